@@ -1,0 +1,470 @@
+"""ctypes bindings for the CPU oracle (liboracle.so) and the reference probe
+(oracle/_ref/libtcref.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline / reference legs, always as the checker or the timed
+CPU baseline -- never by the product path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import struct
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+MAX_DEPTH = 16
+
+LOSS_IDS = {"logloss": 0, "mse": 1, "focal": 2, "softmax": 3}
+
+
+def _ptr(a, t=C.c_void_p):
+    return C.cast(a.ctypes.data, t) if a is not None else None
+
+
+class TreeParams(C.Structure):
+    _fields_ = [
+        ("max_depth", C.c_int32),
+        ("max_bins", C.c_int32),
+        ("min_samples_leaf", C.c_int32),
+        ("lambda_l2", C.c_float),
+        ("lambda_l1", C.c_float),
+        ("min_child_weight", C.c_float),
+        ("min_split_gain", C.c_float),
+        ("max_delta_step", C.c_float),
+    ]
+
+
+class TreeOut(C.Structure):
+    _fields_ = [
+        ("depth", C.c_int32),
+        ("feature", C.c_uint16 * MAX_DEPTH),
+        ("bin", C.c_uint8 * MAX_DEPTH),
+        ("threshold", C.c_float * MAX_DEPTH),
+        ("gain", C.c_float * MAX_DEPTH),
+        ("gain_top", C.c_double * MAX_DEPTH),
+        ("gain_second", C.c_double * MAX_DEPTH),
+        ("n_candidates", C.c_uint32 * MAX_DEPTH),
+    ]
+
+
+class FitParams(C.Structure):
+    _fields_ = [
+        ("loss", C.c_int32),
+        ("n_classes", C.c_int32),
+        ("n_estimators", C.c_int32),
+        ("learning_rate", C.c_float),
+        ("focal_gamma", C.c_float),
+        ("focal_alpha", C.c_float),
+        ("tree", TreeParams),
+    ]
+
+
+class RefParams(C.Structure):
+    _fields_ = [
+        ("loss", C.c_int32),
+        ("n_classes", C.c_int32),
+        ("n_estimators", C.c_int32),
+        ("max_depth", C.c_int32),
+        ("max_bins", C.c_int32),
+        ("min_samples_leaf", C.c_int32),
+        ("learning_rate", C.c_float),
+        ("lambda_l2", C.c_float),
+        ("lambda_l1", C.c_float),
+        ("min_child_weight", C.c_float),
+        ("min_split_gain", C.c_float),
+        ("max_delta_step", C.c_float),
+    ]
+
+
+@dataclass
+class Hyper:
+    """Hyper-parameters shared by the oracle, the reference probe and the device path."""
+
+    loss: str = "logloss"
+    n_classes: int = 1
+    n_estimators: int = 10
+    learning_rate: float = 0.1
+    max_depth: int = 6
+    max_bins: int = 255
+    min_samples_leaf: int = 1
+    lambda_l2: float = 1.0
+    lambda_l1: float = 0.0
+    min_child_weight: float = 1.0
+    min_split_gain: float = 0.0
+    max_delta_step: float = 0.0
+    focal_gamma: float = 2.0
+    focal_alpha: float = 0.25
+
+    def tree(self) -> TreeParams:
+        return TreeParams(self.max_depth, self.max_bins, self.min_samples_leaf, self.lambda_l2,
+                          self.lambda_l1, self.min_child_weight, self.min_split_gain,
+                          self.max_delta_step)
+
+    def fit(self) -> FitParams:
+        return FitParams(LOSS_IDS[self.loss], self.n_classes if self.loss == "softmax" else 1,
+                         self.n_estimators, self.learning_rate, self.focal_gamma,
+                         self.focal_alpha, self.tree())
+
+    def ref(self) -> RefParams:
+        return RefParams(LOSS_IDS[self.loss], self.n_classes if self.loss == "softmax" else 2,
+                         self.n_estimators, self.max_depth, self.max_bins, self.min_samples_leaf,
+                         self.learning_rate, self.lambda_l2, self.lambda_l1,
+                         self.min_child_weight, self.min_split_gain, self.max_delta_step)
+
+
+_lib = None
+_ref = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            raise RuntimeError("oracle/liboracle.so is not built (run `make -C oracle`)")
+        _lib = C.CDLL(path)
+    return _lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "libtcref.so"))
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        path = os.path.join(HERE, "_ref", "libtcref.so")
+        if not os.path.exists(path):
+            raise RuntimeError("oracle/_ref/libtcref.so is not built (make -f oracle/ref.mk)")
+        _ref = C.CDLL(path)
+        _ref.tcref_last_error.restype = C.c_char_p
+    return _ref
+
+
+# ---------------------------------------------------------------- oracle --
+
+@dataclass
+class Binned:
+    bins: np.ndarray      # uint8 [f][n]
+    edges: np.ndarray     # float32 [f][255]
+    n_edges: np.ndarray   # uint16 [f]
+
+    def edge_list(self, j):
+        return self.edges[j, : self.n_edges[j]]
+
+
+def quantize(X: np.ndarray, max_bins: int = 255, compat_u8: bool = True) -> Binned:
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    n, f = X.shape
+    bins = np.zeros((f, n), np.uint8)
+    edges = np.zeros((f, 255), np.float32)
+    ne = np.zeros(f, np.uint16)
+    rc = lib().tco_quantize(_ptr(X), C.c_uint32(n), C.c_uint32(f), C.c_int32(max_bins),
+                            C.c_int32(1 if compat_u8 else 0), _ptr(bins), _ptr(edges), _ptr(ne))
+    if rc:
+        raise ValueError(f"tco_quantize failed ({rc})")
+    return Binned(bins, edges, ne)
+
+
+def gradients(loss: str, y, pred, K: int = 1, gamma=2.0, alpha=0.25):
+    y = np.ascontiguousarray(y, np.float32)
+    pred = np.ascontiguousarray(pred, np.float32)
+    g = np.empty_like(pred)
+    h = np.empty_like(pred)
+    n = y.shape[0]
+    L = lib()
+    if loss == "logloss":
+        L.tco_grad_logloss(_ptr(y), _ptr(pred), _ptr(g), _ptr(h), C.c_uint32(n))
+    elif loss == "mse":
+        L.tco_grad_mse(_ptr(y), _ptr(pred), _ptr(g), _ptr(h), C.c_uint32(n))
+    elif loss == "focal":
+        L.tco_grad_focal(_ptr(y), _ptr(pred), _ptr(g), _ptr(h), C.c_uint32(n), C.c_float(gamma),
+                         C.c_float(alpha))
+    elif loss == "softmax":
+        L.tco_grad_softmax(_ptr(y), _ptr(pred), _ptr(g), _ptr(h), C.c_uint32(n), C.c_uint32(K))
+    else:
+        raise ValueError(loss)
+    return g, h
+
+
+def init_prediction(loss: str, y) -> float:
+    y = np.ascontiguousarray(y, np.float32)
+    L = lib()
+    L.tco_init_prediction.restype = C.c_float
+    return float(L.tco_init_prediction(C.c_int32(LOSS_IDS[loss]), _ptr(y), C.c_uint32(y.shape[0])))
+
+
+@dataclass
+class Tree:
+    depth: int
+    feature: np.ndarray
+    bin: np.ndarray
+    threshold: np.ndarray
+    gain: np.ndarray
+    gain_top: np.ndarray
+    gain_second: np.ndarray
+    leaves: np.ndarray
+    leaf_index: np.ndarray | None = None
+    root_hist: np.ndarray | None = None
+
+    def margins(self):
+        """Relative margin of the chosen split over the runner-up, per level."""
+        out = []
+        for d in range(self.depth):
+            top, sec = self.gain_top[d], self.gain_second[d]
+            out.append(np.inf if sec <= -1e29 else (top - sec) / max(abs(top), 1e-300))
+        return np.array(out)
+
+
+def build_tree(b: Binned, g, h, hp: Hyper, mode: int = 0, want_rows=True, want_hist=False) -> Tree:
+    f, n = b.bins.shape
+    g = np.ascontiguousarray(g, np.float32)
+    h = np.ascontiguousarray(h, np.float32)
+    out = TreeOut()
+    leaves = np.zeros(1 << hp.max_depth, np.float32)
+    li = np.zeros(n, np.uint32) if want_rows else None
+    rh = np.zeros((f, 256, 2), np.float64) if want_hist else None
+    tp = hp.tree()
+    rc = lib().tco_build_tree(_ptr(b.bins), C.c_uint32(n), C.c_uint32(f), _ptr(b.edges),
+                              _ptr(b.n_edges), _ptr(g), _ptr(h), C.byref(tp), C.c_int32(mode),
+                              C.byref(out), _ptr(leaves), _ptr(li), _ptr(rh))
+    if rc:
+        raise RuntimeError(f"tco_build_tree failed ({rc})")
+    d = out.depth
+    return Tree(d, np.array(out.feature[:d], np.uint16), np.array(out.bin[:d], np.uint8),
+                np.array(out.threshold[:d], np.float32), np.array(out.gain[:d], np.float32),
+                np.array(out.gain_top[:MAX_DEPTH]), np.array(out.gain_second[:MAX_DEPTH]),
+                leaves[: 1 << d].copy(), li, rh)
+
+
+def histogram(b: Binned, g, h, node_of_row, n_nodes: int) -> np.ndarray:
+    f, n = b.bins.shape
+    g = np.ascontiguousarray(g, np.float32)
+    h = np.ascontiguousarray(h, np.float32)
+    nodes = np.ascontiguousarray(node_of_row, np.uint32)
+    out = np.zeros((n_nodes, f, 256, 2), np.float64)
+    lib().tco_histogram(_ptr(b.bins), C.c_uint32(n), C.c_uint32(f), _ptr(g), _ptr(h),
+                        _ptr(nodes), C.c_uint32(n_nodes), _ptr(out))
+    return out
+
+
+@dataclass
+class Ensemble:
+    """A flat symmetric ensemble (the FastFloatEnsemble layout)."""
+
+    base: float
+    n_classes: int
+    max_depth: int
+    depth: np.ndarray       # int32 [T]
+    feature: np.ndarray     # uint16 [T][D]
+    bin: np.ndarray         # uint8 [T][D]
+    threshold: np.ndarray   # float32 [T][D]
+    leaves: np.ndarray      # float32 [T][2^D]
+    weights: np.ndarray     # float32 [T]
+    gain: np.ndarray | None = None
+    min_margin: float = np.inf
+    train_pred: np.ndarray | None = None
+    bin_edges: list = field(default_factory=list)
+
+    @property
+    def n_trees(self):
+        return int(self.depth.shape[0])
+
+
+def fit(b: Binned, y, hp: Hyper, mode: int = 0, want_pred=True, trace=False) -> Ensemble:
+    f, n = b.bins.shape
+    y = np.ascontiguousarray(y, np.float32)
+    K = hp.n_classes if hp.loss == "softmax" else 1
+    T = hp.n_estimators * K
+    D = hp.max_depth
+    depth = np.zeros(T, np.int32)
+    feat = np.zeros((T, D), np.uint16)
+    bins_ = np.zeros((T, D), np.uint8)
+    thr = np.zeros((T, D), np.float32)
+    leaves = np.zeros((T, 1 << D), np.float32)
+    tp = np.zeros((n, K), np.float32) if want_pred else None
+    base = C.c_float()
+    mm = C.c_double()
+    gain = np.zeros((T, D), np.float32)
+    gt = np.zeros((hp.n_estimators, n, K), np.float32) if trace else None
+    ht = np.zeros((hp.n_estimators, n, K), np.float32) if trace else None
+    fp = hp.fit()
+    rc = lib().tco_fit(_ptr(b.bins), C.c_uint32(n), C.c_uint32(f), _ptr(b.edges), _ptr(b.n_edges),
+                       _ptr(y), C.byref(fp), C.c_int32(mode), C.byref(base), _ptr(depth),
+                       _ptr(feat), _ptr(bins_), _ptr(thr), _ptr(leaves), _ptr(tp), C.byref(mm),
+                       _ptr(gain), _ptr(gt), _ptr(ht))
+    if rc:
+        raise RuntimeError(f"tco_fit failed ({rc})")
+    e = Ensemble(base.value, K, D, depth, feat, bins_, thr, leaves,
+                 np.full(T, hp.learning_rate, np.float32), gain, mm.value, tp,
+                 [b.edge_list(j).copy() for j in range(f)])
+    e.grad_trace, e.hess_trace = gt, ht
+    return e
+
+
+def predict(ens: Ensemble, X) -> np.ndarray:
+    """FP64 raw scores [n][K] (base included)."""
+    X = np.ascontiguousarray(X, np.float32)
+    n, f = X.shape
+    out = np.zeros((n, ens.n_classes), np.float64)
+    depth = np.ascontiguousarray(ens.depth, np.int32)
+    feat = np.ascontiguousarray(ens.feature, np.uint16)
+    thr = np.ascontiguousarray(ens.threshold, np.float32)
+    leaves = np.ascontiguousarray(ens.leaves, np.float32)
+    w = np.ascontiguousarray(ens.weights, np.float32)
+    lib().tco_predict(_ptr(X), C.c_uint32(n), C.c_uint32(f), C.c_int32(ens.n_trees),
+                      C.c_int32(ens.n_classes), C.c_int32(ens.max_depth), _ptr(depth), _ptr(feat),
+                      _ptr(thr), _ptr(leaves), _ptr(w), C.c_float(ens.base), _ptr(out))
+    return out
+
+
+# ------------------------------------------------------------- reference --
+
+def ref_quantize(X, max_bins=255) -> Binned:
+    X = np.ascontiguousarray(X, np.float32)
+    n, f = X.shape
+    bins = np.zeros((f, n), np.uint8)
+    edges = np.zeros((f, 255), np.float32)
+    ne = np.zeros(f, np.uint16)
+    R = ref()
+    rc = R.tcref_bin(_ptr(X), C.c_uint32(n), C.c_uint16(f), C.c_int32(max_bins), _ptr(bins),
+                     _ptr(edges), _ptr(ne))
+    if rc:
+        raise RuntimeError(R.tcref_last_error().decode())
+    return Binned(bins, edges, ne)
+
+
+def ref_fit(X, y, hp: Hyper, trace=False):
+    """Reference Booster::train; returns (Binned, TCAT bytes, grad trace, hess trace, train raw)."""
+    X = np.ascontiguousarray(X, np.float32)
+    y = np.ascontiguousarray(y, np.float32)
+    n, f = X.shape
+    bins = np.zeros((f, n), np.uint8)
+    edges = np.zeros((f, 255), np.float32)
+    ne = np.zeros(f, np.uint16)
+    gt = np.zeros((hp.n_estimators, n), np.float32) if trace else None
+    ht = np.zeros((hp.n_estimators, n), np.float32) if trace else None
+    tp = np.zeros(n, np.float32)
+    mb = C.c_void_p()
+    ml = C.c_size_t()
+    rp = hp.ref()
+    R = ref()
+    rc = R.tcref_fit(_ptr(X), C.c_uint32(n), C.c_uint16(f), _ptr(y), C.byref(rp), _ptr(bins),
+                     _ptr(edges), _ptr(ne), _ptr(gt), _ptr(ht), _ptr(tp), C.byref(mb), C.byref(ml))
+    if rc < 0:
+        raise RuntimeError(R.tcref_last_error().decode())
+    data = C.string_at(mb, ml.value)
+    R.tcref_free(mb)
+    return Binned(bins, edges, ne), data, gt, ht, tp
+
+
+def ref_predict(model: bytes, X, proba=False) -> np.ndarray:
+    X = np.ascontiguousarray(X, np.float32)
+    n, f = X.shape
+    out = np.zeros(n, np.float32)
+    R = ref()
+    rc = R.tcref_predict(C.c_char_p(model), C.c_size_t(len(model)), _ptr(X), C.c_uint32(n),
+                         C.c_uint16(f), C.c_int32(1 if proba else 0), _ptr(out))
+    if rc:
+        raise RuntimeError(R.tcref_last_error().decode())
+    return out
+
+
+def ref_build_tree(X, g, h, hp: Hyper):
+    X = np.ascontiguousarray(X, np.float32)
+    n, f = X.shape
+    g = np.ascontiguousarray(g, np.float32)
+    h = np.ascontiguousarray(h, np.float32)
+    sf = np.zeros(64, np.uint16)
+    sb = np.zeros(64, np.uint8)
+    st = np.zeros(64, np.float32)
+    sg = np.zeros(64, np.float32)
+    lv = np.zeros(1 << hp.max_depth, np.float32)
+    rp = hp.ref()
+    R = ref()
+    d = R.tcref_build_tree(_ptr(X), C.c_uint32(n), C.c_uint16(f), _ptr(g), _ptr(h), C.byref(rp),
+                           _ptr(sf), _ptr(sb), _ptr(st), _ptr(sg), _ptr(lv))
+    if d < 0:
+        raise RuntimeError(R.tcref_last_error().decode())
+    return d, sf[:d], sb[:d], st[:d], sg[:d], lv[: 1 << d]
+
+
+def ref_fit_multiclass(X, y, hp: Hyper):
+    X = np.ascontiguousarray(X, np.float32)
+    y = np.ascontiguousarray(y, np.float32)
+    n, f = X.shape
+    K, D = hp.n_classes, hp.max_depth
+    T = hp.n_estimators * K
+    depth = np.zeros(T, np.int32)
+    sf = np.zeros((T, D), np.uint16)
+    sb = np.zeros((T, D), np.uint8)
+    st = np.zeros((T, D), np.float32)
+    lv = np.zeros((T, 1 << D), np.float32)
+    tp = np.zeros((n, K), np.float32)
+    rp = hp.ref()
+    R = ref()
+    rc = R.tcref_fit_multiclass(_ptr(X), C.c_uint32(n), C.c_uint16(f), _ptr(y), C.byref(rp),
+                                _ptr(depth), _ptr(sf), _ptr(sb), _ptr(st), _ptr(lv), _ptr(tp))
+    if rc:
+        raise RuntimeError(R.tcref_last_error().decode())
+    return depth, sf, sb, st, lv, tp
+
+
+# --------------------------------------------------------------- TCAT v3 --
+
+def parse_tcat(data: bytes) -> Ensemble:
+    """Parse a TCAT v3 symmetric model (src/boosting/booster.cpp:1049-1118,
+    src/tree/symmetric_tree.cpp:1199-1215); host-endian, size_t = 8 bytes."""
+    off = 0
+
+    def take(fmt):
+        nonlocal off
+        v = struct.unpack_from("<" + fmt, data, off)
+        off += struct.calcsize("<" + fmt)
+        return v
+
+    if data[:4] != b"TCAT":
+        raise ValueError("not a TCAT stream")
+    off = 4
+    (version,) = take("I")
+    if version != 3:
+        raise ValueError(f"TCAT version {version} not supported here")
+    (base,) = take("f")
+    (task,) = take("B")
+    (n_classes,) = take("I")
+    (lr,) = take("f")
+    (max_depth,) = take("H")
+    (lam,) = take("f")
+    (sym,) = take("B")
+    if not sym:
+        raise ValueError("not a symmetric-tree model")
+    (nf,) = take("Q")
+    edges = []
+    for _ in range(nf):
+        (ne,) = take("Q")
+        edges.append(np.array(take(f"{ne}f"), np.float32) if ne else np.zeros(0, np.float32))
+    (nt,) = take("Q")
+    weights = np.array(take(f"{nt}f"), np.float32) if nt else np.zeros(0, np.float32)
+    D = max_depth
+    depth = np.zeros(nt, np.int32)
+    feat = np.zeros((nt, D), np.uint16)
+    bins_ = np.zeros((nt, D), np.uint8)
+    thr = np.zeros((nt, D), np.float32)
+    gain = np.zeros((nt, D), np.float32)
+    leaves = np.zeros((nt, 1 << D), np.float32)
+    for t in range(nt):
+        (d,) = take("H")
+        depth[t] = d
+        for k in range(d):
+            (feat[t, k],) = take("H")
+            (bins_[t, k],) = take("B")
+            (thr[t, k],) = take("f")
+            (gain[t, k],) = take("f")
+        (nl,) = take("Q")
+        leaves[t, :nl] = np.array(take(f"{nl}f"), np.float32)
+    e = Ensemble(base, 1, D, depth, feat, bins_, thr, leaves, weights, gain)
+    e.bin_edges = edges
+    return e
