@@ -1,0 +1,98 @@
+"""Seeded synthetic inputs with the shapes and value distributions of the
+benchmark configurations (no public dataset is involved), plus the small
+cases the golden fixtures and the parity tests use."""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+from oracle import Hyper  # noqa: E402
+
+
+def binary_c1(n=50_000, f=20, seed=1):
+    """Binary: X ~ N(0,1); y ~ Bernoulli(sigmoid(w.x + 0.5*x0*x1))."""
+    rng = np.random.default_rng(seed)
+    X = rng.standard_normal((n, f)).astype(np.float32)
+    w = rng.standard_normal(f)
+    s = X.astype(np.float64) @ w + 0.5 * X[:, 0].astype(np.float64) * X[:, 1]
+    y = (rng.random(n) < 1.0 / (1.0 + np.exp(-s))).astype(np.float32)
+    return X, y
+
+
+def regression_c2(n=1_000_000, f=100, seed=2):
+    """Regression: 60% N(0,1), 30% U(-3,3), 10% Student-t(3) columns;
+    y = sum of sin over 10 random features + x2*x3 + N(0, 0.1)."""
+    rng = np.random.default_rng(seed)
+    a, b = int(round(f * 0.6)), int(round(f * 0.3))
+    c = f - a - b
+    X = np.concatenate([rng.standard_normal((n, a)), rng.uniform(-3, 3, (n, b)),
+                        rng.standard_t(3, (n, c))], axis=1).astype(np.float32)
+    S = rng.choice(f, min(10, f), replace=False)
+    y = (np.sin(X[:, S].astype(np.float64)).sum(1) + X[:, 2].astype(np.float64) * X[:, 3]
+         + rng.normal(0, 0.1, n)).astype(np.float32)
+    return X, y
+
+
+def multiclass_c3(n=2_000_000, f=50, K=10, seed=3):
+    """Multiclass: y = argmax of K random projections plus Gumbel noise."""
+    rng = np.random.default_rng(seed)
+    X = rng.standard_normal((n, f)).astype(np.float32)
+    W = rng.standard_normal((f, K))
+    y = np.argmax(X.astype(np.float64) @ W + rng.gumbel(size=(n, K)), axis=1).astype(np.float32)
+    return X, y
+
+
+def imbalanced_c5(n=10_000_000, f=200, seed=5, active=20):
+    """Imbalanced: half N(0,1), half LogNormal(0,1); ~1% positives from a
+    sparse linear score (20 active features) + N(0, 0.5), thresholded at the
+    99th percentile."""
+    rng = np.random.default_rng(seed)
+    h = f // 2
+    X = np.empty((n, f), np.float32)
+    X[:, :h] = rng.standard_normal((n, h), dtype=np.float32)
+    X[:, h:] = np.exp(rng.standard_normal((n, f - h), dtype=np.float32))
+    A = rng.choice(f, min(active, f), replace=False)
+    beta = rng.standard_normal(len(A)).astype(np.float32)
+    s = X[:, A] @ beta + rng.normal(0, 0.5, n).astype(np.float32)
+    y = (s > np.quantile(s, 0.99)).astype(np.float32)
+    return X, y
+
+
+def serving_rows(n, f=100, seed=4):
+    rng = np.random.default_rng(seed)
+    return rng.standard_normal((n, f)).astype(np.float32)
+
+
+# small cases for golden fixtures / CPU-speed parity: name -> spec
+GOLDEN_CASES = {
+    "c1_small": dict(kind="binary", n=8_000, f=20, seed=11, hyper=dict(loss="logloss", n_estimators=30,
+                                                                          learning_rate=0.1, max_depth=6)),
+    "c1_odd": dict(kind="binary", n=1003, f=7, seed=12, hyper=dict(loss="logloss", n_estimators=20,
+                                                                   learning_rate=0.3, max_depth=4)),
+    "c2_small": dict(kind="regression", n=10_000, f=30, seed=13, hyper=dict(loss="mse", n_estimators=20,
+                                                                            learning_rate=0.05, max_depth=8,
+                                                                            lambda_l2=0.0)),
+    "c3_small": dict(kind="multiclass", n=8_000, f=12, K=4, seed=14, hyper=dict(loss="softmax", n_classes=4,
+                                                                                n_estimators=5,
+                                                                                learning_rate=0.1,
+                                                                                max_depth=5)),
+    "c5_small": dict(kind="imbalanced", n=15_000, f=16, seed=15, hyper=dict(loss="focal", n_estimators=20,
+                                                                            learning_rate=0.1, max_depth=8)),
+}
+
+
+def make_case(spec):
+    kind = spec["kind"]
+    if kind == "binary":
+        X, y = binary_c1(spec["n"], spec["f"], spec["seed"])
+    elif kind == "regression":
+        X, y = regression_c2(spec["n"], spec["f"], spec["seed"])
+    elif kind == "multiclass":
+        X, y = multiclass_c3(spec["n"], spec["f"], spec["K"], spec["seed"])
+    else:
+        X, y = imbalanced_c5(spec["n"], spec["f"], spec["seed"], active=min(20, spec["f"]))
+    return X, y, Hyper(**spec["hyper"])

@@ -1,0 +1,173 @@
+// Internal declarations shared by the libtcgpu.so translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "tcgpu.h"
+
+namespace tc {
+
+constexpr int kNanBin = 255;      // bin of NaN rows; always routed left
+constexpr int kSlots = 256;       // histogram slots per (node, feature): bins 0..254 + NaN
+constexpr int kMaxDepth = 12;     // deepest tree the trainer builds
+constexpr int kMaxClasses = 64;
+
+inline size_t round_up(size_t x, size_t m) { return (x + m - 1) / m * m; }
+
+}  // namespace tc
+
+struct tc_ctx {
+  int device = 0;
+  int sm_count = 148;
+  size_t budget = 0;
+  size_t in_use = 0;
+  size_t peak = 0;
+  int fail_next = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  std::mutex mu;                     // guards allocation accounting and err
+  std::map<void*, size_t> allocs;
+
+  tc_status fail(tc_status code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    std::lock_guard<std::mutex> g(mu);
+    err = buf;
+    return code;
+  }
+  tc_status cuda_fail(cudaError_t e, const char* what) {
+    return fail(TC_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+  }
+  // Device allocation with budget accounting and test fault injection.
+  tc_status alloc(void** p, size_t bytes, const char* what);
+  void release(void* p);
+};
+
+#define TC_CUDA(ctx, call)                                         \
+  do {                                                             \
+    cudaError_t e_ = (call);                                       \
+    if (e_ != cudaSuccess) return (ctx)->cuda_fail(e_, #call);     \
+  } while (0)
+
+#define TC_TRY(expr)                    \
+  do {                                  \
+    tc_status s_ = (expr);              \
+    if (s_ != TC_OK) return s_;         \
+  } while (0)
+
+// A device buffer owned by a context.
+template <class T>
+struct DevBuf {
+  tc_ctx* ctx = nullptr;
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { reset(); }
+  tc_status alloc(tc_ctx* c, size_t count, const char* what) {
+    reset();
+    ctx = c;
+    void* q = nullptr;
+    tc_status s = c->alloc(&q, count * sizeof(T) > 0 ? count * sizeof(T) : 16, what);
+    if (s != TC_OK) return s;
+    p = static_cast<T*>(q);
+    n = count;
+    return TC_OK;
+  }
+  void reset() {
+    if (p && ctx) ctx->release(p);
+    p = nullptr;
+    n = 0;
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+struct tc_dataset {
+  tc_ctx* ctx = nullptr;
+  uint32_t n = 0;
+  uint32_t f = 0;
+  uint32_t fs = 0;           // row stride of the row-major bin matrix (f rounded up to 16)
+  uint32_t np = 0;           // column stride of the column-major bin matrix (n rounded up to 16)
+  bool quantized = false;
+  int max_bins = 255;
+  DevBuf<float> X;           // [n][f] row-major input
+  DevBuf<float> y;           // [n] labels (may be empty)
+  DevBuf<uint8_t> bins_rm;   // [n][fs]
+  DevBuf<uint8_t> bins_cm;   // [f][np]
+  DevBuf<float> edges;       // [f][256]
+  DevBuf<uint16_t> n_edges;  // [f]
+  std::vector<float> h_edges;       // [f][255]
+  std::vector<uint16_t> h_n_edges;  // [f]
+};
+
+// Flat device-resident symmetric ensemble (the FastFloatEnsemble layout,
+// include/turbocat/fast_float_ensemble.hpp:90-100).
+struct tc_model {
+  tc_ctx* ctx = nullptr;
+  tc_model_info info{};
+  std::vector<int32_t> depth;       // [T]
+  std::vector<uint16_t> feature;    // [T][D]
+  std::vector<uint8_t> bin;         // [T][D]
+  std::vector<float> threshold;     // [T][D]
+  std::vector<float> gain;          // [T][D]
+  std::vector<float> leaves;        // [T][2^D]
+  std::vector<float> weights;       // [T]
+  std::vector<float> edges;         // [f][255]
+  std::vector<uint16_t> n_edges;    // [f]
+  // device copies used by the predict kernels
+  DevBuf<uint2> d_splits;           // [T][D] packed (feature | depth flags, threshold bits)
+  DevBuf<float> d_leaves;           // [T][2^D] (weights folded in)
+  DevBuf<int32_t> d_depth;          // [T]
+  tc_status upload();
+};
+
+namespace tc {
+
+// Quantization entry (tc_data.cu).
+tc_status quantize(tc_dataset* ds, int max_bins, int compat_u8);
+
+// Prediction (tc_predict.cu): raw scores [n][K] (+ transform) on device buffers.
+tc_status predict_device(tc_ctx* ctx, const tc_model* m, const float* X, uint32_t n, uint32_t f,
+                         int transform, float* out, cudaStream_t stream);
+
+// Serving request table entry for the coalesced predict kernel.
+struct ReqDesc {
+  const float* X;     // device pointer to the request's rows [n][f]
+  float* out;         // device pointer to its outputs [n][K]
+  uint32_t n;
+  uint32_t row_begin; // first global row of this request in the batch
+  int32_t model;      // index into the model table
+  int32_t transform;
+};
+struct ModelDesc {
+  const uint2* splits;
+  const float* leaves;
+  const int32_t* depth;
+  int32_t n_trees;
+  int32_t max_depth;
+  int32_t n_classes;
+  int32_t n_features;
+  float base;
+  int32_t pad[3];
+};
+// Coalesced prediction over a request table: job j covers tiles
+// [tile_begin[j], tile_begin[j+1]) of PRED_ROWS rows each.
+tc_status predict_batched(tc_ctx* ctx, const ModelDesc* d_models, const ReqDesc* d_reqs, int n_reqs,
+                          const uint32_t* d_tile_begin, uint32_t n_tiles, int max_depth_all, int max_f,
+                          cudaStream_t stream);
+uint32_t predict_tiles(uint32_t n);
+ModelDesc model_desc(const tc_model* m);
+
+}  // namespace tc

@@ -1,0 +1,525 @@
+// Oblivious-ensemble prediction on raw float features, the model object and
+// the TCAT v3 stream.
+//
+// Prediction restates FastFloatEnsemble (include/turbocat/fast_float_ensemble.hpp:122-137,
+// 139-664; src/tree/fast_float_ensemble.cpp:23-276): per tree the leaf index is
+// built from depth bit-compares, bit = !isnan(x) && x >= threshold, first
+// split in the most significant bit, and the weighted leaf values are summed;
+// then the base prediction is added (src/boosting/booster.cpp:920-924) and the
+// sigmoid (include/turbocat/loss.hpp:99-101) or softmax
+// (src/boosting/loss.cpp:320-330) applied.
+//
+// Kernel layout: a block owns a tile of rows of one job (one request of a
+// coalesced serving batch, or the whole input of a single call).  The
+// tile's rows are staged in shared memory (row stride f+1 words, so threads
+// reading the same feature of different rows hit different banks), trees are
+// streamed through shared memory in chunks of packed (feature, threshold)
+// pairs and weight-folded leaves, and every thread walks all trees for its
+// row.
+#include <algorithm>
+#include <cstring>
+
+#include "tc_internal.h"
+
+namespace tc {
+namespace {
+
+constexpr int PRED_ROWS = 128;
+constexpr int PRED_TG = 4;                  // thread groups per row tile (trees split across them)
+constexpr int PRED_THREADS = PRED_ROWS * PRED_TG;
+constexpr int PRED_LEAF_FLOATS = 8192;      // shared floats for one chunk of leaves (32 KB)
+constexpr int PRED_MAX_K = 16;
+
+struct JobTable {
+  const ReqDesc* reqs;         // nullptr: single job held inline
+  const ModelDesc* models;
+  const uint32_t* tile_begin;  // [n_jobs + 1] first tile of each job
+  int n_jobs;
+  int max_depth;               // largest model depth in the batch (shared sizing)
+  int max_f;                   // largest feature count in the batch
+  ReqDesc one_req;
+  ModelDesc one_model;
+};
+
+__device__ __forceinline__ float sigmoidf_ref(float x) { return 1.0f / (1.0f + expf(-x)); }
+
+__global__ void __launch_bounds__(PRED_THREADS) k_predict(JobTable jt) {
+  extern __shared__ float smp[];
+  ReqDesc rq;
+  ModelDesc md;
+  uint32_t tile;
+  if (jt.reqs == nullptr) {
+    rq = jt.one_req;
+    md = jt.one_model;
+    tile = blockIdx.x;
+  } else {
+    // job lookup: last job whose first tile <= blockIdx.x
+    int lo = 0, hi = jt.n_jobs - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (jt.tile_begin[mid] <= blockIdx.x) lo = mid; else hi = mid - 1;
+    }
+    rq = jt.reqs[lo];
+    md = jt.models[rq.model];
+    tile = blockIdx.x - jt.tile_begin[lo];
+  }
+  const uint32_t r0 = tile * PRED_ROWS;
+  if (r0 >= rq.n) return;
+  const uint32_t nr = min((uint32_t)PRED_ROWS, rq.n - r0);
+  const int f = md.n_features;
+  const int fs = f + 1;
+  const int D = md.max_depth;
+  const int L = 1 << D;
+  const int tchunk = max(1, min(256, PRED_LEAF_FLOATS / L));
+  float* s_x = smp;                                  // [PRED_ROWS][f+1]
+  float* s_leaf = s_x + PRED_ROWS * (jt.max_f + 1);  // [tchunk][L]
+  uint2* s_split = reinterpret_cast<uint2*>(s_leaf + PRED_LEAF_FLOATS);  // [tchunk][D]
+  int* s_depth = reinterpret_cast<int*>(s_split + 256 * max(1, jt.max_depth));
+  const float* Xt = rq.X + (size_t)r0 * f;
+  for (uint32_t q = threadIdx.x; q < nr * (uint32_t)f; q += blockDim.x) {
+    const uint32_t i = q / f, j = q % f;
+    s_x[i * fs + j] = Xt[q];
+  }
+  const int K = md.n_classes;
+  float acc[PRED_MAX_K];
+#pragma unroll
+  for (int k = 0; k < PRED_MAX_K; ++k) acc[k] = 0.0f;
+  const int row = threadIdx.x % PRED_ROWS;
+  const int tg = threadIdx.x / PRED_ROWS;
+  const float* xr = s_x + row * fs;
+  for (int t0 = 0; t0 < md.n_trees; t0 += tchunk) {
+    const int tn = min(tchunk, md.n_trees - t0);
+    __syncthreads();
+    for (int q = threadIdx.x; q < tn * L; q += blockDim.x) s_leaf[q] = md.leaves[(size_t)t0 * L + q];
+    for (int q = threadIdx.x; q < tn * D; q += blockDim.x) s_split[q] = md.splits[(size_t)t0 * D + q];
+    for (int q = threadIdx.x; q < tn; q += blockDim.x) s_depth[q] = md.depth[t0 + q];
+    __syncthreads();
+    if ((uint32_t)row < nr) {
+      if (K == 1) {
+        float s = 0.0f;
+        for (int t = tg; t < tn; t += PRED_TG) {
+          const int dep = s_depth[t];
+          const uint2* sp = s_split + t * D;
+          uint32_t idx = 0;
+          for (int d = 0; d < dep; ++d) {
+            const uint2 q = sp[d];
+            idx = (idx << 1) | (uint32_t)(xr[q.x] >= __uint_as_float(q.y));  // false for NaN
+          }
+          s += s_leaf[t * L + idx];
+        }
+        acc[0] += s;
+      } else {
+        for (int t = tg; t < tn; t += PRED_TG) {
+          const int dep = s_depth[t];
+          const uint2* sp = s_split + t * D;
+          uint32_t idx = 0;
+          for (int d = 0; d < dep; ++d) {
+            const uint2 q = sp[d];
+            idx = (idx << 1) | (uint32_t)(xr[q.x] >= __uint_as_float(q.y));
+          }
+          const int cls = (t0 + t) % K;
+          const float v = s_leaf[t * L + idx];
+#pragma unroll
+          for (int k = 0; k < PRED_MAX_K; ++k)
+            if (k == cls) acc[k] += v;
+        }
+      }
+    }
+  }
+  // combine the thread groups' partial sums
+  __syncthreads();
+  float* s_red = s_leaf;  // [PRED_TG][PRED_ROWS][K] (fits: 4*128*16 floats = PRED_LEAF_FLOATS)
+#pragma unroll
+  for (int k = 0; k < PRED_MAX_K; ++k)
+    if (k < K) s_red[(tg * PRED_ROWS + row) * K + k] = acc[k];
+  __syncthreads();
+  if (tg != 0 || (uint32_t)row >= nr) return;
+#pragma unroll
+  for (int k = 0; k < PRED_MAX_K; ++k) {
+    if (k < K) {
+      float v = 0.0f;
+      for (int g = 0; g < PRED_TG; ++g) v += s_red[(g * PRED_ROWS + row) * K + k];
+      acc[k] = v;
+    }
+  }
+  float* o = rq.out + (size_t)(r0 + row) * K;
+  if (rq.transform == TC_TRANSFORM_SOFTMAX && K > 1) {
+    float mx = -INFINITY;
+    for (int k = 0; k < K; ++k) mx = fmaxf(mx, acc[k] + md.base);
+    float sum = 0.0f;
+    float e[PRED_MAX_K];
+#pragma unroll
+    for (int k = 0; k < PRED_MAX_K; ++k) {
+      if (k < K) {
+        e[k] = expf(acc[k] + md.base - mx);
+        sum += e[k];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < PRED_MAX_K; ++k)
+      if (k < K) o[k] = e[k] / sum;
+  } else {
+#pragma unroll
+    for (int k = 0; k < PRED_MAX_K; ++k) {
+      if (k < K) {
+        const float raw = acc[k] + md.base;
+        o[k] = (rq.transform == TC_TRANSFORM_SIGMOID) ? sigmoidf_ref(raw) : raw;
+      }
+    }
+  }
+}
+
+size_t predict_smem(int max_f, int max_depth) {
+  return (size_t)PRED_ROWS * (max_f + 1) * 4 + PRED_LEAF_FLOATS * 4 + (size_t)256 * std::max(1, max_depth) * 8 +
+         256 * 4;
+}
+
+tc_status launch_predict(tc_ctx* ctx, const JobTable& jt, uint32_t n_tiles, cudaStream_t stream) {
+  if (n_tiles == 0) return TC_OK;
+  const size_t smem = predict_smem(jt.max_f, jt.max_depth);
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaFuncSetAttribute(k_predict, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_done = true;
+  }
+  if (smem > 200 * 1024)
+    return ctx->fail(TC_ERR_INVALID_ARG, "too many features for the predict kernel (%d)", jt.max_f);
+  k_predict<<<n_tiles, PRED_THREADS, smem, stream>>>(jt);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return ctx->cuda_fail(e, "k_predict");
+  return TC_OK;
+}
+
+}  // namespace
+
+tc_status predict_batched(tc_ctx* ctx, const ModelDesc* d_models, const ReqDesc* d_reqs, int n_reqs,
+                          const uint32_t* d_tile_begin, uint32_t n_tiles, int max_depth_all, int max_f,
+                          cudaStream_t stream) {
+  JobTable jt{};
+  jt.reqs = d_reqs;
+  jt.models = d_models;
+  jt.tile_begin = d_tile_begin;
+  jt.n_jobs = n_reqs;
+  jt.max_depth = max_depth_all;
+  jt.max_f = max_f;
+  return launch_predict(ctx, jt, n_tiles, stream);
+}
+
+uint32_t predict_tiles(uint32_t n) { return (n + PRED_ROWS - 1) / PRED_ROWS; }
+
+}  // namespace tc
+
+using namespace tc;
+
+// Packs splits as (feature, threshold bits) and folds the tree weights into
+// the leaves (w * leaf in FP32, the product the reference forms per tree).
+tc_status tc_model::upload() {
+  const int T = info.n_trees, D = info.max_depth, L = 1 << D;
+  std::vector<uint2> sp((size_t)std::max(1, T * D));
+  std::vector<float> lv((size_t)std::max(1, T * L));
+  for (int t = 0; t < T; ++t) {
+    for (int d = 0; d < D; ++d) {
+      uint32_t bits;
+      std::memcpy(&bits, &threshold[(size_t)t * D + d], 4);
+      sp[(size_t)t * D + d] = make_uint2(feature[(size_t)t * D + d], bits);
+    }
+    for (int l = 0; l < L; ++l) lv[(size_t)t * L + l] = weights[t] * leaves[(size_t)t * L + l];
+  }
+  TC_TRY(d_splits.alloc(ctx, sp.size(), "model splits"));
+  TC_TRY(d_leaves.alloc(ctx, lv.size(), "model leaves"));
+  TC_TRY(d_depth.alloc(ctx, std::max(1, T), "model depths"));
+  TC_CUDA(ctx, cudaMemcpy(d_splits.p, sp.data(), sp.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+  TC_CUDA(ctx, cudaMemcpy(d_leaves.p, lv.data(), lv.size() * sizeof(float), cudaMemcpyHostToDevice));
+  if (T > 0) TC_CUDA(ctx, cudaMemcpy(d_depth.p, depth.data(), T * sizeof(int32_t), cudaMemcpyHostToDevice));
+  return TC_OK;
+}
+
+namespace tc {
+
+ModelDesc model_desc(const tc_model* m) {
+  ModelDesc d{};
+  d.splits = m->d_splits.p;
+  d.leaves = m->d_leaves.p;
+  d.depth = m->d_depth.p;
+  d.n_trees = m->info.n_trees;
+  d.max_depth = m->info.max_depth;
+  d.n_classes = m->info.n_classes;
+  d.n_features = m->info.n_features;
+  d.base = m->info.base_prediction;
+  return d;
+}
+
+tc_status predict_device(tc_ctx* ctx, const tc_model* m, const float* X, uint32_t n, uint32_t f, int transform,
+                         float* out, cudaStream_t stream) {
+  if (n == 0) return TC_OK;
+  JobTable jt{};
+  jt.reqs = nullptr;
+  jt.n_jobs = 1;
+  jt.max_depth = m->info.max_depth;
+  jt.max_f = (int)f;
+  jt.one_model = model_desc(m);
+  jt.one_req = ReqDesc{X, out, n, 0, 0, transform};
+  return launch_predict(ctx, jt, predict_tiles(n), stream);
+}
+
+}  // namespace tc
+
+// ------------------------------------------------------------------ C ABI --
+
+namespace {
+
+void put(std::vector<uint8_t>& b, const void* p, size_t n) {
+  const uint8_t* q = static_cast<const uint8_t*>(p);
+  b.insert(b.end(), q, q + n);
+}
+
+struct Reader {
+  const uint8_t* p;
+  size_t n, off = 0;
+  bool ok = true;
+  template <class T>
+  T get() {
+    T v{};
+    if (off + sizeof(T) > n) { ok = false; return v; }
+    std::memcpy(&v, p + off, sizeof(T));
+    off += sizeof(T);
+    return v;
+  }
+  bool bytes(void* dst, size_t k) {
+    if (off + k > n) { ok = false; return false; }
+    std::memcpy(dst, p + off, k);
+    off += k;
+    return true;
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+tc_status tc_model_info_get(const tc_model* m, tc_model_info* info) {
+  if (!m || !info) return TC_ERR_INVALID_ARG;
+  *info = m->info;
+  return TC_OK;
+}
+
+tc_status tc_model_export(const tc_model* m, int32_t* depth, uint16_t* feature, uint8_t* bin, float* threshold,
+                          float* gain, float* leaves, float* weights, float* edges, uint16_t* n_edges) {
+  if (!m) return TC_ERR_INVALID_ARG;
+  auto cp = [](void* dst, const auto& v) {
+    if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+  };
+  cp(depth, m->depth);
+  cp(feature, m->feature);
+  cp(bin, m->bin);
+  cp(threshold, m->threshold);
+  cp(gain, m->gain);
+  cp(leaves, m->leaves);
+  cp(weights, m->weights);
+  cp(edges, m->edges);
+  cp(n_edges, m->n_edges);
+  return TC_OK;
+}
+
+tc_status tc_model_import(tc_ctx* ctx, const tc_model_info* info, const int32_t* depth, const uint16_t* feature,
+                          const uint8_t* bin, const float* threshold, const float* gain, const float* leaves,
+                          const float* weights, const float* edges, const uint16_t* n_edges, tc_model** out) {
+  if (!ctx || !info || !out) return TC_ERR_INVALID_ARG;
+  *out = nullptr;
+  const int T = info->n_trees, D = info->max_depth, L = 1 << (D > 0 ? D : 0);
+  if (T < 0 || D < 0 || D > 13 || info->n_classes < 1 || info->n_classes > 16 || info->n_features < 1)
+    return ctx->fail(TC_ERR_INVALID_ARG, "invalid model shape (trees %d, depth %d, classes %d, features %d)", T, D,
+                     info->n_classes, info->n_features);
+  if (T > 0 && (!depth || !feature || !threshold || !leaves))
+    return ctx->fail(TC_ERR_INVALID_ARG, "missing model arrays");
+  cudaSetDevice(ctx->device);
+  tc_model* m = new tc_model();
+  m->ctx = ctx;
+  m->info = *info;
+  m->depth.assign(depth, depth + T);
+  for (int t = 0; t < T; ++t) {
+    if (m->depth[t] < 0 || m->depth[t] > D) {
+      delete m;
+      return ctx->fail(TC_ERR_INVALID_ARG, "tree %d depth %d exceeds max_depth %d", t, depth[t], D);
+    }
+    for (int d = 0; d < m->depth[t]; ++d) {
+      if (feature[(size_t)t * D + d] >= info->n_features) {
+        delete m;
+        return ctx->fail(TC_ERR_INVALID_ARG, "tree %d level %d splits on feature %d >= %d", t, d,
+                         feature[(size_t)t * D + d], info->n_features);
+      }
+    }
+  }
+  m->feature.assign(feature, feature + (size_t)T * D);
+  m->bin = bin ? std::vector<uint8_t>(bin, bin + (size_t)T * D) : std::vector<uint8_t>((size_t)T * D, 0);
+  m->threshold.assign(threshold, threshold + (size_t)T * D);
+  m->gain = gain ? std::vector<float>(gain, gain + (size_t)T * D) : std::vector<float>((size_t)T * D, 0.0f);
+  m->leaves.assign(leaves, leaves + (size_t)T * L);
+  m->weights = weights ? std::vector<float>(weights, weights + T) : std::vector<float>(T, info->learning_rate);
+  if (edges && n_edges) {
+    m->n_edges.assign(n_edges, n_edges + info->n_features);
+    m->edges.assign(edges, edges + (size_t)info->n_features * 255);
+  }
+  tc_status s = m->upload();
+  if (s != TC_OK) {
+    delete m;
+    return s;
+  }
+  *out = m;
+  return TC_OK;
+}
+
+// TCAT v3 writer (src/boosting/booster.cpp:1049-1118, src/tree/symmetric_tree.cpp:1199-1215):
+// host-endian, size_t counts.
+tc_status tc_model_save_tcat(const tc_model* m, uint8_t* buf, size_t* len) {
+  if (!m || !len) return TC_ERR_INVALID_ARG;
+  std::vector<uint8_t> b;
+  put(b, "TCAT", 4);
+  const uint32_t version = 3;
+  put(b, &version, 4);
+  put(b, &m->info.base_prediction, 4);
+  const uint8_t task = (uint8_t)m->info.task;
+  put(b, &task, 1);
+  const uint32_t ncls = m->info.task == TC_TASK_MULTICLASS ? (uint32_t)m->info.n_classes : 2u;
+  put(b, &ncls, 4);
+  put(b, &m->info.learning_rate, 4);
+  const uint16_t md = (uint16_t)m->info.max_depth;
+  put(b, &md, 2);
+  put(b, &m->info.lambda_l2, 4);
+  const uint8_t sym = 1;
+  put(b, &sym, 1);
+  const uint64_t nf = m->n_edges.size();
+  put(b, &nf, 8);
+  for (uint64_t j = 0; j < nf; ++j) {
+    const uint64_t ne = m->n_edges[j];
+    put(b, &ne, 8);
+    if (ne) put(b, &m->edges[j * 255], ne * 4);
+  }
+  const uint64_t nt = (uint64_t)m->info.n_trees;
+  put(b, &nt, 8);
+  for (uint64_t t = 0; t < nt; ++t) put(b, &m->weights[t], 4);
+  const int D = m->info.max_depth;
+  for (uint64_t t = 0; t < nt; ++t) {
+    const uint16_t dep = (uint16_t)m->depth[t];
+    put(b, &dep, 2);
+    for (int d = 0; d < dep; ++d) {
+      const size_t q = t * D + d;
+      put(b, &m->feature[q], 2);
+      put(b, &m->bin[q], 1);
+      put(b, &m->threshold[q], 4);
+      put(b, &m->gain[q], 4);
+    }
+    const uint64_t nl = 1ull << dep;
+    put(b, &nl, 8);
+    put(b, &m->leaves[t << D], nl * 4);
+  }
+  if (!buf) {
+    *len = b.size();
+    return TC_OK;
+  }
+  if (*len < b.size()) {
+    *len = b.size();
+    return m->ctx->fail(TC_ERR_INVALID_ARG, "TCAT buffer too small (%zu bytes needed)", b.size());
+  }
+  std::memcpy(buf, b.data(), b.size());
+  *len = b.size();
+  return TC_OK;
+}
+
+// TCAT v3 reader (Booster::load_binary, src/boosting/booster.cpp:1120-1203);
+// symmetric models only.
+tc_status tc_model_load_tcat(tc_ctx* ctx, const uint8_t* buf, size_t len, tc_model** out) {
+  if (!ctx || !buf || !out) return TC_ERR_INVALID_ARG;
+  Reader r{buf, len};
+  char magic[4];
+  if (!r.bytes(magic, 4) || std::memcmp(magic, "TCAT", 4) != 0)
+    return ctx->fail(TC_ERR_FORMAT, "Invalid TurboCat model file");
+  const uint32_t version = r.get<uint32_t>();
+  if (version != 3) return ctx->fail(TC_ERR_FORMAT, "Unsupported TurboCat model version: %u", version);
+  tc_model_info info{};
+  info.base_prediction = r.get<float>();
+  info.task = r.get<uint8_t>();
+  const uint32_t ncls = r.get<uint32_t>();
+  info.learning_rate = r.get<float>();
+  info.max_depth = r.get<uint16_t>();
+  info.lambda_l2 = r.get<float>();
+  const uint8_t sym = r.get<uint8_t>();
+  if (!r.ok) return ctx->fail(TC_ERR_FORMAT, "truncated TCAT header");
+  if (!sym) return ctx->fail(TC_ERR_FORMAT, "TCAT model holds regular trees; only symmetric trees are served");
+  if (info.max_depth > 16) return ctx->fail(TC_ERR_FORMAT, "TCAT max_depth %d too large", info.max_depth);
+  info.n_classes = info.task == TC_TASK_MULTICLASS ? (int)ncls : 1;
+  if (info.n_classes < 1 || info.n_classes > 16) return ctx->fail(TC_ERR_FORMAT, "TCAT class count %u", ncls);
+  const uint64_t nf = r.get<uint64_t>();
+  if (!r.ok || nf == 0 || nf > 65535) return ctx->fail(TC_ERR_FORMAT, "TCAT feature count");
+  info.n_features = (int)nf;
+  std::vector<float> edges((size_t)nf * 255, 0.0f);
+  std::vector<uint16_t> ne(nf);
+  for (uint64_t j = 0; j < nf; ++j) {
+    const uint64_t k = r.get<uint64_t>();
+    if (!r.ok || k > 255) return ctx->fail(TC_ERR_FORMAT, "TCAT edge count");
+    ne[j] = (uint16_t)k;
+    if (k && !r.bytes(&edges[j * 255], k * 4)) return ctx->fail(TC_ERR_FORMAT, "truncated TCAT edges");
+  }
+  const uint64_t nt = r.get<uint64_t>();
+  if (!r.ok || nt > (1ull << 24)) return ctx->fail(TC_ERR_FORMAT, "TCAT tree count");
+  info.n_trees = (int)nt;
+  const int D = info.max_depth, L = 1 << D;
+  std::vector<float> w(nt);
+  for (uint64_t t = 0; t < nt; ++t) w[t] = r.get<float>();
+  std::vector<int32_t> depth(nt);
+  std::vector<uint16_t> feat(nt * D, 0);
+  std::vector<uint8_t> bin(nt * D, 0);
+  std::vector<float> thr(nt * D, 0.0f), gain(nt * D, 0.0f), leaves(nt * L, 0.0f);
+  for (uint64_t t = 0; t < nt && r.ok; ++t) {
+    const uint16_t dep = r.get<uint16_t>();
+    if (dep > D) return ctx->fail(TC_ERR_FORMAT, "TCAT tree %llu depth %u > max_depth %d", (unsigned long long)t, dep, D);
+    depth[t] = dep;
+    for (int d = 0; d < dep; ++d) {
+      feat[t * D + d] = r.get<uint16_t>();
+      bin[t * D + d] = r.get<uint8_t>();
+      thr[t * D + d] = r.get<float>();
+      gain[t * D + d] = r.get<float>();
+    }
+    const uint64_t nl = r.get<uint64_t>();
+    if (!r.ok || nl > (uint64_t)L) return ctx->fail(TC_ERR_FORMAT, "TCAT leaf count");
+    if (!r.bytes(&leaves[t * L], nl * 4)) return ctx->fail(TC_ERR_FORMAT, "truncated TCAT leaves");
+  }
+  if (!r.ok) return ctx->fail(TC_ERR_FORMAT, "truncated TCAT stream");
+  const tc_status s = tc_model_import(ctx, &info, depth.data(), feat.data(), bin.data(), thr.data(), gain.data(),
+                                      leaves.data(), w.data(), edges.data(), ne.data(), out);
+  if (s == TC_ERR_INVALID_ARG) return TC_ERR_FORMAT;
+  return s;
+}
+
+void tc_model_destroy(tc_model* m) { delete m; }
+
+tc_status tc_predict(tc_ctx* ctx, const tc_model* m, const float* X, uint32_t n, uint16_t f, int32_t transform,
+                     float* out) {
+  if (!ctx || !m || (!X && n) || (!out && n)) return TC_ERR_INVALID_ARG;
+  if (f != (uint32_t)m->info.n_features)
+    return ctx->fail(TC_ERR_INVALID_ARG, "X has %u features, the model expects %d", f, m->info.n_features);
+  if (n == 0) return TC_OK;
+  cudaSetDevice(ctx->device);
+  const int K = m->info.n_classes;
+  DevBuf<float> dx, dout;
+  TC_TRY(dx.alloc(ctx, (size_t)n * f, "predict input"));
+  TC_TRY(dout.alloc(ctx, (size_t)n * K, "predict output"));
+  cudaStream_t st = ctx->stream;
+  TC_CUDA(ctx, cudaMemcpyAsync(dx.p, X, (size_t)n * f * sizeof(float), cudaMemcpyHostToDevice, st));
+  TC_TRY(tc::predict_device(ctx, m, dx.p, n, f, transform, dout.p, st));
+  TC_CUDA(ctx, cudaMemcpyAsync(out, dout.p, (size_t)n * K * sizeof(float), cudaMemcpyDeviceToHost, st));
+  TC_CUDA(ctx, cudaStreamSynchronize(st));
+  return TC_OK;
+}
+
+tc_status tc_predict_device(tc_ctx* ctx, const tc_model* m, const float* X_dev, uint32_t n, uint16_t f,
+                            int32_t transform, float* out_dev, void* stream) {
+  if (!ctx || !m || (!X_dev && n) || (!out_dev && n)) return TC_ERR_INVALID_ARG;
+  if (f != (uint32_t)m->info.n_features)
+    return ctx->fail(TC_ERR_INVALID_ARG, "X has %u features, the model expects %d", f, m->info.n_features);
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  return tc::predict_device(ctx, m, X_dev, n, f, transform, out_dev, st);
+}
+
+}  // extern "C"

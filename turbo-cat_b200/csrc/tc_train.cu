@@ -1,0 +1,1435 @@
+// Symmetric (oblivious) tree boosting on the device.
+//
+// Restates Booster::train (src/boosting/booster.cpp:47-252, 438-463) and
+// SymmetricTree::build (src/tree/symmetric_tree.cpp:34-368) level by level:
+//
+//   grad       pred += lr * leaf(prev tree) (fused), loss gradients/hessians,
+//              leaf ids reset, per-block root sums            [one pass over rows]
+//   per level d = 0 .. D-1, for all classes k at once:
+//     hist     FP32 shared-memory histograms of the level's build set -- the
+//              root at d = 0, the smaller child of every sibling pair after --
+//              over row-major uint8 bins gathered through the node-grouped row
+//              list; one FP32 partial per (segment chunk, feature group)
+//     merge    FP64 sum of the partials (the cross-block merge) and the FP64
+//              sibling subtraction larger = parent - smaller
+//     scan     per (feature, node group): FP64 prefix (left, NaN slot
+//              included: NaN routes left) and suffix (right) sums and the
+//              Newton gain of every bin for every node, summed over nodes
+//     pick     per class: argmax over (feature, bin), lowest feature then
+//              lowest bin on ties (the reference keeps the first strictly
+//              greater gain), stop rules, the split goes into the model
+//     part     leaf = 2*leaf + go_right, go_right = bin != 255 && bin > t;
+//              per-block child counts and FP64 child sums
+//     reduce   child totals, smaller child per pair, scatter offsets
+//     plan     (one block) segment starts, the next level's work items,
+//              the stop pre-check, leaf values when the tree is complete
+//     scatter  node-grouped row list of the smaller children
+//
+// Every kernel reads the per-class "done" flag and returns early once a
+// tree has stopped, so an iteration is a fixed launch sequence that is
+// captured once as a CUDA graph and replayed (the batched path).  The plain
+// path launches one class and one level at a time with a host
+// synchronisation after every level.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+
+#include "tc_internal.h"
+
+namespace tc {
+namespace {
+
+constexpr int HIST_THREADS = 512;
+constexpr int PART_THREADS = 512;
+constexpr int SCAN_NODES = 16;    // nodes per scan block
+constexpr int MERGE_BB = 8;       // bins per merge block
+
+struct NodeStat {
+  double G, H;
+  uint32_t cnt;
+  uint32_t pad;
+};
+
+struct Item {
+  int32_t k, p, g, c;
+};
+
+struct SplitRec {
+  int32_t f, b;
+  double gain, second;
+};
+
+// Per-class, per-tree control block on the device.
+struct ClassState {
+  int32_t done;        // tree stopped
+  int32_t depth;       // accepted splits
+  int32_t f, b;        // split of the current level
+};
+
+struct DevCfg {
+  uint32_t n, f, fs, np;
+  int32_t K, D, nb_scan, loss;
+  int32_t KT, k0;                // classes in the model; first class of this launch view
+  int32_t msl;
+  float lr, lam, l1, mcw, msg, mds, gamma, alpha;
+  int32_t G, W, R;               // feature groups, group width (32*J), rows per chunk
+  int32_t PB;                    // partition blocks
+  int32_t item_cap;              // capacity of the item table
+  int32_t n_scan_groups_max;
+};
+
+struct DevPtrs {
+  const uint8_t* bins_rm;
+  const uint8_t* bins_cm;
+  const float* edges;            // [f][256]
+  const uint16_t* n_edges;
+  const float* y;
+  float* pred;                   // [K][n]
+  float2* gh;                    // [K][n]
+  uint16_t* leaf;                // [K][n]
+  uint32_t* rows;                // [K][n]
+  double2* hist[2];              // [K][2^(D-1)][F][256]
+  float2* part;                  // [item_cap][256][W]
+  Item* items;                   // [item_cap]
+  int32_t* n_items;              // [1]
+  int32_t* seg_start;            // [K][2^(D-1)]
+  int32_t* seg_len;              // [K][2^(D-1)]
+  int32_t* item_base;            // [K][2^(D-1)][G]
+  int32_t* n_chunks;             // [K][2^(D-1)]
+  int32_t* small;                // [K][2^(D-1)] child index of the smaller sibling
+  NodeStat* nstat;               // [K][D+1][2^D]
+  uint32_t* pcnt;                // [K][PB][2^D]
+  double2* psum;                 // [K][PB][2^D]
+  uint32_t* blk_off;             // [K][PB][2^(D-1)]
+  double* gpart;                 // [K][F][NG][256]
+  uint8_t* gany;                 // [K][F][NG][256]
+  ClassState* cs;                // [K]
+  int32_t* iter;                 // [1] boosting iteration (tree slot = iter*K + k)
+  // model arrays (capacity T = n_estimators*K)
+  int32_t* m_depth;              // [T]
+  uint16_t* m_feat;              // [T][D]
+  uint8_t* m_bin;                // [T][D]
+  float* m_thr;                  // [T][D]
+  double* m_gain;                // [T][D]
+  double* m_second;              // [T][D]
+  float* m_leaves;               // [T][2^D]
+  double* root_hist_out;         // optional [F][256][2]
+};
+
+__device__ __forceinline__ size_t hist_index(const DevCfg& c, int k, int node, int f, int b) {
+  return (((size_t)k * (1u << (c.D > 0 ? c.D - 1 : 0)) + node) * c.f + f) * kSlots + b;
+}
+
+// ------------------------------------------------------------------ grad --
+
+// fast_exp_avx2 lane arithmetic of the reference (src/boosting/loss.cpp:34-69).
+__device__ __forceinline__ float ref_fast_exp(float x) {
+  x = fmaxf(x, -88.0f);
+  x = fminf(x, 88.0f);
+  const float t = __fmul_rn(x, 1.4426950408889634f);
+  const float ti = rintf(t);
+  const float tf = __fsub_rn(t, ti);
+  float poly = __fmaf_rn(0.0013333558146428443f, tf, 0.009618129107628477f);
+  poly = __fmaf_rn(poly, tf, 0.05550410866482046f);
+  poly = __fmaf_rn(poly, tf, 0.2402265069591007f);
+  poly = __fmaf_rn(poly, tf, 0.6931471805599453f);
+  poly = __fmaf_rn(poly, tf, 1.0f);
+  const float pow2 = __int_as_float(((int)ti + 127) << 23);
+  return __fmul_rn(poly, pow2);
+}
+
+__device__ __forceinline__ void loss_grad(int loss, float pred, float y, uint32_t i, uint32_t n_vec,
+                                          float gamma, float alpha, float& g, float& h) {
+  if (loss == TC_LOSS_MSE) {  // src/boosting/loss.cpp:348-362
+    g = __fmul_rn(2.0f, __fsub_rn(pred, y));
+    h = 2.0f;
+  } else if (loss == TC_LOSS_LOGLOSS) {  // src/boosting/loss.cpp:123-211
+    float p;
+    if (i < n_vec) {
+      float x = fminf(fmaxf(pred, -15.0f), 15.0f);
+      p = __fdiv_rn(1.0f, __fadd_rn(1.0f, ref_fast_exp(__fsub_rn(0.0f, x))));
+    } else {
+      const float x = fmaxf(-15.0f, fminf(15.0f, pred));
+      p = __fdiv_rn(1.0f, __fadd_rn(1.0f, expf(-x)));
+    }
+    g = __fsub_rn(p, y);
+    h = fmaxf(__fmul_rn(p, __fsub_rn(1.0f, p)), 1e-6f);
+  } else {  // TC_LOSS_FOCAL, src/boosting/loss.cpp:505-539 (class weights 1)
+    const float p = __fdiv_rn(1.0f, __fadd_rn(1.0f, expf(-pred)));
+    float pt = __fmaf_rn(y, p, __fmul_rn(__fsub_rn(1.0f, y), __fsub_rn(1.0f, p)));
+    pt = fmaxf(pt, 1e-7f);
+    const float at = __fmaf_rn(y, alpha, __fmul_rn(__fsub_rn(1.0f, y), __fsub_rn(1.0f, alpha)));
+    const float fw = powf(__fsub_rn(1.0f, pt), gamma);
+    const float coef = __fmul_rn(at, fw);
+    g = __fmul_rn(coef, __fsub_rn(p, y));
+    h = fmaxf(__fmul_rn(__fmul_rn(coef, p), __fsub_rn(1.0f, p)), 1e-6f);
+  }
+}
+
+// One thread per row: applies the previous tree of every class
+// (preds += lr * leaf, fused multiply-add as in src/boosting/booster.cpp:458-463),
+// computes the gradients and resets the leaf ids; then per-block root sums
+// (FP64, fixed order) go to psum[k][block][0] / pcnt.
+__global__ void __launch_bounds__(512) k_grad(DevCfg c, DevPtrs P, int use_given_gh) {
+  __shared__ double sG[16], sH[16];
+  const int K = c.K;
+  const int it = *P.iter;
+  const uint32_t n_vec = (c.n / 8) * 8;
+  const uint32_t rows_per_block = (c.n + gridDim.x - 1) / gridDim.x;
+  const uint32_t r0 = blockIdx.x * rows_per_block;
+  const uint32_t r1 = min(c.n, r0 + rows_per_block);
+  const int L = 1 << c.D;
+  for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+    if (it > 0 && !use_given_gh) {
+      for (int k = 0; k < K; ++k) {
+        const size_t t = (size_t)(it - 1) * c.KT + c.k0 + k;
+        const float v = P.m_leaves[t * L + P.leaf[(size_t)k * c.n + i]];
+        float& pr = P.pred[(size_t)k * c.n + i];
+        pr = __fmaf_rn(c.lr, v, pr);
+      }
+    }
+    if (!use_given_gh) {
+      if (c.loss == TC_LOSS_SOFTMAX) {
+        // CrossEntropyLoss::compute_multiclass_gradients + softmax (src/boosting/loss.cpp:273-318)
+        float mx = P.pred[i];
+        for (int k = 1; k < K; ++k) mx = fmaxf(mx, P.pred[(size_t)k * c.n + i]);
+        float sum = 0.0f;
+        for (int k = 0; k < K; ++k) sum = __fadd_rn(sum, expf(__fsub_rn(P.pred[(size_t)k * c.n + i], mx)));
+        const int label = (int)P.y[i];
+        for (int k = 0; k < K; ++k) {
+          const float p = __fdiv_rn(expf(__fsub_rn(P.pred[(size_t)k * c.n + i], mx)), sum);
+          const float g = __fsub_rn(p, (k == label) ? 1.0f : 0.0f);
+          const float h = fmaxf(__fmul_rn(p, __fsub_rn(1.0f, p)), 1e-6f);
+          P.gh[(size_t)k * c.n + i] = make_float2(g, h);
+        }
+      } else {
+        float g, h;
+        loss_grad(c.loss, P.pred[i], P.y[i], i, n_vec, c.gamma, c.alpha, g, h);
+        P.gh[i] = make_float2(g, h);
+      }
+    }
+    for (int k = 0; k < K; ++k) P.leaf[(size_t)k * c.n + i] = 0;
+  }
+  // root sums per class: thread-local in row order, then a fixed-order block reduction
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int k = 0; k < K; ++k) {
+    double g = 0.0, h = 0.0;
+    for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+      const float2 v = P.gh[(size_t)k * c.n + i];
+      g += (double)v.x;
+      h += (double)v.y;
+    }
+    for (int o = 16; o; o >>= 1) {
+      g += __shfl_down_sync(0xffffffffu, g, o);
+      h += __shfl_down_sync(0xffffffffu, h, o);
+    }
+    if (lane == 0) { sG[warp] = g; sH[warp] = h; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double tg = 0.0, th = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { tg += sG[w]; th += sH[w]; }
+      const size_t o = ((size_t)k * c.PB + blockIdx.x) * L;
+      P.psum[o] = make_double2(tg, th);
+      P.pcnt[o] = r1 > r0 ? r1 - r0 : 0;
+    }
+    __syncthreads();
+  }
+}
+
+// Applies the last tree's leaves to the predictions (end of training / before
+// reading training scores).
+__global__ void k_apply_last(DevCfg c, DevPtrs P) {
+  const int it = *P.iter;
+  if (it <= 0) return;
+  const int L = 1 << c.D;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c.n; i += gridDim.x * blockDim.x) {
+    for (int k = 0; k < c.K; ++k) {
+      const size_t t = (size_t)(it - 1) * c.KT + c.k0 + k;
+      const float v = P.m_leaves[t * L + P.leaf[(size_t)k * c.n + i]];
+      float& pr = P.pred[(size_t)k * c.n + i];
+      pr = __fmaf_rn(c.lr, v, pr);
+      P.leaf[(size_t)k * c.n + i] = 0;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ hist --
+
+// Shared layout: column (feature within the group) fastest, so lane l of a
+// warp always hits bank l: float sm[(2*b + {0:grad,1:hess}) * W + col].
+template <int J>
+__global__ void __launch_bounds__(HIST_THREADS) k_hist(DevCfg c, DevPtrs P, int d) {
+  extern __shared__ float sm[];
+  constexpr int W = 32 * J;
+  const int n_items = *P.n_items;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const Item it = P.items[item];
+    const int k = it.k;
+    const int g0 = it.g * W;
+    const int gsize = min(W, (int)c.f - g0);
+    for (int q = threadIdx.x; q < 2 * kSlots * W; q += blockDim.x) sm[q] = 0.0f;
+    __syncthreads();
+    int start, end;
+    if (d == 0) {
+      start = it.c * c.R;
+      end = min((int)c.n, start + c.R);
+    } else {
+      const int s0 = P.seg_start[k * (1 << (c.D - 1)) + it.p];
+      const int sl = P.seg_len[k * (1 << (c.D - 1)) + it.p];
+      start = s0 + it.c * c.R;
+      end = min(s0 + sl, start + c.R);
+    }
+    const uint32_t* rows = P.rows + (size_t)k * c.n;
+    const float2* gh = P.gh + (size_t)k * c.n;
+    for (int base = start + warp * 4; base < end; base += nwarps * 4) {
+      uint32_t r[4];
+      float2 v[4];
+      uint8_t bb[4][J];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int idx = base + u;
+        r[u] = (idx < end) ? (d == 0 ? (uint32_t)idx : rows[idx]) : 0u;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const bool ok = base + u < end;
+        v[u] = ok ? gh[r[u]] : make_float2(0.f, 0.f);
+        const uint8_t* br = P.bins_rm + (size_t)r[u] * c.fs + g0;
+#pragma unroll
+        for (int j = 0; j < J; ++j) {
+          const int col = lane + 32 * j;
+          bb[u][j] = (ok && col < gsize) ? br[col] : (uint8_t)0;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (base + u < end) {
+#pragma unroll
+          for (int j = 0; j < J; ++j) {
+            const int col = lane + 32 * j;
+            if (col < gsize) {
+              atomicAdd(&sm[(2 * bb[u][j]) * W + col], v[u].x);
+              atomicAdd(&sm[(2 * bb[u][j] + 1) * W + col], v[u].y);
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+    float2* out = P.part + (size_t)item * kSlots * W;
+    for (int q = threadIdx.x; q < kSlots * W; q += blockDim.x) {
+      const int b = q / W, col = q % W;
+      out[q] = make_float2(sm[(2 * b) * W + col], sm[(2 * b + 1) * W + col]);
+    }
+    __syncthreads();
+  }
+}
+
+// ----------------------------------------------------------------- merge --
+
+// grid (256/MERGE_BB, segments, groups).  FP64 sum of a segment's partials
+// (fixed chunk order), then larger = parent - smaller (FP64).
+template <int J>
+__global__ void k_merge(DevCfg c, DevPtrs P, int d) {
+  constexpr int W = 32 * J;
+  __shared__ double2 tile[MERGE_BB][W];
+  const int P2 = d == 0 ? 1 : (1 << (d - 1));
+  const int seg = blockIdx.y;
+  const int k = seg / P2, p = seg % P2, g = blockIdx.z;
+  if (P.cs[k].done) return;
+  const int Pmax = 1 << (c.D - 1);
+  const int g0 = g * W;
+  const int gsize = min(W, (int)c.f - g0);
+  const int b0 = blockIdx.x * MERGE_BB;
+  const int nch = P.n_chunks[k * Pmax + p];
+  const int ib = P.item_base[(k * Pmax + p) * c.G + g];
+  // phase 1: column-fastest reads of the partials
+  for (int q = threadIdx.x; q < MERGE_BB * W; q += blockDim.x) {
+    const int bl = q / W, col = q % W;
+    double sg = 0.0, sh = 0.0;
+    if (col < gsize) {
+      for (int ch = 0; ch < nch; ++ch) {
+        const float2 v = P.part[((size_t)(ib + ch) * kSlots + b0 + bl) * W + col];
+        sg += (double)v.x;
+        sh += (double)v.y;
+      }
+    }
+    tile[bl][col] = make_double2(sg, sh);
+  }
+  __syncthreads();
+  double2* cur = P.hist[d & 1];
+  const double2* par = P.hist[(d & 1) ^ 1];
+  // phase 2: bin-fastest writes of both children
+  for (int q = threadIdx.x; q < MERGE_BB * W; q += blockDim.x) {
+    const int col = q / MERGE_BB, bl = q % MERGE_BB;
+    if (col >= gsize) continue;
+    const int f = g0 + col, b = b0 + bl;
+    const double2 s = tile[bl][col];
+    if (d == 0) {
+      cur[hist_index(c, k, 0, f, b)] = s;
+    } else {
+      const int sn = P.small[k * Pmax + p];
+      const int ln = sn ^ 1;
+      const double2 pv = par[hist_index(c, k, p, f, b)];
+      cur[hist_index(c, k, sn, f, b)] = s;
+      cur[hist_index(c, k, ln, f, b)] = make_double2(pv.x - s.x, pv.y - s.y);
+    }
+  }
+}
+
+// ------------------------------------------------------------------ scan --
+
+// Block-wide inclusive scan of (G, H) pairs over 256 threads.
+__device__ __forceinline__ double2 block_scan256(double2 v, double2* ws) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int o = 1; o < 32; o <<= 1) {
+    const double yg = __shfl_up_sync(0xffffffffu, v.x, o);
+    const double yh = __shfl_up_sync(0xffffffffu, v.y, o);
+    if (lane >= o) { v.x += yg; v.y += yh; }
+  }
+  if (lane == 31) ws[warp] = v;
+  __syncthreads();
+  double2 pre = make_double2(0.0, 0.0);
+  for (int w = 0; w < warp; ++w) { pre.x += ws[w].x; pre.y += ws[w].y; }
+  __syncthreads();
+  return make_double2(pre.x + v.x, pre.y + v.y);
+}
+
+// grid (F, node groups, K), 256 threads = bins.  Gain of every bin summed
+// over the group's nodes, in FP64 (the reference's formula,
+// src/tree/symmetric_tree.cpp:161-178 and 221-236).
+__global__ void __launch_bounds__(256) k_scan(DevCfg c, DevPtrs P, int d) {
+  __shared__ double2 ws[8];
+  const int f = blockIdx.x, ng = blockIdx.y, k = blockIdx.z;
+  if (P.cs[k].done) return;
+  const int nn = 1 << d;
+  const int b = threadIdx.x;
+  const double lam = (double)c.lam;
+  const double2* cur = P.hist[d & 1];
+  const NodeStat* ns = P.nstat + ((size_t)k * (c.D + 1) + d) * (1 << c.D);
+  double acc = 0.0;
+  uint8_t any = 0;
+  const int n0 = ng * SCAN_NODES, n1 = min(nn, n0 + SCAN_NODES);
+  for (int node = n0; node < n1; ++node) {
+    const NodeStat st = ns[node];
+    const double2 h = cur[hist_index(c, k, node, f, b)];
+    const double2 hv = (b < kNanBin) ? h : make_double2(0.0, 0.0);
+    // prefix over regular bins (thread b), NaN slot added to the left side
+    const double2 pre = block_scan256(hv, ws);
+    __shared__ double2 s_nan;
+    if (threadIdx.x == 255) s_nan = h;
+    // suffix: inclusive scan in reverse order
+    const int rb = 255 - b;
+    __shared__ double2 rev[256];
+    rev[rb] = hv;
+    __syncthreads();
+    const double2 rv = rev[b];
+    const double2 rs = block_scan256(rv, ws);  // thread b holds sum of bins >= 255-b
+    rev[255 - b] = rs;                         // rev[j] = sum over bins >= j
+    __syncthreads();
+    const double2 nv = s_nan;
+    if (st.cnt > 0 && b < c.nb_scan) {
+      const double lg = nv.x + pre.x, lh = nv.y + pre.y;
+      const double2 r = rev[b + 1];
+      if (lh >= 1e-10 && r.y >= 1e-10) {
+        const double pg = (st.H > 1e-10) ? (st.G * st.G) / (st.H + lam) : 0.0;
+        acc += 0.5 * ((lg * lg) / (lh + lam) + (r.x * r.x) / (r.y + lam) - pg);
+        any = 1;
+      }
+    }
+    __syncthreads();
+  }
+  const size_t o = (((size_t)k * c.f + f) * c.n_scan_groups_max + ng) * kSlots + b;
+  P.gpart[o] = acc;
+  P.gany[o] = any;
+}
+
+// ------------------------------------------------------------------ pick --
+
+struct Cand {
+  double gain, second;
+  int f, b;
+};
+
+__device__ __forceinline__ bool better(double ga, int fa, int ba, double gb, int fb, int bb) {
+  if (ga != gb) return ga > gb;
+  if (fa != fb) return fa < fb;
+  return ba < bb;
+}
+
+// grid (K), 1024 threads.  Reduces the per-group gain partials, applies the
+// reference's tie rule and stop rule, records the split.
+__global__ void __launch_bounds__(1024) k_pick(DevCfg c, DevPtrs P, int d) {
+  __shared__ double s_g[1024], s_2[1024];
+  __shared__ int s_f[1024], s_b[1024];
+  const int k = blockIdx.x;
+  ClassState& cs = P.cs[k];
+  if (cs.done) return;
+  const int nn = 1 << d;
+  const int ngroups = (nn + SCAN_NODES - 1) / SCAN_NODES;
+  double bg = -1e300, b2 = -1e300;
+  int bf = 0x7fffffff, bbin = 0x7fffffff;
+  const int total = (int)c.f * c.nb_scan;
+  for (int q = threadIdx.x; q < total; q += blockDim.x) {
+    const int f = q / c.nb_scan, b = q % c.nb_scan;
+    double s = 0.0;
+    uint8_t any = 0;
+    const size_t o = ((size_t)k * c.f + f) * c.n_scan_groups_max * kSlots + b;
+    for (int g = 0; g < ngroups; ++g) {
+      s += P.gpart[o + (size_t)g * kSlots];
+      any |= P.gany[o + (size_t)g * kSlots];
+    }
+    if (d == 0 && !any) continue;  // root: a candidate needs both sides non-empty
+    if (better(s, f, b, bg, bf, bbin)) {
+      b2 = bg;
+      bg = s; bf = f; bbin = b;
+    } else if (s > b2) {
+      b2 = s;
+    }
+  }
+  s_g[threadIdx.x] = bg; s_2[threadIdx.x] = b2; s_f[threadIdx.x] = bf; s_b[threadIdx.x] = bbin;
+  __syncthreads();
+  for (int stride = blockDim.x / 2; stride > 0; stride >>= 1) {
+    if (threadIdx.x < stride) {
+      const int o = threadIdx.x + stride;
+      const double g1 = s_g[threadIdx.x], g2 = s_g[o];
+      const double rest = fmax(s_2[threadIdx.x], s_2[o]);
+      if (better(g2, s_f[o], s_b[o], g1, s_f[threadIdx.x], s_b[threadIdx.x])) {
+        s_2[threadIdx.x] = fmax(g1, rest);
+        s_g[threadIdx.x] = g2; s_f[threadIdx.x] = s_f[o]; s_b[threadIdx.x] = s_b[o];
+      } else {
+        s_2[threadIdx.x] = fmax(g2, rest);
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double best = s_g[0];
+    const int f = s_f[0], b = s_b[0];
+    const int t = *P.iter * c.KT + c.k0 + k;
+    // no candidate (gain stays -1e30 in the reference) or below min_split_gain
+    // (src/tree/symmetric_tree.cpp:276-278); the gain compared is FP32 there
+    if (f == 0x7fffffff || (float)best < c.msg) {
+      cs.done = 1;
+      return;
+    }
+    float thr = 0.0f;
+    const int ne = P.n_edges[f];
+    if (b < ne) thr = P.edges[(size_t)f * kSlots + b];
+    else if (ne > 0) thr = P.edges[(size_t)f * kSlots + ne - 1];
+    P.m_feat[(size_t)t * c.D + d] = (uint16_t)f;
+    P.m_bin[(size_t)t * c.D + d] = (uint8_t)b;
+    P.m_thr[(size_t)t * c.D + d] = thr;
+    P.m_gain[(size_t)t * c.D + d] = best;
+    P.m_second[(size_t)t * c.D + d] = s_2[0];
+    cs.f = f;
+    cs.b = b;
+    cs.depth = d + 1;
+  }
+}
+
+// ------------------------------------------------------------- partition --
+
+// grid (PB, K).  Rows of block b: a contiguous range.  Updates leaf ids and
+// writes per-block child counts and FP64 sums.
+__global__ void __launch_bounds__(PART_THREADS) k_partition(DevCfg c, DevPtrs P, int d) {
+  extern __shared__ unsigned char smraw[];
+  const int k = blockIdx.y;
+  const ClassState cs = P.cs[k];
+  if (cs.done || cs.depth != d + 1) return;
+  const int nch = 1 << (d + 1);
+  double* sG = reinterpret_cast<double*>(smraw);
+  double* sH = sG + nch;
+  uint32_t* sC = reinterpret_cast<uint32_t*>(sH + nch);
+  for (int q = threadIdx.x; q < nch; q += blockDim.x) { sG[q] = 0.0; sH[q] = 0.0; sC[q] = 0; }
+  __syncthreads();
+  const uint32_t rpb = (c.n + gridDim.x - 1) / gridDim.x;
+  const uint32_t r0 = blockIdx.x * rpb, r1 = min(c.n, r0 + rpb);
+  const uint8_t* col = P.bins_cm + (size_t)cs.f * c.np;
+  uint16_t* leaf = P.leaf + (size_t)k * c.n;
+  const float2* gh = P.gh + (size_t)k * c.n;
+  const uint8_t t = (uint8_t)cs.b;
+  for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+    const uint8_t b = col[i];
+    const uint32_t right = (b != (uint8_t)kNanBin && b > t) ? 1u : 0u;
+    const uint32_t nl = ((uint32_t)leaf[i] << 1) | right;
+    leaf[i] = (uint16_t)nl;
+    const float2 v = gh[i];
+    atomicAdd(&sG[nl], (double)v.x);
+    atomicAdd(&sH[nl], (double)v.y);
+    atomicAdd(&sC[nl], 1u);
+  }
+  __syncthreads();
+  const int L = 1 << c.D;
+  for (int q = threadIdx.x; q < nch; q += blockDim.x) {
+    const size_t o = ((size_t)k * c.PB + blockIdx.x) * L + q;
+    P.psum[o] = make_double2(sG[q], sH[q]);
+    P.pcnt[o] = sC[q];
+  }
+}
+
+// grid (pairs, K), 256 threads.  Child totals (fixed-order FP64 sums over
+// blocks), the smaller sibling (left on a tie, src/tree/symmetric_tree.cpp:337-339),
+// and the per-block scatter offsets of its rows.
+__global__ void __launch_bounds__(256) k_node_reduce(DevCfg c, DevPtrs P, int d) {
+  const int k = blockIdx.y, p = blockIdx.x;
+  const ClassState cs = P.cs[k];
+  // d < 0 encodes the root reduction after the gradient pass
+  const bool root = d < 0;
+  if (!root && (cs.done || cs.depth != d + 1)) return;
+  const int L = 1 << c.D;
+  __shared__ double sg[2][256], sh[2][256];
+  __shared__ uint32_t sc[2][256];
+  const int nkids = root ? 1 : 2;
+  for (int kid = 0; kid < nkids; ++kid) {
+    const int child = root ? 0 : 2 * p + kid;
+    double g = 0.0, h = 0.0;
+    uint32_t cn = 0;
+    for (int blk = threadIdx.x; blk < c.PB; blk += blockDim.x) {
+      const size_t o = ((size_t)k * c.PB + blk) * L + child;
+      const double2 v = P.psum[o];
+      g += v.x; h += v.y; cn += P.pcnt[o];
+    }
+    sg[kid][threadIdx.x] = g; sh[kid][threadIdx.x] = h; sc[kid][threadIdx.x] = cn;
+  }
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      for (int kid = 0; kid < nkids; ++kid) {
+        sg[kid][threadIdx.x] += sg[kid][threadIdx.x + s];
+        sh[kid][threadIdx.x] += sh[kid][threadIdx.x + s];
+        sc[kid][threadIdx.x] += sc[kid][threadIdx.x + s];
+      }
+    }
+    __syncthreads();
+  }
+  const int lvl = root ? 0 : d + 1;
+  NodeStat* ns = P.nstat + ((size_t)k * (c.D + 1) + lvl) * L;
+  if (root) {
+    if (threadIdx.x == 0) ns[0] = NodeStat{sg[0][0], sh[0][0], sc[0][0], 0};
+    return;
+  }
+  const uint32_t cl = sc[0][0], cr = sc[1][0];
+  const int sm = (cl <= cr) ? 0 : 1;
+  if (threadIdx.x == 0) {
+    ns[2 * p] = NodeStat{sg[0][0], sh[0][0], cl, 0};
+    ns[2 * p + 1] = NodeStat{sg[1][0], sh[1][0], cr, 0};
+    const int Pmax = 1 << (c.D - 1);
+    if (d + 1 < c.D) {
+      P.small[k * Pmax + p] = 2 * p + sm;
+      P.seg_len[k * Pmax + p] = (int)(sm ? cr : cl);
+    }
+  }
+  if (d + 1 < c.D) {
+    // exclusive scan over blocks of the smaller child's counts (serial per
+    // thread 0 chunk; PB is a few hundred)
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int Pmax = 1 << (c.D - 1);
+      uint32_t run = 0;
+      for (int blk = 0; blk < c.PB; ++blk) {
+        const size_t o = ((size_t)k * c.PB + blk) * L + 2 * p + sm;
+        P.blk_off[((size_t)k * c.PB + blk) * Pmax + p] = run;
+        run += P.pcnt[o];
+      }
+    }
+  }
+}
+
+// One block.  Segment starts, work items for the next histogram level, stop
+// pre-check (src/tree/symmetric_tree.cpp:116-124) and leaf values.
+// d = level about to be histogrammed (0 = root, after the gradient pass).
+__global__ void k_plan(DevCfg c, DevPtrs P, int d, int k_only) {
+  __shared__ int s_items;
+  const int Pmax = 1 << (c.D - 1);
+  const int L = 1 << c.D;
+  if (threadIdx.x == 0) s_items = 0;
+  __syncthreads();
+  for (int k = 0; k < c.K; ++k) {
+    if (k_only >= 0 && k != k_only) continue;
+    ClassState& cs = P.cs[k];
+    if (threadIdx.x == 0) {
+      if (d == 0) { cs.done = 0; cs.depth = 0; }
+      bool alive = !cs.done && (d == 0 || cs.depth == d);
+      if (alive && d >= c.D) alive = false;
+      if (alive) {
+        // stop pre-check on the level-d nodes
+        const NodeStat* ns = P.nstat + ((size_t)k * (c.D + 1) + d) * L;
+        bool go = false;
+        const int nn = 1 << d;
+        for (int q = 0; q < nn && !go; ++q)
+          go = ns[q].cnt >= (uint32_t)c.msl * 2u && (float)ns[q].H >= c.mcw * 2.0f;
+        if (!go) alive = false;
+      }
+      if (!alive && !cs.done) cs.done = 1;
+      if (!cs.done) {
+        // segments and items
+        const int np2 = d == 0 ? 1 : (1 << (d - 1));
+        int run = 0;
+        for (int p = 0; p < np2; ++p) {
+          const int len = d == 0 ? (int)c.n : P.seg_len[k * Pmax + p];
+          P.seg_start[k * Pmax + p] = run;
+          run += len;
+          const int nch = (len + c.R - 1) / c.R;
+          P.n_chunks[k * Pmax + p] = nch;
+          for (int g = 0; g < c.G; ++g) {
+            P.item_base[(k * Pmax + p) * c.G + g] = s_items;
+            for (int ch = 0; ch < nch; ++ch) {
+              if (s_items < c.item_cap) P.items[s_items] = Item{k, p, g, ch};
+              ++s_items;
+            }
+          }
+        }
+      }
+      if (cs.done == 1) {
+        // leaf values of the finished tree (src/tree/symmetric_tree.cpp:357-367, 753-775)
+        const int t = *P.iter * c.KT + c.k0 + k;
+        const int dep = cs.depth;
+        P.m_depth[t] = dep;
+        const NodeStat* ns = P.nstat + ((size_t)k * (c.D + 1) + dep) * L;
+        for (int q = 0; q < (1 << dep); ++q) {
+          const double H = ns[q].H;
+          float v = 0.0f;
+          if (H >= 1e-10) {
+            double x = -ns[q].G / (H + (double)c.lam);
+            const double l1 = (double)c.l1;
+            if (l1 > 0) x = x > l1 ? x - l1 : (x < -l1 ? x + l1 : 0.0);
+            const double md = (double)c.mds;
+            if (md > 0) x = fmax(-md, fmin(md, x));
+            v = (float)x;
+          }
+          P.m_leaves[(size_t)t * L + q] = v;
+        }
+        for (int q = (1 << dep); q < L; ++q) P.m_leaves[(size_t)t * L + q] = 0.0f;
+        cs.done = 2;  // finalized
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *P.n_items = min(s_items, c.item_cap);
+}
+
+// grid (PB, K).  Row ids of the smaller children, grouped by pair.
+__global__ void __launch_bounds__(PART_THREADS) k_scatter(DevCfg c, DevPtrs P, int d) {
+  extern __shared__ uint32_t s_cur[];
+  const int k = blockIdx.y;
+  if (P.cs[k].done) return;
+  const int Pmax = 1 << (c.D - 1);
+  const int np2 = 1 << d;  // pairs at level d+1
+  for (int q = threadIdx.x; q < np2; q += blockDim.x) s_cur[q] = 0;
+  __syncthreads();
+  const uint32_t rpb = (c.n + gridDim.x - 1) / gridDim.x;
+  const uint32_t r0 = blockIdx.x * rpb, r1 = min(c.n, r0 + rpb);
+  const uint16_t* leaf = P.leaf + (size_t)k * c.n;
+  uint32_t* rows = P.rows + (size_t)k * c.n;
+  for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+    const int ch = leaf[i];
+    const int p = ch >> 1;
+    if (ch == P.small[k * Pmax + p]) {
+      const uint32_t pos = P.seg_start[k * Pmax + p] + P.blk_off[((size_t)k * c.PB + blockIdx.x) * Pmax + p] +
+                           atomicAdd(&s_cur[p], 1u);
+      rows[pos] = i;
+    }
+  }
+}
+
+__global__ void k_next_iter(DevPtrs P) { *P.iter += 1; }
+
+__global__ void k_root_hist_out(DevCfg c, DevPtrs P) {
+  // root histogram of class 0 (level 0, node 0), FP64 [F][256][2]
+  const double2* h = P.hist[0];
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < (size_t)c.f * kSlots;
+       q += (size_t)gridDim.x * blockDim.x) {
+    const double2 v = h[q];
+    P.root_hist_out[2 * q] = v.x;
+    P.root_hist_out[2 * q + 1] = v.y;
+  }
+}
+
+}  // namespace
+}  // namespace tc
+
+// ---------------------------------------------------------------- trainer --
+
+using namespace tc;
+
+#define TC_CUDA_VOID(call) (void)(call)
+
+struct tc_trainer {
+  tc_ctx* ctx = nullptr;
+  tc_dataset* ds = nullptr;
+  tc_train_params prm{};
+  DevCfg cfg{};
+  DevPtrs ptr{};
+  int J = 2;
+  int hist_grid = 0;
+  int T_cap = 0;
+  int iters_done = 0;
+  float base = 0.0f;
+  double seconds = 0.0;
+  bool scores_dirty = false;
+  cudaGraphExec_t graph = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  DevBuf<float> pred;
+  DevBuf<float2> gh;
+  DevBuf<uint16_t> leaf;
+  DevBuf<uint32_t> rows;
+  DevBuf<double2> hist0, hist1;
+  DevBuf<float2> part;
+  DevBuf<Item> items;
+  DevBuf<int32_t> n_items, seg_start, seg_len, item_base, n_chunks, small, iter;
+  DevBuf<NodeStat> nstat;
+  DevBuf<uint32_t> pcnt, blk_off;
+  DevBuf<double2> psum;
+  DevBuf<double> gpart;
+  DevBuf<uint8_t> gany;
+  DevBuf<ClassState> cs;
+  DevBuf<int32_t> m_depth;
+  DevBuf<uint16_t> m_feat;
+  DevBuf<uint8_t> m_bin;
+  DevBuf<float> m_thr, m_leaves;
+  DevBuf<double> m_gain, m_second;
+  DevBuf<double> root_hist;
+
+  ~tc_trainer() {
+    for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
+    if (graph) cudaGraphExecDestroy(graph);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+  }
+
+  bool given_gh = false;
+  int64_t launches = 0;
+  int launches_per_iter = 0;
+  // profiling: when prof != nullptr every launch is bracketed by events
+  struct ProfRec {
+    int cls;
+    cudaEvent_t a, b;
+    double bytes;
+    int level;
+    double rows;
+  };
+  std::vector<ProfRec>* prof = nullptr;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  int cur_cls = -1;
+  void mark_begin(int cls, cudaStream_t st);
+  void mark_end(cudaStream_t st, double bytes = 0.0);
+  tc_status setup(int given_gh_rows_only);
+  void launch_level(const DevCfg& c, const DevPtrs& P, int d, cudaStream_t st);
+  tc_status enqueue_iteration(cudaStream_t st);
+  tc_status run_plain_iteration(cudaStream_t st);
+  tc_status init_predictions();
+  tc_status step(int iters, bool sync);
+};
+
+namespace {
+
+template <int J>
+void set_hist_attr() {
+  cudaFuncSetAttribute(k_hist<J>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kSlots * 32 * J * 4);
+}
+
+}  // namespace
+
+tc_status tc_trainer::setup(int) {
+  const uint32_t n = ds->n, f = ds->f;
+  const int K = prm.loss == TC_LOSS_SOFTMAX ? prm.n_classes : 1;
+  const int D = prm.max_depth;
+  // feature groups: J*32 columns per block, groups as even as possible
+  int J_ = prm.hist_features_per_block ? prm.hist_features_per_block / 32 : 0;
+  if (J_ < 1 || J_ > 3) {
+    // default: the fewest groups whose width fits in 3*32 columns, then the
+    // narrowest J covering the per-group size
+    int G = (int)((f + 95) / 96);
+    int per = (int)((f + G - 1) / G);
+    J_ = (per + 31) / 32;
+  }
+  J = J_;
+  const int W = 32 * J;
+  const int G = (int)((f + W - 1) / W);
+  int R = prm.hist_rows_per_chunk;
+  const int blocks_per_sm = (2 * kSlots * W * 4 <= 100 * 1024) ? 2 : 1;
+  hist_grid = ctx->sm_count * blocks_per_sm;
+  if (R <= 0) {
+    // about two waves of items at the root
+    const long long target = (long long)hist_grid;
+    R = (int)std::max<long long>(1024, ((long long)n * G + target - 1) / target);
+  }
+  const int PB = ctx->sm_count * 2;
+  const int Pmax = 1 << (D - 1);
+  const int L = 1 << D;
+  // item capacity: chunks of every segment of every class at the widest level
+  const long long cap = (long long)K * G * ((n + R - 1) / R + Pmax + 1);
+  const int ngroups_max = (L / 2 + SCAN_NODES - 1) / SCAN_NODES;
+
+  cfg.n = n; cfg.f = f; cfg.fs = ds->fs; cfg.np = ds->np;
+  cfg.K = K; cfg.KT = K; cfg.k0 = 0; cfg.D = D; cfg.nb_scan = (int)(uint8_t)prm.max_bins - 1; cfg.loss = prm.loss;
+  cfg.msl = prm.min_samples_leaf; cfg.lr = prm.learning_rate; cfg.lam = prm.lambda_l2; cfg.l1 = prm.lambda_l1;
+  cfg.mcw = prm.min_child_weight; cfg.msg = prm.min_split_gain; cfg.mds = prm.max_delta_step;
+  cfg.gamma = prm.focal_gamma; cfg.alpha = prm.focal_alpha;
+  cfg.G = G; cfg.W = W; cfg.R = R; cfg.PB = PB; cfg.item_cap = (int)cap;
+  cfg.n_scan_groups_max = std::max(1, ngroups_max);
+
+  T_cap = prm.n_estimators * K;
+  TC_TRY(pred.alloc(ctx, (size_t)K * n, "predictions"));
+  TC_TRY(gh.alloc(ctx, (size_t)K * n, "gradients"));
+  TC_TRY(leaf.alloc(ctx, (size_t)K * n, "leaf ids"));
+  TC_TRY(rows.alloc(ctx, (size_t)K * n, "row lists"));
+  const size_t hsz = (size_t)K * Pmax * f * kSlots;
+  TC_TRY(hist0.alloc(ctx, hsz, "level histograms"));
+  TC_TRY(hist1.alloc(ctx, hsz, "level histograms"));
+  TC_TRY(part.alloc(ctx, (size_t)cap * kSlots * W, "histogram partials"));
+  TC_TRY(items.alloc(ctx, (size_t)cap, "work items"));
+  TC_TRY(n_items.alloc(ctx, 1, "item count"));
+  TC_TRY(seg_start.alloc(ctx, (size_t)K * Pmax, "segments"));
+  TC_TRY(seg_len.alloc(ctx, (size_t)K * Pmax, "segments"));
+  TC_TRY(item_base.alloc(ctx, (size_t)K * Pmax * G, "segments"));
+  TC_TRY(n_chunks.alloc(ctx, (size_t)K * Pmax, "segments"));
+  TC_TRY(small.alloc(ctx, (size_t)K * Pmax, "segments"));
+  TC_TRY(iter.alloc(ctx, 1, "iteration"));
+  TC_TRY(nstat.alloc(ctx, (size_t)K * (D + 1) * L, "node stats"));
+  TC_TRY(pcnt.alloc(ctx, (size_t)K * PB * L, "partition counts"));
+  TC_TRY(psum.alloc(ctx, (size_t)K * PB * L, "partition sums"));
+  TC_TRY(blk_off.alloc(ctx, (size_t)K * PB * Pmax, "scatter offsets"));
+  TC_TRY(gpart.alloc(ctx, (size_t)K * f * cfg.n_scan_groups_max * kSlots, "gain partials"));
+  TC_TRY(gany.alloc(ctx, (size_t)K * f * cfg.n_scan_groups_max * kSlots, "gain flags"));
+  TC_TRY(cs.alloc(ctx, K, "class state"));
+  TC_TRY(m_depth.alloc(ctx, T_cap, "model"));
+  TC_TRY(m_feat.alloc(ctx, (size_t)T_cap * D, "model"));
+  TC_TRY(m_bin.alloc(ctx, (size_t)T_cap * D, "model"));
+  TC_TRY(m_thr.alloc(ctx, (size_t)T_cap * D, "model"));
+  TC_TRY(m_gain.alloc(ctx, (size_t)T_cap * D, "model"));
+  TC_TRY(m_second.alloc(ctx, (size_t)T_cap * D, "model"));
+  TC_TRY(m_leaves.alloc(ctx, (size_t)T_cap * L, "model"));
+
+  ptr.bins_rm = ds->bins_rm.p; ptr.bins_cm = ds->bins_cm.p; ptr.edges = ds->edges.p; ptr.n_edges = ds->n_edges.p;
+  ptr.y = ds->y.p; ptr.pred = pred.p; ptr.gh = gh.p; ptr.leaf = leaf.p; ptr.rows = rows.p;
+  ptr.hist[0] = hist0.p; ptr.hist[1] = hist1.p; ptr.part = part.p; ptr.items = items.p; ptr.n_items = n_items.p;
+  ptr.seg_start = seg_start.p; ptr.seg_len = seg_len.p; ptr.item_base = item_base.p; ptr.n_chunks = n_chunks.p;
+  ptr.small = small.p; ptr.nstat = nstat.p; ptr.pcnt = pcnt.p; ptr.psum = psum.p; ptr.blk_off = blk_off.p;
+  ptr.gpart = gpart.p; ptr.gany = gany.p; ptr.cs = cs.p; ptr.iter = iter.p;
+  ptr.m_depth = m_depth.p; ptr.m_feat = m_feat.p; ptr.m_bin = m_bin.p; ptr.m_thr = m_thr.p; ptr.m_gain = m_gain.p;
+  ptr.m_second = m_second.p; ptr.m_leaves = m_leaves.p; ptr.root_hist_out = nullptr;
+
+  set_hist_attr<1>();
+  set_hist_attr<2>();
+  set_hist_attr<3>();
+  cudaFuncSetAttribute(k_partition, cudaFuncAttributeMaxDynamicSharedMemorySize, 20 * L);
+  TC_CUDA(ctx, cudaEventCreate(&ev0));
+  TC_CUDA(ctx, cudaEventCreate(&ev1));
+  return TC_OK;
+}
+
+enum { KC_GRAD, KC_HIST, KC_MERGE, KC_SCAN, KC_PICK, KC_PART, KC_REDUCE, KC_PLAN, KC_SCATTER, KC_OTHER, KC_N };
+static const char* kKernelNames[KC_N] = {"grad", "hist", "merge", "scan", "pick", "partition",
+                                         "node_reduce", "plan", "scatter", "other"};
+
+void tc_trainer::mark_begin(int cls, cudaStream_t st) {
+  ++launches;
+  if (!prof) return;
+  if (ev_used + 2 > ev_pool.size()) {
+    for (int i = 0; i < 64; ++i) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      ev_pool.push_back(e);
+    }
+  }
+  ProfRec r{cls, ev_pool[ev_used], ev_pool[ev_used + 1], 0.0, -1, 0.0};
+  ev_used += 2;
+  cudaEventRecord(r.a, st);
+  prof->push_back(r);
+}
+
+void tc_trainer::mark_end(cudaStream_t st, double bytes) {
+  if (!prof) return;
+  cudaEventRecord(prof->back().b, st);
+  prof->back().bytes = bytes;
+}
+
+// All launches of level d for the classes of view (c, P).
+void tc_trainer::launch_level(const DevCfg& c, const DevPtrs& P, int d, cudaStream_t st) {
+  const int K = c.K, D = c.D;
+  const size_t smem = (size_t)2 * kSlots * 32 * J * 4;
+  double hist_bytes = 0.0, hist_rows = 0.0;
+  if (prof) {
+    // algorithmic bytes: rows histogrammed at this level (device counts)
+    TC_CUDA_VOID(cudaStreamSynchronize(st));
+    std::vector<ClassState> h(K);
+    cudaMemcpy(h.data(), P.cs, K * sizeof(ClassState), cudaMemcpyDeviceToHost);
+    const int Pmax = 1 << (D - 1);
+    double rows = 0.0, nodes = 0.0;
+    for (int k = 0; k < K; ++k) {
+      if (h[k].done) continue;
+      if (d == 0) {
+        rows += c.n;
+        nodes += 1;
+      } else {
+        std::vector<int32_t> sl(1 << (d - 1));
+        cudaMemcpy(sl.data(), P.seg_len + (size_t)k * Pmax, sl.size() * sizeof(int32_t), cudaMemcpyDeviceToHost);
+        for (int32_t v : sl) rows += v;
+        nodes += (double)sl.size();
+      }
+    }
+    hist_bytes = rows * (c.f + 8.0) + (d > 0 ? rows * 4.0 : 0.0) + nodes * c.f * kSlots * 8.0;
+    hist_rows = rows;
+  }
+  mark_begin(KC_HIST, st);
+  if (J == 1) k_hist<1><<<hist_grid, HIST_THREADS, smem, st>>>(c, P, d);
+  else if (J == 2) k_hist<2><<<hist_grid, HIST_THREADS, smem, st>>>(c, P, d);
+  else k_hist<3><<<hist_grid, HIST_THREADS, smem, st>>>(c, P, d);
+  mark_end(st, hist_bytes);
+  if (prof) {
+    prof->back().level = d;
+    prof->back().rows = hist_rows;
+  }
+  const int P2 = d == 0 ? 1 : (1 << (d - 1));
+  dim3 mg(kSlots / MERGE_BB, K * P2, c.G);
+  mark_begin(KC_MERGE, st);
+  if (J == 1) k_merge<1><<<mg, 256, 0, st>>>(c, P, d);
+  else if (J == 2) k_merge<2><<<mg, 256, 0, st>>>(c, P, d);
+  else k_merge<3><<<mg, 256, 0, st>>>(c, P, d);
+  mark_end(st);
+  const int ng = ((1 << d) + SCAN_NODES - 1) / SCAN_NODES;
+  mark_begin(KC_SCAN, st);
+  k_scan<<<dim3(c.f, ng, K), 256, 0, st>>>(c, P, d);
+  mark_end(st);
+  mark_begin(KC_PICK, st);
+  k_pick<<<K, 1024, 0, st>>>(c, P, d);
+  mark_end(st);
+  mark_begin(KC_PART, st);
+  k_partition<<<dim3(c.PB, K), PART_THREADS, 20 * (2 << d), st>>>(c, P, d);
+  mark_end(st, (double)c.n * K * (1 + 2 + 2 + 8));
+  mark_begin(KC_REDUCE, st);
+  k_node_reduce<<<dim3(1 << d, K), 256, 0, st>>>(c, P, d);
+  mark_end(st);
+  mark_begin(KC_PLAN, st);
+  k_plan<<<1, 32, 0, st>>>(c, P, d + 1, -1);
+  mark_end(st);
+  if (d + 1 < D) {
+    mark_begin(KC_SCATTER, st);
+    k_scatter<<<dim3(c.PB, K), PART_THREADS, sizeof(uint32_t) * (1 << d), st>>>(c, P, d);
+    mark_end(st);
+  }
+}
+
+// The whole iteration as a fixed launch sequence (graph-capturable).
+tc_status tc_trainer::enqueue_iteration(cudaStream_t st) {
+  const int K = cfg.K, D = cfg.D;
+  mark_begin(KC_GRAD, st);
+  k_grad<<<cfg.PB, 512, 0, st>>>(cfg, ptr, 0);
+  mark_end(st, (double)cfg.n * K * (4 + 4 + 8 + 2 + 8) + (double)cfg.n * 4);
+  mark_begin(KC_REDUCE, st);
+  k_node_reduce<<<dim3(1, K), 256, 0, st>>>(cfg, ptr, -1);
+  mark_end(st);
+  mark_begin(KC_PLAN, st);
+  k_plan<<<1, 32, 0, st>>>(cfg, ptr, 0, -1);
+  mark_end(st);
+  for (int d = 0; d < D; ++d) launch_level(cfg, ptr, d, st);
+  mark_begin(KC_OTHER, st);
+  k_next_iter<<<1, 1, 0, st>>>(ptr);
+  mark_end(st);
+  return TC_OK;
+}
+
+// Class-k view of the device state (K = 1 launches of the plain path).
+static DevPtrs class_view(const DevCfg& c, const DevPtrs& P, int k, DevCfg* one) {
+  DevPtrs pk = P;
+  const size_t n = c.n;
+  const int Pmax = 1 << (c.D - 1), L = 1 << c.D;
+  *one = c;
+  one->K = 1;
+  one->k0 = k;
+  pk.pred += k * n; pk.gh += k * n; pk.leaf += k * n; pk.rows += k * n;
+  pk.hist[0] += (size_t)k * Pmax * c.f * kSlots;
+  pk.hist[1] += (size_t)k * Pmax * c.f * kSlots;
+  pk.seg_start += k * Pmax; pk.seg_len += k * Pmax; pk.item_base += (size_t)k * Pmax * c.G;
+  pk.n_chunks += k * Pmax; pk.small += k * Pmax; pk.nstat += (size_t)k * (c.D + 1) * L;
+  pk.pcnt += (size_t)k * c.PB * L; pk.psum += (size_t)k * c.PB * L; pk.blk_off += (size_t)k * c.PB * Pmax;
+  pk.gpart += (size_t)k * c.f * c.n_scan_groups_max * kSlots;
+  pk.gany += (size_t)k * c.f * c.n_scan_groups_max * kSlots;
+  pk.cs += k;
+  return pk;
+}
+
+// The plain path: one class and one level per launch group, a host
+// synchronisation after every level (the host reads the stop flag), no graph.
+tc_status tc_trainer::run_plain_iteration(cudaStream_t st) {
+  const int K = cfg.K, D = cfg.D;
+  k_grad<<<cfg.PB, 512, 0, st>>>(cfg, ptr, 0);
+  k_node_reduce<<<dim3(1, K), 256, 0, st>>>(cfg, ptr, -1);
+  for (int k = 0; k < K; ++k) {
+    DevCfg one;
+    DevPtrs pk = class_view(cfg, ptr, k, &one);
+    k_plan<<<1, 32, 0, st>>>(one, pk, 0, -1);
+    for (int d = 0; d < D; ++d) {
+      TC_CUDA(ctx, cudaStreamSynchronize(st));
+      ClassState h;
+      TC_CUDA(ctx, cudaMemcpy(&h, pk.cs, sizeof(h), cudaMemcpyDeviceToHost));
+      if (h.done) break;
+      launch_level(one, pk, d, st);
+    }
+  }
+  k_next_iter<<<1, 1, 0, st>>>(ptr);
+  TC_CUDA(ctx, cudaGetLastError());
+  return TC_OK;
+}
+
+tc_status tc_trainer::init_predictions() {
+  cudaStream_t st = ctx->stream;
+  // base prediction on the host from the labels (Loss::init_prediction,
+  // src/boosting/loss.cpp:217-226, 364-370, 545-553; 0 for softmax)
+  base = 0.0f;
+  if (prm.loss != TC_LOSS_SOFTMAX && !given_gh) {
+    std::vector<float> y(cfg.n);
+    TC_CUDA(ctx, cudaMemcpyAsync(y.data(), ds->y.p, cfg.n * sizeof(float), cudaMemcpyDeviceToHost, st));
+    TC_CUDA(ctx, cudaStreamSynchronize(st));
+    float sum = 0.0f;
+    for (uint32_t i = 0; i < cfg.n; ++i) sum += y[i];
+    float p = sum / (float)cfg.n;
+    if (prm.loss == TC_LOSS_MSE) {
+      base = p;
+    } else {
+      p = std::max(1e-7f, std::min(1.0f - 1e-7f, p));
+      base = std::log(p / (1.0f - p));
+    }
+  }
+  std::vector<float> h((size_t)cfg.K * cfg.n, base);
+  TC_CUDA(ctx, cudaMemcpyAsync(pred.p, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+  TC_CUDA(ctx, cudaMemsetAsync(leaf.p, 0, leaf.bytes(), st));
+  TC_CUDA(ctx, cudaMemsetAsync(iter.p, 0, sizeof(int32_t), st));
+  TC_CUDA(ctx, cudaMemsetAsync(cs.p, 0, cs.bytes(), st));
+  TC_CUDA(ctx, cudaMemsetAsync(m_depth.p, 0, m_depth.bytes(), st));
+  TC_CUDA(ctx, cudaMemsetAsync(m_feat.p, 0, m_feat.bytes(), st));
+  TC_CUDA(ctx, cudaMemsetAsync(m_bin.p, 0, m_bin.bytes(), st));
+  TC_CUDA(ctx, cudaMemsetAsync(m_thr.p, 0, m_thr.bytes(), st));
+  TC_CUDA(ctx, cudaMemsetAsync(m_gain.p, 0, m_gain.bytes(), st));
+  TC_CUDA(ctx, cudaMemsetAsync(m_second.p, 0, m_second.bytes(), st));
+  TC_CUDA(ctx, cudaMemsetAsync(m_leaves.p, 0, m_leaves.bytes(), st));
+  TC_CUDA(ctx, cudaStreamSynchronize(st));
+  iters_done = 0;
+  seconds = 0.0;
+  return TC_OK;
+}
+
+tc_status tc_trainer::step(int iters, bool sync) {
+  cudaStream_t st = ctx->stream;
+  if (iters < 0 || iters_done + iters > prm.n_estimators)
+    return ctx->fail(TC_ERR_INVALID_ARG, "step(%d) exceeds n_estimators=%d (done %d)", iters,
+                     prm.n_estimators, iters_done);
+  if (iters == 0) return TC_OK;
+  TC_CUDA(ctx, cudaEventRecord(ev0, st));
+  if (prm.batched) {
+    if (!graph) {
+      cudaGraph_t g;
+      const int64_t l0 = launches;
+      TC_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      enqueue_iteration(st);
+      TC_CUDA(ctx, cudaStreamEndCapture(st, &g));
+      launches_per_iter = (int)(launches - l0);
+      launches = l0;
+      cudaError_t e = cudaGraphInstantiate(&graph, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return ctx->cuda_fail(e, "cudaGraphInstantiate");
+    }
+    for (int i = 0; i < iters; ++i) TC_CUDA(ctx, cudaGraphLaunch(graph, st));
+    launches += (int64_t)launches_per_iter * iters;
+  } else {
+    for (int i = 0; i < iters; ++i) TC_TRY(run_plain_iteration(st));
+  }
+  TC_CUDA(ctx, cudaEventRecord(ev1, st));
+  TC_CUDA(ctx, cudaGetLastError());
+  iters_done += iters;
+  scores_dirty = true;
+  if (sync) {
+    TC_CUDA(ctx, cudaEventSynchronize(ev1));
+    float ms = 0.0f;
+    TC_CUDA(ctx, cudaEventElapsedTime(&ms, ev0, ev1));
+    seconds += ms * 1e-3;
+  }
+  return TC_OK;
+}
+
+// ------------------------------------------------------------------ C ABI --
+
+static tc_status validate(tc_ctx* ctx, const tc_dataset* ds, const tc_train_params* p) {
+  if (!ds->quantized) return ctx->fail(TC_ERR_INVALID_ARG, "dataset is not quantized");
+  if (p->max_depth < 1 || p->max_depth > kMaxDepth)
+    return ctx->fail(TC_ERR_INVALID_ARG, "max_depth must be in [1, %d]", kMaxDepth);
+  if (p->max_bins < 2 || p->max_bins > 255)
+    return ctx->fail(TC_ERR_INVALID_ARG, "max_bins cannot exceed 255 (uint8 limit)");
+  if (!(p->learning_rate > 0.0f) || p->learning_rate > 1.0f)
+    return ctx->fail(TC_ERR_INVALID_ARG, "learning_rate must be in (0, 1]");
+  if (p->loss < TC_LOSS_LOGLOSS || p->loss > TC_LOSS_SOFTMAX) return ctx->fail(TC_ERR_INVALID_ARG, "unknown loss");
+  if (p->loss == TC_LOSS_SOFTMAX && (p->n_classes < 3 || p->n_classes > 16))
+    return ctx->fail(TC_ERR_INVALID_ARG, "softmax needs 3 <= n_classes <= 16");
+  if (p->n_estimators < 0) return ctx->fail(TC_ERR_INVALID_ARG, "n_estimators must be >= 0");
+  if (ds->n == 0) return ctx->fail(TC_ERR_INVALID_ARG, "empty dataset");
+  if (p->loss != TC_LOSS_SOFTMAX || true) {
+    if (!ds->y.p) return ctx->fail(TC_ERR_INVALID_ARG, "dataset has no labels");
+  }
+  return TC_OK;
+}
+
+extern "C" {
+
+tc_status tc_trainer_create(tc_ctx* ctx, tc_dataset* ds, const tc_train_params* p, tc_trainer** out) {
+  if (!ctx || !ds || !p || !out) return TC_ERR_INVALID_ARG;
+  *out = nullptr;
+  cudaSetDevice(ctx->device);
+  TC_TRY(validate(ctx, ds, p));
+  tc_trainer* tr = new tc_trainer();
+  tr->ctx = ctx;
+  tr->ds = ds;
+  tr->prm = *p;
+  tc_status s = tr->setup(0);
+  if (s == TC_OK) s = tr->init_predictions();
+  if (s != TC_OK) {
+    delete tr;
+    return s;
+  }
+  *out = tr;
+  return TC_OK;
+}
+
+tc_status tc_trainer_step(tc_trainer* tr, int32_t iterations, int sync) {
+  if (!tr) return TC_ERR_INVALID_ARG;
+  cudaSetDevice(tr->ctx->device);
+  return tr->step(iterations, sync != 0);
+}
+
+tc_status tc_trainer_reset(tc_trainer* tr) {
+  if (!tr) return TC_ERR_INVALID_ARG;
+  cudaSetDevice(tr->ctx->device);
+  return tr->init_predictions();
+}
+
+tc_status tc_trainer_stats(tc_trainer* tr, tc_train_stats* st) {
+  if (!tr || !st) return TC_ERR_INVALID_ARG;
+  st->n_trees = tr->iters_done * tr->cfg.K;
+  st->iterations_done = tr->iters_done;
+  st->base_prediction = tr->base;
+  st->seconds = tr->seconds;
+  st->hist_features_per_block = tr->cfg.W;
+  st->hist_rows_per_chunk = tr->cfg.R;
+  st->kernel_launches = tr->launches;
+  return TC_OK;
+}
+
+tc_status tc_trainer_profile(tc_trainer* tr, int32_t iterations, tc_profile* out) {
+  if (!tr || !out || iterations < 0) return TC_ERR_INVALID_ARG;
+  tc_ctx* ctx = tr->ctx;
+  cudaSetDevice(ctx->device);
+  if (tr->iters_done + iterations > tr->prm.n_estimators)
+    return ctx->fail(TC_ERR_INVALID_ARG, "profile(%d) exceeds n_estimators", iterations);
+  cudaStream_t st = ctx->stream;
+  std::vector<tc_trainer::ProfRec> recs;
+  tr->prof = &recs;
+  tr->ev_used = 0;
+  for (int i = 0; i < iterations; ++i) {
+    tr->enqueue_iteration(st);
+    // harvest every iteration so that the event pool stays small
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+      tr->prof = nullptr;
+      return ctx->cuda_fail(e, "profiled iteration");
+    }
+    for (const auto& r : recs) {
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, r.a, r.b);
+      tc_kernel_time& k = out->k[r.cls];
+      k.launches += 1;
+      k.ms += ms;
+      k.alg_bytes += r.bytes;
+      if (r.level >= 0 && r.level < 16) {
+        out->hist_level_ms[r.level] += ms;
+        out->hist_level_rows[r.level] += r.rows;
+      }
+    }
+    recs.clear();
+    tr->ev_used = 0;
+  }
+  tr->prof = nullptr;
+  tr->iters_done += iterations;
+  tr->scores_dirty = true;
+  out->n_kernels = KC_N;
+  for (int c = 0; c < KC_N; ++c) {
+    std::strncpy(out->k[c].name, kKernelNames[c], sizeof(out->k[c].name) - 1);
+  }
+  return TC_OK;
+}
+
+tc_status tc_trainer_train_scores(tc_trainer* tr, float* out) {
+  if (!tr || !out) return TC_ERR_INVALID_ARG;
+  tc_ctx* ctx = tr->ctx;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  // apply the last tree to a scratch copy so that training can continue
+  DevBuf<float> tmp;
+  DevBuf<uint16_t> lf;
+  TC_TRY(tmp.alloc(ctx, tr->pred.n, "score copy"));
+  TC_TRY(lf.alloc(ctx, tr->leaf.n, "leaf copy"));
+  TC_CUDA(ctx, cudaMemcpyAsync(tmp.p, tr->pred.p, tr->pred.bytes(), cudaMemcpyDeviceToDevice, st));
+  TC_CUDA(ctx, cudaMemcpyAsync(lf.p, tr->leaf.p, tr->leaf.bytes(), cudaMemcpyDeviceToDevice, st));
+  DevPtrs P = tr->ptr;
+  P.pred = tmp.p;
+  P.leaf = lf.p;
+  k_apply_last<<<tr->ctx->sm_count * 4, 256, 0, st>>>(tr->cfg, P);
+  const uint32_t n = tr->cfg.n;
+  const int K = tr->cfg.K;
+  std::vector<float> h((size_t)K * n);
+  TC_CUDA(ctx, cudaMemcpyAsync(h.data(), tmp.p, h.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+  TC_CUDA(ctx, cudaStreamSynchronize(st));
+  for (uint32_t i = 0; i < n; ++i)
+    for (int k = 0; k < K; ++k) out[(size_t)i * K + k] = h[(size_t)k * n + i];
+  return TC_OK;
+}
+
+tc_status tc_trainer_model(tc_trainer* tr, tc_model** out) {
+  if (!tr || !out) return TC_ERR_INVALID_ARG;
+  tc_ctx* ctx = tr->ctx;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  const int K = tr->cfg.K, D = tr->cfg.D, L = 1 << D;
+  const int T = tr->iters_done * K;
+  tc_model* m = new tc_model();
+  m->ctx = ctx;
+  m->info.n_trees = T;
+  m->info.n_classes = K;
+  m->info.max_depth = D;
+  m->info.n_features = (int)tr->cfg.f;
+  m->info.task = tr->prm.loss == TC_LOSS_SOFTMAX ? TC_TASK_MULTICLASS
+                 : (tr->prm.loss == TC_LOSS_MSE ? TC_TASK_REGRESSION : TC_TASK_BINARY);
+  m->info.base_prediction = tr->base;
+  m->info.learning_rate = tr->prm.learning_rate;
+  m->info.lambda_l2 = tr->prm.lambda_l2;
+  m->depth.resize(T);
+  m->feature.resize((size_t)T * D);
+  m->bin.resize((size_t)T * D);
+  m->threshold.resize((size_t)T * D);
+  m->gain.resize((size_t)T * D);
+  m->leaves.resize((size_t)T * L);
+  m->weights.assign(T, tr->prm.learning_rate);
+  std::vector<double> g64((size_t)T * D);
+  auto cp = [&](void* dst, const void* src, size_t bytes) {
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st);
+  };
+  cudaError_t e = cudaSuccess;
+  if (T > 0) {
+    e = cp(m->depth.data(), tr->m_depth.p, (size_t)T * sizeof(int32_t));
+    if (e == cudaSuccess) e = cp(m->feature.data(), tr->m_feat.p, (size_t)T * D * sizeof(uint16_t));
+    if (e == cudaSuccess) e = cp(m->bin.data(), tr->m_bin.p, (size_t)T * D);
+    if (e == cudaSuccess) e = cp(m->threshold.data(), tr->m_thr.p, (size_t)T * D * sizeof(float));
+    if (e == cudaSuccess) e = cp(g64.data(), tr->m_gain.p, (size_t)T * D * sizeof(double));
+    if (e == cudaSuccess) e = cp(m->leaves.data(), tr->m_leaves.p, (size_t)T * L * sizeof(float));
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    delete m;
+    return ctx->cuda_fail(e, "model download");
+  }
+  for (size_t q = 0; q < g64.size(); ++q) m->gain[q] = (float)g64[q];
+  m->edges = tr->ds->h_edges;
+  m->n_edges = tr->ds->h_n_edges;
+  tc_status s = m->upload();
+  if (s != TC_OK) {
+    delete m;
+    return s;
+  }
+  *out = m;
+  return TC_OK;
+}
+
+void tc_trainer_destroy(tc_trainer* tr) {
+  if (!tr) return;
+  cudaSetDevice(tr->ctx->device);
+  cudaStreamSynchronize(tr->ctx->stream);
+  delete tr;
+}
+
+tc_status tc_train(tc_ctx* ctx, tc_dataset* ds, const tc_train_params* p, tc_model** out, tc_train_stats* st) {
+  if (!ctx || !ds || !p || !out) return TC_ERR_INVALID_ARG;
+  tc_trainer* tr = nullptr;
+  TC_TRY(tc_trainer_create(ctx, ds, p, &tr));
+  tc_status s = tr->step(p->n_estimators, true);
+  if (s == TC_OK) s = tc_trainer_model(tr, out);
+  if (s == TC_OK && st) tc_trainer_stats(tr, st);
+  tc_trainer_destroy(tr);
+  return s;
+}
+
+tc_status tc_build_tree(tc_ctx* ctx, tc_dataset* ds, const float* grad, const float* hess,
+                        const tc_train_params* p, int32_t* depth_out, uint16_t* split_feature,
+                        uint8_t* split_bin, float* split_threshold, double* split_gain,
+                        double* runner_up_gain, float* leaf_values, uint32_t* leaf_index,
+                        double* root_hist) {
+  if (!ctx || !ds || !grad || !hess || !p || !depth_out) return TC_ERR_INVALID_ARG;
+  cudaSetDevice(ctx->device);
+  tc_train_params q = *p;
+  q.loss = TC_LOSS_MSE;  // labels unused: gradients are given
+  q.n_classes = 1;
+  q.n_estimators = 1;
+  if (!ds->quantized) return ctx->fail(TC_ERR_INVALID_ARG, "dataset is not quantized");
+  if (q.max_depth < 1 || q.max_depth > kMaxDepth)
+    return ctx->fail(TC_ERR_INVALID_ARG, "max_depth must be in [1, %d]", kMaxDepth);
+  if (q.max_bins < 2 || q.max_bins > 255) return ctx->fail(TC_ERR_INVALID_ARG, "max_bins must be in [2, 255]");
+  tc_trainer* tr = new tc_trainer();
+  tr->ctx = ctx;
+  tr->ds = ds;
+  tr->prm = q;
+  tr->given_gh = true;
+  tc_status s = tr->setup(1);
+  if (s == TC_OK) s = tr->init_predictions();
+  if (s != TC_OK) {
+    delete tr;
+    return s;
+  }
+  cudaStream_t st = ctx->stream;
+  const uint32_t n = ds->n;
+  std::vector<float2> h(n);
+  for (uint32_t i = 0; i < n; ++i) h[i] = make_float2(grad[i], hess[i]);
+  DevBuf<double> rh;
+  cudaError_t e = cudaMemcpyAsync(tr->gh.p, h.data(), n * sizeof(float2), cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) { delete tr; return ctx->cuda_fail(e, "gradient upload"); }
+  if (root_hist) {
+    s = rh.alloc(ctx, (size_t)ds->f * kSlots * 2, "root histogram");
+    if (s != TC_OK) { delete tr; return s; }
+    tr->ptr.root_hist_out = rh.p;
+  }
+  // one iteration with the given gradients
+  const int D = tr->cfg.D;
+  k_grad<<<tr->cfg.PB, 512, 0, st>>>(tr->cfg, tr->ptr, 1);
+  k_node_reduce<<<dim3(1, 1), 256, 0, st>>>(tr->cfg, tr->ptr, -1);
+  k_plan<<<1, 32, 0, st>>>(tr->cfg, tr->ptr, 0, -1);
+  for (int d = 0; d < D; ++d) {
+    tr->launch_level(tr->cfg, tr->ptr, d, st);
+    if (d == 0 && root_hist) k_root_hist_out<<<64, 256, 0, st>>>(tr->cfg, tr->ptr);
+  }
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) { delete tr; return ctx->cuda_fail(e, "tree build"); }
+  int32_t dep = 0;
+  const int L = 1 << D;
+  std::vector<uint16_t> lf;
+  e = cudaMemcpy(&dep, tr->m_depth.p, sizeof(int32_t), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && split_feature) e = cudaMemcpy(split_feature, tr->m_feat.p, D * sizeof(uint16_t), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && split_bin) e = cudaMemcpy(split_bin, tr->m_bin.p, D, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && split_threshold) e = cudaMemcpy(split_threshold, tr->m_thr.p, D * sizeof(float), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && split_gain) e = cudaMemcpy(split_gain, tr->m_gain.p, D * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && runner_up_gain) e = cudaMemcpy(runner_up_gain, tr->m_second.p, D * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && leaf_values) e = cudaMemcpy(leaf_values, tr->m_leaves.p, L * sizeof(float), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && leaf_index) {
+    lf.resize(n);
+    e = cudaMemcpy(lf.data(), tr->leaf.p, n * sizeof(uint16_t), cudaMemcpyDeviceToHost);
+    for (uint32_t i = 0; i < n && e == cudaSuccess; ++i) leaf_index[i] = lf[i];
+  }
+  if (e == cudaSuccess && root_hist) e = cudaMemcpy(root_hist, rh.p, rh.bytes(), cudaMemcpyDeviceToHost);
+  delete tr;
+  if (e != cudaSuccess) return ctx->cuda_fail(e, "tree download");
+  *depth_out = dep;
+  return TC_OK;
+}
+
+}  // extern "C"
