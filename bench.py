@@ -1,0 +1,332 @@
+"""Benchmark: symmetric-tree training on the regression configuration.
+
+Workload (seeded synthetic data with the configuration's shapes and value
+distributions): 1,000,000 rows x 100 float32 features -- 60 N(0,1),
+30 U(-3,3), 10 Student-t(3) -- target sum_k sin(x_k) over 10 features +
+x2*x3 + N(0, 0.1); MSE ("RMSE" config), 500 symmetric trees, depth 8,
+learning rate 0.05, 255 bins, lambda_l2 0 (the facade default).
+
+Metric: training seconds per 100 trees (lower is better).  A step is 100
+boosting iterations; --steps 5 therefore trains the configuration's 500
+trees.  `value` times the steps on device-resident data (CUDA events on the
+engine's stream, L2 flushed between steps); `e2e` times whole fits through
+the public API (turbocat.TurboCatRegressor.fit) from pinned host memory:
+upload, device binning, 500 trees, model download.
+
+--impl reference runs the reference's own CPU implementation (its pybind
+module built from source in oracle/_ref) on the same data on the host cores.
+Multi-GPU: replicas only (one independent fit per rank, no collective on the
+data path); value aggregates over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "turbo-cat_b200"))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+N_ROWS, N_FEAT, DEPTH, LR, TREES = 1_000_000, 100, 8, 0.05, 500
+TREES_PER_STEP = 100
+METRIC = "train_s_per_100_trees"
+UNIT = "s/100 trees"
+CONFIG = {"workload": "regression 1M x 100 float32 (60 N(0,1), 30 U(-3,3), 10 t(3)), MSE, 500 symmetric trees, "
+                      "depth 8, lr 0.05, 255 bins, lambda_l2 0",
+          "rows": N_ROWS, "features": N_FEAT, "trees": TREES, "depth": DEPTH, "bins": 255,
+          "step": "100 boosting iterations", "l2": "flushed between timed steps (256 MiB write)"}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def hist_traffic_per_launch():
+    """dram bytes per histogram launch from the committed ncu summary (or None)."""
+    path = os.path.join(ROOT, "profiles", "k_hist_c2_regression.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+class Clocks:
+    """nvidia-smi clock sampling during the timed region."""
+
+    def __init__(self, gpu):
+        self.path = os.path.join(ROOT, "gpurun_out", f"bench_clocks_{gpu}.csv")
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.fh = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={gpu}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if not self.p:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.fh.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        loaded = [s for s in sm if mx and s > 0.5 * mx] or sm
+        return {"sm_mhz": float(np.median(loaded)) if loaded else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(backend):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def dist_max(x, ws, device=None):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(x)], device=device) if device is not None else torch.tensor([float(x)])
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def make_data():
+    from datagen import regression_c2
+
+    return regression_c2(N_ROWS, N_FEAT, seed=2)
+
+
+def reference_sample(X, y, n_more=4):
+    """Reference CPU fit through its pybind module (oracle/_ref/_turbocat):
+    a 1-tree fit and a (1+n_more)-tree fit give setup and per-tree cost,
+    extrapolated to the configuration's 500 trees; returns s/100 trees."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
+    import _turbocat as ref  # the reference's own module, built from its sources
+
+    def fit(T):
+        m = ref.TurboCatRegressor(n_estimators=T, learning_rate=LR, max_depth=DEPTH, loss="mse", mode="large",
+                                  subsample=1.0, colsample_bytree=1.0, lambda_l2=0.0, min_child_weight=1.0,
+                                  verbosity=0)
+        t0 = time.perf_counter()
+        m.fit(X, y)
+        return time.perf_counter() - t0
+
+    t1 = fit(1)
+    t2 = fit(1 + n_more)
+    per_tree = max(0.0, (t2 - t1) / n_more)
+    setup = max(0.0, t1 - per_tree)
+    full = setup + TREES * per_tree
+    return full / (TREES / TREES_PER_STEP), dict(setup_s=setup, per_tree_s=per_tree, fit1_s=t1,
+                                                  fit_more_s=t2, extra_trees=n_more)
+
+
+def run_reference(args):
+    ws, rank, _ = dist_setup("gloo")
+    if rank != 0:
+        dist_barrier(ws)
+        return
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref")):
+        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref not present"}))
+        return
+    X, y = make_data()
+    cores = os.cpu_count()
+    for _ in range(args.warmup):
+        reference_sample(X, y, n_more=2)
+    vals = []
+    detail = None
+    for _ in range(args.steps):
+        v, detail = reference_sample(X, y, n_more=2)
+        vals.append(v)
+    value = float(np.mean(vals))
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": CONFIG, "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                             "sample": "reference pybind fit of the 1M x 100 data with 1 and 3 trees per step; "
+                                       "setup + per-tree cost extrapolated to 500 trees", "detail": detail},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    dist_barrier(ws)
+
+
+def run_ours(args):
+    ws, rank, local = dist_setup("nccl")
+    import torch
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    os.environ["TURBOCAT_DEVICE"] = str(local)
+    from turbocat import _capi
+
+    eng = _capi.Engine(local)
+    X, y = make_data()
+    ds = eng.upload(X, y)
+    ds.quantize(255)
+    iters_cap = TREES_PER_STEP * max(args.steps, args.warmup, 1) + 16
+    p = _capi.params(loss="mse", n_estimators=iters_cap, max_depth=DEPTH, learning_rate=LR, lambda_l2=0.0,
+                     max_bins=255)
+    tr = eng.trainer(ds, p)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
+
+    # warm-up: W steps on a fresh model
+    for _ in range(args.warmup):
+        tr.step(TREES_PER_STEP)
+    tr.reset()
+    torch.cuda.synchronize()
+    dist_barrier(ws)
+    clocks = Clocks(local)
+    launches0 = tr.stats().kernel_launches
+    step_s = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        s0 = tr.stats().seconds
+        tr.step(TREES_PER_STEP)  # synchronises; seconds from CUDA events on the engine stream
+        step_s.append(tr.stats().seconds - s0)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = tr.stats().kernel_launches - launches0
+    dist_barrier(ws)
+    total = dist_max(sum(step_s), ws, dev)
+    # whole job: ws replicas x steps x 100 trees in `total` seconds
+    value = total / (args.steps * ws)
+
+    # roofline of the dominant kernel (histogram) from event-timed launches
+    tr.reset()
+    prof = tr.profile(3)
+    prof.pop("_hist_levels", None)
+    hl, hms, hbytes = prof["hist"]
+    peak, peak_kind = load_peaks()
+    achieved = hbytes / (hms * 1e-3) / 1e9 if hms > 0 else None
+    dominant = max((v[1], k) for k, v in prof.items())[1]
+    roofline = {"kernel": "k_hist (histogram)", "bound": "hbm", "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                "traffic": hist_traffic_per_launch(), "peak_kind": peak_kind,
+                "alg_bytes_per_launch": hbytes / max(1, hl), "avg_launch_ms": hms / max(1, hl),
+                "dominant_kernel_by_time": dominant,
+                "kernel_ms_per_iter": {k: round(v[1] / 3, 4) for k, v in prof.items() if v[0]}}
+
+    # end to end through the public API, pinned host inputs
+    import turbocat
+
+    Xp = torch.empty((N_ROWS, N_FEAT), dtype=torch.float32, pin_memory=True).numpy()
+    yp = torch.empty(N_ROWS, dtype=torch.float32, pin_memory=True).numpy()
+    Xp[:] = X
+    yp[:] = y
+    e2e_s = []
+    for i in range(1 + args.e2e_fits):
+        m = turbocat.TurboCatRegressor(n_estimators=TREES, learning_rate=LR, max_depth=DEPTH, loss="mse",
+                                       mode="large", subsample=1.0, colsample_bytree=1.0, lambda_l2=0.0,
+                                       verbosity=0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        m.fit(Xp, yp)
+        dt = time.perf_counter() - t0
+        if i > 0:
+            e2e_s.append(dt)
+    e2e_fit = dist_max(float(np.mean(e2e_s)), ws, dev)
+    steps_per_fit = TREES / TREES_PER_STEP
+    model_bytes = TREES * (DEPTH * 11 + (1 << DEPTH) * 4 + 8)
+    e2e = {"value": e2e_fit / steps_per_fit / ws, "unit": UNIT,
+           "h2d_bytes_per_step": int((X.nbytes + y.nbytes) / steps_per_fit),
+           "d2h_bytes_per_step": int(model_bytes / steps_per_fit),
+           "fit_seconds": e2e_fit, "fits_timed": args.e2e_fits,
+           "path": "turbocat.TurboCatRegressor.fit (pybind -> C ABI): upload, device binning, 500 trees, model"}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            v, detail = reference_sample(X, y, n_more=2)
+            cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": "reference pybind fit of the same 1M x 100 data with 1 and 3 trees; setup + "
+                             "per-tree cost extrapolated to 500 trees", "detail": detail}
+        except Exception as e:  # reference build absent
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3, "higher_is_better": False,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": CONFIG,
+                "parallelism": f"replicas x{ws}", "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "clocks": clk, "gpu_launches": int(launches),
+                "trees_per_s": args.steps * TREES_PER_STEP * ws / total}
+        print(json.dumps(line))
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-fits", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        log("warm-up raised to 3 steps")
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -9,8 +9,6 @@ import sys
 import numpy as np
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-sys.path.insert(0, os.path.join(ROOT, "oracle"))
-from oracle import Hyper  # noqa: E402
 
 
 def binary_c1(n=50_000, f=20, seed=1):
@@ -86,6 +84,11 @@ GOLDEN_CASES = {
 
 
 def make_case(spec):
+    """(X, y, oracle.Hyper) of a small parity case (imports the oracle: tests only)."""
+    if os.path.join(ROOT, "oracle") not in sys.path:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Hyper
+
     kind = spec["kind"]
     if kind == "binary":
         X, y = binary_c1(spec["n"], spec["f"], spec["seed"])

