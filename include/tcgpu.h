@@ -178,6 +178,25 @@ tc_status tc_build_tree(tc_ctx* ctx, tc_dataset* ds, const float* grad, const fl
                         double* runner_up_gain, float* leaf_values, uint32_t* leaf_index,
                         double* root_hist);
 
+/* Root-level gradient/hessian histogram that allocates no device memory.
+ * No counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc -- e.g. a process whose device memory is entirely reserved by
+ * another framework's allocator, or a latency-critical request path where a
+ * driver allocation (which can synchronise the device, and can fail) is not
+ * allowed.  All buffers are the caller's device memory: bins_rm row-major
+ * uint8 [n][row_stride] (NaN rows in bin 255), grad/hess float [n],
+ * hist_out FP64 [f][256][2] (grad, hess).  Scratch is a fixed 16 MiB
+ * device array inside the library (every GPU that loads the library holds it
+ * until the process exits); at most 8192 features, larger f is rejected with
+ * TC_ERR_INVALID_ARG.  The first call on a device resolves that array's
+ * device address, so make the first call before any stream capture.  Calls
+ * share the array: calls that overlap on the GPU race (serialise them on one
+ * stream).  Queued on `stream` (NULL = the context's stream); returns
+ * without synchronising. */
+tc_status tc_histogram_root_noalloc(tc_ctx* ctx, const uint8_t* bins_rm, uint32_t n, uint16_t f,
+                                    uint32_t row_stride, const float* grad, const float* hess,
+                                    double* hist_out, void* stream);
+
 /* ------------------------------------------------------------------ model */
 
 typedef struct {

@@ -28,7 +28,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
                      f"-I{INCLUDE}", f"-I{CSRC}", "--expt-relaxed-constexpr", "-Xptxas", "-v"]
 
-CU_SOURCES = ["tc_context.cu", "tc_data.cu", "tc_train.cu", "tc_predict.cu", "tc_server.cu"]
+CU_SOURCES = ["tc_context.cu", "tc_data.cu", "tc_train.cu", "tc_predict.cu", "tc_server.cu", "tc_noalloc.cu"]
 HOST_SOURCES = ["bindings.cpp"]
 
 LIB = os.path.join(PKG, "libtcgpu.so")

@@ -28,7 +28,8 @@ SYMBOLS = [
     "tc_ctx_synchronize", "tc_dataset_upload", "tc_dataset_destroy", "tc_quantize", "tc_dataset_bins",
     "tc_trainer_create", "tc_trainer_step", "tc_trainer_reset", "tc_trainer_stats", "tc_trainer_profile",
     "tc_trainer_train_scores",
-    "tc_trainer_model", "tc_trainer_destroy", "tc_train", "tc_build_tree", "tc_model_info_get", "tc_model_export",
+    "tc_trainer_model", "tc_trainer_destroy", "tc_train", "tc_build_tree", "tc_histogram_root_noalloc",
+    "tc_model_info_get", "tc_model_export",
     "tc_model_import", "tc_model_save_tcat", "tc_model_load_tcat", "tc_model_destroy", "tc_predict",
     "tc_predict_device", "tc_server_create", "tc_server_add_model", "tc_server_submit", "tc_server_poll",
     "tc_server_replay", "tc_server_stats", "tc_server_destroy",
