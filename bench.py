@@ -172,9 +172,8 @@ def reference_sample(X, y, n_more=4):
 
 
 def run_reference(args):
-    ws, rank, _ = dist_setup("gloo")
-    if rank != 0:
-        dist_barrier(ws)
+    # rank 0 alone measures the host CPU; other ranks exit without work
+    if int(os.environ.get("RANK", "0")) != 0:
         return
     if not os.path.exists(os.path.join(ROOT, "oracle", "_ref")):
         print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref not present"}))
@@ -197,7 +196,6 @@ def run_reference(args):
                                        "setup + per-tree cost extrapolated to 500 trees", "detail": detail},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
-    dist_barrier(ws)
 
 
 def run_ours(args):
@@ -310,6 +308,201 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------- suite --
+# Secondary configurations (not the headline line): run with --suite; writes
+# one JSON object per configuration to stdout.
+
+def _pct(a, q):
+    return float(np.percentile(np.asarray(a), q)) if len(a) else None
+
+
+def suite_c1(eng, _capi, ref_ok):
+    from datagen import binary_c1
+
+    X, y = binary_c1()
+    ds = eng.upload(X, y)
+    ds.quantize(255)
+    tr = eng.trainer(ds, _capi.params(loss="logloss", n_estimators=400, max_depth=6, learning_rate=0.1))
+    tr.step(100)
+    tr.reset()
+    s0 = tr.stats().seconds
+    tr.step(100)
+    dev = tr.stats().seconds - s0
+    out = {"config": "binary 50k x 20, logloss, 100 trees, depth 6", "device_s_per_100_trees": dev}
+    if ref_ok:
+        sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
+        import _turbocat as ref
+
+        m = ref.TurboCatClassifier(n_estimators=100, learning_rate=0.1, max_depth=6, max_bins=255, subsample=1.0,
+                                   colsample_bytree=1.0, min_child_weight=1.0, lambda_l2=1.0, loss="logloss",
+                                   mode="large", verbosity=0)
+        t0 = time.perf_counter()
+        m.fit(X, y)
+        out["reference_cpu_fit_s"] = time.perf_counter() - t0
+        out["reference_cores"] = os.cpu_count()
+    return out
+
+
+def suite_c3(eng, _capi, iters=10):
+    from datagen import multiclass_c3
+
+    X, y = multiclass_c3()
+    ds = eng.upload(X, y)
+    ds.quantize(255)
+    res = {"config": "multiclass 2M x 50, K=10 softmax, depth 6 (200 iterations x 10 trees in the config)"}
+    for batched in (1, 0):
+        tr = eng.trainer(ds, _capi.params(loss="softmax", n_classes=10, n_estimators=iters + 3, max_depth=6,
+                                          learning_rate=0.1, batched=batched))
+        tr.step(2)
+        s0 = tr.stats().seconds
+        tr.step(iters)
+        dt = (tr.stats().seconds - s0) / iters
+        res["batched_s_per_iter" if batched else "plain_s_per_iter"] = dt
+        tr.close()
+    res["batched_speedup_vs_plain"] = res["plain_s_per_iter"] / res["batched_s_per_iter"]
+    res["batched_s_per_100_trees"] = res["batched_s_per_iter"] * 10
+    return res
+
+
+def _train_serving_models(eng, _capi):
+    rng = np.random.default_rng(4)
+    n, f = 200_000, 100
+    X = rng.standard_normal((n, f)).astype(np.float32)
+    w = rng.standard_normal(f).astype(np.float32)
+    y = ((X @ w + rng.normal(0, 1.0, n).astype(np.float32)) > 0).astype(np.float32)
+    ds = eng.upload(X, y)
+    ds.quantize(255)
+    models = []
+    for T, D in ((1000, 6), (200, 4), (500, 8), (2000, 10)):
+        m, _ = eng.train(ds, _capi.params(loss="logloss", n_estimators=T, max_depth=D, learning_rate=0.1))
+        models.append(m)
+    return models
+
+
+def suite_c4(eng, _capi, seconds=3.0, rate=20_000.0, ref_ok=False):
+    import torch
+
+    models = _train_serving_models(eng, _capi)
+    f = 100
+    rng = np.random.default_rng(44)
+    pool = torch.empty((65536 + 65536, f), dtype=torch.float32, pin_memory=True).numpy()
+    pool[:] = rng.standard_normal(pool.shape).astype(np.float32)
+    res = {"config": "serving: 4 resident models (1000xd6, 200xd4, 500xd8, 2000xd10) on 100 features; "
+                     f"Poisson {rate:.0f} req/s for {seconds:.1f} s, rows log-uniform [1, 65536]"}
+    # fixed-batch latency of the 1000 x depth-6 model (host buffers, H2D + kernel + D2H)
+    lat = {}
+    for rows in (1, 64, 4096, 65536):
+        Xb = pool[:rows]
+        for _ in range(3):
+            models[0].predict(Xb, "sigmoid")
+        ts = []
+        for _ in range(30):
+            t0 = time.perf_counter()
+            models[0].predict(Xb, "sigmoid")
+            ts.append(time.perf_counter() - t0)
+        lat[str(rows)] = {"p50_us": _pct(ts, 50) * 1e6, "p99_us": _pct(ts, 99) * 1e6,
+                          "rows_per_s": rows / _pct(ts, 50)}
+    res["fixed_batch_1000xd6"] = lat
+    if ref_ok:
+        sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
+        import tempfile
+
+        import _turbocat as ref
+
+        path = os.path.join(tempfile.mkdtemp(), "m.tcat")
+        with open(path, "wb") as fh:
+            fh.write(models[0].tcat())
+        rm = ref.TurboCatClassifier(verbosity=0)
+        rm.load(path)
+        rl = {}
+        for rows in (1, 64, 4096, 65536):
+            Xb = np.ascontiguousarray(pool[:rows])
+            rm.predict_proba(Xb)
+            ts = []
+            for _ in range(30):
+                t0 = time.perf_counter()
+                rm.predict_proba(Xb)
+                ts.append(time.perf_counter() - t0)
+            rl[str(rows)] = {"p50_us": _pct(ts, 50) * 1e6, "p99_us": _pct(ts, 99) * 1e6,
+                             "rows_per_s": rows / _pct(ts, 50)}
+        res["reference_cpu_fixed_batch_1000xd6"] = rl
+        res["reference_cores"] = os.cpu_count()
+    # open-loop Poisson stream
+    n_req = int(seconds * rate)
+    arr = np.cumsum(rng.exponential(1.0 / rate, n_req))
+    sizes = np.minimum(65536, np.floor(np.exp(rng.uniform(0, np.log(65537), n_req)))).astype(np.int64)
+    mids = rng.integers(0, 4, n_req)
+    offs = rng.integers(0, 65536, n_req)
+    n_out = 2048
+    outs = [torch.empty((65536, 1), dtype=torch.float32, pin_memory=True).numpy() for _ in range(n_out)]
+    for mode in ("coalesced", "plain"):
+        srv = _capi.Server(eng, staging_bytes=0, max_batch_rows=262144, coalesce=(mode == "coalesced"),
+                           max_inflight=4)
+        ids = [srv.add_model(m) for m in models]
+        reqs = [(float(arr[i]), ids[mids[i]], pool[offs[i]:offs[i] + sizes[i]], outs[i % n_out][:sizes[i]],
+                 "sigmoid") for i in range(n_req)]
+        lat_s, wall = srv.replay(reqs)
+        done, launches, rows = srv.stats()
+        res[mode] = {"p50_ms": _pct(lat_s, 50) * 1e3, "p99_ms": _pct(lat_s, 99) * 1e3,
+                     "rows_per_s": float(rows) / wall, "requests": int(done), "launches": int(launches),
+                     "wall_s": wall}
+        srv.close()
+    res["p99_improvement_vs_plain"] = res["plain"]["p99_ms"] / res["coalesced"]["p99_ms"]
+    return res
+
+
+def suite_c5(eng, _capi, trees=20):
+    from datagen import imbalanced_c5
+
+    X, y = imbalanced_c5()
+    t0 = time.perf_counter()
+    ds = eng.upload(X, y)
+    up = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ds.quantize(255)
+    qt = time.perf_counter() - t0
+    del X
+    tr = eng.trainer(ds, _capi.params(loss="focal", n_estimators=trees + 6, max_depth=8, learning_rate=0.1))
+    tr.step(3)
+    s0 = tr.stats().seconds
+    tr.step(trees)
+    per_tree = (tr.stats().seconds - s0) / trees
+    prof = tr.profile(3)
+    prof.pop("_hist_levels", None)
+    hl, hms, hbytes = prof["hist"]
+    peak, kind = load_peaks()
+    return {"config": "imbalanced 10M x 200, focal, depth 8 (1000 trees in the config)",
+            "upload_s": up, "quantize_s": qt, "device_s_per_tree": per_tree,
+            "extrapolated_1000_trees_s": per_tree * 1000 + qt,
+            "hist_alg_gbs": hbytes / (hms * 1e-3) / 1e9, "hist_frac_of_hbm": hbytes / (hms * 1e-3) / 1e9 / peak,
+            "kernel_ms_per_iter": {k: round(v[1] / 3, 4) for k, v in prof.items() if v[0]}}
+
+
+def run_suite(args):
+    import torch
+
+    torch.cuda.set_device(0)
+    from turbocat import _capi
+
+    eng = _capi.Engine(0)
+    ref_ok = os.path.exists(os.path.join(ROOT, "oracle", "_ref")) and not args.no_cpu_baseline
+    for name in args.suite.split(","):
+        t0 = time.perf_counter()
+        if name == "c1":
+            r = suite_c1(eng, _capi, ref_ok)
+        elif name == "c3":
+            r = suite_c3(eng, _capi)
+        elif name == "c4":
+            r = suite_c4(eng, _capi, ref_ok=ref_ok)
+        elif name == "c5":
+            r = suite_c5(eng, _capi)
+        else:
+            continue
+        r["suite"] = name
+        r["wall_s"] = time.perf_counter() - t0
+        print(json.dumps(r), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -318,7 +511,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-fits", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--suite", default="", help="secondary configurations, e.g. c1,c3,c4,c5")
     args = ap.parse_args()
+    if args.suite:
+        run_suite(args)
+        return
     if args.warmup < 3:
         log("warm-up raised to 3 steps")
         args.warmup = 3

@@ -305,3 +305,45 @@ def test_bad_tcat_is_rejected(engine, capi):
         with pytest.raises(capi.TCError) as ei:
             engine.load_tcat(bad)
         assert ei.value.status == 6
+
+
+# ---------------------------------------------- tile shapes and the tuner --
+
+@pytest.mark.parametrize("width,rows", [(32, 0), (64, 0), (96, 0), (64, 700), (32, 5000)])
+def test_fit_identical_across_histogram_tilings(engine, capi, width, rows):
+    """Every histogram tiling (feature-group width, rows per chunk) must grow
+    the same trees: tilings change only FP32 summation order inside blocks."""
+    X, y = regression_c2(40_000, 70, seed=61)
+    hp = O.Hyper(loss="mse", n_estimators=6, learning_rate=0.1, max_depth=7, lambda_l2=0.0)
+    ob = O.quantize(X)
+    f64 = O.fit(ob, y, hp, mode=1)
+    ds = engine.upload(X, y)
+    ds.quantize(255)
+    tr = engine.trainer(ds, _params(capi, hp, hist_features_per_block=width, hist_rows_per_chunk=rows))
+    tr.step(hp.n_estimators)
+    st = tr.stats()
+    assert st.hist_features_per_block == width
+    ex = tr.model().export()
+    assert f64.min_margin > MARGIN
+    assert np.array_equal(ex["feature"], f64.feature) and np.array_equal(ex["bin"], f64.bin)
+    assert np.allclose(ex["leaves"], f64.leaves, rtol=REL, atol=1e-6)
+
+
+def test_autotuner_and_profile(engine, capi):
+    X, y = binary_c1(30_000, 40, seed=62)
+    ds = engine.upload(X, y)
+    ds.quantize(255)
+    tr = engine.trainer(ds, capi.params(loss="logloss", n_estimators=12, max_depth=6))
+    st = tr.stats()
+    assert st.hist_features_per_block in (32, 64) and st.iterations_done == 0 and st.kernel_launches == 0
+    tr.step(4)
+    prof = tr.profile(3)
+    levels = prof.pop("_hist_levels")
+    assert prof["hist"][0] == 3 * 6 and prof["hist"][1] > 0 and prof["hist"][2] > 0
+    assert levels[0][1] == 3 * 30_000  # root rows histogrammed per profiled iteration
+    assert tr.stats().iterations_done == 7
+    # the tuned model equals an untuned one on the same data
+    ref = O.fit(O.quantize(X), y, O.Hyper(loss="logloss", n_estimators=7, max_depth=6), mode=1)
+    ex = tr.model().export()
+    if ref.min_margin > MARGIN:
+        assert np.array_equal(ex["feature"], ref.feature)

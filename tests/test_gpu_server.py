@@ -1,0 +1,143 @@
+"""Serving loop through the C ABI: every request's result is the same when
+served alone (tc_predict) and when coalesced with others (continuous
+batching), in both the coalescing and the plain per-request modes, with
+pinned and pageable buffers, and under a tight staging-memory budget."""
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _random_model(engine, capi, seed, T, D, F, K=1):
+    rng = np.random.default_rng(seed)
+    arrays = dict(depth=rng.integers(max(0, D - 2), D + 1, T).astype(np.int32),
+                  feature=rng.integers(0, F, (T, D)).astype(np.uint16),
+                  threshold=rng.standard_normal((T, D)).astype(np.float32),
+                  leaves=(0.1 * rng.standard_normal((T, 1 << D))).astype(np.float32),
+                  weights=np.full(T, 0.1, np.float32))
+    info = capi.ModelInfo(T, K, D, F, 1 if K > 1 else 0, 0.3, 0.1, 1.0)
+    return engine.import_model(info, arrays), arrays
+
+
+def _requests(F, sizes, seed, pinned):
+    import torch
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for n in sizes:
+        X = rng.standard_normal((n, F)).astype(np.float32)
+        if pinned:
+            t = torch.empty((n, F), dtype=torch.float32, pin_memory=True)
+            t.numpy()[:] = X
+            X = t.numpy()
+        out.append(X)
+    return out
+
+
+@pytest.mark.parametrize("coalesce,pinned", [(True, True), (True, False), (False, True)])
+def test_results_same_alone_and_in_the_mix(engine, capi, coalesce, pinned):
+    import torch
+
+    F = 24
+    m1, a1 = _random_model(engine, capi, 1, 300, 6, F)
+    m2, a2 = _random_model(engine, capi, 2, 40, 10, F)
+    m3, a3 = _random_model(engine, capi, 3, 50, 5, F, K=4)
+    sizes = [1, 7, 128, 129, 1000, 4096, 33, 5000, 2, 700, 16384, 64, 3, 900]
+    reqs = _requests(F, sizes, 11, pinned)
+    models = [m1, m2, m3]
+    transforms = ["sigmoid", "raw", "softmax"]
+    alone = []
+    for i, X in enumerate(reqs):
+        m = models[i % 3]
+        alone.append(m.predict(X, transforms[i % 3]))
+    srv = capi.Server(engine, staging_bytes=0, max_batch_rows=65536, coalesce=coalesce, max_inflight=4)
+    ids = [srv.add_model(m) for m in models]
+    outs = []
+    tickets = []
+    for i, X in enumerate(reqs):
+        K = models[i % 3].info.n_classes
+        if pinned:
+            o = torch.empty((X.shape[0], K), dtype=torch.float32, pin_memory=True).numpy()
+        else:
+            o = np.zeros((X.shape[0], K), np.float32)
+        outs.append(o)
+        tickets.append(srv.submit(ids[i % 3], X, o, transforms[i % 3]))
+    for t in tickets:
+        done, lat = srv.poll(t, 10_000_000)
+        assert done and lat is not None and lat >= 0
+    for i in range(len(reqs)):
+        assert np.array_equal(outs[i], alone[i]), i
+    done_n, launches, rows = srv.stats()
+    assert done_n == len(reqs) and rows == sum(sizes)
+    if not coalesce:
+        assert launches == len(reqs)
+    srv.close()
+    # and the single-call predictor matches the FP64 oracle
+    e = O.Ensemble(0.3, 1, 6, a1["depth"], a1["feature"], np.zeros((300, 6), np.uint8), a1["threshold"],
+                   a1["leaves"], a1["weights"])
+    p64 = O.predict(e, reqs[3])[:, 0]  # request 3 went to model 1 with the sigmoid
+    assert np.max(np.abs(alone[3][:, 0] - 1 / (1 + np.exp(-p64)))) < 1e-5
+
+
+def test_coalescing_happens_under_a_burst(engine, capi):
+    import torch
+
+    F = 16
+    m, _ = _random_model(engine, capi, 5, 200, 6, F)
+    reqs = _requests(F, [256] * 64, 3, True)
+    srv = capi.Server(engine, staging_bytes=0, max_batch_rows=65536, coalesce=True, max_inflight=2)
+    mid = srv.add_model(m)
+    outs = [torch.empty((256, 1), dtype=torch.float32, pin_memory=True).numpy() for _ in reqs]
+    tickets = [srv.submit(mid, X, o, "raw") for X, o in zip(reqs, outs)]
+    for t in tickets:
+        assert srv.poll(t, 10_000_000)[0]
+    _, launches, _ = srv.stats()
+    assert launches < len(reqs)  # requests that arrived while a batch ran shared a launch
+    for X, o in zip(reqs, outs):
+        assert np.array_equal(o, m.predict(X, "raw"))
+    srv.close()
+
+
+def test_admission_by_staging_memory(engine, capi):
+    F = 32
+    m, _ = _random_model(engine, capi, 7, 100, 6, F)
+    # room for ~3000 rows per slot: requests queue until a slot frees
+    budget = 2 * 3000 * (F + 16) * 4
+    srv = capi.Server(engine, staging_bytes=budget, max_batch_rows=65536, coalesce=True, max_inflight=2)
+    mid = srv.add_model(m)
+    reqs = _requests(F, [1000, 2500, 3000, 10, 2999, 1500, 700, 3000], 9, False)
+    outs = [np.zeros((X.shape[0], 1), np.float32) for X in reqs]
+    tickets = [srv.submit(mid, X, o, "raw") for X, o in zip(reqs, outs)]
+    for t in tickets:
+        assert srv.poll(t, 10_000_000)[0]
+    for X, o in zip(reqs, outs):
+        assert np.array_equal(o, m.predict(X, "raw"))
+    # a request larger than a slot is refused up front
+    big = np.zeros((3001, F), np.float32)
+    with pytest.raises(capi.TCError) as ei:
+        srv.submit(mid, big, np.zeros((3001, 1), np.float32), "raw")
+    assert ei.value.status == 1
+    with pytest.raises(capi.TCError):
+        srv.submit(mid, np.zeros((5, F + 1), np.float32), np.zeros((5, 1), np.float32), "raw")
+    srv.close()
+
+
+def test_replay_open_loop(engine, capi):
+    import torch
+
+    F = 20
+    m, _ = _random_model(engine, capi, 8, 120, 6, F)
+    srv = capi.Server(engine, staging_bytes=0, max_batch_rows=65536, coalesce=True, max_inflight=4)
+    mid = srv.add_model(m)
+    rng = np.random.default_rng(4)
+    sizes = np.floor(np.exp(rng.uniform(0, np.log(4097), 200))).astype(int)
+    reqs = _requests(F, sizes, 12, True)
+    outs = [torch.empty((X.shape[0], 1), dtype=torch.float32, pin_memory=True).numpy() for X in reqs]
+    arrivals = np.cumsum(rng.exponential(1 / 5000.0, len(reqs)))
+    lat, wall = srv.replay([(float(t), mid, X, o, "raw") for t, X, o in zip(arrivals, reqs, outs)])
+    assert np.all(lat > 0) and wall >= arrivals[-1]
+    for X, o in zip(reqs, outs):
+        assert np.array_equal(o, m.predict(X, "raw"))
+    srv.close()

@@ -21,7 +21,8 @@
 //     part     leaf = 2*leaf + go_right, go_right = bin != 255 && bin > t;
 //              per-block child counts and FP64 child sums
 //     reduce   child totals, smaller child per pair, scatter offsets
-//     plan     (one block) segment starts, the next level's work items,
+//     plan     (one block) segment starts, rows per chunk and the chunk counts
+//              the histogram kernel decodes into work items,
 //              the stop pre-check, leaf values when the tree is complete
 //     scatter  node-grouped row list of the smaller children
 //
@@ -34,6 +35,9 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
 
 #include "tc_internal.h"
 
@@ -41,9 +45,12 @@ namespace tc {
 namespace {
 
 constexpr int HIST_THREADS = 512;
+constexpr int HIST_TILE = 128;    // rows per staged tile
 constexpr int PART_THREADS = 512;
-constexpr int SCAN_NODES = 16;    // nodes per scan block
+constexpr int SCAN_WARPS = 8;     // warps per scan block
+constexpr int SCAN_NODES = 32;    // nodes per scan block (4 per warp)
 constexpr int MERGE_BB = 8;       // bins per merge block
+constexpr int PLAN_THREADS = 1024;
 
 struct NodeStat {
   double G, H;
@@ -51,20 +58,17 @@ struct NodeStat {
   uint32_t pad;
 };
 
-struct Item {
-  int32_t k, p, g, c;
-};
-
-struct SplitRec {
-  int32_t f, b;
-  double gain, second;
-};
-
 // Per-class, per-tree control block on the device.
 struct ClassState {
-  int32_t done;        // tree stopped
+  int32_t done;        // 0 growing, 1 stopped (leaves pending), 2 finalized
   int32_t depth;       // accepted splits
   int32_t f, b;        // split of the current level
+};
+
+// Per-(class, feature) best candidate of a level.
+struct FeatBest {
+  double gain, second;
+  int32_t b, valid;
 };
 
 struct DevCfg {
@@ -73,10 +77,14 @@ struct DevCfg {
   int32_t KT, k0;                // classes in the model; first class of this launch view
   int32_t msl;
   float lr, lam, l1, mcw, msg, mds, gamma, alpha;
-  int32_t G, W, R;               // feature groups, group width (32*J), rows per chunk
+  int32_t G, W;                  // feature groups, group width (32*J)
   int32_t PB;                    // partition blocks
-  int32_t item_cap;              // capacity of the item table
+  int32_t item_cap;              // capacity of the partial buffer (items)
   int32_t n_scan_groups_max;
+  int32_t hist_grid;             // persistent histogram blocks
+  int32_t target_items;          // work items aimed for per histogram launch
+  int32_t rows_min;              // smallest rows per histogram chunk
+  int32_t rows_fixed;            // > 0: fixed rows per chunk (tuning override)
 };
 
 struct DevPtrs {
@@ -91,12 +99,10 @@ struct DevPtrs {
   uint32_t* rows;                // [K][n]
   double2* hist[2];              // [K][2^(D-1)][F][256]
   float2* part;                  // [item_cap][256][W]
-  Item* items;                   // [item_cap]
-  int32_t* n_items;              // [1]
+  int32_t* cum;                  // [K*2^(D-1)*G + 1] cumulative chunk counts (segment-group order)
+  int32_t* rchunk;               // [1] rows per chunk at the current level
   int32_t* seg_start;            // [K][2^(D-1)]
   int32_t* seg_len;              // [K][2^(D-1)]
-  int32_t* item_base;            // [K][2^(D-1)][G]
-  int32_t* n_chunks;             // [K][2^(D-1)]
   int32_t* small;                // [K][2^(D-1)] child index of the smaller sibling
   NodeStat* nstat;               // [K][D+1][2^D]
   uint32_t* pcnt;                // [K][PB][2^D]
@@ -104,8 +110,10 @@ struct DevPtrs {
   uint32_t* blk_off;             // [K][PB][2^(D-1)]
   double* gpart;                 // [K][F][NG][256]
   uint8_t* gany;                 // [K][F][NG][256]
+  FeatBest* fbest;               // [K][F]
+  uint32_t* counters;            // [K] completion counters of the pick blocks
   ClassState* cs;                // [K]
-  int32_t* iter;                 // [1] boosting iteration (tree slot = iter*K + k)
+  int32_t* iter;                 // [1] boosting iteration (tree slot = iter*KT + k0 + k)
   // model arrays (capacity T = n_estimators*K)
   int32_t* m_depth;              // [T]
   uint16_t* m_feat;              // [T][D]
@@ -120,6 +128,8 @@ struct DevPtrs {
 __device__ __forceinline__ size_t hist_index(const DevCfg& c, int k, int node, int f, int b) {
   return (((size_t)k * (1u << (c.D > 0 ? c.D - 1 : 0)) + node) * c.f + f) * kSlots + b;
 }
+
+__device__ __forceinline__ int pairs_at(int d) { return d == 0 ? 1 : (1 << (d - 1)); }
 
 // ------------------------------------------------------------------ grad --
 
@@ -254,74 +264,150 @@ __global__ void k_apply_last(DevCfg c, DevPtrs P) {
   }
 }
 
+
 // ------------------------------------------------------------------ hist --
 
-// Shared layout: column (feature within the group) fastest, so lane l of a
-// warp always hits bank l: float sm[(2*b + {0:grad,1:hess}) * W + col].
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+template <int J>
+struct HistShape {
+  static constexpr int W = 32 * J;
+  static constexpr int S = J == 3 ? 2 : 3;             // staging depth
+  static constexpr int CH = W / 16;                    // 16-byte chunks per staged row slice
+  static constexpr size_t hist_bytes = (size_t)2 * kSlots * W * 4;
+  static constexpr size_t stage_bytes = (size_t)HIST_TILE * (W + 8);
+  static constexpr size_t smem = hist_bytes + S * stage_bytes;
+};
+
+// Work item -> (segment-group, chunk) through the cumulative chunk counts.
+__device__ __forceinline__ int find_sg(const int32_t* cum, int nsg, int item) {
+  int lo = 0, hi = nsg - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (cum[mid] <= item) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Persistent blocks over work items; an item is a chunk of one segment's
+// rows (the root at d = 0, a smaller child after) for one feature group.
+// Row slices (the group's bytes of each row) and the rows' (grad, hess) are
+// staged into shared memory by cp.async, S tiles ahead of the compute, so
+// the gathered rows' latency overlaps the atomic updates of earlier tiles.
+// Shared histogram layout: column (feature in the group) fastest, so lane l
+// of a warp always hits bank l: float hist[(2*bin + {0 grad, 1 hess}) * W + col].
 template <int J>
 __global__ void __launch_bounds__(HIST_THREADS) k_hist(DevCfg c, DevPtrs P, int d) {
-  extern __shared__ float sm[];
-  constexpr int W = 32 * J;
-  const int n_items = *P.n_items;
+  using S_ = HistShape<J>;
+  constexpr int W = S_::W, S = S_::S, CH = S_::CH, T = HIST_TILE;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float* hist = reinterpret_cast<float*>(smraw);
+  uint8_t* s_bins = smraw + S_::hist_bytes;                                  // [S][T][W]
+  float2* s_gh = reinterpret_cast<float2*>(s_bins + (size_t)S * T * W);      // [S][T]
+  const int P2 = pairs_at(d);
+  const int nsg = c.K * P2 * c.G;
+  const int n_items = P.cum[nsg];
+  const int R = *P.rchunk;
+  const int Pmax = 1 << (c.D - 1);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
-    const Item it = P.items[item];
-    const int k = it.k;
-    const int g0 = it.g * W;
+    const int sg = find_sg(P.cum, nsg, item);
+    const int ch_idx = item - P.cum[sg];
+    const int g = sg % c.G;
+    const int kp = sg / c.G;
+    const int k = kp / P2, p = kp % P2;
+    const int g0 = g * W;
     const int gsize = min(W, (int)c.f - g0);
-    for (int q = threadIdx.x; q < 2 * kSlots * W; q += blockDim.x) sm[q] = 0.0f;
-    __syncthreads();
     int start, end;
     if (d == 0) {
-      start = it.c * c.R;
-      end = min((int)c.n, start + c.R);
+      start = ch_idx * R;
+      end = min((int)c.n, start + R);
     } else {
-      const int s0 = P.seg_start[k * (1 << (c.D - 1)) + it.p];
-      const int sl = P.seg_len[k * (1 << (c.D - 1)) + it.p];
-      start = s0 + it.c * c.R;
-      end = min(s0 + sl, start + c.R);
+      const int s0 = P.seg_start[k * Pmax + p];
+      const int sl = P.seg_len[k * Pmax + p];
+      start = s0 + ch_idx * R;
+      end = min(s0 + sl, start + R);
     }
     const uint32_t* rows = P.rows + (size_t)k * c.n;
     const float2* gh = P.gh + (size_t)k * c.n;
-    for (int base = start + warp * 4; base < end; base += nwarps * 4) {
-      uint32_t r[4];
-      float2 v[4];
-      uint8_t bb[4][J];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int idx = base + u;
-        r[u] = (idx < end) ? (d == 0 ? (uint32_t)idx : rows[idx]) : 0u;
+    for (int q = threadIdx.x; q < 2 * kSlots * W; q += blockDim.x) hist[q] = 0.0f;
+    const int n_tiles = (end - start + T - 1) / T;
+    // stage tile t into buffer t % S
+    auto issue = [&](int t) {
+      if (t < n_tiles) {
+        const int st = t % S;
+        const int base = start + t * T;
+        for (int q = threadIdx.x; q < T * CH; q += blockDim.x) {
+          const int i = q / CH, chn = q % CH;
+          const int idx = base + i;
+          if (idx < end && g0 + 16 * chn < (int)c.fs) {
+            const uint32_t r = d == 0 ? (uint32_t)idx : rows[idx];
+            cp_async16(s_bins + ((size_t)st * T + i) * W + 16 * chn, P.bins_rm + (size_t)r * c.fs + g0 + 16 * chn);
+          }
+        }
+        for (int i = threadIdx.x; i < T; i += blockDim.x) {
+          const int idx = base + i;
+          if (idx < end) {
+            const uint32_t r = d == 0 ? (uint32_t)idx : rows[idx];
+            cp_async8(s_gh + (size_t)st * T + i, gh + r);
+          }
+        }
       }
+      cp_async_commit();
+    };
+    __syncthreads();
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const bool ok = base + u < end;
-        v[u] = ok ? gh[r[u]] : make_float2(0.f, 0.f);
-        const uint8_t* br = P.bins_rm + (size_t)r[u] * c.fs + g0;
+    for (int t = 0; t < S - 1; ++t) issue(t);
+    for (int t = 0; t < n_tiles; ++t) {
+      issue(t + S - 1);
+      cp_async_wait<S - 1>();
+      __syncthreads();
+      const int st = t % S;
+      const int nvalid = min(T, end - (start + t * T));
+      const uint8_t* sb = s_bins + (size_t)st * T * W;
+      const float2* sv = s_gh + (size_t)st * T;
+      for (int i = warp; i < nvalid; i += 2 * nwarps) {
+        const int i2 = i + nwarps;
+        const bool has2 = i2 < nvalid;
+        const float2 v1 = sv[i];
+        const float2 v2 = has2 ? sv[i2] : make_float2(0.f, 0.f);
+        int b1[J], b2[J];
 #pragma unroll
         for (int j = 0; j < J; ++j) {
           const int col = lane + 32 * j;
-          bb[u][j] = (ok && col < gsize) ? br[col] : (uint8_t)0;
+          b1[j] = sb[(size_t)i * W + col];
+          b2[j] = has2 ? sb[(size_t)i2 * W + col] : 0;
         }
-      }
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        if (base + u < end) {
-#pragma unroll
-          for (int j = 0; j < J; ++j) {
-            const int col = lane + 32 * j;
-            if (col < gsize) {
-              atomicAdd(&sm[(2 * bb[u][j]) * W + col], v[u].x);
-              atomicAdd(&sm[(2 * bb[u][j] + 1) * W + col], v[u].y);
+        for (int j = 0; j < J; ++j) {
+          const int col = lane + 32 * j;
+          if (col < gsize) {
+            atomicAdd(&hist[(2 * b1[j]) * W + col], v1.x);
+            atomicAdd(&hist[(2 * b1[j] + 1) * W + col], v1.y);
+            if (has2) {
+              atomicAdd(&hist[(2 * b2[j]) * W + col], v2.x);
+              atomicAdd(&hist[(2 * b2[j] + 1) * W + col], v2.y);
             }
           }
         }
       }
+      __syncthreads();
     }
-    __syncthreads();
+    cp_async_wait<0>();
     float2* out = P.part + (size_t)item * kSlots * W;
     for (int q = threadIdx.x; q < kSlots * W; q += blockDim.x) {
       const int b = q / W, col = q % W;
-      out[q] = make_float2(sm[(2 * b) * W + col], sm[(2 * b + 1) * W + col]);
+      out[q] = make_float2(hist[(2 * b) * W + col], hist[(2 * b + 1) * W + col]);
     }
     __syncthreads();
   }
@@ -335,7 +421,7 @@ template <int J>
 __global__ void k_merge(DevCfg c, DevPtrs P, int d) {
   constexpr int W = 32 * J;
   __shared__ double2 tile[MERGE_BB][W];
-  const int P2 = d == 0 ? 1 : (1 << (d - 1));
+  const int P2 = pairs_at(d);
   const int seg = blockIdx.y;
   const int k = seg / P2, p = seg % P2, g = blockIdx.z;
   if (P.cs[k].done) return;
@@ -343,25 +429,24 @@ __global__ void k_merge(DevCfg c, DevPtrs P, int d) {
   const int g0 = g * W;
   const int gsize = min(W, (int)c.f - g0);
   const int b0 = blockIdx.x * MERGE_BB;
-  const int nch = P.n_chunks[k * Pmax + p];
-  const int ib = P.item_base[(k * Pmax + p) * c.G + g];
-  // phase 1: column-fastest reads of the partials
+  const int sg = (k * P2 + p) * c.G + g;
+  const int ib = P.cum[sg];
+  const int nch = P.cum[sg + 1] - ib;
   for (int q = threadIdx.x; q < MERGE_BB * W; q += blockDim.x) {
     const int bl = q / W, col = q % W;
-    double sg = 0.0, sh = 0.0;
+    double sg_ = 0.0, sh = 0.0;
     if (col < gsize) {
       for (int ch = 0; ch < nch; ++ch) {
         const float2 v = P.part[((size_t)(ib + ch) * kSlots + b0 + bl) * W + col];
-        sg += (double)v.x;
+        sg_ += (double)v.x;
         sh += (double)v.y;
       }
     }
-    tile[bl][col] = make_double2(sg, sh);
+    tile[bl][col] = make_double2(sg_, sh);
   }
   __syncthreads();
   double2* cur = P.hist[d & 1];
   const double2* par = P.hist[(d & 1) ^ 1];
-  // phase 2: bin-fastest writes of both children
   for (int q = threadIdx.x; q < MERGE_BB * W; q += blockDim.x) {
     const int col = q / MERGE_BB, bl = q % MERGE_BB;
     if (col >= gsize) continue;
@@ -381,77 +466,100 @@ __global__ void k_merge(DevCfg c, DevPtrs P, int d) {
 
 // ------------------------------------------------------------------ scan --
 
-// Block-wide inclusive scan of (G, H) pairs over 256 threads.
-__device__ __forceinline__ double2 block_scan256(double2 v, double2* ws) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int o = 1; o < 32; o <<= 1) {
-    const double yg = __shfl_up_sync(0xffffffffu, v.x, o);
-    const double yh = __shfl_up_sync(0xffffffffu, v.y, o);
-    if (lane >= o) { v.x += yg; v.y += yh; }
-  }
-  if (lane == 31) ws[warp] = v;
-  __syncthreads();
-  double2 pre = make_double2(0.0, 0.0);
-  for (int w = 0; w < warp; ++w) { pre.x += ws[w].x; pre.y += ws[w].y; }
-  __syncthreads();
-  return make_double2(pre.x + v.x, pre.y + v.y);
-}
-
-// grid (F, node groups, K), 256 threads = bins.  Gain of every bin summed
-// over the group's nodes, in FP64 (the reference's formula,
-// src/tree/symmetric_tree.cpp:161-178 and 221-236).
-__global__ void __launch_bounds__(256) k_scan(DevCfg c, DevPtrs P, int d) {
-  __shared__ double2 ws[8];
+// grid (F, node groups, K), SCAN_WARPS warps.  A warp scores one node at a
+// time: lane l holds bins 8l .. 8l+7 (bin 255 = NaN rows, added to the left
+// side); left sums are NaN + prefix, right sums an independent suffix, so an
+// empty side is exactly zero.  Per-bin gains (the reference's formula,
+// src/tree/symmetric_tree.cpp:161-178 and 221-236) accumulate in FP64 over
+// the warp's nodes; the block then sums its warps in a fixed order.
+__global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(DevCfg c, DevPtrs P, int d) {
+  __shared__ double s_acc[SCAN_WARPS][kSlots];
+  __shared__ uint8_t s_any[SCAN_WARPS][kSlots];
   const int f = blockIdx.x, ng = blockIdx.y, k = blockIdx.z;
   if (P.cs[k].done) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nn = 1 << d;
-  const int b = threadIdx.x;
   const double lam = (double)c.lam;
   const double2* cur = P.hist[d & 1];
   const NodeStat* ns = P.nstat + ((size_t)k * (c.D + 1) + d) * (1 << c.D);
-  double acc = 0.0;
-  uint8_t any = 0;
+  double acc[8];
+  uint32_t anyb = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) acc[i] = 0.0;
   const int n0 = ng * SCAN_NODES, n1 = min(nn, n0 + SCAN_NODES);
-  for (int node = n0; node < n1; ++node) {
+  for (int node = n0 + warp; node < n1; node += SCAN_WARPS) {
     const NodeStat st = ns[node];
-    const double2 h = cur[hist_index(c, k, node, f, b)];
-    const double2 hv = (b < kNanBin) ? h : make_double2(0.0, 0.0);
-    // prefix over regular bins (thread b), NaN slot added to the left side
-    const double2 pre = block_scan256(hv, ws);
-    __shared__ double2 s_nan;
-    if (threadIdx.x == 255) s_nan = h;
-    // suffix: inclusive scan in reverse order
-    const int rb = 255 - b;
-    __shared__ double2 rev[256];
-    rev[rb] = hv;
-    __syncthreads();
-    const double2 rv = rev[b];
-    const double2 rs = block_scan256(rv, ws);  // thread b holds sum of bins >= 255-b
-    rev[255 - b] = rs;                         // rev[j] = sum over bins >= j
-    __syncthreads();
-    const double2 nv = s_nan;
-    if (st.cnt > 0 && b < c.nb_scan) {
-      const double lg = nv.x + pre.x, lh = nv.y + pre.y;
-      const double2 r = rev[b + 1];
-      if (lh >= 1e-10 && r.y >= 1e-10) {
-        const double pg = (st.H > 1e-10) ? (st.G * st.G) / (st.H + lam) : 0.0;
-        acc += 0.5 * ((lg * lg) / (lh + lam) + (r.x * r.x) / (r.y + lam) - pg);
-        any = 1;
+    if (st.cnt == 0) continue;
+    const double2* hp = cur + hist_index(c, k, node, f, 0) + lane * 8;
+    double hg[8], hh[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const double2 v = hp[i];
+      hg[i] = v.x;
+      hh[i] = v.y;
+    }
+    const double nan_g = __shfl_sync(0xffffffffu, hg[7], 31);
+    const double nan_h = __shfl_sync(0xffffffffu, hh[7], 31);
+    if (lane == 31) { hg[7] = 0.0; hh[7] = 0.0; }  // NaN slot is not a regular bin
+    double tg = 0.0, th = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) { tg += hg[i]; th += hh[i]; }
+    // exclusive prefix and suffix of the lane totals
+    double pg = tg, ph = th, sg = tg, sh = th;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const double ug = __shfl_up_sync(0xffffffffu, pg, o), uh = __shfl_up_sync(0xffffffffu, ph, o);
+      const double dg = __shfl_down_sync(0xffffffffu, sg, o), dh = __shfl_down_sync(0xffffffffu, sh, o);
+      if (lane >= o) { pg += ug; ph += uh; }
+      if (lane + o < 32) { sg += dg; sh += dh; }
+    }
+    pg -= tg; ph -= th;  // exclusive prefix
+    sg -= tg; sh -= th;  // exclusive suffix
+    const double pgain = (st.H > 1e-10) ? (st.G * st.G) / (st.H + lam) : 0.0;
+    // right side of bin 8l+i: this lane's bins above i plus all lanes above
+    double rsg[8], rsh[8];
+    {
+      double ag = sg, ah = sh;
+#pragma unroll
+      for (int i = 7; i >= 0; --i) {
+        rsg[i] = ag;
+        rsh[i] = ah;
+        ag += hg[i];
+        ah += hh[i];
       }
     }
-    __syncthreads();
+    double lg = nan_g + pg, lh = nan_h + ph;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      lg += hg[i];
+      lh += hh[i];
+      const int b = lane * 8 + i;
+      if (b < c.nb_scan && lh >= 1e-10 && rsh[i] >= 1e-10) {
+        acc[i] += 0.5 * ((lg * lg) / (lh + lam) + (rsg[i] * rsg[i]) / (rsh[i] + lam) - pgain);
+        anyb |= 1u << i;
+      }
+    }
   }
-  const size_t o = (((size_t)k * c.f + f) * c.n_scan_groups_max + ng) * kSlots + b;
-  P.gpart[o] = acc;
-  P.gany[o] = any;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    s_acc[warp][lane * 8 + i] = acc[i];
+    s_any[warp][lane * 8 + i] = (anyb >> i) & 1u;
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < kSlots; b += blockDim.x) {
+    double s = 0.0;
+    uint8_t a = 0;
+    for (int w = 0; w < SCAN_WARPS; ++w) {
+      s += s_acc[w][b];
+      a |= s_any[w][b];
+    }
+    const size_t o = (((size_t)k * c.f + f) * c.n_scan_groups_max + ng) * kSlots + b;
+    P.gpart[o] = s;
+    P.gany[o] = a;
+  }
 }
 
 // ------------------------------------------------------------------ pick --
-
-struct Cand {
-  double gain, second;
-  int f, b;
-};
 
 __device__ __forceinline__ bool better(double ga, int fa, int ba, double gb, int fb, int bb) {
   if (ga != gb) return ga > gb;
@@ -459,73 +567,115 @@ __device__ __forceinline__ bool better(double ga, int fa, int ba, double gb, int
   return ba < bb;
 }
 
-// grid (K), 1024 threads.  Reduces the per-group gain partials, applies the
-// reference's tie rule and stop rule, records the split.
-__global__ void __launch_bounds__(1024) k_pick(DevCfg c, DevPtrs P, int d) {
-  __shared__ double s_g[1024], s_2[1024];
-  __shared__ int s_f[1024], s_b[1024];
-  const int k = blockIdx.x;
+// grid (F, K), 256 threads = bins.  Sums the node-group partials of every
+// bin of one feature, keeps the best bin (lowest bin on equal gain) and the
+// runner-up; the last block of a class to finish (completion counter, no
+// waiting) reduces the features in ascending order -- the reference keeps
+// the first strictly greater gain, i.e. lowest feature then lowest bin --
+// applies the stop rule and records the split.
+__global__ void __launch_bounds__(256) k_pick(DevCfg c, DevPtrs P, int d) {
+  __shared__ double s_g[256], s_2[256];
+  __shared__ int s_b[256];
+  __shared__ bool s_last;
+  const int f = blockIdx.x, k = blockIdx.y;
   ClassState& cs = P.cs[k];
   if (cs.done) return;
-  const int nn = 1 << d;
-  const int ngroups = (nn + SCAN_NODES - 1) / SCAN_NODES;
-  double bg = -1e300, b2 = -1e300;
-  int bf = 0x7fffffff, bbin = 0x7fffffff;
-  const int total = (int)c.f * c.nb_scan;
-  for (int q = threadIdx.x; q < total; q += blockDim.x) {
-    const int f = q / c.nb_scan, b = q % c.nb_scan;
-    double s = 0.0;
-    uint8_t any = 0;
-    const size_t o = ((size_t)k * c.f + f) * c.n_scan_groups_max * kSlots + b;
-    for (int g = 0; g < ngroups; ++g) {
-      s += P.gpart[o + (size_t)g * kSlots];
-      any |= P.gany[o + (size_t)g * kSlots];
-    }
-    if (d == 0 && !any) continue;  // root: a candidate needs both sides non-empty
-    if (better(s, f, b, bg, bf, bbin)) {
-      b2 = bg;
-      bg = s; bf = f; bbin = b;
-    } else if (s > b2) {
-      b2 = s;
-    }
+  const int b = threadIdx.x;
+  const int ngroups = ((1 << d) + SCAN_NODES - 1) / SCAN_NODES;
+  double s = 0.0;
+  uint8_t any = 0;
+  const size_t o = ((size_t)k * c.f + f) * c.n_scan_groups_max * kSlots + b;
+  for (int g = 0; g < ngroups; ++g) {
+    s += P.gpart[o + (size_t)g * kSlots];
+    any |= P.gany[o + (size_t)g * kSlots];
   }
-  s_g[threadIdx.x] = bg; s_2[threadIdx.x] = b2; s_f[threadIdx.x] = bf; s_b[threadIdx.x] = bbin;
+  const bool cand = b < c.nb_scan && (d > 0 || any);
+  s_g[b] = cand ? s : -1e300;
+  s_2[b] = -1e300;
+  s_b[b] = cand ? b : 0x7fffffff;
   __syncthreads();
-  for (int stride = blockDim.x / 2; stride > 0; stride >>= 1) {
-    if (threadIdx.x < stride) {
-      const int o = threadIdx.x + stride;
-      const double g1 = s_g[threadIdx.x], g2 = s_g[o];
-      const double rest = fmax(s_2[threadIdx.x], s_2[o]);
-      if (better(g2, s_f[o], s_b[o], g1, s_f[threadIdx.x], s_b[threadIdx.x])) {
-        s_2[threadIdx.x] = fmax(g1, rest);
-        s_g[threadIdx.x] = g2; s_f[threadIdx.x] = s_f[o]; s_b[threadIdx.x] = s_b[o];
+  for (int stride = 128; stride > 0; stride >>= 1) {
+    if (b < stride) {
+      const int q = b + stride;
+      const double rest = fmax(s_2[b], s_2[q]);
+      if (better(s_g[q], 0, s_b[q], s_g[b], 0, s_b[b])) {
+        s_2[b] = fmax(s_g[b], rest);
+        s_g[b] = s_g[q];
+        s_b[b] = s_b[q];
       } else {
-        s_2[threadIdx.x] = fmax(g2, rest);
+        s_2[b] = fmax(s_g[q], rest);
       }
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) {
+  if (b == 0) {
+    FeatBest fb;
+    fb.gain = s_g[0];
+    fb.second = s_2[0];
+    fb.b = s_b[0];
+    fb.valid = s_b[0] != 0x7fffffff;
+    P.fbest[(size_t)k * c.f + f] = fb;
+    __threadfence();
+    const uint32_t prev = atomicAdd(&P.counters[k], 1u);
+    s_last = prev == c.f - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  // last block of class k: reduce the features (fixed order per thread, then a tree)
+  __threadfence();
+  double bg = -1e300, b2 = -1e300;
+  int bf = 0x7fffffff, bbin = 0x7fffffff;
+  for (int ff = b; ff < (int)c.f; ff += blockDim.x) {
+    const FeatBest fb = P.fbest[(size_t)k * c.f + ff];
+    if (!fb.valid) continue;
+    const double rest = fmax(b2, fb.second);
+    if (better(fb.gain, ff, fb.b, bg, bf, bbin)) {
+      b2 = fmax(bg, rest);
+      bg = fb.gain; bf = ff; bbin = fb.b;
+    } else {
+      b2 = fmax(fb.gain, rest);
+    }
+  }
+  __syncthreads();
+  s_g[b] = bg; s_2[b] = b2; s_b[b] = bbin;
+  __shared__ int s_f[256];
+  s_f[b] = bf;
+  __syncthreads();
+  for (int stride = 128; stride > 0; stride >>= 1) {
+    if (b < stride) {
+      const int q = b + stride;
+      const double rest = fmax(s_2[b], s_2[q]);
+      if (better(s_g[q], s_f[q], s_b[q], s_g[b], s_f[b], s_b[b])) {
+        s_2[b] = fmax(s_g[b], rest);
+        s_g[b] = s_g[q]; s_f[b] = s_f[q]; s_b[b] = s_b[q];
+      } else {
+        s_2[b] = fmax(s_g[q], rest);
+      }
+    }
+    __syncthreads();
+  }
+  if (b == 0) {
+    P.counters[k] = 0;  // re-armed for the next level / graph replay
     const double best = s_g[0];
-    const int f = s_f[0], b = s_b[0];
+    const int bf0 = s_f[0], bb0 = s_b[0];
     const int t = *P.iter * c.KT + c.k0 + k;
-    // no candidate (gain stays -1e30 in the reference) or below min_split_gain
-    // (src/tree/symmetric_tree.cpp:276-278); the gain compared is FP32 there
-    if (f == 0x7fffffff || (float)best < c.msg) {
+    // no candidate (the reference's gain stays -1e30) or below
+    // min_split_gain (src/tree/symmetric_tree.cpp:276-278; FP32 compare there)
+    if (bf0 == 0x7fffffff || (float)best < c.msg) {
       cs.done = 1;
       return;
     }
     float thr = 0.0f;
-    const int ne = P.n_edges[f];
-    if (b < ne) thr = P.edges[(size_t)f * kSlots + b];
-    else if (ne > 0) thr = P.edges[(size_t)f * kSlots + ne - 1];
-    P.m_feat[(size_t)t * c.D + d] = (uint16_t)f;
-    P.m_bin[(size_t)t * c.D + d] = (uint8_t)b;
+    const int ne = P.n_edges[bf0];
+    if (bb0 < ne) thr = P.edges[(size_t)bf0 * kSlots + bb0];
+    else if (ne > 0) thr = P.edges[(size_t)bf0 * kSlots + ne - 1];
+    P.m_feat[(size_t)t * c.D + d] = (uint16_t)bf0;
+    P.m_bin[(size_t)t * c.D + d] = (uint8_t)bb0;
     P.m_thr[(size_t)t * c.D + d] = thr;
     P.m_gain[(size_t)t * c.D + d] = best;
     P.m_second[(size_t)t * c.D + d] = s_2[0];
-    cs.f = f;
-    cs.b = b;
+    cs.f = bf0;
+    cs.b = bb0;
     cs.depth = d + 1;
   }
 }
@@ -533,17 +683,20 @@ __global__ void __launch_bounds__(1024) k_pick(DevCfg c, DevPtrs P, int d) {
 // ------------------------------------------------------------- partition --
 
 // grid (PB, K).  Rows of block b: a contiguous range.  Updates leaf ids and
-// writes per-block child counts and FP64 sums.
+// writes per-block child counts and sums (FP32 within the block, handed on
+// as FP64 for the cross-block merge).  With few children, a warp reduces
+// each child's contributions through shuffles first (one shared update per
+// warp and child) instead of letting every lane hit the same two addresses.
 __global__ void __launch_bounds__(PART_THREADS) k_partition(DevCfg c, DevPtrs P, int d) {
   extern __shared__ unsigned char smraw[];
   const int k = blockIdx.y;
   const ClassState cs = P.cs[k];
   if (cs.done || cs.depth != d + 1) return;
   const int nch = 1 << (d + 1);
-  double* sG = reinterpret_cast<double*>(smraw);
-  double* sH = sG + nch;
+  float* sG = reinterpret_cast<float*>(smraw);
+  float* sH = sG + nch;
   uint32_t* sC = reinterpret_cast<uint32_t*>(sH + nch);
-  for (int q = threadIdx.x; q < nch; q += blockDim.x) { sG[q] = 0.0; sH[q] = 0.0; sC[q] = 0; }
+  for (int q = threadIdx.x; q < nch; q += blockDim.x) { sG[q] = 0.0f; sH[q] = 0.0f; sC[q] = 0; }
   __syncthreads();
   const uint32_t rpb = (c.n + gridDim.x - 1) / gridDim.x;
   const uint32_t r0 = blockIdx.x * rpb, r1 = min(c.n, r0 + rpb);
@@ -551,56 +704,83 @@ __global__ void __launch_bounds__(PART_THREADS) k_partition(DevCfg c, DevPtrs P,
   uint16_t* leaf = P.leaf + (size_t)k * c.n;
   const float2* gh = P.gh + (size_t)k * c.n;
   const uint8_t t = (uint8_t)cs.b;
-  for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-    const uint8_t b = col[i];
-    const uint32_t right = (b != (uint8_t)kNanBin && b > t) ? 1u : 0u;
-    const uint32_t nl = ((uint32_t)leaf[i] << 1) | right;
-    leaf[i] = (uint16_t)nl;
-    const float2 v = gh[i];
-    atomicAdd(&sG[nl], (double)v.x);
-    atomicAdd(&sH[nl], (double)v.y);
-    atomicAdd(&sC[nl], 1u);
+  const int lane = threadIdx.x & 31;
+  for (uint32_t base = r0; base < r1; base += blockDim.x) {
+    const uint32_t i = base + threadIdx.x;
+    const bool ok = i < r1;
+    int nl = -1;
+    float2 v = make_float2(0.f, 0.f);
+    if (ok) {
+      const uint8_t b = col[i];
+      const uint32_t right = (b != (uint8_t)kNanBin && b > t) ? 1u : 0u;
+      nl = (int)(((uint32_t)leaf[i] << 1) | right);
+      leaf[i] = (uint16_t)nl;
+      v = gh[i];
+    }
+    if (nch <= 8) {
+      for (int cc = 0; cc < nch; ++cc) {
+        float g = nl == cc ? v.x : 0.0f, h = nl == cc ? v.y : 0.0f;
+        const uint32_t cnt = __popc(__ballot_sync(0xffffffffu, nl == cc));
+        for (int o = 16; o; o >>= 1) {
+          g += __shfl_xor_sync(0xffffffffu, g, o);
+          h += __shfl_xor_sync(0xffffffffu, h, o);
+        }
+        if (lane == 0 && cnt) {
+          atomicAdd(&sG[cc], g);
+          atomicAdd(&sH[cc], h);
+          atomicAdd(&sC[cc], cnt);
+        }
+      }
+    } else if (ok) {
+      atomicAdd(&sG[nl], v.x);
+      atomicAdd(&sH[nl], v.y);
+      atomicAdd(&sC[nl], 1u);
+    }
   }
   __syncthreads();
   const int L = 1 << c.D;
   for (int q = threadIdx.x; q < nch; q += blockDim.x) {
     const size_t o = ((size_t)k * c.PB + blockIdx.x) * L + q;
-    P.psum[o] = make_double2(sG[q], sH[q]);
+    P.psum[o] = make_double2((double)sG[q], (double)sH[q]);
     P.pcnt[o] = sC[q];
   }
 }
 
-// grid (pairs, K), 256 threads.  Child totals (fixed-order FP64 sums over
-// blocks), the smaller sibling (left on a tie, src/tree/symmetric_tree.cpp:337-339),
-// and the per-block scatter offsets of its rows.
-__global__ void __launch_bounds__(256) k_node_reduce(DevCfg c, DevPtrs P, int d) {
+// grid (pairs, K), 512 threads (>= PB).  Child totals (fixed-order FP64
+// sums over blocks), the smaller sibling (left on a tie,
+// src/tree/symmetric_tree.cpp:337-339) and each block's scatter offset of
+// its rows of the smaller child (exclusive scan over blocks).
+__global__ void __launch_bounds__(512) k_node_reduce(DevCfg c, DevPtrs P, int d) {
   const int k = blockIdx.y, p = blockIdx.x;
   const ClassState cs = P.cs[k];
-  // d < 0 encodes the root reduction after the gradient pass
-  const bool root = d < 0;
+  const bool root = d < 0;  // root reduction after the gradient pass
   if (!root && (cs.done || cs.depth != d + 1)) return;
   const int L = 1 << c.D;
-  __shared__ double sg[2][256], sh[2][256];
-  __shared__ uint32_t sc[2][256];
+  __shared__ double s_g[2][512], s_h[2][512];
+  __shared__ uint32_t s_c[2][512];
+  __shared__ uint32_t s_w[16];
   const int nkids = root ? 1 : 2;
+  const int blk = threadIdx.x;
+  uint32_t my_cnt[2] = {0, 0};
   for (int kid = 0; kid < nkids; ++kid) {
     const int child = root ? 0 : 2 * p + kid;
     double g = 0.0, h = 0.0;
     uint32_t cn = 0;
-    for (int blk = threadIdx.x; blk < c.PB; blk += blockDim.x) {
+    if (blk < c.PB) {
       const size_t o = ((size_t)k * c.PB + blk) * L + child;
       const double2 v = P.psum[o];
-      g += v.x; h += v.y; cn += P.pcnt[o];
+      g = v.x; h = v.y; cn = P.pcnt[o];
     }
-    sg[kid][threadIdx.x] = g; sh[kid][threadIdx.x] = h; sc[kid][threadIdx.x] = cn;
+    my_cnt[kid] = cn;
+    s_g[kid][blk] = g; s_h[kid][blk] = h; s_c[kid][blk] = cn;
   }
   __syncthreads();
-  for (int s = 128; s > 0; s >>= 1) {
-    if (threadIdx.x < s) {
+  for (int s = 256; s > 0; s >>= 1) {
+    if (blk < s) {
       for (int kid = 0; kid < nkids; ++kid) {
-        sg[kid][threadIdx.x] += sg[kid][threadIdx.x + s];
-        sh[kid][threadIdx.x] += sh[kid][threadIdx.x + s];
-        sc[kid][threadIdx.x] += sc[kid][threadIdx.x + s];
+        s_g[kid][blk] += s_g[kid][blk + s];
+        s_h[kid][blk] += s_h[kid][blk + s];
+        s_c[kid][blk] += s_c[kid][blk + s];
       }
     }
     __syncthreads();
@@ -608,90 +788,75 @@ __global__ void __launch_bounds__(256) k_node_reduce(DevCfg c, DevPtrs P, int d)
   const int lvl = root ? 0 : d + 1;
   NodeStat* ns = P.nstat + ((size_t)k * (c.D + 1) + lvl) * L;
   if (root) {
-    if (threadIdx.x == 0) ns[0] = NodeStat{sg[0][0], sh[0][0], sc[0][0], 0};
+    if (blk == 0) ns[0] = NodeStat{s_g[0][0], s_h[0][0], s_c[0][0], 0};
     return;
   }
-  const uint32_t cl = sc[0][0], cr = sc[1][0];
+  const uint32_t cl = s_c[0][0], cr = s_c[1][0];
   const int sm = (cl <= cr) ? 0 : 1;
-  if (threadIdx.x == 0) {
-    ns[2 * p] = NodeStat{sg[0][0], sh[0][0], cl, 0};
-    ns[2 * p + 1] = NodeStat{sg[1][0], sh[1][0], cr, 0};
-    const int Pmax = 1 << (c.D - 1);
+  const int Pmax = 1 << (c.D - 1);
+  if (blk == 0) {
+    ns[2 * p] = NodeStat{s_g[0][0], s_h[0][0], cl, 0};
+    ns[2 * p + 1] = NodeStat{s_g[1][0], s_h[1][0], cr, 0};
     if (d + 1 < c.D) {
       P.small[k * Pmax + p] = 2 * p + sm;
       P.seg_len[k * Pmax + p] = (int)(sm ? cr : cl);
     }
   }
-  if (d + 1 < c.D) {
-    // exclusive scan over blocks of the smaller child's counts (serial per
-    // thread 0 chunk; PB is a few hundred)
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      const int Pmax = 1 << (c.D - 1);
-      uint32_t run = 0;
-      for (int blk = 0; blk < c.PB; ++blk) {
-        const size_t o = ((size_t)k * c.PB + blk) * L + 2 * p + sm;
-        P.blk_off[((size_t)k * c.PB + blk) * Pmax + p] = run;
-        run += P.pcnt[o];
-      }
-    }
+  if (d + 1 >= c.D) return;
+  // exclusive scan over blocks of the smaller child's counts
+  const uint32_t v = my_cnt[sm];
+  const int lane = blk & 31, warp = blk >> 5;
+  uint32_t x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
   }
+  if (lane == 31) s_w[warp] = x;
+  __syncthreads();
+  uint32_t before = 0;
+  for (int w = 0; w < warp; ++w) before += s_w[w];
+  if (blk < c.PB) P.blk_off[((size_t)k * c.PB + blk) * Pmax + p] = before + x - v;
 }
 
-// One block.  Segment starts, work items for the next histogram level, stop
-// pre-check (src/tree/symmetric_tree.cpp:116-124) and leaf values.
-// d = level about to be histogrammed (0 = root, after the gradient pass).
-__global__ void k_plan(DevCfg c, DevPtrs P, int d, int k_only) {
-  __shared__ int s_items;
+// One block.  For the level d about to be histogrammed: per class the stop
+// pre-check (src/tree/symmetric_tree.cpp:116-124) and, for a finished tree,
+// its leaf values (src/tree/symmetric_tree.cpp:357-367, 753-775); then the
+// rows per chunk for this level and the cumulative chunk counts over
+// (class, pair, feature group), which the histogram kernel decodes into work
+// items.
+__global__ void __launch_bounds__(PLAN_THREADS) k_plan(DevCfg c, DevPtrs P, int d) {
+  __shared__ int s_go;
+  __shared__ long long s_rows;
+  __shared__ int s_warp[PLAN_THREADS / 32];
+  __shared__ int s_carry;
   const int Pmax = 1 << (c.D - 1);
   const int L = 1 << c.D;
-  if (threadIdx.x == 0) s_items = 0;
-  __syncthreads();
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_rows = 0;
   for (int k = 0; k < c.K; ++k) {
-    if (k_only >= 0 && k != k_only) continue;
     ClassState& cs = P.cs[k];
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
       if (d == 0) { cs.done = 0; cs.depth = 0; }
-      bool alive = !cs.done && (d == 0 || cs.depth == d);
-      if (alive && d >= c.D) alive = false;
-      if (alive) {
-        // stop pre-check on the level-d nodes
-        const NodeStat* ns = P.nstat + ((size_t)k * (c.D + 1) + d) * L;
-        bool go = false;
-        const int nn = 1 << d;
-        for (int q = 0; q < nn && !go; ++q)
-          go = ns[q].cnt >= (uint32_t)c.msl * 2u && (float)ns[q].H >= c.mcw * 2.0f;
-        if (!go) alive = false;
-      }
-      if (!alive && !cs.done) cs.done = 1;
-      if (!cs.done) {
-        // segments and items
-        const int np2 = d == 0 ? 1 : (1 << (d - 1));
-        int run = 0;
-        for (int p = 0; p < np2; ++p) {
-          const int len = d == 0 ? (int)c.n : P.seg_len[k * Pmax + p];
-          P.seg_start[k * Pmax + p] = run;
-          run += len;
-          const int nch = (len + c.R - 1) / c.R;
-          P.n_chunks[k * Pmax + p] = nch;
-          for (int g = 0; g < c.G; ++g) {
-            P.item_base[(k * Pmax + p) * c.G + g] = s_items;
-            for (int ch = 0; ch < nch; ++ch) {
-              if (s_items < c.item_cap) P.items[s_items] = Item{k, p, g, ch};
-              ++s_items;
-            }
-          }
-        }
-      }
-      if (cs.done == 1) {
-        // leaf values of the finished tree (src/tree/symmetric_tree.cpp:357-367, 753-775)
-        const int t = *P.iter * c.KT + c.k0 + k;
-        const int dep = cs.depth;
-        P.m_depth[t] = dep;
-        const NodeStat* ns = P.nstat + ((size_t)k * (c.D + 1) + dep) * L;
-        for (int q = 0; q < (1 << dep); ++q) {
+      s_go = 0;
+    }
+    __syncthreads();
+    const bool alive = !cs.done && (d == 0 || cs.depth == d) && d < c.D;
+    if (alive) {
+      const NodeStat* ns = P.nstat + ((size_t)k * (c.D + 1) + d) * L;
+      for (int q = tid; q < (1 << d); q += blockDim.x)
+        if (ns[q].cnt >= (uint32_t)c.msl * 2u && (float)ns[q].H >= c.mcw * 2.0f) s_go = 1;
+    }
+    __syncthreads();
+    if (tid == 0 && !cs.done && !(alive && s_go)) cs.done = 1;
+    __syncthreads();
+    if (cs.done == 1) {
+      const int t = *P.iter * c.KT + c.k0 + k;
+      const int dep = cs.depth;
+      const NodeStat* ns = P.nstat + ((size_t)k * (c.D + 1) + dep) * L;
+      for (int q = tid; q < L; q += blockDim.x) {
+        float v = 0.0f;
+        if (q < (1 << dep)) {
           const double H = ns[q].H;
-          float v = 0.0f;
           if (H >= 1e-10) {
             double x = -ns[q].G / (H + (double)c.lam);
             const double l1 = (double)c.l1;
@@ -700,15 +865,83 @@ __global__ void k_plan(DevCfg c, DevPtrs P, int d, int k_only) {
             if (md > 0) x = fmax(-md, fmin(md, x));
             v = (float)x;
           }
-          P.m_leaves[(size_t)t * L + q] = v;
         }
-        for (int q = (1 << dep); q < L; ++q) P.m_leaves[(size_t)t * L + q] = 0.0f;
-        cs.done = 2;  // finalized
+        P.m_leaves[(size_t)t * L + q] = v;
       }
+      __syncthreads();
+      if (tid == 0) {
+        P.m_depth[t] = dep;
+        cs.done = 2;
+      }
+    } else if (!cs.done) {
+      // segment starts (exclusive scan over the pairs' lengths)
+      const int np2 = pairs_at(d);
+      if (tid == 0) s_carry = 0;
+      __syncthreads();
+      for (int base = 0; base < np2; base += blockDim.x) {
+        const int p = base + tid;
+        const int len = p < np2 ? (d == 0 ? (int)c.n : P.seg_len[k * Pmax + p]) : 0;
+        int x = len;
+        for (int o = 1; o < 32; o <<= 1) {
+          const int y = __shfl_up_sync(0xffffffffu, x, o);
+          if (lane >= o) x += y;
+        }
+        if (lane == 31) s_warp[warp] = x;
+        __syncthreads();
+        int before = s_carry;
+        for (int w = 0; w < warp; ++w) before += s_warp[w];
+        if (p < np2) P.seg_start[k * Pmax + p] = before + x - len;
+        __syncthreads();
+        if (tid == blockDim.x - 1) s_carry = before + x;
+        __syncthreads();
+      }
+      if (tid == 0) s_rows += s_carry;
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) *P.n_items = min(s_items, c.item_cap);
+  // rows per chunk for this level: about two items per histogram block
+  __shared__ int s_R;
+  if (tid == 0) {
+    int R = c.rows_fixed;
+    if (R <= 0) {
+      const long long target = c.target_items;
+      R = (int)max((long long)c.rows_min, (s_rows * c.G + target - 1) / target);
+    }
+    s_R = R;
+    *P.rchunk = R;
+    s_carry = 0;
+  }
+  __syncthreads();
+  const int R = s_R;
+  // cumulative chunk counts over segment-groups (class, pair, group)
+  const int np2 = pairs_at(d);
+  const int nsg = c.K * np2 * c.G;
+  for (int base = 0; base < nsg; base += blockDim.x) {
+    const int sgi = base + tid;
+    int chunks = 0;
+    if (sgi < nsg) {
+      const int kp = sgi / c.G;
+      const int k = kp / np2, p = kp % np2;
+      if (!P.cs[k].done) {
+        const int len = d == 0 ? (int)c.n : P.seg_len[k * Pmax + p];
+        chunks = (len + R - 1) / R;
+      }
+    }
+    int x = chunks;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    int before = s_carry;
+    for (int w = 0; w < warp; ++w) before += s_warp[w];
+    if (sgi < nsg) P.cum[sgi] = min(before + x - chunks, c.item_cap);
+    __syncthreads();
+    if (tid == blockDim.x - 1) s_carry = before + x;
+    __syncthreads();
+  }
+  if (tid == 0) P.cum[nsg] = min(s_carry, c.item_cap);
 }
 
 // grid (PB, K).  Row ids of the smaller children, grouped by pair.
@@ -778,8 +1011,9 @@ struct tc_trainer {
   DevBuf<uint32_t> rows;
   DevBuf<double2> hist0, hist1;
   DevBuf<float2> part;
-  DevBuf<Item> items;
-  DevBuf<int32_t> n_items, seg_start, seg_len, item_base, n_chunks, small, iter;
+  DevBuf<int32_t> cum, rchunk, seg_start, seg_len, small, iter;
+  DevBuf<FeatBest> fbest;
+  DevBuf<uint32_t> counters;
   DevBuf<NodeStat> nstat;
   DevBuf<uint32_t> pcnt, blk_off;
   DevBuf<double2> psum;
@@ -801,6 +1035,8 @@ struct tc_trainer {
   }
 
   bool given_gh = false;
+  bool tuned = false;
+  int hist_waves = 2;
   int64_t launches = 0;
   int launches_per_iter = 0;
   // profiling: when prof != nullptr every launch is bracketed by events
@@ -818,6 +1054,8 @@ struct tc_trainer {
   void mark_begin(int cls, cudaStream_t st);
   void mark_end(cudaStream_t st, double bytes = 0.0);
   tc_status setup(int given_gh_rows_only);
+  tc_status configure(int J, int waves);
+  tc_status autotune();
   void launch_level(const DevCfg& c, const DevPtrs& P, int d, cudaStream_t st);
   tc_status enqueue_iteration(cudaStream_t st);
   tc_status run_plain_iteration(cudaStream_t st);
@@ -825,53 +1063,26 @@ struct tc_trainer {
   tc_status step(int iters, bool sync);
 };
 
-namespace {
-
-template <int J>
-void set_hist_attr() {
-  cudaFuncSetAttribute(k_hist<J>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kSlots * 32 * J * 4);
-}
-
-}  // namespace
-
 tc_status tc_trainer::setup(int) {
   const uint32_t n = ds->n, f = ds->f;
   const int K = prm.loss == TC_LOSS_SOFTMAX ? prm.n_classes : 1;
   const int D = prm.max_depth;
-  // feature groups: J*32 columns per block, groups as even as possible
-  int J_ = prm.hist_features_per_block ? prm.hist_features_per_block / 32 : 0;
-  if (J_ < 1 || J_ > 3) {
-    // default: the fewest groups whose width fits in 3*32 columns, then the
-    // narrowest J covering the per-group size
-    int G = (int)((f + 95) / 96);
-    int per = (int)((f + G - 1) / G);
-    J_ = (per + 31) / 32;
-  }
-  J = J_;
-  const int W = 32 * J;
-  const int G = (int)((f + W - 1) / W);
-  int R = prm.hist_rows_per_chunk;
-  const int blocks_per_sm = (2 * kSlots * W * 4 <= 100 * 1024) ? 2 : 1;
-  hist_grid = ctx->sm_count * blocks_per_sm;
-  if (R <= 0) {
-    // about two waves of items at the root
-    const long long target = (long long)hist_grid;
-    R = (int)std::max<long long>(1024, ((long long)n * G + target - 1) / target);
-  }
   const int PB = ctx->sm_count * 2;
+  if (PB > 512) return ctx->fail(TC_ERR_INVALID_ARG, "too many SMs for the partition reduction");
   const int Pmax = 1 << (D - 1);
   const int L = 1 << D;
-  // item capacity: chunks of every segment of every class at the widest level
-  const long long cap = (long long)K * G * ((n + R - 1) / R + Pmax + 1);
   const int ngroups_max = (L / 2 + SCAN_NODES - 1) / SCAN_NODES;
+  const int G = 1, W = 32;  // placeholders until configure()
 
   cfg.n = n; cfg.f = f; cfg.fs = ds->fs; cfg.np = ds->np;
   cfg.K = K; cfg.KT = K; cfg.k0 = 0; cfg.D = D; cfg.nb_scan = (int)(uint8_t)prm.max_bins - 1; cfg.loss = prm.loss;
   cfg.msl = prm.min_samples_leaf; cfg.lr = prm.learning_rate; cfg.lam = prm.lambda_l2; cfg.l1 = prm.lambda_l1;
   cfg.mcw = prm.min_child_weight; cfg.msg = prm.min_split_gain; cfg.mds = prm.max_delta_step;
   cfg.gamma = prm.focal_gamma; cfg.alpha = prm.focal_alpha;
-  cfg.G = G; cfg.W = W; cfg.R = R; cfg.PB = PB; cfg.item_cap = (int)cap;
+  cfg.G = G; cfg.W = W; cfg.PB = PB;
   cfg.n_scan_groups_max = std::max(1, ngroups_max);
+  cfg.rows_min = 512;
+  cfg.rows_fixed = prm.hist_rows_per_chunk > 0 ? prm.hist_rows_per_chunk : 0;
 
   T_cap = prm.n_estimators * K;
   TC_TRY(pred.alloc(ctx, (size_t)K * n, "predictions"));
@@ -881,13 +1092,9 @@ tc_status tc_trainer::setup(int) {
   const size_t hsz = (size_t)K * Pmax * f * kSlots;
   TC_TRY(hist0.alloc(ctx, hsz, "level histograms"));
   TC_TRY(hist1.alloc(ctx, hsz, "level histograms"));
-  TC_TRY(part.alloc(ctx, (size_t)cap * kSlots * W, "histogram partials"));
-  TC_TRY(items.alloc(ctx, (size_t)cap, "work items"));
-  TC_TRY(n_items.alloc(ctx, 1, "item count"));
+  TC_TRY(rchunk.alloc(ctx, 1, "chunk rows"));
   TC_TRY(seg_start.alloc(ctx, (size_t)K * Pmax, "segments"));
   TC_TRY(seg_len.alloc(ctx, (size_t)K * Pmax, "segments"));
-  TC_TRY(item_base.alloc(ctx, (size_t)K * Pmax * G, "segments"));
-  TC_TRY(n_chunks.alloc(ctx, (size_t)K * Pmax, "segments"));
   TC_TRY(small.alloc(ctx, (size_t)K * Pmax, "segments"));
   TC_TRY(iter.alloc(ctx, 1, "iteration"));
   TC_TRY(nstat.alloc(ctx, (size_t)K * (D + 1) * L, "node stats"));
@@ -896,6 +1103,8 @@ tc_status tc_trainer::setup(int) {
   TC_TRY(blk_off.alloc(ctx, (size_t)K * PB * Pmax, "scatter offsets"));
   TC_TRY(gpart.alloc(ctx, (size_t)K * f * cfg.n_scan_groups_max * kSlots, "gain partials"));
   TC_TRY(gany.alloc(ctx, (size_t)K * f * cfg.n_scan_groups_max * kSlots, "gain flags"));
+  TC_TRY(fbest.alloc(ctx, (size_t)K * f, "feature bests"));
+  TC_TRY(counters.alloc(ctx, K, "pick counters"));
   TC_TRY(cs.alloc(ctx, K, "class state"));
   TC_TRY(m_depth.alloc(ctx, T_cap, "model"));
   TC_TRY(m_feat.alloc(ctx, (size_t)T_cap * D, "model"));
@@ -904,22 +1113,114 @@ tc_status tc_trainer::setup(int) {
   TC_TRY(m_gain.alloc(ctx, (size_t)T_cap * D, "model"));
   TC_TRY(m_second.alloc(ctx, (size_t)T_cap * D, "model"));
   TC_TRY(m_leaves.alloc(ctx, (size_t)T_cap * L, "model"));
+  TC_CUDA(ctx, cudaMemset(counters.p, 0, counters.bytes()));
 
   ptr.bins_rm = ds->bins_rm.p; ptr.bins_cm = ds->bins_cm.p; ptr.edges = ds->edges.p; ptr.n_edges = ds->n_edges.p;
   ptr.y = ds->y.p; ptr.pred = pred.p; ptr.gh = gh.p; ptr.leaf = leaf.p; ptr.rows = rows.p;
-  ptr.hist[0] = hist0.p; ptr.hist[1] = hist1.p; ptr.part = part.p; ptr.items = items.p; ptr.n_items = n_items.p;
-  ptr.seg_start = seg_start.p; ptr.seg_len = seg_len.p; ptr.item_base = item_base.p; ptr.n_chunks = n_chunks.p;
-  ptr.small = small.p; ptr.nstat = nstat.p; ptr.pcnt = pcnt.p; ptr.psum = psum.p; ptr.blk_off = blk_off.p;
-  ptr.gpart = gpart.p; ptr.gany = gany.p; ptr.cs = cs.p; ptr.iter = iter.p;
+  ptr.hist[0] = hist0.p; ptr.hist[1] = hist1.p; ptr.rchunk = rchunk.p;
+  ptr.seg_start = seg_start.p; ptr.seg_len = seg_len.p; ptr.small = small.p; ptr.nstat = nstat.p;
+  ptr.pcnt = pcnt.p; ptr.psum = psum.p; ptr.blk_off = blk_off.p; ptr.gpart = gpart.p; ptr.gany = gany.p;
+  ptr.fbest = fbest.p; ptr.counters = counters.p; ptr.cs = cs.p; ptr.iter = iter.p;
   ptr.m_depth = m_depth.p; ptr.m_feat = m_feat.p; ptr.m_bin = m_bin.p; ptr.m_thr = m_thr.p; ptr.m_gain = m_gain.p;
   ptr.m_second = m_second.p; ptr.m_leaves = m_leaves.p; ptr.root_hist_out = nullptr;
 
-  set_hist_attr<1>();
-  set_hist_attr<2>();
-  set_hist_attr<3>();
-  cudaFuncSetAttribute(k_partition, cudaFuncAttributeMaxDynamicSharedMemorySize, 20 * L);
+  cudaFuncSetAttribute(k_hist<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape<1>::smem);
+  cudaFuncSetAttribute(k_hist<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape<2>::smem);
+  cudaFuncSetAttribute(k_hist<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape<3>::smem);
+  cudaFuncSetAttribute(k_partition, cudaFuncAttributeMaxDynamicSharedMemorySize, 12 * L);
   TC_CUDA(ctx, cudaEventCreate(&ev0));
   TC_CUDA(ctx, cudaEventCreate(&ev1));
+  int J0 = prm.hist_features_per_block / 32;
+  if (J0 < 1 || J0 > 3) {
+    // default before tuning: the fewest 96-column groups, narrowest J covering them
+    const int G0 = (int)((f + 95) / 96);
+    const int per = (int)((f + G0 - 1) / G0);
+    J0 = (per + 31) / 32;
+  }
+  return configure(J0, 2);
+}
+
+// Feature-group width (32*J columns) and work items per histogram launch
+// (waves x resident histogram blocks); (re)sizes the partial buffer.
+tc_status tc_trainer::configure(int J_, int waves) {
+  const uint32_t f = cfg.f;
+  const int K = cfg.K, D = cfg.D;
+  const int Pmax = 1 << (D - 1);
+  J = J_;
+  const int W = 32 * J;
+  const int G = (int)((f + W - 1) / W);
+  const size_t hsm = J == 1 ? HistShape<1>::smem : (J == 2 ? HistShape<2>::smem : HistShape<3>::smem);
+  const int blocks_per_sm = std::max<int>(1, (int)((227 * 1024) / (hsm + 1024)));
+  hist_grid = ctx->sm_count * std::min(blocks_per_sm, 4);
+  hist_waves = waves;
+  long long cap = (long long)waves * hist_grid + (long long)K * Pmax * G + 1;
+  if (cfg.rows_fixed) cap += (long long)K * G * ((cfg.n + cfg.rows_fixed - 1) / cfg.rows_fixed + 1);
+  cfg.G = G;
+  cfg.W = W;
+  cfg.hist_grid = hist_grid;
+  cfg.target_items = waves * hist_grid;
+  cfg.item_cap = (int)cap;
+  TC_TRY(part.alloc(ctx, (size_t)cap * kSlots * W, "histogram partials"));
+  TC_TRY(cum.alloc(ctx, (size_t)K * Pmax * G + 1, "chunk counts"));
+  ptr.part = part.p;
+  ptr.cum = cum.p;
+  if (graph) {
+    cudaGraphExecDestroy(graph);
+    graph = nullptr;
+  }
+  return TC_OK;
+}
+
+namespace {
+std::mutex g_tune_mu;
+std::map<std::string, std::pair<int, int>> g_tune_cache;  // shape -> (J, waves)
+}  // namespace
+
+// Project autotuner: times a few launch-by-launch iterations for every
+// (feature-group width, items per launch) candidate on this dataset shape,
+// keeps the fastest, caches it per (rows, features, depth, classes, SMs) and
+// restarts the model from the base prediction.
+tc_status tc_trainer::autotune() {
+  char key[160];
+  snprintf(key, sizeof(key), "%u/%u/%d/%d/%d/%d", cfg.n, cfg.f, cfg.D, cfg.K, ctx->sm_count, prm.loss);
+  {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      TC_TRY(configure(it->second.first, it->second.second));
+      tuned = true;
+      return TC_OK;
+    }
+  }
+  cudaStream_t st = ctx->stream;
+  const int jmax = std::min(3, (int)((cfg.f + 31) / 32));
+  double best = 1e30;
+  int bj = J, bw = hist_waves;
+  const int trial_iters = 2;  // + 1 warm-up: 3 <= n_estimators iterations (checked by the caller)
+  for (int j = 1; j <= jmax; ++j) {
+    for (int waves : {1, 2, 4}) {
+      TC_TRY(configure(j, waves));
+      TC_TRY(init_predictions());
+      enqueue_iteration(st);  // warm-up (first touch of the buffers)
+      TC_CUDA(ctx, cudaEventRecord(ev0, st));
+      for (int i = 0; i < trial_iters; ++i) enqueue_iteration(st);
+      TC_CUDA(ctx, cudaEventRecord(ev1, st));
+      TC_CUDA(ctx, cudaEventSynchronize(ev1));
+      float ms = 0.0f;
+      TC_CUDA(ctx, cudaEventElapsedTime(&ms, ev0, ev1));
+      if (ms < best) {
+        best = ms;
+        bj = j;
+        bw = waves;
+      }
+    }
+  }
+  TC_TRY(configure(bj, bw));
+  TC_TRY(init_predictions());
+  launches = 0;
+  tuned = true;
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  g_tune_cache[key] = {bj, bw};
   return TC_OK;
 }
 
@@ -952,7 +1253,6 @@ void tc_trainer::mark_end(cudaStream_t st, double bytes) {
 // All launches of level d for the classes of view (c, P).
 void tc_trainer::launch_level(const DevCfg& c, const DevPtrs& P, int d, cudaStream_t st) {
   const int K = c.K, D = c.D;
-  const size_t smem = (size_t)2 * kSlots * 32 * J * 4;
   double hist_bytes = 0.0, hist_rows = 0.0;
   if (prof) {
     // algorithmic bytes: rows histogrammed at this level (device counts)
@@ -977,9 +1277,9 @@ void tc_trainer::launch_level(const DevCfg& c, const DevPtrs& P, int d, cudaStre
     hist_rows = rows;
   }
   mark_begin(KC_HIST, st);
-  if (J == 1) k_hist<1><<<hist_grid, HIST_THREADS, smem, st>>>(c, P, d);
-  else if (J == 2) k_hist<2><<<hist_grid, HIST_THREADS, smem, st>>>(c, P, d);
-  else k_hist<3><<<hist_grid, HIST_THREADS, smem, st>>>(c, P, d);
+  if (J == 1) k_hist<1><<<hist_grid, HIST_THREADS, HistShape<1>::smem, st>>>(c, P, d);
+  else if (J == 2) k_hist<2><<<hist_grid, HIST_THREADS, HistShape<2>::smem, st>>>(c, P, d);
+  else k_hist<3><<<hist_grid, HIST_THREADS, HistShape<3>::smem, st>>>(c, P, d);
   mark_end(st, hist_bytes);
   if (prof) {
     prof->back().level = d;
@@ -994,19 +1294,19 @@ void tc_trainer::launch_level(const DevCfg& c, const DevPtrs& P, int d, cudaStre
   mark_end(st);
   const int ng = ((1 << d) + SCAN_NODES - 1) / SCAN_NODES;
   mark_begin(KC_SCAN, st);
-  k_scan<<<dim3(c.f, ng, K), 256, 0, st>>>(c, P, d);
+  k_scan<<<dim3(c.f, ng, K), SCAN_WARPS * 32, 0, st>>>(c, P, d);
   mark_end(st);
   mark_begin(KC_PICK, st);
-  k_pick<<<K, 1024, 0, st>>>(c, P, d);
+  k_pick<<<dim3(c.f, K), 256, 0, st>>>(c, P, d);
   mark_end(st);
   mark_begin(KC_PART, st);
-  k_partition<<<dim3(c.PB, K), PART_THREADS, 20 * (2 << d), st>>>(c, P, d);
+  k_partition<<<dim3(c.PB, K), PART_THREADS, 12 * (2 << d), st>>>(c, P, d);
   mark_end(st, (double)c.n * K * (1 + 2 + 2 + 8));
   mark_begin(KC_REDUCE, st);
-  k_node_reduce<<<dim3(1 << d, K), 256, 0, st>>>(c, P, d);
+  k_node_reduce<<<dim3(1 << d, K), 512, 0, st>>>(c, P, d);
   mark_end(st);
   mark_begin(KC_PLAN, st);
-  k_plan<<<1, 32, 0, st>>>(c, P, d + 1, -1);
+  k_plan<<<1, PLAN_THREADS, 0, st>>>(c, P, d + 1);
   mark_end(st);
   if (d + 1 < D) {
     mark_begin(KC_SCATTER, st);
@@ -1022,10 +1322,10 @@ tc_status tc_trainer::enqueue_iteration(cudaStream_t st) {
   k_grad<<<cfg.PB, 512, 0, st>>>(cfg, ptr, 0);
   mark_end(st, (double)cfg.n * K * (4 + 4 + 8 + 2 + 8) + (double)cfg.n * 4);
   mark_begin(KC_REDUCE, st);
-  k_node_reduce<<<dim3(1, K), 256, 0, st>>>(cfg, ptr, -1);
+  k_node_reduce<<<dim3(1, K), 512, 0, st>>>(cfg, ptr, -1);
   mark_end(st);
   mark_begin(KC_PLAN, st);
-  k_plan<<<1, 32, 0, st>>>(cfg, ptr, 0, -1);
+  k_plan<<<1, PLAN_THREADS, 0, st>>>(cfg, ptr, 0);
   mark_end(st);
   for (int d = 0; d < D; ++d) launch_level(cfg, ptr, d, st);
   mark_begin(KC_OTHER, st);
@@ -1045,8 +1345,9 @@ static DevPtrs class_view(const DevCfg& c, const DevPtrs& P, int k, DevCfg* one)
   pk.pred += k * n; pk.gh += k * n; pk.leaf += k * n; pk.rows += k * n;
   pk.hist[0] += (size_t)k * Pmax * c.f * kSlots;
   pk.hist[1] += (size_t)k * Pmax * c.f * kSlots;
-  pk.seg_start += k * Pmax; pk.seg_len += k * Pmax; pk.item_base += (size_t)k * Pmax * c.G;
-  pk.n_chunks += k * Pmax; pk.small += k * Pmax; pk.nstat += (size_t)k * (c.D + 1) * L;
+  pk.seg_start += k * Pmax; pk.seg_len += k * Pmax;
+  pk.small += k * Pmax; pk.nstat += (size_t)k * (c.D + 1) * L;
+  pk.fbest += (size_t)k * c.f; pk.counters += k;
   pk.pcnt += (size_t)k * c.PB * L; pk.psum += (size_t)k * c.PB * L; pk.blk_off += (size_t)k * c.PB * Pmax;
   pk.gpart += (size_t)k * c.f * c.n_scan_groups_max * kSlots;
   pk.gany += (size_t)k * c.f * c.n_scan_groups_max * kSlots;
@@ -1059,11 +1360,11 @@ static DevPtrs class_view(const DevCfg& c, const DevPtrs& P, int k, DevCfg* one)
 tc_status tc_trainer::run_plain_iteration(cudaStream_t st) {
   const int K = cfg.K, D = cfg.D;
   k_grad<<<cfg.PB, 512, 0, st>>>(cfg, ptr, 0);
-  k_node_reduce<<<dim3(1, K), 256, 0, st>>>(cfg, ptr, -1);
+  k_node_reduce<<<dim3(1, K), 512, 0, st>>>(cfg, ptr, -1);
   for (int k = 0; k < K; ++k) {
     DevCfg one;
     DevPtrs pk = class_view(cfg, ptr, k, &one);
-    k_plan<<<1, 32, 0, st>>>(one, pk, 0, -1);
+    k_plan<<<1, PLAN_THREADS, 0, st>>>(one, pk, 0);
     for (int d = 0; d < D; ++d) {
       TC_CUDA(ctx, cudaStreamSynchronize(st));
       ClassState h;
@@ -1186,6 +1487,8 @@ tc_status tc_trainer_create(tc_ctx* ctx, tc_dataset* ds, const tc_train_params* 
   tr->prm = *p;
   tc_status s = tr->setup(0);
   if (s == TC_OK) s = tr->init_predictions();
+  // tuning runs up to three throw-away iterations: it needs that many tree slots
+  if (s == TC_OK && p->hist_features_per_block == 0 && p->n_estimators >= 3) s = tr->autotune();
   if (s != TC_OK) {
     delete tr;
     return s;
@@ -1213,7 +1516,7 @@ tc_status tc_trainer_stats(tc_trainer* tr, tc_train_stats* st) {
   st->base_prediction = tr->base;
   st->seconds = tr->seconds;
   st->hist_features_per_block = tr->cfg.W;
-  st->hist_rows_per_chunk = tr->cfg.R;
+  st->hist_rows_per_chunk = tr->cfg.rows_fixed ? tr->cfg.rows_fixed : -tr->cfg.target_items;
   st->kernel_launches = tr->launches;
   return TC_OK;
 }
@@ -1401,8 +1704,8 @@ tc_status tc_build_tree(tc_ctx* ctx, tc_dataset* ds, const float* grad, const fl
   // one iteration with the given gradients
   const int D = tr->cfg.D;
   k_grad<<<tr->cfg.PB, 512, 0, st>>>(tr->cfg, tr->ptr, 1);
-  k_node_reduce<<<dim3(1, 1), 256, 0, st>>>(tr->cfg, tr->ptr, -1);
-  k_plan<<<1, 32, 0, st>>>(tr->cfg, tr->ptr, 0, -1);
+  k_node_reduce<<<dim3(1, 1), 512, 0, st>>>(tr->cfg, tr->ptr, -1);
+  k_plan<<<1, PLAN_THREADS, 0, st>>>(tr->cfg, tr->ptr, 0);
   for (int d = 0; d < D; ++d) {
     tr->launch_level(tr->cfg, tr->ptr, d, st);
     if (d == 0 && root_hist) k_root_hist_out<<<64, 256, 0, st>>>(tr->cfg, tr->ptr);
