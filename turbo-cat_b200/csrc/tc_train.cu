@@ -85,6 +85,7 @@ struct DevCfg {
   int32_t target_items;          // work items aimed for per histogram launch
   int32_t rows_min;              // smallest rows per histogram chunk
   int32_t rows_fixed;            // > 0: fixed rows per chunk (tuning override)
+  float hconst;                  // > 0: every row's hessian equals this (histogram counts rows)
 };
 
 struct DevPtrs {
@@ -282,8 +283,10 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 template <int J>
 struct HistShape {
   static constexpr int W = 32 * J;
-  static constexpr int S = J == 3 ? 2 : 3;             // staging depth
+  static constexpr int S = 2;                          // staging depth (tiles in flight)
   static constexpr int CH = W / 16;                    // 16-byte chunks per staged row slice
+  static constexpr int SLOTS = HIST_TILE * CH;         // copy slots per tile
+  static constexpr int SLOT_ROUNDS = (SLOTS + HIST_THREADS - 1) / HIST_THREADS;
   static constexpr size_t hist_bytes = (size_t)2 * kSlots * W * 4;
   static constexpr size_t stage_bytes = (size_t)HIST_TILE * (W + 8);
   static constexpr size_t smem = hist_bytes + S * stage_bytes;
@@ -302,16 +305,26 @@ __device__ __forceinline__ int find_sg(const int32_t* cum, int nsg, int item) {
 // Persistent blocks over work items; an item is a chunk of one segment's
 // rows (the root at d = 0, a smaller child after) for one feature group.
 // Row slices (the group's bytes of each row) and the rows' (grad, hess) are
-// staged into shared memory by cp.async, S tiles ahead of the compute, so
-// the gathered rows' latency overlaps the atomic updates of earlier tiles.
-// Shared histogram layout: column (feature in the group) fastest, so lane l
-// of a warp always hits bank l: float hist[(2*bin + {0 grad, 1 hess}) * W + col].
+// staged into shared memory by cp.async one tile ahead of the compute (row
+// ids of gathered rows are fetched one further tile ahead, into registers),
+// so the gathered rows' latency overlaps the updates of the current tile.
+//
+// Shared histogram layout: column fastest, so lane l of a warp always hits
+// bank l: float hist[(2*bin + {0 grad, 1 hess}) * W + column].  A group of at
+// most 16 features is packed: with p2 = next power of two >= its width, the
+// 32 columns hold 32/p2 private copies and one warp instruction updates
+// 32/p2 rows; the copies are summed when the partial is written.
+//
+// Constant-hessian losses (MSE: h = 2 for every row) count rows per bin with
+// 32-bit integer shared atomics (2.7x the throughput of FP32 shared atomics
+// on this part) and write hess = count * h exactly.
 template <int J>
 __global__ void __launch_bounds__(HIST_THREADS) k_hist(DevCfg c, DevPtrs P, int d) {
   using S_ = HistShape<J>;
-  constexpr int W = S_::W, S = S_::S, CH = S_::CH, T = HIST_TILE;
+  constexpr int W = S_::W, S = S_::S, CH = S_::CH, T = HIST_TILE, RND = S_::SLOT_ROUNDS;
   extern __shared__ __align__(16) unsigned char smraw[];
   float* hist = reinterpret_cast<float*>(smraw);
+  uint32_t* histu = reinterpret_cast<uint32_t*>(smraw);
   uint8_t* s_bins = smraw + S_::hist_bytes;                                  // [S][T][W]
   float2* s_gh = reinterpret_cast<float2*>(s_bins + (size_t)S * T * W);      // [S][T]
   const int P2 = pairs_at(d);
@@ -319,6 +332,7 @@ __global__ void __launch_bounds__(HIST_THREADS) k_hist(DevCfg c, DevPtrs P, int 
   const int n_items = P.cum[nsg];
   const int R = *P.rchunk;
   const int Pmax = 1 << (c.D - 1);
+  const bool cnt_mode = c.hconst > 0.0f;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
     const int sg = find_sg(P.cum, nsg, item);
@@ -328,6 +342,10 @@ __global__ void __launch_bounds__(HIST_THREADS) k_hist(DevCfg c, DevPtrs P, int 
     const int k = kp / P2, p = kp % P2;
     const int g0 = g * W;
     const int gsize = min(W, (int)c.f - g0);
+    const int p2 = gsize <= 1 ? 1 : (gsize <= 2 ? 2 : (gsize <= 4 ? 4 : (gsize <= 8 ? 8 : (gsize <= 16 ? 16 : 32))));
+    const bool narrow = p2 <= 16;
+    const int rpi = narrow ? 32 / p2 : 1;   // rows per warp instruction
+    const int my_row = lane / p2, my_col = lane % p2;
     int start, end;
     if (d == 0) {
       start = ch_idx * R;
@@ -342,72 +360,111 @@ __global__ void __launch_bounds__(HIST_THREADS) k_hist(DevCfg c, DevPtrs P, int 
     const float2* gh = P.gh + (size_t)k * c.n;
     for (int q = threadIdx.x; q < 2 * kSlots * W; q += blockDim.x) hist[q] = 0.0f;
     const int n_tiles = (end - start + T - 1) / T;
-    // stage tile t into buffer t % S
-    auto issue = [&](int t) {
-      if (t < n_tiles) {
-        const int st = t % S;
-        const int base = start + t * T;
-        for (int q = threadIdx.x; q < T * CH; q += blockDim.x) {
-          const int i = q / CH, chn = q % CH;
-          const int idx = base + i;
-          if (idx < end && g0 + 16 * chn < (int)c.fs) {
-            const uint32_t r = d == 0 ? (uint32_t)idx : rows[idx];
-            cp_async16(s_bins + ((size_t)st * T + i) * W + 16 * chn, P.bins_rm + (size_t)r * c.fs + g0 + 16 * chn);
-          }
-        }
-        for (int i = threadIdx.x; i < T; i += blockDim.x) {
-          const int idx = base + i;
-          if (idx < end) {
-            const uint32_t r = d == 0 ? (uint32_t)idx : rows[idx];
-            cp_async8(s_gh + (size_t)st * T + i, gh + r);
-          }
-        }
-      }
-      cp_async_commit();
-    };
+    // row ids of this thread's copy slots (at most two per tile), fetched one
+    // tile ahead of the copies that use them
+    uint32_t rid0 = 0, rid1 = 0, rgh = 0;
+#define TC_FETCH_IDS(t)                                                                       \
+    {                                                                                         \
+      const int base_ = start + (t) * T;                                                      \
+      const int q0_ = threadIdx.x, q1_ = threadIdx.x + HIST_THREADS;                          \
+      const int i0_ = base_ + q0_ / CH, i1_ = base_ + q1_ / CH, ig_ = base_ + threadIdx.x;      \
+      rid0 = (q0_ < T * CH && i0_ < end) ? (d == 0 ? (uint32_t)i0_ : rows[i0_]) : 0u;          \
+      if (RND > 1) rid1 = (q1_ < T * CH && i1_ < end) ? (d == 0 ? (uint32_t)i1_ : rows[i1_]) : 0u; \
+      rgh = (threadIdx.x < T && ig_ < end) ? (d == 0 ? (uint32_t)ig_ : rows[ig_]) : 0u;        \
+    }
+#define TC_ISSUE(t)                                                                           \
+    {                                                                                         \
+      if ((t) < n_tiles) {                                                                    \
+        const int st_ = (t) % S;                                                              \
+        const int base_ = start + (t) * T;                                                    \
+        _Pragma("unroll") for (int u = 0; u < RND; ++u) {                                     \
+          const int q = threadIdx.x + u * HIST_THREADS;                                       \
+          const int i = q / CH, chn = q % CH;                                                 \
+          if (q < T * CH && base_ + i < end && g0 + 16 * chn < (int)c.fs)                     \
+            cp_async16(s_bins + ((size_t)st_ * T + i) * W + 16 * chn,                         \
+                       P.bins_rm + (size_t)(u == 0 ? rid0 : rid1) * c.fs + g0 + 16 * chn);    \
+        }                                                                                     \
+        if (threadIdx.x < T && base_ + (int)threadIdx.x < end)                                \
+          cp_async8(s_gh + (size_t)st_ * T + threadIdx.x, gh + rgh);                           \
+      }                                                                                       \
+      cp_async_commit();                                                                      \
+    }
     __syncthreads();
-#pragma unroll
-    for (int t = 0; t < S - 1; ++t) issue(t);
+    TC_FETCH_IDS(0);
+    TC_ISSUE(0);
+    TC_FETCH_IDS(1);
     for (int t = 0; t < n_tiles; ++t) {
-      issue(t + S - 1);
-      cp_async_wait<S - 1>();
+      TC_ISSUE(t + 1);       // S = 2: the next tile streams in while this one is counted
+      TC_FETCH_IDS(t + 2);   // ids for the tile after, hidden behind this tile's updates
+      cp_async_wait<1>();
       __syncthreads();
       const int st = t % S;
       const int nvalid = min(T, end - (start + t * T));
       const uint8_t* sb = s_bins + (size_t)st * T * W;
       const float2* sv = s_gh + (size_t)st * T;
-      for (int i = warp; i < nvalid; i += 2 * nwarps) {
-        const int i2 = i + nwarps;
-        const bool has2 = i2 < nvalid;
-        const float2 v1 = sv[i];
-        const float2 v2 = has2 ? sv[i2] : make_float2(0.f, 0.f);
-        int b1[J], b2[J];
+      if (!narrow) {
+        for (int i = warp; i < nvalid; i += 2 * nwarps) {
+          const int i2 = i + nwarps;
+          const bool has2 = i2 < nvalid;
+          const float2 v1 = sv[i];
+          const float2 v2 = has2 ? sv[i2] : make_float2(0.f, 0.f);
+          int b1[J], b2[J];
 #pragma unroll
-        for (int j = 0; j < J; ++j) {
-          const int col = lane + 32 * j;
-          b1[j] = sb[(size_t)i * W + col];
-          b2[j] = has2 ? sb[(size_t)i2 * W + col] : 0;
-        }
+          for (int j = 0; j < J; ++j) {
+            const int col = lane + 32 * j;
+            b1[j] = sb[(size_t)i * W + col];
+            b2[j] = has2 ? sb[(size_t)i2 * W + col] : 0;
+          }
 #pragma unroll
-        for (int j = 0; j < J; ++j) {
-          const int col = lane + 32 * j;
-          if (col < gsize) {
-            atomicAdd(&hist[(2 * b1[j]) * W + col], v1.x);
-            atomicAdd(&hist[(2 * b1[j] + 1) * W + col], v1.y);
-            if (has2) {
-              atomicAdd(&hist[(2 * b2[j]) * W + col], v2.x);
-              atomicAdd(&hist[(2 * b2[j] + 1) * W + col], v2.y);
+          for (int j = 0; j < J; ++j) {
+            const int col = lane + 32 * j;
+            if (col < gsize) {
+              atomicAdd(&hist[(2 * b1[j]) * W + col], v1.x);
+              if (cnt_mode) atomicAdd(&histu[(2 * b1[j] + 1) * W + col], 1u);
+              else atomicAdd(&hist[(2 * b1[j] + 1) * W + col], v1.y);
+              if (has2) {
+                atomicAdd(&hist[(2 * b2[j]) * W + col], v2.x);
+                if (cnt_mode) atomicAdd(&histu[(2 * b2[j] + 1) * W + col], 1u);
+                else atomicAdd(&hist[(2 * b2[j] + 1) * W + col], v2.y);
+              }
             }
+          }
+        }
+      } else {
+        // packed narrow group: lane (my_row, my_col) of rows i .. i+rpi-1
+        for (int i = warp * rpi; i < nvalid; i += nwarps * rpi) {
+          const int r = i + my_row;
+          if (r < nvalid && my_col < gsize) {
+            const float2 v = sv[r];
+            const int b = sb[(size_t)r * W + my_col];
+            atomicAdd(&hist[(2 * b) * W + lane], v.x);
+            if (cnt_mode) atomicAdd(&histu[(2 * b + 1) * W + lane], 1u);
+            else atomicAdd(&hist[(2 * b + 1) * W + lane], v.y);
           }
         }
       }
       __syncthreads();
     }
+#undef TC_FETCH_IDS
+#undef TC_ISSUE
     cp_async_wait<0>();
     float2* out = P.part + (size_t)item * kSlots * W;
     for (int q = threadIdx.x; q < kSlots * W; q += blockDim.x) {
       const int b = q / W, col = q % W;
-      out[q] = make_float2(hist[(2 * b) * W + col], hist[(2 * b + 1) * W + col]);
+      float sgv = 0.0f, shv = 0.0f;
+      if (!narrow) {
+        sgv = hist[(2 * b) * W + col];
+        shv = cnt_mode ? c.hconst * (float)histu[(2 * b + 1) * W + col] : hist[(2 * b + 1) * W + col];
+      } else if (col < gsize) {
+        uint32_t cnt = 0;
+        for (int cp = 0; cp < rpi; ++cp) {
+          sgv += hist[(2 * b) * W + cp * p2 + col];
+          if (cnt_mode) cnt += histu[(2 * b + 1) * W + cp * p2 + col];
+          else shv += hist[(2 * b + 1) * W + cp * p2 + col];
+        }
+        if (cnt_mode) shv = c.hconst * (float)cnt;
+      }
+      out[q] = make_float2(sgv, shv);
     }
     __syncthreads();
   }
@@ -1083,6 +1140,8 @@ tc_status tc_trainer::setup(int) {
   cfg.n_scan_groups_max = std::max(1, ngroups_max);
   cfg.rows_min = 512;
   cfg.rows_fixed = prm.hist_rows_per_chunk > 0 ? prm.hist_rows_per_chunk : 0;
+  // MSE's hessian is 2 for every row (src/boosting/loss.cpp:348-362)
+  cfg.hconst = (prm.loss == TC_LOSS_MSE && !given_gh) ? 2.0f : 0.0f;
 
   T_cap = prm.n_estimators * K;
   TC_TRY(pred.alloc(ctx, (size_t)K * n, "predictions"));
