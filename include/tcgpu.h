@@ -109,7 +109,7 @@ typedef struct {
   int32_t batched;          /* 1: all classes and nodes of a level per launch, one CUDA graph per
                                iteration; 0: the plain path, one tree and one level at a time with a
                                host synchronisation per level */
-  int32_t hist_features_per_block; /* 0 = autotune; else 32, 64 or 96 */
+  int32_t hist_features_per_block; /* 0 = autotune; else 32 or 64 (other values: 32) */
   int32_t hist_rows_per_chunk;     /* 0 = autotune */
 } tc_train_params;
 

@@ -309,7 +309,7 @@ def test_bad_tcat_is_rejected(engine, capi):
 
 # ---------------------------------------------- tile shapes and the tuner --
 
-@pytest.mark.parametrize("width,rows", [(32, 0), (64, 0), (96, 0), (64, 700), (32, 5000)])
+@pytest.mark.parametrize("width,rows", [(32, 0), (64, 0), (32, 700), (64, 700), (32, 5000)])
 def test_fit_identical_across_histogram_tilings(engine, capi, width, rows):
     """Every histogram tiling (feature-group width, rows per chunk) must grow
     the same trees: tilings change only FP32 summation order inside blocks."""

@@ -45,7 +45,7 @@ namespace tc {
 namespace {
 
 constexpr int HIST_THREADS = 512;
-constexpr int HIST_TILE = 128;    // rows per staged tile
+constexpr int HIST_BATCH = 32;    // rows per warp batch (one per lane)
 constexpr int PART_THREADS = 512;
 constexpr int SCAN_WARPS = 8;     // warps per scan block
 constexpr int SCAN_NODES = 32;    // nodes per scan block (4 per warp)
@@ -100,7 +100,7 @@ struct DevPtrs {
   uint32_t* rows;                // [K][n]
   double2* hist[2];              // [K][2^(D-1)][F][256]
   float2* part;                  // [item_cap][256][W]
-  int32_t* cum;                  // [K*2^(D-1)*G + 1] cumulative chunk counts (segment-group order)
+  int32_t* cum;                  // [K*2^(D-1) + 1] cumulative item counts per segment (chunk-major)
   int32_t* rchunk;               // [1] rows per chunk at the current level
   int32_t* seg_start;            // [K][2^(D-1)]
   int32_t* seg_len;              // [K][2^(D-1)]
@@ -282,19 +282,17 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 
 template <int J>
 struct HistShape {
-  static constexpr int W = 32 * J;
-  static constexpr int S = 2;                          // staging depth (tiles in flight)
-  static constexpr int CH = W / 16;                    // 16-byte chunks per staged row slice
-  static constexpr int SLOTS = HIST_TILE * CH;         // copy slots per tile
-  static constexpr int SLOT_ROUNDS = (SLOTS + HIST_THREADS - 1) / HIST_THREADS;
+  static constexpr int W = 32 * J;                      // histogram columns of a block
+  static constexpr int WARPS = HIST_THREADS / 32;
+  static constexpr int S = 2;                           // staging depth per warp (batches in flight)
   static constexpr size_t hist_bytes = (size_t)2 * kSlots * W * 4;
-  static constexpr size_t stage_bytes = (size_t)HIST_TILE * (W + 8);
-  static constexpr size_t smem = hist_bytes + S * stage_bytes;
+  static constexpr size_t warp_bytes = (size_t)S * HIST_BATCH * (W + 8);   // bins + (grad, hess)
+  static constexpr size_t smem = hist_bytes + WARPS * warp_bytes;
 };
 
-// Work item -> (segment-group, chunk) through the cumulative chunk counts.
-__device__ __forceinline__ int find_sg(const int32_t* cum, int nsg, int item) {
-  int lo = 0, hi = nsg - 1;
+// Work item -> segment (class, pair) through the cumulative item counts.
+__device__ __forceinline__ int find_seg(const int32_t* cum, int nseg, int item) {
+  int lo = 0, hi = nseg - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
     if (cum[mid] <= item) lo = mid; else hi = mid - 1;
@@ -302,50 +300,87 @@ __device__ __forceinline__ int find_sg(const int32_t* cum, int nsg, int item) {
   return lo;
 }
 
-// Persistent blocks over work items; an item is a chunk of one segment's
-// rows (the root at d = 0, a smaller child after) for one feature group.
-// Row slices (the group's bytes of each row) and the rows' (grad, hess) are
-// staged into shared memory by cp.async one tile ahead of the compute (row
-// ids of gathered rows are fetched one further tile ahead, into registers),
-// so the gathered rows' latency overlaps the updates of the current tile.
+// Bin slots of a histogram column: a feature with n_edges edges uses bins
+// 0 .. n_edges (span = n_edges + 1) and the NaN slot 255, so the slots past
+// its span are free.  They hold private copies of the column for different
+// warps (copy c of bin b in slot c*span + b, NaN always in slot 255), which
+// spreads the updates of few-bin features over more addresses: concurrent
+// atomics on one shared address serialise.
+__device__ __forceinline__ int hist_span(const uint16_t* ne, int f, int nf) {
+  return f < nf ? (int)ne[f] + 1 : 255;
+}
+__device__ __forceinline__ int hist_copies(int span) { return min(HIST_THREADS / 32, max(1, 255 / span)); }
+// slot offset of this warp's copy of a column
+__device__ __forceinline__ int hist_copy_offset(const uint16_t* ne, int f, int nf, int warp) {
+  const int span = hist_span(ne, f, nf);
+  return (warp % hist_copies(span)) * span;
+}
+
+// Persistent blocks over work items; an item is one chunk of one segment's
+// rows (the root at d = 0, a smaller child after) for one feature group, and
+// the items of a chunk's groups are adjacent (chunk-major), so blocks that run
+// together read the same rows and the L2 serves a row's bytes and its
+// (grad, hess) to every group.
 //
-// Shared histogram layout: column fastest, so lane l of a warp always hits
-// bank l: float hist[(2*bin + {0 grad, 1 hess}) * W + column].  A group of at
-// most 16 features is packed: with p2 = next power of two >= its width, the
-// 32 columns hold 32/p2 private copies and one warp instruction updates
-// 32/p2 rows; the copies are summed when the partial is written.
+// Every warp runs its own copy pipeline: lane l stages row l of a 32-row
+// batch (its group slice and its (grad, hess)) by cp.async into the warp's
+// private buffers, one batch ahead of the updates, with the row ids of
+// gathered rows fetched a further batch ahead; no block barrier is taken
+// until the item is done.
+//
+// Shared histogram layout: column fastest, so a column always hits the same
+// bank: float hist[(2*bin + {0 grad, 1 hess}) * W + column].  A wide group
+// is updated four rows at a time: lane (r = l/8, c = l%8) loads the 4 bins
+// of columns 4c..4c+3 of row r of the quad as one word and, in step s,
+// updates column 4c + (s + r) % 4, so the 32 lanes of every step hit 32
+// different columns (banks).  A group of at most 16 features is packed: with
+// p2 = next power of two >= its width, the 32 columns hold 32/p2 private
+// copies and one warp instruction updates 32/p2 rows; the copies are summed
+// when the partial is written.  Columns past a group's width collect the
+// padding bytes of the row and are never read.  A bin goes to slot
+// min(bin + copy offset, 255) of its column (the copies above).
 //
 // Constant-hessian losses (MSE: h = 2 for every row) count rows per bin with
 // 32-bit integer shared atomics (2.7x the throughput of FP32 shared atomics
 // on this part) and write hess = count * h exactly.
 template <int J>
-__global__ void __launch_bounds__(HIST_THREADS) k_hist(DevCfg c, DevPtrs P, int d) {
+__global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs P, int d) {
   using S_ = HistShape<J>;
-  constexpr int W = S_::W, S = S_::S, CH = S_::CH, T = HIST_TILE, RND = S_::SLOT_ROUNDS;
+  constexpr int W = S_::W, S = S_::S, B = HIST_BATCH;
   extern __shared__ __align__(16) unsigned char smraw[];
   float* hist = reinterpret_cast<float*>(smraw);
   uint32_t* histu = reinterpret_cast<uint32_t*>(smraw);
-  uint8_t* s_bins = smraw + S_::hist_bytes;                                  // [S][T][W]
-  float2* s_gh = reinterpret_cast<float2*>(s_bins + (size_t)S * T * W);      // [S][T]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  uint8_t* w_bins = smraw + S_::hist_bytes + (size_t)warp * S_::warp_bytes;        // [S][B][W]
+  float2* w_gh = reinterpret_cast<float2*>(w_bins + (size_t)S * B * W);            // [S][B]
   const int P2 = pairs_at(d);
-  const int nsg = c.K * P2 * c.G;
-  const int n_items = P.cum[nsg];
+  const int nseg = c.K * P2;
+  const int n_items = P.cum[nseg];
   const int R = *P.rchunk;
   const int Pmax = 1 << (c.D - 1);
   const bool cnt_mode = c.hconst > 0.0f;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  // quad mapping of this lane: row r of a quad, columns 4*c4 .. 4*c4+3
+  const int qr = lane >> 3, c4 = lane & 7;
+  for (int q = threadIdx.x; q < 2 * kSlots * W; q += blockDim.x) hist[q] = 0.0f;
+  __syncthreads();
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
-    const int sg = find_sg(P.cum, nsg, item);
-    const int ch_idx = item - P.cum[sg];
-    const int g = sg % c.G;
-    const int kp = sg / c.G;
-    const int k = kp / P2, p = kp % P2;
+    const int seg = find_seg(P.cum, nseg, item);
+    const int local = item - P.cum[seg];
+    const int ch_idx = local / c.G;
+    const int g = local - ch_idx * c.G;
+    const int k = seg / P2, p = seg - k * P2;
     const int g0 = g * W;
     const int gsize = min(W, (int)c.f - g0);
     const int p2 = gsize <= 1 ? 1 : (gsize <= 2 ? 2 : (gsize <= 4 ? 4 : (gsize <= 8 ? 8 : (gsize <= 16 ? 16 : 32))));
     const bool narrow = p2 <= 16;
-    const int rpi = narrow ? 32 / p2 : 1;   // rows per warp instruction
-    const int my_row = lane / p2, my_col = lane % p2;
+    const int nchunk16 = (gsize + 15) >> 4;  // 16-byte pieces of the slice that hold features
+    // slot offsets of this warp's copies of the lane's columns
+    int off[J][4];
+#pragma unroll
+    for (int j = 0; j < J; ++j)
+#pragma unroll
+      for (int s = 0; s < 4; ++s)
+        off[j][s] = hist_copy_offset(P.n_edges, g0 + 32 * j + 4 * c4 + ((s + qr) & 3), (int)c.f, warp);
     int start, end;
     if (d == 0) {
       start = ch_idx * R;
@@ -358,113 +393,143 @@ __global__ void __launch_bounds__(HIST_THREADS) k_hist(DevCfg c, DevPtrs P, int 
     }
     const uint32_t* rows = P.rows + (size_t)k * c.n;
     const float2* gh = P.gh + (size_t)k * c.n;
-    for (int q = threadIdx.x; q < 2 * kSlots * W; q += blockDim.x) hist[q] = 0.0f;
-    const int n_tiles = (end - start + T - 1) / T;
-    // row ids of this thread's copy slots (at most two per tile), fetched one
-    // tile ahead of the copies that use them
-    uint32_t rid0 = 0, rid1 = 0, rgh = 0;
-#define TC_FETCH_IDS(t)                                                                       \
-    {                                                                                         \
-      const int base_ = start + (t) * T;                                                      \
-      const int q0_ = threadIdx.x, q1_ = threadIdx.x + HIST_THREADS;                          \
-      const int i0_ = base_ + q0_ / CH, i1_ = base_ + q1_ / CH, ig_ = base_ + threadIdx.x;      \
-      rid0 = (q0_ < T * CH && i0_ < end) ? (d == 0 ? (uint32_t)i0_ : rows[i0_]) : 0u;          \
-      if (RND > 1) rid1 = (q1_ < T * CH && i1_ < end) ? (d == 0 ? (uint32_t)i1_ : rows[i1_]) : 0u; \
-      rgh = (threadIdx.x < T && ig_ < end) ? (d == 0 ? (uint32_t)ig_ : rows[ig_]) : 0u;        \
+    const uint8_t* bsrc = P.bins_rm + g0;
+    const int nb = (end - start + B - 1) / B;   // batches in the item; warp w takes w, w+nwarps, ...
+    uint32_t rid_next = 0;
+#define TC_FETCH_ID(bi)                                                                      \
+    {                                                                                        \
+      const int r_ = start + (bi) * B + lane;                                                \
+      rid_next = ((bi) < nb && r_ < end) ? (d == 0 ? (uint32_t)r_ : rows[r_]) : 0u;          \
     }
-#define TC_ISSUE(t)                                                                           \
-    {                                                                                         \
-      if ((t) < n_tiles) {                                                                    \
-        const int st_ = (t) % S;                                                              \
-        const int base_ = start + (t) * T;                                                    \
-        _Pragma("unroll") for (int u = 0; u < RND; ++u) {                                     \
-          const int q = threadIdx.x + u * HIST_THREADS;                                       \
-          const int i = q / CH, chn = q % CH;                                                 \
-          if (q < T * CH && base_ + i < end && g0 + 16 * chn < (int)c.fs)                     \
-            cp_async16(s_bins + ((size_t)st_ * T + i) * W + 16 * chn,                         \
-                       P.bins_rm + (size_t)(u == 0 ? rid0 : rid1) * c.fs + g0 + 16 * chn);    \
-        }                                                                                     \
-        if (threadIdx.x < T && base_ + (int)threadIdx.x < end)                                \
-          cp_async8(s_gh + (size_t)st_ * T + threadIdx.x, gh + rgh);                           \
-      }                                                                                       \
-      cp_async_commit();                                                                      \
+#define TC_ISSUE(bi, st_)                                                                    \
+    {                                                                                        \
+      if ((bi) < nb && start + (bi) * B + lane < end) {                                      \
+        const uint8_t* src_ = bsrc + (size_t)rid_next * c.fs;                                \
+        uint8_t* dst_ = w_bins + ((size_t)(st_) * B + lane) * W;                             \
+        _Pragma("unroll") for (int u = 0; u < 2 * J; ++u)                                    \
+          if (u < nchunk16) cp_async16(dst_ + 16 * u, src_ + 16 * u);                        \
+        cp_async8(w_gh + (st_) * B + lane, gh + rid_next);                                   \
+      }                                                                                      \
+      cp_async_commit();                                                                     \
     }
-    __syncthreads();
-    TC_FETCH_IDS(0);
-    TC_ISSUE(0);
-    TC_FETCH_IDS(1);
-    for (int t = 0; t < n_tiles; ++t) {
-      TC_ISSUE(t + 1);       // S = 2: the next tile streams in while this one is counted
-      TC_FETCH_IDS(t + 2);   // ids for the tile after, hidden behind this tile's updates
+    int bi = warp;
+    TC_FETCH_ID(bi);
+    TC_ISSUE(bi, 0);
+    TC_FETCH_ID(bi + nwarps);
+    for (int t = 0; bi < nb; ++t, bi += nwarps) {
+      const int st = t & 1;
+      TC_ISSUE(bi + nwarps, st ^ 1);       // the next batch streams in while this one is counted
+      TC_FETCH_ID(bi + 2 * nwarps);        // row ids for the batch after, behind this batch's updates
       cp_async_wait<1>();
-      __syncthreads();
-      const int st = t % S;
-      const int nvalid = min(T, end - (start + t * T));
-      const uint8_t* sb = s_bins + (size_t)st * T * W;
-      const float2* sv = s_gh + (size_t)st * T;
+      __syncwarp();
+      const int nvalid = min(B, end - (start + bi * B));
+      const uint8_t* sb = w_bins + (size_t)st * B * W;
+      const float2* sv = w_gh + st * B;
       if (!narrow) {
-        for (int i = warp; i < nvalid; i += 2 * nwarps) {
-          const int i2 = i + nwarps;
-          const bool has2 = i2 < nvalid;
-          const float2 v1 = sv[i];
-          const float2 v2 = has2 ? sv[i2] : make_float2(0.f, 0.f);
-          int b1[J], b2[J];
+        // the batch's bins and (grad, hess) go to registers first, so the
+        // loads are not ordered behind the updates (they share the memory space)
+        const uint32_t* sw = reinterpret_cast<const uint32_t*>(sb);
+        uint32_t wd[B / 4][J];
+        float vx[B / 4], vy[B / 4];
+#pragma unroll
+        for (int qd = 0; qd < B / 4; ++qd) {
+          const int row = 4 * qd + qr;
+          const float2 v = sv[row];
+          vx[qd] = v.x;
+          vy[qd] = v.y;
 #pragma unroll
           for (int j = 0; j < J; ++j) {
-            const int col = lane + 32 * j;
-            b1[j] = sb[(size_t)i * W + col];
-            b2[j] = has2 ? sb[(size_t)i2 * W + col] : 0;
+            const uint32_t w = sw[row * (W / 4) + 8 * j + c4];
+            wd[qd][j] = __funnelshift_r(w, w, 8 * qr);  // byte s is column 4*c4 + (s + qr) % 4
           }
+        }
 #pragma unroll
-          for (int j = 0; j < J; ++j) {
-            const int col = lane + 32 * j;
-            if (col < gsize) {
-              atomicAdd(&hist[(2 * b1[j]) * W + col], v1.x);
-              if (cnt_mode) atomicAdd(&histu[(2 * b1[j] + 1) * W + col], 1u);
-              else atomicAdd(&hist[(2 * b1[j] + 1) * W + col], v1.y);
-              if (has2) {
-                atomicAdd(&hist[(2 * b2[j]) * W + col], v2.x);
-                if (cnt_mode) atomicAdd(&histu[(2 * b2[j] + 1) * W + col], 1u);
-                else atomicAdd(&hist[(2 * b2[j] + 1) * W + col], v2.y);
+        for (int qd = 0; qd < B / 4; ++qd) {
+          if (4 * qd + qr < nvalid) {
+#pragma unroll
+            for (int j = 0; j < J; ++j) {
+              if (32 * j < gsize) {
+#pragma unroll
+                for (int s = 0; s < 4; ++s) {
+                  const int col = 32 * j + 4 * c4 + ((s + qr) & 3);
+                  const int slot = min((int)((wd[qd][j] >> (8 * s)) & 0xFF) + off[j][s], 255);
+                  const int o = 2 * slot * W + col;
+                  atomicAdd(&hist[o], vx[qd]);
+                  if (cnt_mode) atomicAdd(&histu[o + W], 1u);
+                  else atomicAdd(&hist[o + W], vy[qd]);
+                }
               }
             }
           }
         }
       } else {
-        // packed narrow group: lane (my_row, my_col) of rows i .. i+rpi-1
-        for (int i = warp * rpi; i < nvalid; i += nwarps * rpi) {
-          const int r = i + my_row;
-          if (r < nvalid && my_col < gsize) {
-            const float2 v = sv[r];
-            const int b = sb[(size_t)r * W + my_col];
-            atomicAdd(&hist[(2 * b) * W + lane], v.x);
-            if (cnt_mode) atomicAdd(&histu[(2 * b + 1) * W + lane], 1u);
-            else atomicAdd(&hist[(2 * b + 1) * W + lane], v.y);
+        // packed narrow group: lane (copy, column) of rows i .. i + 32/p2 - 1,
+        // four instructions' rows loaded ahead of their updates
+        const int rpi = 32 / p2;
+        const int my_row = lane / p2, my_col = lane - my_row * p2;
+        const int noff = hist_copy_offset(P.n_edges, g0 + my_col, (int)c.f, warp);
+        for (int i0 = 0; i0 < B; i0 += 4 * rpi) {
+          int bb[4];
+          float gx[4], gy[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int row = min(i0 + u * rpi + my_row, B - 1);
+            const float2 v = sv[row];
+            gx[u] = v.x;
+            gy[u] = v.y;
+            bb[u] = min((int)sb[row * W + my_col] + noff, 255);
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            if (i0 + u * rpi + my_row < nvalid) {
+              atomicAdd(&hist[2 * bb[u] * W + lane], gx[u]);
+              if (cnt_mode) atomicAdd(&histu[(2 * bb[u] + 1) * W + lane], 1u);
+              else atomicAdd(&hist[(2 * bb[u] + 1) * W + lane], gy[u]);
+            }
           }
         }
       }
-      __syncthreads();
+      __syncwarp();
     }
-#undef TC_FETCH_IDS
+#undef TC_FETCH_ID
 #undef TC_ISSUE
     cp_async_wait<0>();
+    __syncthreads();
     float2* out = P.part + (size_t)item * kSlots * W;
+    // write the partial (copies summed in a fixed order) and clear the
+    // histogram for the next item; a thread clears exactly the slots it reads
+    const int ncp = narrow ? 32 / p2 : 1;     // packed copies of a narrow group
+    // blockDim.x is a multiple of W: a thread's column is the same on every pass
+    const int fcol = threadIdx.x % W;
+    const int fspan = hist_span(P.n_edges, g0 + fcol, (int)c.f);
+    const int fcopies = hist_copies(fspan);
     for (int q = threadIdx.x; q < kSlots * W; q += blockDim.x) {
-      const int b = q / W, col = q % W;
+      const int b = q / W, col = fcol;
       float sgv = 0.0f, shv = 0.0f;
-      if (!narrow) {
-        sgv = hist[(2 * b) * W + col];
-        shv = cnt_mode ? c.hconst * (float)histu[(2 * b + 1) * W + col] : hist[(2 * b + 1) * W + col];
-      } else if (col < gsize) {
-        uint32_t cnt = 0;
-        for (int cp = 0; cp < rpi; ++cp) {
-          sgv += hist[(2 * b) * W + cp * p2 + col];
-          if (cnt_mode) cnt += histu[(2 * b + 1) * W + cp * p2 + col];
-          else shv += hist[(2 * b + 1) * W + cp * p2 + col];
+      uint32_t cnt = 0;
+      if (!narrow || col < p2) {
+        const int span = fspan;
+        const int kc = b == kNanBin ? 1 : (b < span ? fcopies : 0);
+        for (int cc = 0; cc < kc; ++cc) {
+          const int slot = b == kNanBin ? kNanBin : cc * span + b;
+          for (int cp = 0; cp < ncp; ++cp) {
+            const int o = 2 * slot * W + cp * p2 * (narrow ? 1 : 0) + col;
+            sgv += hist[o];
+            if (cnt_mode) cnt += histu[o + W];
+            else shv += hist[o + W];
+            if (!narrow) {
+              hist[o] = 0.0f;
+              hist[o + W] = 0.0f;
+            }
+          }
         }
         if (cnt_mode) shv = c.hconst * (float)cnt;
       }
       out[q] = make_float2(sgv, shv);
+    }
+    if (narrow) {
+      __syncthreads();
+      for (int q = threadIdx.x; q < 2 * kSlots * 32; q += blockDim.x) hist[(q >> 5) * W + (q & 31)] = 0.0f;
     }
     __syncthreads();
   }
@@ -486,15 +551,14 @@ __global__ void k_merge(DevCfg c, DevPtrs P, int d) {
   const int g0 = g * W;
   const int gsize = min(W, (int)c.f - g0);
   const int b0 = blockIdx.x * MERGE_BB;
-  const int sg = (k * P2 + p) * c.G + g;
-  const int ib = P.cum[sg];
-  const int nch = P.cum[sg + 1] - ib;
+  const int ib = P.cum[seg] + g;                        // chunk-major: chunk ch is item ib + ch*G
+  const int nch = (P.cum[seg + 1] - P.cum[seg]) / c.G;
   for (int q = threadIdx.x; q < MERGE_BB * W; q += blockDim.x) {
     const int bl = q / W, col = q % W;
     double sg_ = 0.0, sh = 0.0;
     if (col < gsize) {
       for (int ch = 0; ch < nch; ++ch) {
-        const float2 v = P.part[((size_t)(ib + ch) * kSlots + b0 + bl) * W + col];
+        const float2 v = P.part[((size_t)(ib + ch * c.G) * kSlots + b0 + bl) * W + col];
         sg_ += (double)v.x;
         sh += (double)v.y;
       }
@@ -970,18 +1034,17 @@ __global__ void __launch_bounds__(PLAN_THREADS) k_plan(DevCfg c, DevPtrs P, int 
   }
   __syncthreads();
   const int R = s_R;
-  // cumulative chunk counts over segment-groups (class, pair, group)
+  // cumulative item counts over segments (class, pair): chunks x groups
   const int np2 = pairs_at(d);
-  const int nsg = c.K * np2 * c.G;
+  const int nsg = c.K * np2;
   for (int base = 0; base < nsg; base += blockDim.x) {
     const int sgi = base + tid;
     int chunks = 0;
     if (sgi < nsg) {
-      const int kp = sgi / c.G;
-      const int k = kp / np2, p = kp % np2;
+      const int k = sgi / np2, p = sgi % np2;
       if (!P.cs[k].done) {
         const int len = d == 0 ? (int)c.n : P.seg_len[k * Pmax + p];
-        chunks = (len + R - 1) / R;
+        chunks = (len + R - 1) / R * c.G;
       }
     }
     int x = chunks;
@@ -1185,17 +1248,11 @@ tc_status tc_trainer::setup(int) {
 
   cudaFuncSetAttribute(k_hist<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape<1>::smem);
   cudaFuncSetAttribute(k_hist<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape<2>::smem);
-  cudaFuncSetAttribute(k_hist<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape<3>::smem);
   cudaFuncSetAttribute(k_partition, cudaFuncAttributeMaxDynamicSharedMemorySize, 12 * L);
   TC_CUDA(ctx, cudaEventCreate(&ev0));
   TC_CUDA(ctx, cudaEventCreate(&ev1));
   int J0 = prm.hist_features_per_block / 32;
-  if (J0 < 1 || J0 > 3) {
-    // default before tuning: the fewest 96-column groups, narrowest J covering them
-    const int G0 = (int)((f + 95) / 96);
-    const int per = (int)((f + G0 - 1) / G0);
-    J0 = (per + 31) / 32;
-  }
+  if (J0 < 1 || J0 > 2) J0 = 1;  // default before tuning: 32-column groups
   return configure(J0, 2);
 }
 
@@ -1208,7 +1265,7 @@ tc_status tc_trainer::configure(int J_, int waves) {
   J = J_;
   const int W = 32 * J;
   const int G = (int)((f + W - 1) / W);
-  const size_t hsm = J == 1 ? HistShape<1>::smem : (J == 2 ? HistShape<2>::smem : HistShape<3>::smem);
+  const size_t hsm = J == 1 ? HistShape<1>::smem : HistShape<2>::smem;
   const int blocks_per_sm = std::max<int>(1, (int)((227 * 1024) / (hsm + 1024)));
   hist_grid = ctx->sm_count * std::min(blocks_per_sm, 4);
   hist_waves = waves;
@@ -1252,7 +1309,7 @@ tc_status tc_trainer::autotune() {
     }
   }
   cudaStream_t st = ctx->stream;
-  const int jmax = std::min(3, (int)((cfg.f + 31) / 32));
+  const int jmax = std::min(2, (int)((cfg.f + 31) / 32));
   double best = 1e30;
   int bj = J, bw = hist_waves;
   const int trial_iters = 2;  // + 1 warm-up: 3 <= n_estimators iterations (checked by the caller)
@@ -1337,8 +1394,7 @@ void tc_trainer::launch_level(const DevCfg& c, const DevPtrs& P, int d, cudaStre
   }
   mark_begin(KC_HIST, st);
   if (J == 1) k_hist<1><<<hist_grid, HIST_THREADS, HistShape<1>::smem, st>>>(c, P, d);
-  else if (J == 2) k_hist<2><<<hist_grid, HIST_THREADS, HistShape<2>::smem, st>>>(c, P, d);
-  else k_hist<3><<<hist_grid, HIST_THREADS, HistShape<3>::smem, st>>>(c, P, d);
+  else k_hist<2><<<hist_grid, HIST_THREADS, HistShape<2>::smem, st>>>(c, P, d);
   mark_end(st, hist_bytes);
   if (prof) {
     prof->back().level = d;
@@ -1348,8 +1404,7 @@ void tc_trainer::launch_level(const DevCfg& c, const DevPtrs& P, int d, cudaStre
   dim3 mg(kSlots / MERGE_BB, K * P2, c.G);
   mark_begin(KC_MERGE, st);
   if (J == 1) k_merge<1><<<mg, 256, 0, st>>>(c, P, d);
-  else if (J == 2) k_merge<2><<<mg, 256, 0, st>>>(c, P, d);
-  else k_merge<3><<<mg, 256, 0, st>>>(c, P, d);
+  else k_merge<2><<<mg, 256, 0, st>>>(c, P, d);
   mark_end(st);
   const int ng = ((1 << d) + SCAN_NODES - 1) / SCAN_NODES;
   mark_begin(KC_SCAN, st);
