@@ -237,17 +237,21 @@ constexpr int AB_ROWS = 256;
 __global__ void k_assign_bins(const float* __restrict__ X, uint32_t n, uint32_t f,
                               const float* __restrict__ edges, const uint16_t* __restrict__ n_edges,
                               uint8_t* __restrict__ bins_rm, uint32_t fs, uint8_t* __restrict__ bins_cm,
-                              uint32_t np) {
+                              uint32_t np, uint32_t* __restrict__ nan_any) {
   __shared__ float s_e[32][kSlots + 1];
   __shared__ int s_ne[32];
   __shared__ uint8_t s_b[32][AB_ROWS + 4];
+  __shared__ int s_nan[32];
   const uint32_t j0 = blockIdx.y * 32, r0 = blockIdx.x * AB_ROWS;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
   for (int q = tid; q < 32 * kSlots; q += blockDim.x) {
     const int jj = q / kSlots, e = q % kSlots;
     s_e[jj][e] = (j0 + jj < f) ? edges[(size_t)(j0 + jj) * kSlots + e] : 0.0f;
   }
-  if (tid < 32) s_ne[tid] = (j0 + tid < f) ? (int)n_edges[j0 + tid] : 0;
+  if (tid < 32) {
+    s_ne[tid] = (j0 + tid < f) ? (int)n_edges[j0 + tid] : 0;
+    s_nan[tid] = 0;
+  }
   __syncthreads();
   const uint32_t j = j0 + lane;
   for (int i = warp; i < AB_ROWS; i += nw) {
@@ -257,6 +261,7 @@ __global__ void k_assign_bins(const float* __restrict__ X, uint32_t n, uint32_t 
       const float x = X[(size_t)r * f + j];
       if (isnan(x)) {
         b = (uint8_t)kNanBin;
+        s_nan[lane] = 1;
       } else {
         int lo = 0, hi = s_ne[lane];
         while (lo < hi) {
@@ -269,6 +274,7 @@ __global__ void k_assign_bins(const float* __restrict__ X, uint32_t n, uint32_t 
     s_b[lane][i] = b;
   }
   __syncthreads();
+  if (tid < 32 && s_nan[tid] && j0 + tid < f) atomicOr(&nan_any[j0 + tid], 1u);
   // column-major rows of this tile
   for (int q = tid; q < 32 * AB_ROWS; q += blockDim.x) {
     const int jj = q / AB_ROWS, i = q % AB_ROWS;
@@ -298,6 +304,8 @@ tc_status quantize(tc_dataset* ds, int max_bins, int compat_u8) {
   TC_TRY(U.alloc(ctx, f, "unique counts"));
   TC_TRY(ds->edges.alloc(ctx, (size_t)f * kSlots, "bin edges"));
   TC_TRY(ds->n_edges.alloc(ctx, f, "edge counts"));
+  TC_TRY(ds->nan_any.alloc(ctx, f, "NaN flags"));
+  TC_CUDA(ctx, cudaMemsetAsync(ds->nan_any.p, 0, ds->nan_any.bytes(), st));
   TC_TRY(ds->bins_rm.alloc(ctx, (size_t)n * ds->fs, "row-major bins"));
   TC_TRY(ds->bins_cm.alloc(ctx, (size_t)f * ds->np, "column-major bins"));
   TC_CUDA(ctx, cudaMemsetAsync(ds->edges.p, 0, ds->edges.bytes(), st));
@@ -325,7 +333,7 @@ tc_status quantize(tc_dataset* ds, int max_bins, int compat_u8) {
   if (n > 0) {
     dim3 ag((n + AB_ROWS - 1) / AB_ROWS, (ds->fs + 31) / 32);
     k_assign_bins<<<ag, 256, 0, st>>>(ds->X.p, n, f, ds->edges.p, ds->n_edges.p, ds->bins_rm.p, ds->fs,
-                                      ds->bins_cm.p, ds->np);
+                                      ds->bins_cm.p, ds->np, ds->nan_any.p);
   }
   TC_CUDA(ctx, cudaGetLastError());
   // host copy of the edges for model export / thresholds

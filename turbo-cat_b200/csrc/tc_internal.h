@@ -108,6 +108,7 @@ struct tc_dataset {
   DevBuf<uint8_t> bins_cm;   // [f][np]
   DevBuf<float> edges;       // [f][256]
   DevBuf<uint16_t> n_edges;  // [f]
+  DevBuf<uint32_t> nan_any;  // [f] nonzero: the feature has NaN rows
   std::vector<float> h_edges;       // [f][255]
   std::vector<uint16_t> h_n_edges;  // [f]
 };

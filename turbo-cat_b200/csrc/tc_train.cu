@@ -93,6 +93,7 @@ struct DevPtrs {
   const uint8_t* bins_cm;
   const float* edges;            // [f][256]
   const uint16_t* n_edges;
+  const uint32_t* nan_any;       // [f] nonzero: the feature has NaN rows
   const float* y;
   float* pred;                   // [K][n]
   float2* gh;                    // [K][n]
@@ -113,6 +114,7 @@ struct DevPtrs {
   uint8_t* gany;                 // [K][F][NG][256]
   FeatBest* fbest;               // [K][F]
   uint32_t* counters;            // [K] completion counters of the pick blocks
+  int32_t* hist_ctr;             // [1] next histogram work item (reset by the plan kernel)
   ClassState* cs;                // [K]
   int32_t* iter;                 // [1] boosting iteration (tree slot = iter*KT + k0 + k)
   // model arrays (capacity T = n_estimators*K)
@@ -302,18 +304,25 @@ __device__ __forceinline__ int find_seg(const int32_t* cum, int nseg, int item) 
 
 // Bin slots of a histogram column: a feature with n_edges edges uses bins
 // 0 .. n_edges (span = n_edges + 1) and the NaN slot 255, so the slots past
-// its span are free.  They hold private copies of the column for different
-// warps (copy c of bin b in slot c*span + b, NaN always in slot 255), which
-// spreads the updates of few-bin features over more addresses: concurrent
-// atomics on one shared address serialise.
-__device__ __forceinline__ int hist_span(const uint16_t* ne, int f, int nf) {
-  return f < nf ? (int)ne[f] + 1 : 255;
+// its span are free.  A feature without NaN rows keeps private copies of its
+// column there for different warps (copy c of bin b in slot c*span + b, at
+// most 255/span copies, so bin + offset never reaches 255), which spreads the
+// updates of few-bin features over more addresses: concurrent atomics on one
+// shared address serialise.  A feature with NaN rows keeps one copy.
+struct HistCol {
+  int span, copies;
+};
+__device__ __forceinline__ HistCol hist_col(const DevPtrs& P, int f, int nf) {
+  if (f >= nf) return {255, 1};
+  const int span = (int)P.n_edges[f] + 1;
+  return {span, P.nan_any[f] ? 1 : min(HIST_THREADS / 32, max(1, 255 / span))};
 }
-__device__ __forceinline__ int hist_copies(int span) { return min(HIST_THREADS / 32, max(1, 255 / span)); }
-// slot offset of this warp's copy of a column
-__device__ __forceinline__ int hist_copy_offset(const uint16_t* ne, int f, int nf, int warp) {
-  const int span = hist_span(ne, f, nf);
-  return (warp % hist_copies(span)) * span;
+
+__device__ __forceinline__ void red_add_f32(uint32_t a, float v) {
+  asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
+}
+__device__ __forceinline__ void red_add_u32(uint32_t a, uint32_t v) {
+  asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(a), "r"(v) : "memory");
 }
 
 // Persistent blocks over work items; an item is one chunk of one segment's
@@ -329,7 +338,7 @@ __device__ __forceinline__ int hist_copy_offset(const uint16_t* ne, int f, int n
 // until the item is done.
 //
 // Shared histogram layout: column fastest, so a column always hits the same
-// bank: float hist[(2*bin + {0 grad, 1 hess}) * W + column].  A wide group
+// bank: float hist[(2*slot + {0 grad, 1 hess}) * W + column].  A wide group
 // is updated four rows at a time: lane (r = l/8, c = l%8) loads the 4 bins
 // of columns 4c..4c+3 of row r of the quad as one word and, in step s,
 // updates column 4c + (s + r) % 4, so the 32 lanes of every step hit 32
@@ -337,19 +346,22 @@ __device__ __forceinline__ int hist_copy_offset(const uint16_t* ne, int f, int n
 // p2 = next power of two >= its width, the 32 columns hold 32/p2 private
 // copies and one warp instruction updates 32/p2 rows; the copies are summed
 // when the partial is written.  Columns past a group's width collect the
-// padding bytes of the row and are never read.  A bin goes to slot
-// min(bin + copy offset, 255) of its column (the copies above).
+// padding bytes of the row and are never read.  Each lane keeps the shared
+// address of (its warp's copy of) every column it updates, so an update is a
+// byte permute, an add and the atomics.
 //
-// Constant-hessian losses (MSE: h = 2 for every row) count rows per bin with
-// 32-bit integer shared atomics (2.7x the throughput of FP32 shared atomics
-// on this part) and write hess = count * h exactly.
-template <int J>
+// CNT: every row's hessian is the same constant (MSE: h = 2); rows are
+// counted with 32-bit integer shared atomics (2.7x the throughput of FP32
+// shared atomics on this part) and hess = count * h is exact.
+template <int J, bool CNT>
 __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs P, int d) {
   using S_ = HistShape<J>;
   constexpr int W = S_::W, S = S_::S, B = HIST_BATCH;
+  constexpr uint32_t BIN_BYTES = 8 * W;   // grad and hess rows of one slot
   extern __shared__ __align__(16) unsigned char smraw[];
   float* hist = reinterpret_cast<float*>(smraw);
   uint32_t* histu = reinterpret_cast<uint32_t*>(smraw);
+  const uint32_t hbase = (uint32_t)__cvta_generic_to_shared(hist);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   uint8_t* w_bins = smraw + S_::hist_bytes + (size_t)warp * S_::warp_bytes;        // [S][B][W]
   float2* w_gh = reinterpret_cast<float2*>(w_bins + (size_t)S * B * W);            // [S][B]
@@ -358,12 +370,31 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
   const int n_items = P.cum[nseg];
   const int R = *P.rchunk;
   const int Pmax = 1 << (c.D - 1);
-  const bool cnt_mode = c.hconst > 0.0f;
-  // quad mapping of this lane: row r of a quad, columns 4*c4 .. 4*c4+3
+  // quad mapping of this lane: row qr of a quad, columns 4*c4 .. 4*c4+3;
+  // byte-permute selectors that move byte (s + qr) % 4 of the word to bits 8..15
   const int qr = lane >> 3, c4 = lane & 7;
+  uint32_t sel[4];
+#pragma unroll
+  for (int s = 0; s < 4; ++s) sel[s] = 0x4404u | ((uint32_t)((s + qr) & 3) << 4);
   for (int q = threadIdx.x; q < 2 * kSlots * W; q += blockDim.x) hist[q] = 0.0f;
   __syncthreads();
-  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+  // Items are claimed from a counter (blocks that drew cheap items take
+  // more), the next one while the current one runs.  Item ci*G + g is chunk
+  // ci (over all segments) of group g; a narrow last group costs a fraction
+  // of a wide one, so its items are handed out after all the wide ones and
+  // fill the gaps at the end.
+  const int n_chunks = n_items / c.G;
+  const int gw = (c.G > 1 && (int)c.f - (c.G - 1) * W <= 16) ? c.G - 1 : c.G;  // wide groups
+  auto claim_to_item = [&](int cl) {
+    if (gw == c.G || cl >= n_items) return cl;
+    return cl < n_chunks * gw ? (cl / gw) * c.G + cl % gw : (cl - n_chunks * gw) * c.G + gw;
+  };
+  __shared__ int s_item[2];
+  if (threadIdx.x == 0) s_item[0] = claim_to_item(atomicAdd(P.hist_ctr, 1));
+  __syncthreads();
+  int item = s_item[0];
+  for (int it = 1; item < n_items; ++it) {
+    if (threadIdx.x == 0) s_item[it & 1] = claim_to_item(atomicAdd(P.hist_ctr, 1));
     const int seg = find_seg(P.cum, nseg, item);
     const int local = item - P.cum[seg];
     const int ch_idx = local / c.G;
@@ -374,23 +405,22 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
     const int p2 = gsize <= 1 ? 1 : (gsize <= 2 ? 2 : (gsize <= 4 ? 4 : (gsize <= 8 ? 8 : (gsize <= 16 ? 16 : 32))));
     const bool narrow = p2 <= 16;
     const int nchunk16 = (gsize + 15) >> 4;  // 16-byte pieces of the slice that hold features
-    // slot offsets of this warp's copies of the lane's columns
-    int off[J][4];
+    // shared address of this warp's copy of each column the lane updates
+    uint32_t ab[J][4];
 #pragma unroll
     for (int j = 0; j < J; ++j)
 #pragma unroll
-      for (int s = 0; s < 4; ++s)
-        off[j][s] = hist_copy_offset(P.n_edges, g0 + 32 * j + 4 * c4 + ((s + qr) & 3), (int)c.f, warp);
-    int start, end;
-    if (d == 0) {
-      start = ch_idx * R;
-      end = min((int)c.n, start + R);
-    } else {
-      const int s0 = P.seg_start[k * Pmax + p];
-      const int sl = P.seg_len[k * Pmax + p];
-      start = s0 + ch_idx * R;
-      end = min(s0 + sl, start + R);
-    }
+      for (int s = 0; s < 4; ++s) {
+        const int col = 32 * j + 4 * c4 + ((s + qr) & 3);
+        const HistCol hc = hist_col(P, g0 + col, (int)c.f);
+        ab[j][s] = hbase + BIN_BYTES * (uint32_t)((warp % hc.copies) * hc.span) + 4u * col;
+      }
+    // the segment's ceil(len / R) chunks have equal sizes (within one row)
+    const int s0 = d == 0 ? 0 : P.seg_start[k * Pmax + p];
+    const int sl = d == 0 ? (int)c.n : P.seg_len[k * Pmax + p];
+    const int nch = (sl + R - 1) / R;
+    const int start = s0 + (int)((long long)sl * ch_idx / nch);
+    const int end = s0 + (int)((long long)sl * (ch_idx + 1) / nch);
     const uint32_t* rows = P.rows + (size_t)k * c.n;
     const float2* gh = P.gh + (size_t)k * c.n;
     const uint8_t* bsrc = P.bins_rm + g0;
@@ -438,10 +468,7 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
           vx[qd] = v.x;
           vy[qd] = v.y;
 #pragma unroll
-          for (int j = 0; j < J; ++j) {
-            const uint32_t w = sw[row * (W / 4) + 8 * j + c4];
-            wd[qd][j] = __funnelshift_r(w, w, 8 * qr);  // byte s is column 4*c4 + (s + qr) % 4
-          }
+          for (int j = 0; j < J; ++j) wd[qd][j] = sw[row * (W / 4) + 8 * j + c4];
         }
 #pragma unroll
         for (int qd = 0; qd < B / 4; ++qd) {
@@ -451,12 +478,11 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
               if (32 * j < gsize) {
 #pragma unroll
                 for (int s = 0; s < 4; ++s) {
-                  const int col = 32 * j + 4 * c4 + ((s + qr) & 3);
-                  const int slot = min((int)((wd[qd][j] >> (8 * s)) & 0xFF) + off[j][s], 255);
-                  const int o = 2 * slot * W + col;
-                  atomicAdd(&hist[o], vx[qd]);
-                  if (cnt_mode) atomicAdd(&histu[o + W], 1u);
-                  else atomicAdd(&hist[o + W], vy[qd]);
+                  // __byte_perm gives bin * 256; a slot is BIN_BYTES = 256 * J bytes
+                  const uint32_t a = ab[j][s] + __byte_perm(wd[qd][j], 0u, sel[s]) * J;
+                  red_add_f32(a, vx[qd]);
+                  if (CNT) red_add_u32(a + 4 * W, 1u);
+                  else red_add_f32(a + 4 * W, vy[qd]);
                 }
               }
             }
@@ -467,9 +493,10 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
         // four instructions' rows loaded ahead of their updates
         const int rpi = 32 / p2;
         const int my_row = lane / p2, my_col = lane - my_row * p2;
-        const int noff = hist_copy_offset(P.n_edges, g0 + my_col, (int)c.f, warp);
+        const HistCol hc = hist_col(P, g0 + my_col, (int)c.f);
+        const uint32_t abn = hbase + BIN_BYTES * (uint32_t)((warp % hc.copies) * hc.span) + 4u * lane;
         for (int i0 = 0; i0 < B; i0 += 4 * rpi) {
-          int bb[4];
+          uint32_t bb[4];
           float gx[4], gy[4];
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
@@ -477,14 +504,15 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
             const float2 v = sv[row];
             gx[u] = v.x;
             gy[u] = v.y;
-            bb[u] = min((int)sb[row * W + my_col] + noff, 255);
+            bb[u] = sb[row * W + my_col];
           }
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
             if (i0 + u * rpi + my_row < nvalid) {
-              atomicAdd(&hist[2 * bb[u] * W + lane], gx[u]);
-              if (cnt_mode) atomicAdd(&histu[(2 * bb[u] + 1) * W + lane], 1u);
-              else atomicAdd(&hist[(2 * bb[u] + 1) * W + lane], gy[u]);
+              const uint32_t a = abn + BIN_BYTES * bb[u];
+              red_add_f32(a, gx[u]);
+              if (CNT) red_add_u32(a + 4 * W, 1u);
+              else red_add_f32(a + 4 * W, gy[u]);
             }
           }
         }
@@ -500,22 +528,20 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
     // histogram for the next item; a thread clears exactly the slots it reads
     const int ncp = narrow ? 32 / p2 : 1;     // packed copies of a narrow group
     // blockDim.x is a multiple of W: a thread's column is the same on every pass
-    const int fcol = threadIdx.x % W;
-    const int fspan = hist_span(P.n_edges, g0 + fcol, (int)c.f);
-    const int fcopies = hist_copies(fspan);
+    const int col = threadIdx.x % W;
+    const HistCol fc = hist_col(P, g0 + col, (int)c.f);
     for (int q = threadIdx.x; q < kSlots * W; q += blockDim.x) {
-      const int b = q / W, col = fcol;
+      const int b = q / W;
       float sgv = 0.0f, shv = 0.0f;
       uint32_t cnt = 0;
       if (!narrow || col < p2) {
-        const int span = fspan;
-        const int kc = b == kNanBin ? 1 : (b < span ? fcopies : 0);
+        const int kc = b == kNanBin ? 1 : (b < fc.span ? fc.copies : 0);
         for (int cc = 0; cc < kc; ++cc) {
-          const int slot = b == kNanBin ? kNanBin : cc * span + b;
+          const int slot = b == kNanBin ? kNanBin : cc * fc.span + b;
           for (int cp = 0; cp < ncp; ++cp) {
             const int o = 2 * slot * W + cp * p2 * (narrow ? 1 : 0) + col;
             sgv += hist[o];
-            if (cnt_mode) cnt += histu[o + W];
+            if (CNT) cnt += histu[o + W];
             else shv += hist[o + W];
             if (!narrow) {
               hist[o] = 0.0f;
@@ -523,7 +549,7 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
             }
           }
         }
-        if (cnt_mode) shv = c.hconst * (float)cnt;
+        if (CNT) shv = c.hconst * (float)cnt;
       }
       out[q] = make_float2(sgv, shv);
     }
@@ -532,6 +558,7 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
       for (int q = threadIdx.x; q < 2 * kSlots * 32; q += blockDim.x) hist[(q >> 5) * W + (q & 31)] = 0.0f;
     }
     __syncthreads();
+    item = s_item[it & 1];
   }
 }
 
@@ -1061,7 +1088,10 @@ __global__ void __launch_bounds__(PLAN_THREADS) k_plan(DevCfg c, DevPtrs P, int 
     if (tid == blockDim.x - 1) s_carry = before + x;
     __syncthreads();
   }
-  if (tid == 0) P.cum[nsg] = min(s_carry, c.item_cap);
+  if (tid == 0) {
+    P.cum[nsg] = min(s_carry, c.item_cap);
+    *P.hist_ctr = 0;
+  }
 }
 
 // grid (PB, K).  Row ids of the smaller children, grouped by pair.
@@ -1134,6 +1164,7 @@ struct tc_trainer {
   DevBuf<int32_t> cum, rchunk, seg_start, seg_len, small, iter;
   DevBuf<FeatBest> fbest;
   DevBuf<uint32_t> counters;
+  DevBuf<int32_t> hist_ctr;
   DevBuf<NodeStat> nstat;
   DevBuf<uint32_t> pcnt, blk_off;
   DevBuf<double2> psum;
@@ -1227,6 +1258,7 @@ tc_status tc_trainer::setup(int) {
   TC_TRY(gany.alloc(ctx, (size_t)K * f * cfg.n_scan_groups_max * kSlots, "gain flags"));
   TC_TRY(fbest.alloc(ctx, (size_t)K * f, "feature bests"));
   TC_TRY(counters.alloc(ctx, K, "pick counters"));
+  TC_TRY(hist_ctr.alloc(ctx, 1, "histogram item counter"));
   TC_TRY(cs.alloc(ctx, K, "class state"));
   TC_TRY(m_depth.alloc(ctx, T_cap, "model"));
   TC_TRY(m_feat.alloc(ctx, (size_t)T_cap * D, "model"));
@@ -1238,16 +1270,19 @@ tc_status tc_trainer::setup(int) {
   TC_CUDA(ctx, cudaMemset(counters.p, 0, counters.bytes()));
 
   ptr.bins_rm = ds->bins_rm.p; ptr.bins_cm = ds->bins_cm.p; ptr.edges = ds->edges.p; ptr.n_edges = ds->n_edges.p;
+  ptr.nan_any = ds->nan_any.p;
   ptr.y = ds->y.p; ptr.pred = pred.p; ptr.gh = gh.p; ptr.leaf = leaf.p; ptr.rows = rows.p;
   ptr.hist[0] = hist0.p; ptr.hist[1] = hist1.p; ptr.rchunk = rchunk.p;
   ptr.seg_start = seg_start.p; ptr.seg_len = seg_len.p; ptr.small = small.p; ptr.nstat = nstat.p;
   ptr.pcnt = pcnt.p; ptr.psum = psum.p; ptr.blk_off = blk_off.p; ptr.gpart = gpart.p; ptr.gany = gany.p;
-  ptr.fbest = fbest.p; ptr.counters = counters.p; ptr.cs = cs.p; ptr.iter = iter.p;
+  ptr.fbest = fbest.p; ptr.counters = counters.p; ptr.hist_ctr = hist_ctr.p; ptr.cs = cs.p; ptr.iter = iter.p;
   ptr.m_depth = m_depth.p; ptr.m_feat = m_feat.p; ptr.m_bin = m_bin.p; ptr.m_thr = m_thr.p; ptr.m_gain = m_gain.p;
   ptr.m_second = m_second.p; ptr.m_leaves = m_leaves.p; ptr.root_hist_out = nullptr;
 
-  cudaFuncSetAttribute(k_hist<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape<1>::smem);
-  cudaFuncSetAttribute(k_hist<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape<2>::smem);
+  cudaFuncSetAttribute(k_hist<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape<1>::smem);
+  cudaFuncSetAttribute(k_hist<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape<2>::smem);
+  cudaFuncSetAttribute(k_hist<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape<1>::smem);
+  cudaFuncSetAttribute(k_hist<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape<2>::smem);
   cudaFuncSetAttribute(k_partition, cudaFuncAttributeMaxDynamicSharedMemorySize, 12 * L);
   TC_CUDA(ctx, cudaEventCreate(&ev0));
   TC_CUDA(ctx, cudaEventCreate(&ev1));
@@ -1314,7 +1349,7 @@ tc_status tc_trainer::autotune() {
   int bj = J, bw = hist_waves;
   const int trial_iters = 2;  // + 1 warm-up: 3 <= n_estimators iterations (checked by the caller)
   for (int j = 1; j <= jmax; ++j) {
-    for (int waves : {1, 2, 4}) {
+    for (int waves : {1, 2, 4, 8}) {
       TC_TRY(configure(j, waves));
       TC_TRY(init_predictions());
       enqueue_iteration(st);  // warm-up (first touch of the buffers)
@@ -1393,8 +1428,11 @@ void tc_trainer::launch_level(const DevCfg& c, const DevPtrs& P, int d, cudaStre
     hist_rows = rows;
   }
   mark_begin(KC_HIST, st);
-  if (J == 1) k_hist<1><<<hist_grid, HIST_THREADS, HistShape<1>::smem, st>>>(c, P, d);
-  else k_hist<2><<<hist_grid, HIST_THREADS, HistShape<2>::smem, st>>>(c, P, d);
+  const bool cnt = c.hconst > 0.0f;
+  if (J == 1 && cnt) k_hist<1, true><<<hist_grid, HIST_THREADS, HistShape<1>::smem, st>>>(c, P, d);
+  else if (J == 1) k_hist<1, false><<<hist_grid, HIST_THREADS, HistShape<1>::smem, st>>>(c, P, d);
+  else if (cnt) k_hist<2, true><<<hist_grid, HIST_THREADS, HistShape<2>::smem, st>>>(c, P, d);
+  else k_hist<2, false><<<hist_grid, HIST_THREADS, HistShape<2>::smem, st>>>(c, P, d);
   mark_end(st, hist_bytes);
   if (prof) {
     prof->back().level = d;
