@@ -835,8 +835,17 @@ __global__ void __launch_bounds__(256) k_pick(DevCfg c, DevPtrs P, int d) {
 // as FP64 for the cross-block merge).  With few children, a warp reduces
 // each child's contributions through shuffles first (one shared update per
 // warp and child) instead of letting every lane hit the same two addresses.
+// grid (PB, K).  Rows of the split level get their child leaf index
+// (2*leaf + right, right = bin != 255 && bin > t) and every block sums its
+// rows' (grad, hess) and counts per child: FP32 within the block (rows in a
+// fixed order inside each warp), FP64 across blocks in the reduce kernel.
+// A warp's rows are first combined per distinct child (ballots for up to 4
+// children, a match over the warp beyond), so a child gets one shared
+// atomic per warp; four rows per thread are loaded before any is used.
+constexpr int PART_UNROLL = 4;
 __global__ void __launch_bounds__(PART_THREADS) k_partition(DevCfg c, DevPtrs P, int d) {
   extern __shared__ unsigned char smraw[];
+  __shared__ float2 s_wv[PART_THREADS / 32][32];
   const int k = blockIdx.y;
   const ClassState cs = P.cs[k];
   if (cs.done || cs.depth != d + 1) return;
@@ -852,37 +861,63 @@ __global__ void __launch_bounds__(PART_THREADS) k_partition(DevCfg c, DevPtrs P,
   uint16_t* leaf = P.leaf + (size_t)k * c.n;
   const float2* gh = P.gh + (size_t)k * c.n;
   const uint8_t t = (uint8_t)cs.b;
-  const int lane = threadIdx.x & 31;
-  for (uint32_t base = r0; base < r1; base += blockDim.x) {
-    const uint32_t i = base + threadIdx.x;
-    const bool ok = i < r1;
-    int nl = -1;
-    float2 v = make_float2(0.f, 0.f);
-    if (ok) {
-      const uint8_t b = col[i];
-      const uint32_t right = (b != (uint8_t)kNanBin && b > t) ? 1u : 0u;
-      nl = (int)(((uint32_t)leaf[i] << 1) | right);
-      leaf[i] = (uint16_t)nl;
-      v = gh[i];
-    }
-    if (nch <= 8) {
-      for (int cc = 0; cc < nch; ++cc) {
-        float g = nl == cc ? v.x : 0.0f, h = nl == cc ? v.y : 0.0f;
-        const uint32_t cnt = __popc(__ballot_sync(0xffffffffu, nl == cc));
-        for (int o = 16; o; o >>= 1) {
-          g += __shfl_xor_sync(0xffffffffu, g, o);
-          h += __shfl_xor_sync(0xffffffffu, h, o);
-        }
-        if (lane == 0 && cnt) {
-          atomicAdd(&sG[cc], g);
-          atomicAdd(&sH[cc], h);
-          atomicAdd(&sC[cc], cnt);
-        }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (uint32_t base = r0; base < r1; base += blockDim.x * PART_UNROLL) {
+    uint8_t bb[PART_UNROLL];
+    uint16_t lf[PART_UNROLL];
+    float2 v[PART_UNROLL];
+#pragma unroll
+    for (int u = 0; u < PART_UNROLL; ++u) {
+      const uint32_t i = base + u * blockDim.x + threadIdx.x;
+      if (i < r1) {
+        bb[u] = col[i];
+        lf[u] = leaf[i];
+        v[u] = gh[i];
       }
-    } else if (ok) {
-      atomicAdd(&sG[nl], v.x);
-      atomicAdd(&sH[nl], v.y);
-      atomicAdd(&sC[nl], 1u);
+    }
+#pragma unroll
+    for (int u = 0; u < PART_UNROLL; ++u) {
+      const uint32_t i = base + u * blockDim.x + threadIdx.x;
+      int nl = -1;
+      float2 w = make_float2(0.f, 0.f);
+      if (i < r1) {
+        const uint32_t right = (bb[u] != (uint8_t)kNanBin && bb[u] > t) ? 1u : 0u;
+        nl = (int)(((uint32_t)lf[u] << 1) | right);
+        leaf[i] = (uint16_t)nl;
+        w = v[u];
+      }
+      if (nch <= 4) {
+        for (int cc = 0; cc < nch; ++cc) {
+          float g = nl == cc ? w.x : 0.0f, h = nl == cc ? w.y : 0.0f;
+          const uint32_t cnt = __popc(__ballot_sync(0xffffffffu, nl == cc));
+          for (int o = 16; o; o >>= 1) {
+            g += __shfl_xor_sync(0xffffffffu, g, o);
+            h += __shfl_xor_sync(0xffffffffu, h, o);
+          }
+          if (lane == 0 && cnt) {
+            atomicAdd(&sG[cc], g);
+            atomicAdd(&sH[cc], h);
+            atomicAdd(&sC[cc], cnt);
+          }
+        }
+      } else {
+        // the first lane of each child's group sums the group in lane order
+        const unsigned m = __match_any_sync(0xffffffffu, nl);
+        s_wv[warp][lane] = w;
+        __syncwarp();
+        if (nl >= 0 && lane == __ffs(m) - 1) {
+          float g = 0.0f, h = 0.0f;
+          for (unsigned mm = m; mm; mm &= mm - 1) {
+            const float2 x = s_wv[warp][__ffs(mm) - 1];
+            g += x.x;
+            h += x.y;
+          }
+          atomicAdd(&sG[nl], g);
+          atomicAdd(&sH[nl], h);
+          atomicAdd(&sC[nl], (uint32_t)__popc(m));
+        }
+        __syncwarp();
+      }
     }
   }
   __syncthreads();
@@ -1107,14 +1142,23 @@ __global__ void __launch_bounds__(PART_THREADS) k_scatter(DevCfg c, DevPtrs P, i
   const uint32_t r0 = blockIdx.x * rpb, r1 = min(c.n, r0 + rpb);
   const uint16_t* leaf = P.leaf + (size_t)k * c.n;
   uint32_t* rows = P.rows + (size_t)k * c.n;
-  for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-    const int ch = leaf[i];
-    const int p = ch >> 1;
-    if (ch == P.small[k * Pmax + p]) {
-      const uint32_t pos = P.seg_start[k * Pmax + p] + P.blk_off[((size_t)k * c.PB + blockIdx.x) * Pmax + p] +
-                           atomicAdd(&s_cur[p], 1u);
-      rows[pos] = i;
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  for (uint32_t base = r0; base < r1; base += blockDim.x) {
+    const uint32_t i = base + threadIdx.x;
+    int key = -1;  // pair of a smaller-child row, else -1
+    if (i < r1) {
+      const int ch = leaf[i];
+      if (ch == P.small[k * Pmax + (ch >> 1)]) key = ch >> 1;
     }
+    // one shared atomic per distinct pair of the warp; lanes keep their order
+    const unsigned m = __match_any_sync(0xffffffffu, key);
+    const int leader = __ffs(m) - 1;
+    uint32_t slot = 0;
+    if (key >= 0 && lane == leader) slot = atomicAdd(&s_cur[key], (uint32_t)__popc(m));
+    slot = __shfl_sync(0xffffffffu, slot, leader) + __popc(m & lt);
+    if (key >= 0)
+      rows[P.seg_start[k * Pmax + key] + P.blk_off[((size_t)k * c.PB + blockIdx.x) * Pmax + key] + slot] = i;
   }
 }
 
