@@ -35,6 +35,10 @@ struct tc_ctx {
   std::string err;
   std::mutex mu;                     // guards allocation accounting and err
   std::map<void*, size_t> allocs;
+  // tc_predict's device staging (grow-only, one caller at a time)
+  std::mutex pred_mu;
+  void* pred_scratch = nullptr;
+  size_t pred_scratch_bytes = 0;
 
   tc_status fail(tc_status code, const char* fmt, ...) {
     char buf[512];

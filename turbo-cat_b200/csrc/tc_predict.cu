@@ -25,8 +25,7 @@ namespace tc {
 namespace {
 
 constexpr int PRED_ROWS = 128;
-constexpr int PRED_TG = 4;                  // thread groups per row tile (trees split across them)
-constexpr int PRED_THREADS = PRED_ROWS * PRED_TG;
+constexpr int PRED_THREADS = 512;                 // a row tile: up to 128 rows x 4 tree groups
 constexpr int PRED_LEAF_FLOATS = 8192;      // shared floats for one chunk of leaves (32 KB)
 constexpr int PRED_MAX_K = 16;
 
@@ -66,6 +65,11 @@ __global__ void __launch_bounds__(PRED_THREADS) k_predict(JobTable jt) {
   const uint32_t r0 = tile * PRED_ROWS;
   if (r0 >= rq.n) return;
   const uint32_t nr = min((uint32_t)PRED_ROWS, rq.n - r0);
+  // row slots of this tile (a power of two >= nr); the block's other threads
+  // split the trees, so a small request still uses every thread
+  int RT = PRED_ROWS;
+  while (RT > 1 && (uint32_t)(RT >> 1) >= nr) RT >>= 1;
+  const int TG = PRED_THREADS / RT;
   const int f = md.n_features;
   const int fs = f + 1;
   const int D = md.max_depth;
@@ -84,8 +88,8 @@ __global__ void __launch_bounds__(PRED_THREADS) k_predict(JobTable jt) {
   float acc[PRED_MAX_K];
 #pragma unroll
   for (int k = 0; k < PRED_MAX_K; ++k) acc[k] = 0.0f;
-  const int row = threadIdx.x % PRED_ROWS;
-  const int tg = threadIdx.x / PRED_ROWS;
+  const int row = threadIdx.x % RT;
+  const int tg = threadIdx.x / RT;
   const float* xr = s_x + row * fs;
   for (int t0 = 0; t0 < md.n_trees; t0 += tchunk) {
     const int tn = min(tchunk, md.n_trees - t0);
@@ -97,7 +101,7 @@ __global__ void __launch_bounds__(PRED_THREADS) k_predict(JobTable jt) {
     if ((uint32_t)row < nr) {
       if (K == 1) {
         float s = 0.0f;
-        for (int t = tg; t < tn; t += PRED_TG) {
+        for (int t = tg; t < tn; t += TG) {
           const int dep = s_depth[t];
           const uint2* sp = s_split + t * D;
           uint32_t idx = 0;
@@ -109,7 +113,7 @@ __global__ void __launch_bounds__(PRED_THREADS) k_predict(JobTable jt) {
         }
         acc[0] += s;
       } else {
-        for (int t = tg; t < tn; t += PRED_TG) {
+        for (int t = tg; t < tn; t += TG) {
           const int dep = s_depth[t];
           const uint2* sp = s_split + t * D;
           uint32_t idx = 0;
@@ -126,22 +130,23 @@ __global__ void __launch_bounds__(PRED_THREADS) k_predict(JobTable jt) {
       }
     }
   }
-  // combine the thread groups' partial sums
+  // combine the thread groups' partial sums (pairwise, fixed order)
   __syncthreads();
-  float* s_red = s_leaf;  // [PRED_TG][PRED_ROWS][K] (fits: 4*128*16 floats = PRED_LEAF_FLOATS)
+  float* s_red = s_leaf;  // [TG][RT][K]: TG*RT = PRED_THREADS, 512*16 floats = PRED_LEAF_FLOATS
 #pragma unroll
   for (int k = 0; k < PRED_MAX_K; ++k)
-    if (k < K) s_red[(tg * PRED_ROWS + row) * K + k] = acc[k];
+    if (k < K) s_red[(tg * RT + row) * K + k] = acc[k];
   __syncthreads();
+  for (int h = TG >> 1; h > 0; h >>= 1) {
+    if (tg < h) {
+      for (int k = 0; k < K; ++k) s_red[(tg * RT + row) * K + k] += s_red[((tg + h) * RT + row) * K + k];
+    }
+    __syncthreads();
+  }
   if (tg != 0 || (uint32_t)row >= nr) return;
 #pragma unroll
-  for (int k = 0; k < PRED_MAX_K; ++k) {
-    if (k < K) {
-      float v = 0.0f;
-      for (int g = 0; g < PRED_TG; ++g) v += s_red[(g * PRED_ROWS + row) * K + k];
-      acc[k] = v;
-    }
-  }
+  for (int k = 0; k < PRED_MAX_K; ++k)
+    if (k < K) acc[k] = s_red[row * K + k];
   float* o = rq.out + (size_t)(r0 + row) * K;
   if (rq.transform == TC_TRANSFORM_SOFTMAX && K > 1) {
     float mx = -INFINITY;
@@ -501,13 +506,28 @@ tc_status tc_predict(tc_ctx* ctx, const tc_model* m, const float* X, uint32_t n,
   if (n == 0) return TC_OK;
   cudaSetDevice(ctx->device);
   const int K = m->info.n_classes;
-  DevBuf<float> dx, dout;
-  TC_TRY(dx.alloc(ctx, (size_t)n * f, "predict input"));
-  TC_TRY(dout.alloc(ctx, (size_t)n * K, "predict output"));
+  // input and output share one grow-only device buffer of the context, so a
+  // call allocates nothing once the largest batch has been seen
+  const size_t in_bytes = ((size_t)n * f * sizeof(float) + 255) / 256 * 256;
+  const size_t need = in_bytes + (size_t)n * K * sizeof(float);
+  std::lock_guard<std::mutex> g(ctx->pred_mu);
+  if (ctx->pred_scratch_bytes < need) {
+    if (ctx->pred_scratch) {
+      cudaStreamSynchronize(ctx->stream);
+      ctx->release(ctx->pred_scratch);
+      ctx->pred_scratch = nullptr;
+      ctx->pred_scratch_bytes = 0;
+    }
+    const size_t cap = std::max(need, (size_t)1 << 20);
+    TC_TRY(ctx->alloc(&ctx->pred_scratch, cap, "predict staging"));
+    ctx->pred_scratch_bytes = cap;
+  }
+  float* dx = static_cast<float*>(ctx->pred_scratch);
+  float* dout = reinterpret_cast<float*>(static_cast<char*>(ctx->pred_scratch) + in_bytes);
   cudaStream_t st = ctx->stream;
-  TC_CUDA(ctx, cudaMemcpyAsync(dx.p, X, (size_t)n * f * sizeof(float), cudaMemcpyHostToDevice, st));
-  TC_TRY(tc::predict_device(ctx, m, dx.p, n, f, transform, dout.p, st));
-  TC_CUDA(ctx, cudaMemcpyAsync(out, dout.p, (size_t)n * K * sizeof(float), cudaMemcpyDeviceToHost, st));
+  TC_CUDA(ctx, cudaMemcpyAsync(dx, X, (size_t)n * f * sizeof(float), cudaMemcpyHostToDevice, st));
+  TC_TRY(tc::predict_device(ctx, m, dx, n, f, transform, dout, st));
+  TC_CUDA(ctx, cudaMemcpyAsync(out, dout, (size_t)n * K * sizeof(float), cudaMemcpyDeviceToHost, st));
   TC_CUDA(ctx, cudaStreamSynchronize(st));
   return TC_OK;
 }
