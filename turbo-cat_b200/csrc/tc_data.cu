@@ -364,7 +364,7 @@ tc_status tc_dataset_upload(tc_ctx* ctx, const float* X, uint32_t n, uint16_t f,
   ds->ctx = ctx;
   ds->n = n;
   ds->f = f;
-  ds->fs = (uint32_t)tc::round_up(f, 16);
+  ds->fs = (uint32_t)tc::round_up(f, 32);
   ds->np = (uint32_t)tc::round_up(n > 0 ? n : 1, 16);
   tc_status s = ds->X.alloc(ctx, (size_t)n * f, "training matrix");
   if (s == TC_OK && y) s = ds->y.alloc(ctx, n, "labels");

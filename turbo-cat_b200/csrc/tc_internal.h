@@ -102,7 +102,8 @@ struct tc_dataset {
   tc_ctx* ctx = nullptr;
   uint32_t n = 0;
   uint32_t f = 0;
-  uint32_t fs = 0;           // row stride of the row-major bin matrix (f rounded up to 16)
+  uint32_t fs = 0;           // row stride of the row-major bin matrix (f rounded up to 32:
+                             // a 32-feature group of a row is one 32-byte sector)
   uint32_t np = 0;           // column stride of the column-major bin matrix (n rounded up to 16)
   bool quantized = false;
   int max_bins = 255;

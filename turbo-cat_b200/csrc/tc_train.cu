@@ -97,6 +97,7 @@ struct DevPtrs {
   const float* y;
   float* pred;                   // [K][n]
   float2* gh;                    // [K][n]
+  float2* cgh;                   // [K][n] (grad, hess) of the rows list, in its order
   uint16_t* leaf;                // [K][n]
   uint32_t* rows;                // [K][n]
   double2* hist[2];              // [K][2^(D-1)][F][256]
@@ -422,7 +423,9 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
     const int start = s0 + (int)((long long)sl * ch_idx / nch);
     const int end = s0 + (int)((long long)sl * (ch_idx + 1) / nch);
     const uint32_t* rows = P.rows + (size_t)k * c.n;
-    const float2* gh = P.gh + (size_t)k * c.n;
+    // (grad, hess) in list order: the root's rows are 0..n-1, a smaller
+    // child's were copied next to its row ids by the scatter kernel
+    const float2* gh = (d == 0 ? P.gh : P.cgh) + (size_t)k * c.n;
     const uint8_t* bsrc = P.bins_rm + g0;
     const int nb = (end - start + B - 1) / B;   // batches in the item; warp w takes w, w+nwarps, ...
     uint32_t rid_next = 0;
@@ -438,7 +441,7 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
         uint8_t* dst_ = w_bins + ((size_t)(st_) * B + lane) * W;                             \
         _Pragma("unroll") for (int u = 0; u < 2 * J; ++u)                                    \
           if (u < nchunk16) cp_async16(dst_ + 16 * u, src_ + 16 * u);                        \
-        cp_async8(w_gh + (st_) * B + lane, gh + rid_next);                                   \
+        cp_async8(w_gh + (st_) * B + lane, gh + start + (bi) * B + lane);                     \
       }                                                                                      \
       cp_async_commit();                                                                     \
     }
@@ -1129,7 +1132,9 @@ __global__ void __launch_bounds__(PLAN_THREADS) k_plan(DevCfg c, DevPtrs P, int 
   }
 }
 
-// grid (PB, K).  Row ids of the smaller children, grouped by pair.
+// grid (PB, K).  Row ids of the smaller children, grouped by pair, and their
+// (grad, hess) in the same order (the next level's histogram reads them
+// contiguously).
 __global__ void __launch_bounds__(PART_THREADS) k_scatter(DevCfg c, DevPtrs P, int d) {
   extern __shared__ uint32_t s_cur[];
   const int k = blockIdx.y;
@@ -1142,6 +1147,8 @@ __global__ void __launch_bounds__(PART_THREADS) k_scatter(DevCfg c, DevPtrs P, i
   const uint32_t r0 = blockIdx.x * rpb, r1 = min(c.n, r0 + rpb);
   const uint16_t* leaf = P.leaf + (size_t)k * c.n;
   uint32_t* rows = P.rows + (size_t)k * c.n;
+  const float2* gh = P.gh + (size_t)k * c.n;
+  float2* cgh = P.cgh + (size_t)k * c.n;
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
   for (uint32_t base = r0; base < r1; base += blockDim.x) {
@@ -1157,8 +1164,11 @@ __global__ void __launch_bounds__(PART_THREADS) k_scatter(DevCfg c, DevPtrs P, i
     uint32_t slot = 0;
     if (key >= 0 && lane == leader) slot = atomicAdd(&s_cur[key], (uint32_t)__popc(m));
     slot = __shfl_sync(0xffffffffu, slot, leader) + __popc(m & lt);
-    if (key >= 0)
-      rows[P.seg_start[k * Pmax + key] + P.blk_off[((size_t)k * c.PB + blockIdx.x) * Pmax + key] + slot] = i;
+    if (key >= 0) {
+      const uint32_t pos = P.seg_start[k * Pmax + key] + P.blk_off[((size_t)k * c.PB + blockIdx.x) * Pmax + key] + slot;
+      rows[pos] = i;
+      cgh[pos] = gh[i];
+    }
   }
 }
 
@@ -1200,7 +1210,7 @@ struct tc_trainer {
   cudaGraphExec_t graph = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   DevBuf<float> pred;
-  DevBuf<float2> gh;
+  DevBuf<float2> gh, cgh;
   DevBuf<uint16_t> leaf;
   DevBuf<uint32_t> rows;
   DevBuf<double2> hist0, hist1;
@@ -1284,6 +1294,7 @@ tc_status tc_trainer::setup(int) {
   T_cap = prm.n_estimators * K;
   TC_TRY(pred.alloc(ctx, (size_t)K * n, "predictions"));
   TC_TRY(gh.alloc(ctx, (size_t)K * n, "gradients"));
+  TC_TRY(cgh.alloc(ctx, (size_t)K * n, "gradients of the row lists"));
   TC_TRY(leaf.alloc(ctx, (size_t)K * n, "leaf ids"));
   TC_TRY(rows.alloc(ctx, (size_t)K * n, "row lists"));
   const size_t hsz = (size_t)K * Pmax * f * kSlots;
@@ -1315,7 +1326,7 @@ tc_status tc_trainer::setup(int) {
 
   ptr.bins_rm = ds->bins_rm.p; ptr.bins_cm = ds->bins_cm.p; ptr.edges = ds->edges.p; ptr.n_edges = ds->n_edges.p;
   ptr.nan_any = ds->nan_any.p;
-  ptr.y = ds->y.p; ptr.pred = pred.p; ptr.gh = gh.p; ptr.leaf = leaf.p; ptr.rows = rows.p;
+  ptr.y = ds->y.p; ptr.pred = pred.p; ptr.gh = gh.p; ptr.cgh = cgh.p; ptr.leaf = leaf.p; ptr.rows = rows.p;
   ptr.hist[0] = hist0.p; ptr.hist[1] = hist1.p; ptr.rchunk = rchunk.p;
   ptr.seg_start = seg_start.p; ptr.seg_len = seg_len.p; ptr.small = small.p; ptr.nstat = nstat.p;
   ptr.pcnt = pcnt.p; ptr.psum = psum.p; ptr.blk_off = blk_off.p; ptr.gpart = gpart.p; ptr.gany = gany.p;
@@ -1538,7 +1549,7 @@ static DevPtrs class_view(const DevCfg& c, const DevPtrs& P, int k, DevCfg* one)
   *one = c;
   one->K = 1;
   one->k0 = k;
-  pk.pred += k * n; pk.gh += k * n; pk.leaf += k * n; pk.rows += k * n;
+  pk.pred += k * n; pk.gh += k * n; pk.cgh += k * n; pk.leaf += k * n; pk.rows += k * n;
   pk.hist[0] += (size_t)k * Pmax * c.f * kSlots;
   pk.hist[1] += (size_t)k * Pmax * c.f * kSlots;
   pk.seg_start += k * Pmax; pk.seg_len += k * Pmax;
