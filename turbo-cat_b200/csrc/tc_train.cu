@@ -1085,23 +1085,49 @@ __global__ void __launch_bounds__(PLAN_THREADS) k_plan(DevCfg c, DevPtrs P, int 
     }
     __syncthreads();
   }
-  // rows per chunk for this level: about two items per histogram block
+  // Rows per chunk for this level: the smallest R (from the even split up)
+  // for which the level has at most target_items items.  Every group counts,
+  // the narrow last one too: measured, items that all run in one wave beat
+  // a second wave of cheap narrow items after the wide ones.
   __shared__ int s_R;
+  __shared__ long long s_cnt;
+  const int np2 = pairs_at(d);
+  const int nsg = c.K * np2;
+  const int gw = c.G;
   if (tid == 0) {
     int R = c.rows_fixed;
-    if (R <= 0) {
-      const long long target = c.target_items;
-      R = (int)max((long long)c.rows_min, (s_rows * c.G + target - 1) / target);
-    }
+    if (R <= 0) R = (int)max((long long)c.rows_min, (s_rows * gw + c.target_items - 1) / c.target_items);
     s_R = R;
-    *P.rchunk = R;
+  }
+  __syncthreads();
+  for (int round = 0; c.rows_fixed <= 0 && round < 16; ++round) {
+    const int Rt = s_R;
+    if (tid == 0) s_cnt = 0;
+    __syncthreads();
+    long long mine = 0;
+    for (int sgi = tid; sgi < nsg; sgi += blockDim.x) {
+      const int k = sgi / np2, p = sgi % np2;
+      if (!P.cs[k].done) {
+        const int len = d == 0 ? (int)c.n : P.seg_len[k * Pmax + p];
+        mine += (len + Rt - 1) / Rt;
+      }
+    }
+    for (int o = 16; o; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
+    if (lane == 0 && mine) atomicAdd(reinterpret_cast<unsigned long long*>(&s_cnt), (unsigned long long)mine);
+    __syncthreads();
+    const long long items = s_cnt * gw;
+    __syncthreads();
+    if (items <= c.target_items) break;
+    if (tid == 0) s_R = (int)min((long long)INT32_MAX / 2, (long long)Rt * items / c.target_items + 1);
+    __syncthreads();
+  }
+  if (tid == 0) {
+    *P.rchunk = s_R;
     s_carry = 0;
   }
   __syncthreads();
   const int R = s_R;
   // cumulative item counts over segments (class, pair): chunks x groups
-  const int np2 = pairs_at(d);
-  const int nsg = c.K * np2;
   for (int base = 0; base < nsg; base += blockDim.x) {
     const int sgi = base + tid;
     int chunks = 0;
