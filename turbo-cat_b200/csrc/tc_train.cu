@@ -346,8 +346,8 @@ __device__ __forceinline__ void red_add_u32(uint32_t a, uint32_t v) {
 // different columns (banks).  A group of at most 16 features is packed: with
 // p2 = next power of two >= its width, the 32 columns hold 32/p2 private
 // copies and one warp instruction updates 32/p2 rows; the copies are summed
-// when the partial is written.  Columns past a group's width collect the
-// padding bytes of the row and are never read.  Each lane keeps the shared
+// when the partial is written.  Columns past a group's width (padding bytes,
+// all bin 0: one hot address) are not updated.  Each lane keeps the shared
 // address of (its warp's copy of) every column it updates, so an update is a
 // byte permute, an add and the atomics.
 //
@@ -406,8 +406,11 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
     const int p2 = gsize <= 1 ? 1 : (gsize <= 2 ? 2 : (gsize <= 4 ? 4 : (gsize <= 8 ? 8 : (gsize <= 16 ? 16 : 32))));
     const bool narrow = p2 <= 16;
     const int nchunk16 = (gsize + 15) >> 4;  // 16-byte pieces of the slice that hold features
-    // shared address of this warp's copy of each column the lane updates
+    // shared address of this warp's copy of each column the lane updates;
+    // columns past the group's width are skipped (their padding bytes are
+    // all bin 0, a single hot address)
     uint32_t ab[J][4];
+    uint32_t live = 0;
 #pragma unroll
     for (int j = 0; j < J; ++j)
 #pragma unroll
@@ -415,6 +418,7 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
         const int col = 32 * j + 4 * c4 + ((s + qr) & 3);
         const HistCol hc = hist_col(P, g0 + col, (int)c.f);
         ab[j][s] = hbase + BIN_BYTES * (uint32_t)((warp % hc.copies) * hc.span) + 4u * col;
+        if (col < gsize) live |= 1u << (4 * j + s);
       }
     // the segment's ceil(len / R) chunks have equal sizes (within one row)
     const int s0 = d == 0 ? 0 : P.seg_start[k * Pmax + p];
@@ -483,9 +487,11 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
                 for (int s = 0; s < 4; ++s) {
                   // __byte_perm gives bin * 256; a slot is BIN_BYTES = 256 * J bytes
                   const uint32_t a = ab[j][s] + __byte_perm(wd[qd][j], 0u, sel[s]) * J;
-                  red_add_f32(a, vx[qd]);
-                  if (CNT) red_add_u32(a + 4 * W, 1u);
-                  else red_add_f32(a + 4 * W, vy[qd]);
+                  if (live & (1u << (4 * j + s))) {
+                    red_add_f32(a, vx[qd]);
+                    if (CNT) red_add_u32(a + 4 * W, 1u);
+                    else red_add_f32(a + 4 * W, vy[qd]);
+                  }
                 }
               }
             }
@@ -511,7 +517,7 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
           }
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
-            if (i0 + u * rpi + my_row < nvalid) {
+            if (i0 + u * rpi + my_row < nvalid && my_col < gsize) {
               const uint32_t a = abn + BIN_BYTES * bb[u];
               red_add_f32(a, gx[u]);
               if (CNT) red_add_u32(a + 4 * W, 1u);
