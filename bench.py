@@ -403,6 +403,36 @@ def suite_c4(eng, _capi, seconds=3.0, rate=20_000.0, ref_ok=False):
         lat[str(rows)] = {"p50_us": _pct(ts, 50) * 1e6, "p99_us": _pct(ts, 99) * 1e6,
                           "rows_per_s": rows / _pct(ts, 50)}
     res["fixed_batch_1000xd6"] = lat
+    # device-resident throughput of every model (kernel only, CUDA events on the launching stream)
+    n_dev = 1 << 20
+    Xd = torch.randn((n_dev, f), dtype=torch.float32, device="cuda")
+    od = torch.empty((n_dev, 1), dtype=torch.float32, device="cuda")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.Stream()  # a real stream handle (0 would select the engine's own stream)
+    torch.cuda.synchronize()
+    dev_tp = {}
+    for m in models:
+        info = m.info
+        exp = m.export()
+        compares = float(np.sum(exp["depth"])) * n_dev
+        for _ in range(3):
+            m.predict_device(Xd.data_ptr(), n_dev, f, od.data_ptr(), "sigmoid", stream.cuda_stream)
+        ts = []
+        for _ in range(10):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            m.predict_device(Xd.data_ptr(), n_dev, f, od.data_ptr(), "sigmoid", stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1) * 1e-3)
+        t = float(np.median(ts))
+        dev_tp[f"{info.n_trees}xd{info.max_depth}"] = {
+            "rows": n_dev, "ms": t * 1e3, "rows_per_s": n_dev / t, "gcompare_per_s": compares / t / 1e9,
+            "input_gbs": n_dev * f * 4 / t / 1e9}
+    res["device_predict_1M_rows"] = dev_tp
+    del Xd, od, flush
     if ref_ok:
         sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
         import tempfile

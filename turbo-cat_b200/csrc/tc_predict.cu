@@ -42,6 +42,37 @@ struct JobTable {
 
 __device__ __forceinline__ float sigmoidf_ref(float x) { return 1.0f / (1.0f + expf(-x)); }
 
+// NT full-depth trees of depth DD walked together: every split is loaded
+// first, then every feature value, then the compares, so the shared-memory
+// loads of the NT trees are in flight together instead of one dependent
+// chain per level.
+template <int NT, int DD>
+__device__ __forceinline__ void walk_full(const uint2* __restrict__ s_split, const float* __restrict__ xr,
+                                          const float* __restrict__ lv, int t, int TG, float4& sum) {
+  constexpr int L = 1 << DD;
+  uint2 q[NT][DD];
+#pragma unroll
+  for (int u = 0; u < NT; ++u)
+#pragma unroll
+    for (int d = 0; d < DD; ++d) q[u][d] = s_split[(t + u * TG) * DD + d];
+  float xv[NT][DD];
+#pragma unroll
+  for (int u = 0; u < NT; ++u)
+#pragma unroll
+    for (int d = 0; d < DD; ++d) xv[u][d] = xr[q[u][d].x];
+#pragma unroll
+  for (int u = 0; u < NT; ++u) {
+    uint32_t idx = 0;
+#pragma unroll
+    for (int d = 0; d < DD; ++d) idx = (idx << 1) | (uint32_t)(xv[u][d] >= __uint_as_float(q[u][d].y));
+    const float v = lv[(t + u * TG) * L + idx];
+    if (u == 0) sum.x += v;
+    else if (u == 1) sum.y += v;
+    else if (u == 2) sum.z += v;
+    else sum.w += v;
+  }
+}
+
 __global__ void __launch_bounds__(PRED_THREADS) k_predict(JobTable jt) {
   extern __shared__ float smp[];
   ReqDesc rq;
@@ -74,16 +105,19 @@ __global__ void __launch_bounds__(PRED_THREADS) k_predict(JobTable jt) {
   const int fs = f + 1;
   const int D = md.max_depth;
   const int L = 1 << D;
-  const int tchunk = max(1, min(256, PRED_LEAF_FLOATS / L));
+  // leaves of shallow trees are staged in shared memory with the splits;
+  // deep trees (more than 256 leaves) gather their leaf from global memory
+  // (L2), so a chunk still holds 256 trees' splits
+  const bool leaves_global = L > 256;
+  const int tchunk = leaves_global ? 256 : max(1, min(256, PRED_LEAF_FLOATS / L));
   float* s_x = smp;                                  // [PRED_ROWS][f+1]
   float* s_leaf = s_x + PRED_ROWS * (jt.max_f + 1);  // [tchunk][L]
   uint2* s_split = reinterpret_cast<uint2*>(s_leaf + PRED_LEAF_FLOATS);  // [tchunk][D]
   int* s_depth = reinterpret_cast<int*>(s_split + 256 * max(1, jt.max_depth));
   const float* Xt = rq.X + (size_t)r0 * f;
-  for (uint32_t q = threadIdx.x; q < nr * (uint32_t)f; q += blockDim.x) {
-    const uint32_t i = q / f, j = q % f;
-    s_x[i * fs + j] = Xt[q];
-  }
+  // a warp copies whole rows (lane = feature), no division by f
+  for (uint32_t i = threadIdx.x >> 5; i < nr; i += blockDim.x >> 5)
+    for (int j = threadIdx.x & 31; j < f; j += 32) s_x[i * fs + j] = Xt[(size_t)i * f + j];
   const int K = md.n_classes;
   float acc[PRED_MAX_K];
 #pragma unroll
@@ -94,14 +128,39 @@ __global__ void __launch_bounds__(PRED_THREADS) k_predict(JobTable jt) {
   for (int t0 = 0; t0 < md.n_trees; t0 += tchunk) {
     const int tn = min(tchunk, md.n_trees - t0);
     __syncthreads();
-    for (int q = threadIdx.x; q < tn * L; q += blockDim.x) s_leaf[q] = md.leaves[(size_t)t0 * L + q];
+    if (!leaves_global)
+      for (int q = threadIdx.x; q < tn * L; q += blockDim.x) s_leaf[q] = md.leaves[(size_t)t0 * L + q];
+    const float* lv = leaves_global ? md.leaves + (size_t)t0 * L : s_leaf;
     for (int q = threadIdx.x; q < tn * D; q += blockDim.x) s_split[q] = md.splits[(size_t)t0 * D + q];
     for (int q = threadIdx.x; q < tn; q += blockDim.x) s_depth[q] = md.depth[t0 + q];
     __syncthreads();
     if ((uint32_t)row < nr) {
       if (K == 1) {
-        float s = 0.0f;
-        for (int t = tg; t < tn; t += TG) {
+        // full-depth trees in groups (depth <= 8: 4 at a time, 9-10: 2),
+        // partial sums combined in a fixed order; other trees one by one
+        float4 s4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        int t = tg;
+        const int NT = D <= 8 ? 4 : 2;
+        if (D <= 10) {
+          for (; t + (NT - 1) * TG < tn; t += NT * TG) {
+            bool full = true;
+            for (int u = 0; u < NT; ++u) full = full && s_depth[t + u * TG] == D;
+            if (!full) break;
+            switch (D) {
+              case 1: walk_full<4, 1>(s_split, xr, lv, t, TG, s4); break;
+              case 2: walk_full<4, 2>(s_split, xr, lv, t, TG, s4); break;
+              case 3: walk_full<4, 3>(s_split, xr, lv, t, TG, s4); break;
+              case 4: walk_full<4, 4>(s_split, xr, lv, t, TG, s4); break;
+              case 5: walk_full<4, 5>(s_split, xr, lv, t, TG, s4); break;
+              case 6: walk_full<4, 6>(s_split, xr, lv, t, TG, s4); break;
+              case 7: walk_full<4, 7>(s_split, xr, lv, t, TG, s4); break;
+              case 8: walk_full<4, 8>(s_split, xr, lv, t, TG, s4); break;
+              case 9: walk_full<2, 9>(s_split, xr, lv, t, TG, s4); break;
+              default: walk_full<2, 10>(s_split, xr, lv, t, TG, s4); break;
+            }
+          }
+        }
+        for (; t < tn; t += TG) {
           const int dep = s_depth[t];
           const uint2* sp = s_split + t * D;
           uint32_t idx = 0;
@@ -109,9 +168,9 @@ __global__ void __launch_bounds__(PRED_THREADS) k_predict(JobTable jt) {
             const uint2 q = sp[d];
             idx = (idx << 1) | (uint32_t)(xr[q.x] >= __uint_as_float(q.y));  // false for NaN
           }
-          s += s_leaf[t * L + idx];
+          s4.x += lv[t * L + idx];
         }
-        acc[0] += s;
+        acc[0] += (s4.x + s4.y) + (s4.z + s4.w);
       } else {
         for (int t = tg; t < tn; t += TG) {
           const int dep = s_depth[t];
@@ -122,7 +181,7 @@ __global__ void __launch_bounds__(PRED_THREADS) k_predict(JobTable jt) {
             idx = (idx << 1) | (uint32_t)(xr[q.x] >= __uint_as_float(q.y));
           }
           const int cls = (t0 + t) % K;
-          const float v = s_leaf[t * L + idx];
+          const float v = lv[t * L + idx];
 #pragma unroll
           for (int k = 0; k < PRED_MAX_K; ++k)
             if (k == cls) acc[k] += v;

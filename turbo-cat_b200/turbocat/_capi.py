@@ -147,6 +147,14 @@ class Model:
                                        C.c_int32(TRANSFORM[transform]), _p(out)))
         return out
 
+    def predict_device(self, x_ptr, n, f, out_ptr, transform="raw", stream=0):
+        """tc_predict_device: inputs and outputs already in device memory
+        (raw pointers), launched on `stream` (0: the engine's stream); no
+        synchronisation."""
+        self.eng._chk(lib().tc_predict_device(self.eng.ctx, self.h, C.c_void_p(x_ptr), C.c_uint32(n),
+                                              C.c_uint16(f), C.c_int32(TRANSFORM[transform]),
+                                              C.c_void_p(out_ptr), C.c_void_p(stream)))
+
     def close(self):
         if self.h:
             lib().tc_model_destroy(self.h)
