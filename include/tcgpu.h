@@ -18,6 +18,14 @@
  *   trees      T trees, iteration-major and class-minor for multiclass;
  *              per tree: depth, (feature, bin, float threshold, gain) per
  *              level padded to max_depth, 2^max_depth leaf values (padded)
+ *
+ * Threads: dataset and training calls (tc_dataset_*, tc_quantize, tc_train,
+ * tc_build_tree, tc_trainer_*) on one context run one at a time; tc_predict
+ * calls on one context run one at a time, on a stream of their own, so they
+ * may run while another thread trains; tc_server_submit/poll may be called
+ * from any thread.  The reference
+ * is not thread-safe at all (thread_local pools and mutable caches,
+ * src/tree/symmetric_tree.cpp:57-89).
  */
 #ifndef TCGPU_H
 #define TCGPU_H
@@ -240,7 +248,8 @@ void tc_model_destroy(tc_model* m);
 tc_status tc_predict(tc_ctx* ctx, const tc_model* m, const float* X, uint32_t n, uint16_t f,
                      int32_t transform, float* out);
 /* Same on device buffers, queued on `stream` (a cudaStream_t, NULL = the
- * context's stream); returns without synchronising. */
+ * context's prediction stream, not the one training runs on); returns
+ * without synchronising. */
 tc_status tc_predict_device(tc_ctx* ctx, const tc_model* m, const float* X_dev, uint32_t n,
                             uint16_t f, int32_t transform, float* out_dev, void* stream);
 

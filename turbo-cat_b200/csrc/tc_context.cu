@@ -70,6 +70,11 @@ tc_status tc_ctx_create(int device, size_t mem_budget, tc_ctx** out) {
     delete c;
     return TC_ERR_CUDA;
   }
+  if (cudaStreamCreateWithFlags(&c->pred_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return TC_ERR_CUDA;
+  }
   *out = c;
   return TC_OK;
 }
@@ -78,9 +83,11 @@ void tc_ctx_destroy(tc_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  cudaStreamSynchronize(ctx->pred_stream);
   for (auto& kv : ctx->allocs) cudaFree(kv.first);
   ctx->allocs.clear();
   cudaStreamDestroy(ctx->stream);
+  cudaStreamDestroy(ctx->pred_stream);
   delete ctx;
 }
 

@@ -358,6 +358,7 @@ extern "C" {
 tc_status tc_dataset_upload(tc_ctx* ctx, const float* X, uint32_t n, uint16_t f, const float* y,
                             tc_dataset** out) {
   if (!ctx || !out || (!X && n > 0) || f == 0) return TC_ERR_INVALID_ARG;
+  std::lock_guard<std::recursive_mutex> train_lock(ctx->train_mu);
   *out = nullptr;
   cudaSetDevice(ctx->device);
   tc_dataset* ds = new tc_dataset();
@@ -385,12 +386,21 @@ tc_status tc_dataset_upload(tc_ctx* ctx, const float* X, uint32_t n, uint16_t f,
   return TC_OK;
 }
 
-void tc_dataset_destroy(tc_dataset* ds) { delete ds; }
+void tc_dataset_destroy(tc_dataset* ds) {
+  if (!ds) return;
+  if (!ds->ctx) {
+    delete ds;
+    return;
+  }
+  std::lock_guard<std::recursive_mutex> train_lock(ds->ctx->train_mu);
+  delete ds;
+}
 
 tc_status tc_quantize(tc_dataset* ds, uint16_t max_bins, int compat_uint8_count, float* edges_out,
                       uint16_t* n_edges_out) {
   if (!ds) return TC_ERR_INVALID_ARG;
   tc_ctx* ctx = ds->ctx;
+  std::lock_guard<std::recursive_mutex> train_lock(ctx->train_mu);
   if (max_bins < 2 || max_bins > 255)
     return ctx->fail(TC_ERR_INVALID_ARG, "max_bins must be in [2, 255] (uint8 bins; got %u)", max_bins);
   cudaSetDevice(ctx->device);
@@ -403,6 +413,7 @@ tc_status tc_quantize(tc_dataset* ds, uint16_t max_bins, int compat_uint8_count,
 tc_status tc_dataset_bins(const tc_dataset* ds, uint8_t* bins_out) {
   if (!ds || !bins_out) return TC_ERR_INVALID_ARG;
   tc_ctx* ctx = ds->ctx;
+  std::lock_guard<std::recursive_mutex> train_lock(ctx->train_mu);
   if (!ds->quantized) return ctx->fail(TC_ERR_NOT_FITTED, "dataset not quantized");
   cudaSetDevice(ctx->device);
   TC_CUDA(ctx, cudaMemcpy2DAsync(bins_out, ds->n, ds->bins_cm.p, ds->np, ds->n, ds->f,

@@ -31,10 +31,14 @@ struct tc_ctx {
   size_t in_use = 0;
   size_t peak = 0;
   int fail_next = 0;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;       // training, binning, uploads
+  cudaStream_t pred_stream = nullptr;  // tc_predict / tc_predict_device (NULL stream)
   std::string err;
   std::mutex mu;                     // guards allocation accounting and err
   std::map<void*, size_t> allocs;
+  // training calls (tc_train, tc_build_tree, tc_trainer_*) on one context
+  // run one at a time: they share the context's stream and tuner state
+  std::recursive_mutex train_mu;
   // tc_predict's device staging (grow-only, one caller at a time)
   std::mutex pred_mu;
   void* pred_scratch = nullptr;

@@ -572,7 +572,7 @@ tc_status tc_predict(tc_ctx* ctx, const tc_model* m, const float* X, uint32_t n,
   std::lock_guard<std::mutex> g(ctx->pred_mu);
   if (ctx->pred_scratch_bytes < need) {
     if (ctx->pred_scratch) {
-      cudaStreamSynchronize(ctx->stream);
+      cudaStreamSynchronize(ctx->pred_stream);
       ctx->release(ctx->pred_scratch);
       ctx->pred_scratch = nullptr;
       ctx->pred_scratch_bytes = 0;
@@ -583,7 +583,7 @@ tc_status tc_predict(tc_ctx* ctx, const tc_model* m, const float* X, uint32_t n,
   }
   float* dx = static_cast<float*>(ctx->pred_scratch);
   float* dout = reinterpret_cast<float*>(static_cast<char*>(ctx->pred_scratch) + in_bytes);
-  cudaStream_t st = ctx->stream;
+  cudaStream_t st = ctx->pred_stream;  // not the training stream, which another thread may be capturing
   TC_CUDA(ctx, cudaMemcpyAsync(dx, X, (size_t)n * f * sizeof(float), cudaMemcpyHostToDevice, st));
   TC_TRY(tc::predict_device(ctx, m, dx, n, f, transform, dout, st));
   TC_CUDA(ctx, cudaMemcpyAsync(out, dout, (size_t)n * K * sizeof(float), cudaMemcpyDeviceToHost, st));
@@ -597,7 +597,7 @@ tc_status tc_predict_device(tc_ctx* ctx, const tc_model* m, const float* X_dev, 
   if (f != (uint32_t)m->info.n_features)
     return ctx->fail(TC_ERR_INVALID_ARG, "X has %u features, the model expects %d", f, m->info.n_features);
   cudaSetDevice(ctx->device);
-  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->pred_stream;
   return tc::predict_device(ctx, m, X_dev, n, f, transform, out_dev, st);
 }
 

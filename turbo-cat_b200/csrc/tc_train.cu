@@ -1728,6 +1728,7 @@ extern "C" {
 
 tc_status tc_trainer_create(tc_ctx* ctx, tc_dataset* ds, const tc_train_params* p, tc_trainer** out) {
   if (!ctx || !ds || !p || !out) return TC_ERR_INVALID_ARG;
+  std::lock_guard<std::recursive_mutex> train_lock(ctx->train_mu);
   *out = nullptr;
   cudaSetDevice(ctx->device);
   TC_TRY(validate(ctx, ds, p));
@@ -1749,12 +1750,14 @@ tc_status tc_trainer_create(tc_ctx* ctx, tc_dataset* ds, const tc_train_params* 
 
 tc_status tc_trainer_step(tc_trainer* tr, int32_t iterations, int sync) {
   if (!tr) return TC_ERR_INVALID_ARG;
+  std::lock_guard<std::recursive_mutex> train_lock(tr->ctx->train_mu);
   cudaSetDevice(tr->ctx->device);
   return tr->step(iterations, sync != 0);
 }
 
 tc_status tc_trainer_reset(tc_trainer* tr) {
   if (!tr) return TC_ERR_INVALID_ARG;
+  std::lock_guard<std::recursive_mutex> train_lock(tr->ctx->train_mu);
   cudaSetDevice(tr->ctx->device);
   return tr->init_predictions();
 }
@@ -1773,6 +1776,7 @@ tc_status tc_trainer_stats(tc_trainer* tr, tc_train_stats* st) {
 
 tc_status tc_trainer_profile(tc_trainer* tr, int32_t iterations, tc_profile* out) {
   if (!tr || !out || iterations < 0) return TC_ERR_INVALID_ARG;
+  std::lock_guard<std::recursive_mutex> train_lock(tr->ctx->train_mu);
   tc_ctx* ctx = tr->ctx;
   cudaSetDevice(ctx->device);
   if (tr->iters_done + iterations > tr->prm.n_estimators)
@@ -1817,6 +1821,7 @@ tc_status tc_trainer_profile(tc_trainer* tr, int32_t iterations, tc_profile* out
 tc_status tc_trainer_train_scores(tc_trainer* tr, float* out) {
   if (!tr || !out) return TC_ERR_INVALID_ARG;
   tc_ctx* ctx = tr->ctx;
+  std::lock_guard<std::recursive_mutex> train_lock(ctx->train_mu);
   cudaSetDevice(ctx->device);
   cudaStream_t st = ctx->stream;
   // apply the last tree to a scratch copy so that training can continue
@@ -1843,6 +1848,7 @@ tc_status tc_trainer_train_scores(tc_trainer* tr, float* out) {
 tc_status tc_trainer_model(tc_trainer* tr, tc_model** out) {
   if (!tr || !out) return TC_ERR_INVALID_ARG;
   tc_ctx* ctx = tr->ctx;
+  std::lock_guard<std::recursive_mutex> train_lock(ctx->train_mu);
   cudaSetDevice(ctx->device);
   cudaStream_t st = ctx->stream;
   const int K = tr->cfg.K, D = tr->cfg.D, L = 1 << D;
@@ -1904,6 +1910,7 @@ void tc_trainer_destroy(tc_trainer* tr) {
 
 tc_status tc_train(tc_ctx* ctx, tc_dataset* ds, const tc_train_params* p, tc_model** out, tc_train_stats* st) {
   if (!ctx || !ds || !p || !out) return TC_ERR_INVALID_ARG;
+  std::lock_guard<std::recursive_mutex> train_lock(ctx->train_mu);
   tc_trainer* tr = nullptr;
   TC_TRY(tc_trainer_create(ctx, ds, p, &tr));
   tc_status s = tr->step(p->n_estimators, true);
@@ -1919,6 +1926,7 @@ tc_status tc_build_tree(tc_ctx* ctx, tc_dataset* ds, const float* grad, const fl
                         double* runner_up_gain, float* leaf_values, uint32_t* leaf_index,
                         double* root_hist) {
   if (!ctx || !ds || !grad || !hess || !p || !depth_out) return TC_ERR_INVALID_ARG;
+  std::lock_guard<std::recursive_mutex> train_lock(ctx->train_mu);
   cudaSetDevice(ctx->device);
   tc_train_params q = *p;
   q.loss = TC_LOSS_MSE;  // labels unused: gradients are given
