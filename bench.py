@@ -273,13 +273,13 @@ def run_ours(args):
         dt = time.perf_counter() - t0
         if i > 0:
             e2e_s.append(dt)
-    e2e_fit = dist_max(float(np.mean(e2e_s)), ws, dev)
+    e2e_fit = dist_max(float(np.median(e2e_s)), ws, dev)  # median: one fit can catch host noise
     steps_per_fit = TREES / TREES_PER_STEP
     model_bytes = TREES * (DEPTH * 11 + (1 << DEPTH) * 4 + 8)
     e2e = {"value": e2e_fit / steps_per_fit / ws, "unit": UNIT,
            "h2d_bytes_per_step": int((X.nbytes + y.nbytes) / steps_per_fit),
            "d2h_bytes_per_step": int(model_bytes / steps_per_fit),
-           "fit_seconds": e2e_fit, "fits_timed": args.e2e_fits,
+           "fit_seconds": e2e_fit, "fits_timed": args.e2e_fits, "fit_seconds_each": e2e_s,
            "path": "turbocat.TurboCatRegressor.fit (pybind -> C ABI): upload, device binning, 500 trees, model"}
 
     cpu = None
@@ -457,27 +457,33 @@ def suite_c4(eng, _capi, seconds=3.0, rate=20_000.0, ref_ok=False):
                              "rows_per_s": rows / _pct(ts, 50)}
         res["reference_cpu_fixed_batch_1000xd6"] = rl
         res["reference_cores"] = os.cpu_count()
-    # open-loop Poisson stream
-    n_req = int(seconds * rate)
-    arr = np.cumsum(rng.exponential(1.0 / rate, n_req))
-    sizes = np.minimum(65536, np.floor(np.exp(rng.uniform(0, np.log(65537), n_req)))).astype(np.int64)
-    mids = rng.integers(0, 4, n_req)
-    offs = rng.integers(0, 65536, n_req)
+    # open-loop Poisson streams: the configuration's rate (its mean request,
+    # ~5.9k rows x 400 B, asks ~47 GB/s of host-to-device copies, about what
+    # the PCIe link carries, so queues build up), and half of it
     n_out = 2048
     outs = [torch.empty((65536, 1), dtype=torch.float32, pin_memory=True).numpy() for _ in range(n_out)]
-    for mode in ("coalesced", "plain"):
-        srv = _capi.Server(eng, staging_bytes=0, max_batch_rows=262144, coalesce=(mode == "coalesced"),
-                           max_inflight=4)
-        ids = [srv.add_model(m) for m in models]
-        reqs = [(float(arr[i]), ids[mids[i]], pool[offs[i]:offs[i] + sizes[i]], outs[i % n_out][:sizes[i]],
-                 "sigmoid") for i in range(n_req)]
-        lat_s, wall = srv.replay(reqs)
-        done, launches, rows = srv.stats()
-        res[mode] = {"p50_ms": _pct(lat_s, 50) * 1e3, "p99_ms": _pct(lat_s, 99) * 1e3,
-                     "rows_per_s": float(rows) / wall, "requests": int(done), "launches": int(launches),
-                     "wall_s": wall}
-        srv.close()
+    for r in (rate, rate / 2):
+        n_req = int(seconds * r)
+        arr = np.cumsum(rng.exponential(1.0 / r, n_req))
+        sizes = np.minimum(65536, np.floor(np.exp(rng.uniform(0, np.log(65537), n_req)))).astype(np.int64)
+        mids = rng.integers(0, 4, n_req)
+        offs = rng.integers(0, 65536, n_req)
+        tag = "" if r == rate else f"_at_{int(r)}_per_s"
+        for mode in ("coalesced", "plain"):
+            srv = _capi.Server(eng, staging_bytes=0, max_batch_rows=262144, coalesce=(mode == "coalesced"),
+                               max_inflight=4)
+            ids = [srv.add_model(m) for m in models]
+            reqs = [(float(arr[i]), ids[mids[i]], pool[offs[i]:offs[i] + sizes[i]], outs[i % n_out][:sizes[i]],
+                     "sigmoid") for i in range(n_req)]
+            lat_s, wall = srv.replay(reqs)
+            done, launches, rows = srv.stats()
+            res[mode + tag] = {"p50_ms": _pct(lat_s, 50) * 1e3, "p99_ms": _pct(lat_s, 99) * 1e3,
+                               "rows_per_s": float(rows) / wall, "h2d_gbs": float(rows) * f * 4 / wall / 1e9,
+                               "requests": int(done), "launches": int(launches), "wall_s": wall}
+            srv.close()
     res["p99_improvement_vs_plain"] = res["plain"]["p99_ms"] / res["coalesced"]["p99_ms"]
+    half = f"_at_{int(rate / 2)}_per_s"
+    res["p99_improvement_vs_plain" + half] = res["plain" + half]["p99_ms"] / res["coalesced" + half]["p99_ms"]
     return res
 
 
@@ -539,7 +545,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--e2e-fits", type=int, default=2)
+    ap.add_argument("--e2e-fits", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--suite", default="", help="secondary configurations, e.g. c1,c3,c4,c5")
     args = ap.parse_args()

@@ -156,7 +156,7 @@ class Model:
                                               C.c_void_p(out_ptr), C.c_void_p(stream)))
 
     def close(self):
-        if self.h:
+        if self.h and lib is not None:  # at interpreter exit the module globals may be gone
             lib().tc_model_destroy(self.h)
             self.h = None
 
@@ -180,7 +180,7 @@ class Dataset:
         return out
 
     def close(self):
-        if self.h:
+        if self.h and lib is not None:  # at interpreter exit the module globals may be gone
             lib().tc_dataset_destroy(self.h)
             self.h = None
 
@@ -223,7 +223,7 @@ class Trainer:
         return Model(self.eng, m)
 
     def close(self):
-        if self.h:
+        if self.h and lib is not None:  # at interpreter exit the module globals may be gone
             lib().tc_trainer_destroy(self.h)
             self.h = None
 
@@ -355,7 +355,7 @@ class Server:
         return a.value, b.value, c.value
 
     def close(self):
-        if self.h:
+        if self.h and lib is not None:  # at interpreter exit the module globals may be gone
             lib().tc_server_destroy(self.h)
             self.h = None
 
