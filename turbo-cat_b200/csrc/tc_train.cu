@@ -49,7 +49,7 @@ constexpr int HIST_BATCH = 32;    // rows per warp batch (one per lane)
 constexpr int PART_THREADS = 512;
 constexpr int SCAN_WARPS = 8;     // warps per scan block
 constexpr int SCAN_NODES = 32;    // nodes per scan block (4 per warp)
-constexpr int MERGE_BB = 8;       // bins per merge block
+constexpr int MERGE_BB = 4;       // bins per merge block
 constexpr int PLAN_THREADS = 1024;
 
 struct NodeStat {
@@ -593,8 +593,20 @@ __global__ void k_merge(DevCfg c, DevPtrs P, int d) {
     const int bl = q / W, col = q % W;
     double sg_ = 0.0, sh = 0.0;
     if (col < gsize) {
-      for (int ch = 0; ch < nch; ++ch) {
-        const float2 v = P.part[((size_t)(ib + ch * c.G) * kSlots + b0 + bl) * W + col];
+      // four partials loaded ahead of their (in-order) FP64 adds
+      const float2* src = P.part + ((size_t)ib * kSlots + b0 + bl) * W + col;
+      const size_t step = (size_t)c.G * kSlots * W;
+      int ch = 0;
+      for (; ch + 4 <= nch; ch += 4) {
+        const float2 v0 = src[(size_t)ch * step], v1 = src[(size_t)(ch + 1) * step];
+        const float2 v2 = src[(size_t)(ch + 2) * step], v3 = src[(size_t)(ch + 3) * step];
+        sg_ += (double)v0.x; sh += (double)v0.y;
+        sg_ += (double)v1.x; sh += (double)v1.y;
+        sg_ += (double)v2.x; sh += (double)v2.y;
+        sg_ += (double)v3.x; sh += (double)v3.y;
+      }
+      for (; ch < nch; ++ch) {
+        const float2 v = src[(size_t)ch * step];
         sg_ += (double)v.x;
         sh += (double)v.y;
       }
@@ -1538,8 +1550,8 @@ void tc_trainer::launch_level(const DevCfg& c, const DevPtrs& P, int d, cudaStre
   const int P2 = d == 0 ? 1 : (1 << (d - 1));
   dim3 mg(kSlots / MERGE_BB, K * P2, c.G);
   mark_begin(KC_MERGE, st);
-  if (J == 1) k_merge<1><<<mg, 256, 0, st>>>(c, P, d);
-  else k_merge<2><<<mg, 256, 0, st>>>(c, P, d);
+  if (J == 1) k_merge<1><<<mg, MERGE_BB * 32, 0, st>>>(c, P, d);
+  else k_merge<2><<<mg, MERGE_BB * 64, 0, st>>>(c, P, d);
   mark_end(st);
   const int ng = ((1 << d) + SCAN_NODES - 1) / SCAN_NODES;
   mark_begin(KC_SCAN, st);
