@@ -1179,13 +1179,20 @@ __global__ void __launch_bounds__(PLAN_THREADS) k_plan(DevCfg c, DevPtrs P, int 
 // grid (PB, K).  Row ids of the smaller children, grouped by pair, and their
 // (grad, hess) in the same order (the next level's histogram reads them
 // contiguously).
+constexpr int SCAT_UNROLL = 4;
 __global__ void __launch_bounds__(PART_THREADS) k_scatter(DevCfg c, DevPtrs P, int d) {
-  extern __shared__ uint32_t s_cur[];
+  extern __shared__ uint32_t s_cur[];  // [np2] counters, [np2] list offsets of this block, [np2] smaller child
   const int k = blockIdx.y;
   if (P.cs[k].done) return;
   const int Pmax = 1 << (c.D - 1);
   const int np2 = 1 << d;  // pairs at level d+1
-  for (int q = threadIdx.x; q < np2; q += blockDim.x) s_cur[q] = 0;
+  uint32_t* s_base = s_cur + np2;
+  int* s_small = reinterpret_cast<int*>(s_base + np2);
+  for (int q = threadIdx.x; q < np2; q += blockDim.x) {
+    s_cur[q] = 0;
+    s_base[q] = P.seg_start[k * Pmax + q] + P.blk_off[((size_t)k * c.PB + blockIdx.x) * Pmax + q];
+    s_small[q] = P.small[k * Pmax + q];
+  }
   __syncthreads();
   const uint32_t rpb = (c.n + gridDim.x - 1) / gridDim.x;
   const uint32_t r0 = blockIdx.x * rpb, r1 = min(c.n, r0 + rpb);
@@ -1195,23 +1202,35 @@ __global__ void __launch_bounds__(PART_THREADS) k_scatter(DevCfg c, DevPtrs P, i
   float2* cgh = P.cgh + (size_t)k * c.n;
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
-  for (uint32_t base = r0; base < r1; base += blockDim.x) {
-    const uint32_t i = base + threadIdx.x;
-    int key = -1;  // pair of a smaller-child row, else -1
-    if (i < r1) {
-      const int ch = leaf[i];
-      if (ch == P.small[k * Pmax + (ch >> 1)]) key = ch >> 1;
+  for (uint32_t base = r0; base < r1; base += blockDim.x * SCAT_UNROLL) {
+    // SCAT_UNROLL rows per thread: leaf indices, then the kept rows' (grad, hess)
+    int key[SCAT_UNROLL];  // pair of a smaller-child row, else -1
+    float2 g[SCAT_UNROLL];
+#pragma unroll
+    for (int u = 0; u < SCAT_UNROLL; ++u) {
+      const uint32_t i = base + u * blockDim.x + threadIdx.x;
+      key[u] = -1;
+      if (i < r1) {
+        const int ch = leaf[i];
+        if (ch == s_small[ch >> 1]) key[u] = ch >> 1;
+      }
     }
-    // one shared atomic per distinct pair of the warp; lanes keep their order
-    const unsigned m = __match_any_sync(0xffffffffu, key);
-    const int leader = __ffs(m) - 1;
-    uint32_t slot = 0;
-    if (key >= 0 && lane == leader) slot = atomicAdd(&s_cur[key], (uint32_t)__popc(m));
-    slot = __shfl_sync(0xffffffffu, slot, leader) + __popc(m & lt);
-    if (key >= 0) {
-      const uint32_t pos = P.seg_start[k * Pmax + key] + P.blk_off[((size_t)k * c.PB + blockIdx.x) * Pmax + key] + slot;
-      rows[pos] = i;
-      cgh[pos] = gh[i];
+#pragma unroll
+    for (int u = 0; u < SCAT_UNROLL; ++u)
+      if (key[u] >= 0) g[u] = gh[base + u * blockDim.x + threadIdx.x];
+#pragma unroll
+    for (int u = 0; u < SCAT_UNROLL; ++u) {
+      // one shared atomic per distinct pair of the warp; lanes keep their order
+      const unsigned m = __match_any_sync(0xffffffffu, key[u]);
+      const int leader = __ffs(m) - 1;
+      uint32_t slot = 0;
+      if (key[u] >= 0 && lane == leader) slot = atomicAdd(&s_cur[key[u]], (uint32_t)__popc(m));
+      slot = __shfl_sync(0xffffffffu, slot, leader) + __popc(m & lt);
+      if (key[u] >= 0) {
+        const uint32_t pos = s_base[key[u]] + slot;
+        rows[pos] = base + u * blockDim.x + threadIdx.x;
+        cgh[pos] = g[u];
+      }
     }
   }
 }
@@ -1571,7 +1590,7 @@ void tc_trainer::launch_level(const DevCfg& c, const DevPtrs& P, int d, cudaStre
   mark_end(st);
   if (d + 1 < D) {
     mark_begin(KC_SCATTER, st);
-    k_scatter<<<dim3(c.PB, K), PART_THREADS, sizeof(uint32_t) * (1 << d), st>>>(c, P, d);
+    k_scatter<<<dim3(c.PB, K), PART_THREADS, 3 * sizeof(uint32_t) * (1 << d), st>>>(c, P, d);
     mark_end(st);
   }
 }
