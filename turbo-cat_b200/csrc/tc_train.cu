@@ -116,6 +116,7 @@ struct DevPtrs {
   FeatBest* fbest;               // [K][F]
   uint32_t* counters;            // [K] completion counters of the pick blocks
   int32_t* hist_ctr;             // [1] next histogram work item (reset by the plan kernel)
+  uint32_t* red_ctr;             // [1] completion counter of the fused reduce + plan kernel
   ClassState* cs;                // [K]
   int32_t* iter;                 // [1] boosting iteration (tree slot = iter*KT + k0 + k)
   // model arrays (capacity T = n_estimators*K)
@@ -954,7 +955,7 @@ __global__ void __launch_bounds__(PART_THREADS) k_partition(DevCfg c, DevPtrs P,
 // sums over blocks), the smaller sibling (left on a tie,
 // src/tree/symmetric_tree.cpp:337-339) and each block's scatter offset of
 // its rows of the smaller child (exclusive scan over blocks).
-__global__ void __launch_bounds__(512) k_node_reduce(DevCfg c, DevPtrs P, int d) {
+__device__ __forceinline__ void node_reduce_body(const DevCfg& c, const DevPtrs& P, int d) {
   const int k = blockIdx.y, p = blockIdx.x;
   const ClassState cs = P.cs[k];
   const bool root = d < 0;  // root reduction after the gradient pass
@@ -1028,7 +1029,7 @@ __global__ void __launch_bounds__(512) k_node_reduce(DevCfg c, DevPtrs P, int d)
 // rows per chunk for this level and the cumulative chunk counts over
 // (class, pair, feature group), which the histogram kernel decodes into work
 // items.
-__global__ void __launch_bounds__(PLAN_THREADS) k_plan(DevCfg c, DevPtrs P, int d) {
+__device__ __forceinline__ void plan_body(const DevCfg& c, const DevPtrs& P, int d) {
   __shared__ int s_go;
   __shared__ long long s_rows;
   __shared__ int s_warp[PLAN_THREADS / 32];
@@ -1176,6 +1177,31 @@ __global__ void __launch_bounds__(PLAN_THREADS) k_plan(DevCfg c, DevPtrs P, int 
   }
 }
 
+__global__ void __launch_bounds__(PLAN_THREADS) k_plan(DevCfg c, DevPtrs P, int d) { plan_body(c, P, d); }
+
+// grid (nodes of level d, K): the reduce above; with FUSE_PLAN the last block
+// to finish (completion counter, nobody waits) also plans level d + 1, so a
+// level needs one launch less.
+template <bool FUSE_PLAN>
+__global__ void __launch_bounds__(512) k_node_reduce(DevCfg c, DevPtrs P, int d) {
+  node_reduce_body(c, P, d);
+  if (FUSE_PLAN) {
+    __shared__ bool s_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      const uint32_t prev = atomicAdd(P.red_ctr, 1u);
+      s_last = prev == gridDim.x * gridDim.y - 1;
+    }
+    __syncthreads();
+    if (s_last) {
+      __threadfence();
+      if (threadIdx.x == 0) *P.red_ctr = 0;  // re-armed for the next launch / graph replay
+      plan_body(c, P, d + 1);
+    }
+  }
+}
+
 // grid (PB, K).  Row ids of the smaller children, grouped by pair, and their
 // (grad, hess) in the same order (the next level's histogram reads them
 // contiguously).
@@ -1287,6 +1313,7 @@ struct tc_trainer {
   DevBuf<FeatBest> fbest;
   DevBuf<uint32_t> counters;
   DevBuf<int32_t> hist_ctr;
+  DevBuf<uint32_t> red_ctr;
   DevBuf<NodeStat> nstat;
   DevBuf<uint32_t> pcnt, blk_off;
   DevBuf<double2> psum;
@@ -1382,6 +1409,7 @@ tc_status tc_trainer::setup(int) {
   TC_TRY(fbest.alloc(ctx, (size_t)K * f, "feature bests"));
   TC_TRY(counters.alloc(ctx, K, "pick counters"));
   TC_TRY(hist_ctr.alloc(ctx, 1, "histogram item counter"));
+  TC_TRY(red_ctr.alloc(ctx, 1, "reduce completion counter"));
   TC_TRY(cs.alloc(ctx, K, "class state"));
   TC_TRY(m_depth.alloc(ctx, T_cap, "model"));
   TC_TRY(m_feat.alloc(ctx, (size_t)T_cap * D, "model"));
@@ -1391,6 +1419,7 @@ tc_status tc_trainer::setup(int) {
   TC_TRY(m_second.alloc(ctx, (size_t)T_cap * D, "model"));
   TC_TRY(m_leaves.alloc(ctx, (size_t)T_cap * L, "model"));
   TC_CUDA(ctx, cudaMemset(counters.p, 0, counters.bytes()));
+  TC_CUDA(ctx, cudaMemset(red_ctr.p, 0, red_ctr.bytes()));
 
   ptr.bins_rm = ds->bins_rm.p; ptr.bins_cm = ds->bins_cm.p; ptr.edges = ds->edges.p; ptr.n_edges = ds->n_edges.p;
   ptr.nan_any = ds->nan_any.p;
@@ -1398,7 +1427,7 @@ tc_status tc_trainer::setup(int) {
   ptr.hist[0] = hist0.p; ptr.hist[1] = hist1.p; ptr.rchunk = rchunk.p;
   ptr.seg_start = seg_start.p; ptr.seg_len = seg_len.p; ptr.small = small.p; ptr.nstat = nstat.p;
   ptr.pcnt = pcnt.p; ptr.psum = psum.p; ptr.blk_off = blk_off.p; ptr.gpart = gpart.p; ptr.gany = gany.p;
-  ptr.fbest = fbest.p; ptr.counters = counters.p; ptr.hist_ctr = hist_ctr.p; ptr.cs = cs.p; ptr.iter = iter.p;
+  ptr.fbest = fbest.p; ptr.counters = counters.p; ptr.hist_ctr = hist_ctr.p; ptr.red_ctr = red_ctr.p; ptr.cs = cs.p; ptr.iter = iter.p;
   ptr.m_depth = m_depth.p; ptr.m_feat = m_feat.p; ptr.m_bin = m_bin.p; ptr.m_thr = m_thr.p; ptr.m_gain = m_gain.p;
   ptr.m_second = m_second.p; ptr.m_leaves = m_leaves.p; ptr.root_hist_out = nullptr;
 
@@ -1505,7 +1534,7 @@ tc_status tc_trainer::autotune() {
 
 enum { KC_GRAD, KC_HIST, KC_MERGE, KC_SCAN, KC_PICK, KC_PART, KC_REDUCE, KC_PLAN, KC_SCATTER, KC_OTHER, KC_N };
 static const char* kKernelNames[KC_N] = {"grad", "hist", "merge", "scan", "pick", "partition",
-                                         "node_reduce", "plan", "scatter", "other"};
+                                         "reduce_plan", "plan", "scatter", "other"};
 
 void tc_trainer::mark_begin(int cls, cudaStream_t st) {
   ++launches;
@@ -1583,10 +1612,7 @@ void tc_trainer::launch_level(const DevCfg& c, const DevPtrs& P, int d, cudaStre
   k_partition<<<dim3(c.PB, K), PART_THREADS, 12 * (2 << d), st>>>(c, P, d);
   mark_end(st, (double)c.n * K * (1 + 2 + 2 + 8));
   mark_begin(KC_REDUCE, st);
-  k_node_reduce<<<dim3(1 << d, K), 512, 0, st>>>(c, P, d);
-  mark_end(st);
-  mark_begin(KC_PLAN, st);
-  k_plan<<<1, PLAN_THREADS, 0, st>>>(c, P, d + 1);
+  k_node_reduce<true><<<dim3(1 << d, K), 512, 0, st>>>(c, P, d);  // + plan of level d + 1
   mark_end(st);
   if (d + 1 < D) {
     mark_begin(KC_SCATTER, st);
@@ -1602,10 +1628,7 @@ tc_status tc_trainer::enqueue_iteration(cudaStream_t st) {
   k_grad<<<cfg.PB, 512, 0, st>>>(cfg, ptr, 0);
   mark_end(st, (double)cfg.n * K * (4 + 4 + 8 + 2 + 8) + (double)cfg.n * 4);
   mark_begin(KC_REDUCE, st);
-  k_node_reduce<<<dim3(1, K), 512, 0, st>>>(cfg, ptr, -1);
-  mark_end(st);
-  mark_begin(KC_PLAN, st);
-  k_plan<<<1, PLAN_THREADS, 0, st>>>(cfg, ptr, 0);
+  k_node_reduce<true><<<dim3(1, K), 512, 0, st>>>(cfg, ptr, -1);  // + plan of level 0
   mark_end(st);
   for (int d = 0; d < D; ++d) launch_level(cfg, ptr, d, st);
   mark_begin(KC_OTHER, st);
@@ -1640,7 +1663,7 @@ static DevPtrs class_view(const DevCfg& c, const DevPtrs& P, int k, DevCfg* one)
 tc_status tc_trainer::run_plain_iteration(cudaStream_t st) {
   const int K = cfg.K, D = cfg.D;
   k_grad<<<cfg.PB, 512, 0, st>>>(cfg, ptr, 0);
-  k_node_reduce<<<dim3(1, K), 512, 0, st>>>(cfg, ptr, -1);
+  k_node_reduce<false><<<dim3(1, K), 512, 0, st>>>(cfg, ptr, -1);
   for (int k = 0; k < K; ++k) {
     DevCfg one;
     DevPtrs pk = class_view(cfg, ptr, k, &one);
@@ -1993,7 +2016,7 @@ tc_status tc_build_tree(tc_ctx* ctx, tc_dataset* ds, const float* grad, const fl
   // one iteration with the given gradients
   const int D = tr->cfg.D;
   k_grad<<<tr->cfg.PB, 512, 0, st>>>(tr->cfg, tr->ptr, 1);
-  k_node_reduce<<<dim3(1, 1), 512, 0, st>>>(tr->cfg, tr->ptr, -1);
+  k_node_reduce<false><<<dim3(1, 1), 512, 0, st>>>(tr->cfg, tr->ptr, -1);
   k_plan<<<1, PLAN_THREADS, 0, st>>>(tr->cfg, tr->ptr, 0);
   for (int d = 0; d < D; ++d) {
     tr->launch_level(tr->cfg, tr->ptr, d, st);
