@@ -49,6 +49,7 @@ constexpr int HIST_BATCH = 32;    // rows per warp batch (one per lane)
 constexpr int PART_THREADS = 512;
 constexpr int SCAN_WARPS = 8;     // warps per scan block
 constexpr int SCAN_NODES = 32;    // nodes per scan block (4 per warp)
+static_assert(SCAN_WARPS * 32 == 256, "a scan block also runs the 256-thread pick");
 constexpr int MERGE_BB = 4;       // bins per merge block
 constexpr int PLAN_THREADS = 1024;
 
@@ -115,6 +116,7 @@ struct DevPtrs {
   uint8_t* gany;                 // [K][F][NG][256]
   FeatBest* fbest;               // [K][F]
   uint32_t* counters;            // [K] completion counters of the pick blocks
+  uint32_t* fcnt;                // [K][F] completion counters of a feature's scan blocks
   int32_t* hist_ctr;             // [1] next histogram work item (reset by the plan kernel)
   uint32_t* red_ctr;             // [1] completion counter of the fused reduce + plan kernel
   ClassState* cs;                // [K]
@@ -636,6 +638,8 @@ __global__ void k_merge(DevCfg c, DevPtrs P, int d) {
 
 // ------------------------------------------------------------------ scan --
 
+__device__ void pick_body(const DevCfg& c, const DevPtrs& P, int d, int f, int k);
+
 // grid (F, node groups, K), SCAN_WARPS warps.  A warp scores one node at a
 // time: lane l holds bins 8l .. 8l+7 (bin 255 = NaN rows, added to the left
 // side); left sums are NaN + prefix, right sums an independent suffix, so an
@@ -727,6 +731,20 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(DevCfg c, DevPtrs P, i
     P.gpart[o] = s;
     P.gany[o] = a;
   }
+  // the last node-group block of feature f (completion counter; nobody
+  // waits) picks the feature's best bin, and the class's last feature its split
+  __shared__ bool s_fdone;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const uint32_t prev = atomicAdd(&P.fcnt[(size_t)k * c.f + f], 1u);
+    s_fdone = prev == gridDim.y - 1;
+  }
+  __syncthreads();
+  if (!s_fdone) return;
+  __threadfence();
+  if (threadIdx.x == 0) P.fcnt[(size_t)k * c.f + f] = 0;  // re-armed for the next level / graph replay
+  pick_body(c, P, d, f, k);
 }
 
 // ------------------------------------------------------------------ pick --
@@ -743,13 +761,14 @@ __device__ __forceinline__ bool better(double ga, int fa, int ba, double gb, int
 // waiting) reduces the features in ascending order -- the reference keeps
 // the first strictly greater gain, i.e. lowest feature then lowest bin --
 // applies the stop rule and records the split.
-__global__ void __launch_bounds__(256) k_pick(DevCfg c, DevPtrs P, int d) {
+// Best bin of feature f of class k over the level's node groups, then, in the
+// last feature block of the class (completion counter), the level's split.
+// Called by the 256 threads of a scan block once its feature is complete.
+__device__ void pick_body(const DevCfg& c, const DevPtrs& P, int d, int f, int k) {
   __shared__ double s_g[256], s_2[256];
   __shared__ int s_b[256];
   __shared__ bool s_last;
-  const int f = blockIdx.x, k = blockIdx.y;
   ClassState& cs = P.cs[k];
-  if (cs.done) return;
   const int b = threadIdx.x;
   const int ngroups = ((1 << d) + SCAN_NODES - 1) / SCAN_NODES;
   double s = 0.0;
@@ -1313,7 +1332,7 @@ struct tc_trainer {
   DevBuf<FeatBest> fbest;
   DevBuf<uint32_t> counters;
   DevBuf<int32_t> hist_ctr;
-  DevBuf<uint32_t> red_ctr;
+  DevBuf<uint32_t> red_ctr, fcnt;
   DevBuf<NodeStat> nstat;
   DevBuf<uint32_t> pcnt, blk_off;
   DevBuf<double2> psum;
@@ -1410,6 +1429,7 @@ tc_status tc_trainer::setup(int) {
   TC_TRY(counters.alloc(ctx, K, "pick counters"));
   TC_TRY(hist_ctr.alloc(ctx, 1, "histogram item counter"));
   TC_TRY(red_ctr.alloc(ctx, 1, "reduce completion counter"));
+  TC_TRY(fcnt.alloc(ctx, (size_t)K * f, "scan completion counters"));
   TC_TRY(cs.alloc(ctx, K, "class state"));
   TC_TRY(m_depth.alloc(ctx, T_cap, "model"));
   TC_TRY(m_feat.alloc(ctx, (size_t)T_cap * D, "model"));
@@ -1420,6 +1440,7 @@ tc_status tc_trainer::setup(int) {
   TC_TRY(m_leaves.alloc(ctx, (size_t)T_cap * L, "model"));
   TC_CUDA(ctx, cudaMemset(counters.p, 0, counters.bytes()));
   TC_CUDA(ctx, cudaMemset(red_ctr.p, 0, red_ctr.bytes()));
+  TC_CUDA(ctx, cudaMemset(fcnt.p, 0, fcnt.bytes()));
 
   ptr.bins_rm = ds->bins_rm.p; ptr.bins_cm = ds->bins_cm.p; ptr.edges = ds->edges.p; ptr.n_edges = ds->n_edges.p;
   ptr.nan_any = ds->nan_any.p;
@@ -1427,7 +1448,7 @@ tc_status tc_trainer::setup(int) {
   ptr.hist[0] = hist0.p; ptr.hist[1] = hist1.p; ptr.rchunk = rchunk.p;
   ptr.seg_start = seg_start.p; ptr.seg_len = seg_len.p; ptr.small = small.p; ptr.nstat = nstat.p;
   ptr.pcnt = pcnt.p; ptr.psum = psum.p; ptr.blk_off = blk_off.p; ptr.gpart = gpart.p; ptr.gany = gany.p;
-  ptr.fbest = fbest.p; ptr.counters = counters.p; ptr.hist_ctr = hist_ctr.p; ptr.red_ctr = red_ctr.p; ptr.cs = cs.p; ptr.iter = iter.p;
+  ptr.fbest = fbest.p; ptr.counters = counters.p; ptr.hist_ctr = hist_ctr.p; ptr.red_ctr = red_ctr.p; ptr.fcnt = fcnt.p; ptr.cs = cs.p; ptr.iter = iter.p;
   ptr.m_depth = m_depth.p; ptr.m_feat = m_feat.p; ptr.m_bin = m_bin.p; ptr.m_thr = m_thr.p; ptr.m_gain = m_gain.p;
   ptr.m_second = m_second.p; ptr.m_leaves = m_leaves.p; ptr.root_hist_out = nullptr;
 
@@ -1533,7 +1554,7 @@ tc_status tc_trainer::autotune() {
 }
 
 enum { KC_GRAD, KC_HIST, KC_MERGE, KC_SCAN, KC_PICK, KC_PART, KC_REDUCE, KC_PLAN, KC_SCATTER, KC_OTHER, KC_N };
-static const char* kKernelNames[KC_N] = {"grad", "hist", "merge", "scan", "pick", "partition",
+static const char* kKernelNames[KC_N] = {"grad", "hist", "merge", "scan_pick", "pick", "partition",
                                          "reduce_plan", "plan", "scatter", "other"};
 
 void tc_trainer::mark_begin(int cls, cudaStream_t st) {
@@ -1603,10 +1624,7 @@ void tc_trainer::launch_level(const DevCfg& c, const DevPtrs& P, int d, cudaStre
   mark_end(st);
   const int ng = ((1 << d) + SCAN_NODES - 1) / SCAN_NODES;
   mark_begin(KC_SCAN, st);
-  k_scan<<<dim3(c.f, ng, K), SCAN_WARPS * 32, 0, st>>>(c, P, d);
-  mark_end(st);
-  mark_begin(KC_PICK, st);
-  k_pick<<<dim3(c.f, K), 256, 0, st>>>(c, P, d);
+  k_scan<<<dim3(c.f, ng, K), SCAN_WARPS * 32, 0, st>>>(c, P, d);  // + pick
   mark_end(st);
   mark_begin(KC_PART, st);
   k_partition<<<dim3(c.PB, K), PART_THREADS, 12 * (2 << d), st>>>(c, P, d);
@@ -1650,7 +1668,7 @@ static DevPtrs class_view(const DevCfg& c, const DevPtrs& P, int k, DevCfg* one)
   pk.hist[1] += (size_t)k * Pmax * c.f * kSlots;
   pk.seg_start += k * Pmax; pk.seg_len += k * Pmax;
   pk.small += k * Pmax; pk.nstat += (size_t)k * (c.D + 1) * L;
-  pk.fbest += (size_t)k * c.f; pk.counters += k;
+  pk.fbest += (size_t)k * c.f; pk.counters += k; pk.fcnt += (size_t)k * c.f;
   pk.pcnt += (size_t)k * c.PB * L; pk.psum += (size_t)k * c.PB * L; pk.blk_off += (size_t)k * c.PB * Pmax;
   pk.gpart += (size_t)k * c.f * c.n_scan_groups_max * kSlots;
   pk.gany += (size_t)k * c.f * c.n_scan_groups_max * kSlots;
