@@ -129,6 +129,8 @@ typedef struct {
   int32_t hist_features_per_block;
   int32_t hist_rows_per_chunk;
   int64_t kernel_launches;  /* kernels launched by the iterations run so far */
+  int32_t best_iteration;   /* validation set: iteration of the best validation loss (else -1) */
+  int32_t stopped_early;    /* validation set: 1 once the early-stopping rule has fired */
 } tc_train_stats;
 
 /* Per-kernel timing of profiled iterations (CUDA events on the launching
@@ -166,6 +168,21 @@ tc_status tc_trainer_profile(tc_trainer* tr, int32_t iterations, tc_profile* out
 tc_status tc_trainer_train_scores(tc_trainer* tr, float* out);
 /* Snapshot of the ensemble trained so far as an immutable model. */
 tc_status tc_trainer_model(tc_trainer* tr, tc_model** out);
+/* Validation set and early stopping, Booster::train's valid_data branch
+ * (src/boosting/booster.cpp:255-371; multiclass 1405-1435).  After every
+ * iteration its trees are added to the validation predictions (FP32
+ * lr * leaf), the validation loss is the loss's compute_loss (mean logloss
+ * with p clipped to [1e-7, 1 - 1e-7], mean squared error, robust focal,
+ * multiclass cross entropy; summed in FP64 here), an improvement is
+ * loss < best - 1e-10, and training stops once the iteration is
+ * >= max(50, n_estimators / 10) and `early_stopping_rounds` iterations in a
+ * row did not improve (< 0: never stop).  The model keeps every tree up to
+ * and including the stopping iteration, as the reference's loop breaks
+ * there.  `valid` needs labels and the training set's feature count (raw
+ * features; it need not be quantized); call before the first iteration. */
+tc_status tc_trainer_set_validation(tc_trainer* tr, const tc_dataset* valid, int32_t early_stopping_rounds);
+/* Validation loss of every iteration run so far (iterations_done values). */
+tc_status tc_trainer_valid_loss(tc_trainer* tr, double* out);
 void tc_trainer_destroy(tc_trainer* tr);
 
 /* One-shot fit: create + step(n_estimators) + model.  Replaces

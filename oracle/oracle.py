@@ -468,3 +468,64 @@ def parse_tcat(data: bytes) -> Ensemble:
     e = Ensemble(base, 1, D, depth, feat, bins_, thr, leaves, weights, gain)
     e.bin_edges = edges
     return e
+
+
+# --------------------------------------------------------- early stopping --
+
+def early_stopping(ens: Ensemble, Xv, yv, loss: str, n_estimators: int, rounds: int,
+                   learning_rate: float, focal_gamma=2.0, focal_alpha=0.25):
+    """Validation loss per iteration and the stopping iteration of
+    Booster::train's valid_data branch (src/boosting/booster.cpp:255-371;
+    multiclass 1405-1435), replayed over the iterations of `ens`:
+    valid_pred += lr * leaf (FP32, fused multiply-add as the compiled
+    reference), the loss's compute_loss term per row in FP32
+    (src/boosting/loss.cpp:110-121, 232-244, 336-346, 475-503) summed in
+    FP64, improvement when loss < best - 1e-10 (FP32), stop once
+    iteration >= max(50, n_estimators / 10) and `rounds` iterations in a row
+    did not improve.  Returns (losses, stop_iteration or -1, best_iteration)."""
+    Xv = np.ascontiguousarray(Xv, np.float32)
+    yv = np.ascontiguousarray(yv, np.float32)
+    K = ens.n_classes
+    nv = Xv.shape[0]
+    iters = ens.n_trees // K
+    pred = np.full((nv, K), np.float32(ens.base), np.float32)
+    best, best_it, no_imp = np.float32(1e30), 0, 0
+    min_it = max(50, n_estimators // 10)
+    losses = []
+    f32 = np.float32
+    for it in range(iters):
+        for k in range(K):
+            t = it * K + k
+            idx = np.zeros(nv, np.int64)
+            for d in range(int(ens.depth[t])):
+                idx = idx * 2 + (Xv[:, ens.feature[t, d]] >= ens.threshold[t, d])
+            v = ens.leaves[t, idx].astype(np.float64)
+            pred[:, k] = (np.float64(f32(learning_rate)) * v + pred[:, k].astype(np.float64)).astype(np.float32)
+        if loss == "mse":
+            diff = pred[:, 0] - yv
+            term = diff * diff
+        elif loss == "logloss":
+            p = f32(1) / (f32(1) + np.exp(-pred[:, 0]))
+            p = np.clip(p, f32(1e-7), f32(1) - f32(1e-7))
+            term = -yv * np.log(p) - (f32(1) - yv) * np.log(f32(1) - p)
+        elif loss == "focal":
+            p = f32(1) / (f32(1) + np.exp(-pred[:, 0]))
+            pt = yv * p + (f32(1) - yv) * (f32(1) - p)
+            robust = f32(1) - f32(0.1) * np.abs(f32(2) * pt - f32(1)) ** f32(2)
+            pt = np.maximum(pt, f32(1e-7))
+            at = yv * f32(focal_alpha) + (f32(1) - yv) * (f32(1) - f32(focal_alpha))
+            term = -at * (f32(1) - pt) ** f32(focal_gamma) * robust * np.log(pt)
+        else:  # softmax cross entropy
+            z = pred - pred.max(axis=1, keepdims=True)
+            e = np.exp(z)
+            pl = e[np.arange(nv), yv.astype(np.int64)] / e.sum(axis=1)
+            term = -np.log(np.maximum(pl, f32(1e-7)))
+        lv = float(np.sum(term.astype(np.float64)) / nv)
+        losses.append(lv)
+        if f32(lv) < best - f32(1e-10):
+            best, best_it, no_imp = f32(lv), it, 0
+        else:
+            no_imp += 1
+        if rounds >= 0 and it >= min_it and no_imp >= rounds:
+            return np.array(losses), it, best_it
+    return np.array(losses), -1, best_it

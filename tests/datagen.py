@@ -99,3 +99,14 @@ def make_case(spec):
     else:
         X, y = imbalanced_c5(spec["n"], spec["f"], spec["seed"], active=min(20, spec["f"]))
     return X, y, Hyper(**spec["hyper"])
+
+
+def noisy_binary_split(n=3000, nv=2000, f=10, seed=81, noise=2.0):
+    """A small noisy binary problem with a held-out validation split: training
+    overfits within a few dozen iterations at a high learning rate, so the
+    validation loss turns and early stopping fires."""
+    rng = np.random.default_rng(seed)
+    X = rng.standard_normal((n + nv, f)).astype(np.float32)
+    w = rng.standard_normal(f)
+    y = ((X @ w + rng.normal(0, noise, n + nv)) > 0).astype(np.float32)
+    return X[:n], y[:n], X[n:], y[n:]

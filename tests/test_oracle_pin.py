@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from datagen import GOLDEN_CASES, binary_c1, make_case, regression_c2
+from datagen import GOLDEN_CASES, binary_c1, make_case, noisy_binary_split, regression_c2
 
 
 def _u32(a):
@@ -109,3 +109,41 @@ def test_oracle_matches_reference_live(seed):
     assert np.array_equal(r.feature, e.feature) and np.array_equal(r.bin, e.bin)
     assert np.array_equal(_u32(r.leaves), _u32(e.leaves))
     assert np.array_equal(_u32(gt), _u32(e.grad_trace[:, :, 0]))
+
+
+_ES_SCRIPT = r"""
+import sys
+sys.path[:0] = [sys.argv[1], sys.argv[2]]
+import numpy as np
+import _turbocat as ref
+from datagen import noisy_binary_split
+Xt, yt, Xv, yv = noisy_binary_split()
+m = ref.TurboCatClassifier(n_estimators=200, learning_rate=0.3, max_depth=6, max_bins=255, subsample=1.0,
+                           colsample_bytree=1.0, min_child_weight=1.0, lambda_l2=1.0, loss="logloss",
+                           mode="large", early_stopping_rounds=10, verbosity=0)
+m.fit(Xt, yt, Xv, yv)
+print(m.n_trees)
+"""
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference build (oracle/_ref) not present")
+def test_early_stopping_replay_matches_reference():
+    """The oracle's replay of the validation/early-stopping rule over its own
+    (reference-identical) trees stops where the reference's fit with a
+    validation set stops.  The reference runs in a process of its own (one
+    fit per process)."""
+    import os
+    import subprocess
+    import sys
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    out = subprocess.run([sys.executable, "-c", _ES_SCRIPT, here, os.path.join(O.HERE, "_ref")],
+                         capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr
+    ref_trees = int(out.stdout.strip().splitlines()[-1])
+    Xt, yt, Xv, yv = noisy_binary_split()
+    hp = O.Hyper(loss="logloss", n_estimators=200, learning_rate=0.3, max_depth=6, lambda_l2=1.0)
+    e = O.fit(O.quantize(Xt), yt, hp, mode=0)
+    losses, stop, best = O.early_stopping(e, Xv, yv, "logloss", 200, 10, 0.3)
+    assert stop >= 50 and best < stop  # the rule fired after the minimum iterations
+    assert ref_trees == stop + 1

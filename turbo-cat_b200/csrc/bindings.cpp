@@ -67,13 +67,29 @@ class GpuBooster {
   tc_model_info info{};
   tc_train_stats stats{};
 
-  void fit(const float* X, uint32_t n, uint16_t f, const float* y, const tc_train_params& p) {
+  // With a validation set (Xv, yv, nv > 0) the fit follows Booster::train's
+  // valid_data branch: validation loss every iteration, early stopping after
+  // `es_rounds` iterations without improvement (src/boosting/booster.cpp:255-371).
+  void fit(const float* X, uint32_t n, uint16_t f, const float* y, const tc_train_params& p,
+           const float* Xv = nullptr, const float* yv = nullptr, uint32_t nv = 0, int es_rounds = 50) {
     tc_ctx* ctx = device_context();
     tc_dataset* ds = nullptr;
+    tc_dataset* vds = nullptr;
     check(tc_dataset_upload(ctx, X, n, f, y, &ds), ctx);
     tc_status s = tc_quantize(ds, (uint16_t)p.max_bins, 1, nullptr, nullptr);
     tc_model* m = nullptr;
-    if (s == TC_OK) s = tc_train(ctx, ds, &p, &m, &stats);
+    if (s == TC_OK && nv == 0) s = tc_train(ctx, ds, &p, &m, &stats);
+    if (s == TC_OK && nv > 0) {
+      tc_trainer* tr = nullptr;
+      s = tc_dataset_upload(ctx, Xv, nv, f, yv, &vds);
+      if (s == TC_OK) s = tc_trainer_create(ctx, ds, &p, &tr);
+      if (s == TC_OK) s = tc_trainer_set_validation(tr, vds, es_rounds);
+      if (s == TC_OK) s = tc_trainer_step(tr, p.n_estimators, 1);
+      if (s == TC_OK) s = tc_trainer_model(tr, &m);
+      if (s == TC_OK) s = tc_trainer_stats(tr, &stats);
+      if (tr) tc_trainer_destroy(tr);
+    }
+    if (vds) tc_dataset_destroy(vds);
     tc_dataset_destroy(ds);
     check(s, ctx);
     model.reset(new ModelPtr());
@@ -214,7 +230,11 @@ class TurboCatClassifier {
     p_.min_child_weight = min_child_weight;
     p_.lambda_l2 = lambda_l2;
     (void)goss_top_rate; (void)goss_other_rate; (void)use_symmetric; (void)grow_policy;
-    (void)early_stopping_rounds; (void)early_stopping_metric; (void)cat_encoding; (void)max_interactions;
+    es_rounds_ = early_stopping_rounds;
+    if (early_stopping_metric != "loss" && early_stopping_metric != "logloss")
+      warn("early_stopping_metric '" + early_stopping_metric + "' is not on the device path; the validation "
+           "loss is used (the reference's fallback for metrics it does not know)");
+    (void)cat_encoding; (void)max_interactions;
     (void)interaction_method; (void)n_threads; (void)seed;
   }
 
@@ -230,7 +250,12 @@ class TurboCatClassifier {
     if (use_gradtree_ || use_ordered_ || auto_interactions_)
       warn("use_gradtree / use_ordered_boosting / auto_interactions are not on the device path and are ignored");
     if (!cat_features.empty()) throw std::invalid_argument("cat_features are not supported on the device path");
-    if (X_val.size() > 0 || y_val.size() > 0) warn("validation data (early stopping) is not used on the device path");
+    const bool has_val = X_val.size() > 0 && y_val.size() > 0;
+    if (has_val) {
+      check_2d(X_val, "X_val");
+      if (X_val.shape(1) != X.shape(1)) throw std::invalid_argument("X_val must have as many features as X");
+      if ((size_t)y_val.size() != (size_t)X_val.shape(0)) throw std::invalid_argument("y_val does not match X_val");
+    }
     const float* yp = y.data();
     float mx = 0.0f;
     for (uint32_t i = 0; i < n; ++i) mx = std::max(mx, yp[i]);
@@ -248,7 +273,10 @@ class TurboCatClassifier {
     {
       py::gil_scoped_release nogil;
       booster_.reset(new GpuBooster());
-      booster_->fit(X.data(), n, f, yp, p);
+      if (has_val)
+        booster_->fit(X.data(), n, f, yp, p, X_val.data(), y_val.data(), (uint32_t)X_val.shape(0), es_rounds_);
+      else
+        booster_->fit(X.data(), n, f, yp, p);
     }
     n_features_ = f;
     is_fitted_ = true;
@@ -363,6 +391,7 @@ class TurboCatClassifier {
   float subsample_, colsample_;
   bool use_goss_, use_gradtree_, use_ordered_, auto_interactions_;
   int verbosity_;
+  int es_rounds_ = 50;
   std::unique_ptr<GpuBooster> booster_;
   uint32_t n_classes_ = 2;
   int n_features_ = 0;

@@ -52,6 +52,7 @@ constexpr int SCAN_NODES = 32;    // nodes per scan block (4 per warp)
 static_assert(SCAN_WARPS * 32 == 256, "a scan block also runs the 256-thread pick");
 constexpr int MERGE_BB = 4;       // bins per merge block
 constexpr int PLAN_THREADS = 1024;
+constexpr int VALID_BLOCKS = 296;  // blocks of the validation kernel (fixed: its partial sums have a fixed order)
 
 struct NodeStat {
   double G, H;
@@ -64,6 +65,16 @@ struct ClassState {
   int32_t done;        // 0 growing, 1 stopped (leaves pending), 2 finalized
   int32_t depth;       // accepted splits
   int32_t f, b;        // split of the current level
+};
+
+// Early-stopping state of a validation set (device).
+struct EsState {
+  float best;          // best validation loss so far (the reference keeps it in FP32)
+  int32_t best_iter;
+  int32_t no_improve;  // iterations in a row without improvement
+  int32_t stopped;     // set once the stopping rule fires
+  int32_t stop_iter;
+  uint32_t ctr;        // completion counter of the loss blocks
 };
 
 // Per-(class, feature) best candidate of a level.
@@ -87,6 +98,9 @@ struct DevCfg {
   int32_t rows_min;              // smallest rows per histogram chunk
   int32_t rows_fixed;            // > 0: fixed rows per chunk (tuning override)
   float hconst;                  // > 0: every row's hessian equals this (histogram counts rows)
+  uint32_t nv;                   // validation rows (0: no validation set)
+  int32_t es_rounds;             // early_stopping_rounds (< 0: never stop)
+  int32_t es_min_iter;           // first iteration the stopping rule may fire at
 };
 
 struct DevPtrs {
@@ -130,6 +144,13 @@ struct DevPtrs {
   double* m_second;              // [T][D]
   float* m_leaves;               // [T][2^D]
   double* root_hist_out;         // optional [F][256][2]
+  // validation set
+  const float* xv;               // [nv][f] raw features
+  const float* yv;               // [nv] labels
+  float* vpred;                  // [K][nv] raw validation predictions
+  double* vpart;                 // [VALID_BLOCKS] partial loss sums
+  double* vloss;                 // [n_estimators] validation loss per iteration
+  EsState* es;
 };
 
 __device__ __forceinline__ size_t hist_index(const DevCfg& c, int k, int node, int f, int b) {
@@ -1061,6 +1082,7 @@ __device__ __forceinline__ void plan_body(const DevCfg& c, const DevPtrs& P, int
     ClassState& cs = P.cs[k];
     if (tid == 0) {
       if (d == 0) { cs.done = 0; cs.depth = 0; }
+      if (d == 0 && c.nv > 0 && P.es->stopped) cs.done = 2;  // early-stopped: no more trees
       s_go = 0;
     }
     __syncthreads();
@@ -1282,6 +1304,109 @@ __global__ void __launch_bounds__(PART_THREADS) k_scatter(DevCfg c, DevPtrs P, i
 
 __global__ void k_next_iter(DevPtrs P) { *P.iter += 1; }
 
+// Validation set after an iteration (Booster::train's valid_data branch,
+// src/boosting/booster.cpp:255-371; multiclass src/boosting/booster.cpp:1405-1435):
+// the iteration's trees are added to the validation predictions (lr * leaf,
+// FP32 fused multiply-add as the reference's compiled update), the loss is
+// each loss's compute_loss term (FP32 per row as the reference,
+// src/boosting/loss.cpp:110-121, 232-244, 336-346, 475-503; the sum in FP64
+// here, in a fixed order), and the last block applies the stopping rule:
+// improvement when loss < best - 1e-10 (FP32 compare); stop once
+// iteration >= max(50, n_estimators/10) and early_stopping_rounds
+// iterations in a row did not improve.
+__device__ __forceinline__ float valid_term(const DevCfg& c, const float* pr, float y) {
+  if (c.loss == TC_LOSS_MSE) {
+    const float diff = pr[0] - y;
+    return diff * diff;
+  }
+  if (c.loss == TC_LOSS_LOGLOSS) {
+    float p = 1.0f / (1.0f + expf(-pr[0]));
+    p = fmaxf(1e-7f, fminf(1.0f - 1e-7f, p));
+    return -y * logf(p) - (1.0f - y) * logf(1.0f - p);
+  }
+  if (c.loss == TC_LOSS_FOCAL) {
+    // RobustFocalLoss with the reference's defaults: mu = 0.1 (config robust_mu),
+    // class weights 1 (set_class_weights is never called)
+    const float p = 1.0f / (1.0f + expf(-pr[0]));
+    float pt = y * p + (1.0f - y) * (1.0f - p);
+    const float robust = 1.0f - 0.1f * powf(fabsf(2.0f * pt - 1.0f), 2.0f);
+    pt = fmaxf(pt, 1e-7f);
+    const float at = y * c.alpha + (1.0f - y) * (1.0f - c.alpha);
+    const float focal = powf(1.0f - pt, c.gamma);
+    return -at * focal * robust * 1.0f * logf(pt);
+  }
+  // softmax cross entropy (src/boosting/loss.cpp:273-285 softmax)
+  float mx = pr[0];
+  for (int k = 1; k < c.K; ++k) mx = fmaxf(mx, pr[k]);
+  float sum = 0.0f, el = 0.0f;
+  const int label = (int)y;
+  for (int k = 0; k < c.K; ++k) {
+    const float e = expf(pr[k] - mx);
+    sum += e;
+    if (k == label) el = e;
+  }
+  return -logf(fmaxf(el / sum, 1e-7f));
+}
+
+__global__ void __launch_bounds__(256) k_valid(DevCfg c, DevPtrs P) {
+  __shared__ double s_part[256];
+  __shared__ bool s_last;
+  const int it = *P.iter;
+  EsState* es = P.es;
+  const bool stopped = es->stopped != 0;
+  const int L = 1 << c.D;
+  double part = 0.0;
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < c.nv; r += gridDim.x * blockDim.x) {
+    float pr[kMaxClasses];
+    const float* xr = P.xv + (size_t)r * c.f;
+    for (int k = 0; k < c.K; ++k) {
+      float vp = P.vpred[(size_t)k * c.nv + r];
+      if (!stopped) {
+        const size_t t = (size_t)it * c.KT + c.k0 + k;
+        const int dep = P.m_depth[t];
+        uint32_t idx = 0;
+        for (int d = 0; d < dep; ++d)
+          idx = (idx << 1) | (uint32_t)(xr[P.m_feat[t * c.D + d]] >= P.m_thr[t * c.D + d]);  // false for NaN
+        vp = __fmaf_rn(c.lr, P.m_leaves[t * L + idx], vp);
+        P.vpred[(size_t)k * c.nv + r] = vp;
+      }
+      pr[k] = vp;
+    }
+    part += (double)valid_term(c, pr, P.yv[r]);
+  }
+  s_part[threadIdx.x] = part;
+  __syncthreads();
+  for (int h = 128; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h) s_part[threadIdx.x] += s_part[threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    P.vpart[blockIdx.x] = s_part[0];
+    __threadfence();
+    s_last = atomicAdd(&es->ctr, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last || threadIdx.x != 0) return;
+  __threadfence();
+  es->ctr = 0;
+  double sum = 0.0;
+  for (int b = 0; b < (int)gridDim.x; ++b) sum += P.vpart[b];
+  const float loss = (float)(sum / (double)c.nv);
+  P.vloss[it] = sum / (double)c.nv;
+  if (stopped) return;
+  if (loss < es->best - 1e-10f) {
+    es->best = loss;
+    es->best_iter = it;
+    es->no_improve = 0;
+  } else {
+    ++es->no_improve;
+  }
+  if (c.es_rounds >= 0 && it >= c.es_min_iter && es->no_improve >= c.es_rounds) {
+    es->stopped = 1;
+    es->stop_iter = it;
+  }
+}
+
 __global__ void k_fill_f32(float* p, size_t n, float v) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
 }
@@ -1345,6 +1470,13 @@ struct tc_trainer {
   DevBuf<float> m_thr, m_leaves;
   DevBuf<double> m_gain, m_second;
   DevBuf<double> root_hist;
+  // validation set and early stopping (optional)
+  const tc_dataset* vds = nullptr;
+  DevBuf<float> vpred;
+  DevBuf<double> vpart, vloss;
+  DevBuf<EsState> es;
+  bool es_stopped = false;       // the host has seen the stopping rule fire
+  int best_iter = -1;
 
   ~tc_trainer() {
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
@@ -1379,6 +1511,8 @@ struct tc_trainer {
   tc_status enqueue_iteration(cudaStream_t st);
   tc_status run_plain_iteration(cudaStream_t st);
   tc_status init_predictions();
+  tc_status init_validation();
+  tc_status set_validation(const tc_dataset* v, int rounds);
   tc_status step(int iters, bool sync);
 };
 
@@ -1649,6 +1783,11 @@ tc_status tc_trainer::enqueue_iteration(cudaStream_t st) {
   k_node_reduce<true><<<dim3(1, K), 512, 0, st>>>(cfg, ptr, -1);  // + plan of level 0
   mark_end(st);
   for (int d = 0; d < D; ++d) launch_level(cfg, ptr, d, st);
+  if (cfg.nv > 0) {
+    mark_begin(KC_OTHER, st);
+    k_valid<<<VALID_BLOCKS, 256, 0, st>>>(cfg, ptr);
+    mark_end(st, (double)cfg.nv * (cfg.f * 4.0 + 4.0 + cfg.K * 8.0));
+  }
   mark_begin(KC_OTHER, st);
   k_next_iter<<<1, 1, 0, st>>>(ptr);
   mark_end(st);
@@ -1694,6 +1833,7 @@ tc_status tc_trainer::run_plain_iteration(cudaStream_t st) {
       launch_level(one, pk, d, st);
     }
   }
+  if (cfg.nv > 0) k_valid<<<VALID_BLOCKS, 256, 0, st>>>(cfg, ptr);
   k_next_iter<<<1, 1, 0, st>>>(ptr);
   TC_CUDA(ctx, cudaGetLastError());
   return TC_OK;
@@ -1734,7 +1874,52 @@ tc_status tc_trainer::init_predictions() {
   TC_CUDA(ctx, cudaStreamSynchronize(st));
   iters_done = 0;
   seconds = 0.0;
+  if (cfg.nv > 0) TC_TRY(init_validation());
   return TC_OK;
+}
+
+// Validation predictions start at the base prediction (booster.cpp:93-96),
+// the stopping state at best = 1e30 (booster.cpp:119-121).
+tc_status tc_trainer::init_validation() {
+  cudaStream_t st = ctx->stream;
+  k_fill_f32<<<4 * ctx->sm_count, 256, 0, st>>>(vpred.p, (size_t)cfg.K * cfg.nv, base);
+  TC_CUDA(ctx, cudaGetLastError());
+  EsState h{};
+  h.best = 1e30f;
+  h.best_iter = 0;
+  h.stop_iter = -1;
+  TC_CUDA(ctx, cudaMemcpyAsync(es.p, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+  TC_CUDA(ctx, cudaMemsetAsync(vloss.p, 0, vloss.bytes(), st));
+  TC_CUDA(ctx, cudaStreamSynchronize(st));
+  es_stopped = false;
+  best_iter = -1;
+  return TC_OK;
+}
+
+tc_status tc_trainer::set_validation(const tc_dataset* v, int rounds) {
+  if (v->ctx != ctx) return ctx->fail(TC_ERR_INVALID_ARG, "validation set belongs to another context");
+  if (v->f != cfg.f) return ctx->fail(TC_ERR_INVALID_ARG, "validation set has %u features, training %u", v->f, cfg.f);
+  if (v->n == 0 || v->y.n < v->n) return ctx->fail(TC_ERR_INVALID_ARG, "validation set needs rows and labels");
+  if (iters_done > 0) return ctx->fail(TC_ERR_INVALID_ARG, "set the validation set before the first iteration");
+  vds = v;
+  cfg.nv = v->n;
+  cfg.es_rounds = rounds;
+  cfg.es_min_iter = std::max(50, prm.n_estimators / 10);
+  TC_TRY(vpred.alloc(ctx, (size_t)cfg.K * v->n, "validation predictions"));
+  TC_TRY(vpart.alloc(ctx, VALID_BLOCKS, "validation partial losses"));
+  TC_TRY(vloss.alloc(ctx, std::max(1, prm.n_estimators), "validation losses"));
+  TC_TRY(es.alloc(ctx, 1, "early-stopping state"));
+  ptr.xv = v->X.p;
+  ptr.yv = v->y.p;
+  ptr.vpred = vpred.p;
+  ptr.vpart = vpart.p;
+  ptr.vloss = vloss.p;
+  ptr.es = es.p;
+  if (graph) {
+    cudaGraphExecDestroy(graph);
+    graph = nullptr;
+  }
+  return init_validation();
 }
 
 tc_status tc_trainer::step(int iters, bool sync) {
@@ -1742,8 +1927,53 @@ tc_status tc_trainer::step(int iters, bool sync) {
   if (iters < 0 || iters_done + iters > prm.n_estimators)
     return ctx->fail(TC_ERR_INVALID_ARG, "step(%d) exceeds n_estimators=%d (done %d)", iters,
                      prm.n_estimators, iters_done);
-  if (iters == 0) return TC_OK;
+  if (iters == 0 || es_stopped) return TC_OK;
   TC_CUDA(ctx, cudaEventRecord(ev0, st));
+  if (cfg.nv > 0) {
+    // with a validation set: chunks of iterations, then a look at the
+    // stopping state; iterations launched past the stop grow no tree
+    const int chunk = 8;
+    int done = 0;
+    while (done < iters && !es_stopped) {
+      const int m = std::min(chunk, iters - done);
+      if (prm.batched) {
+        if (!graph) {
+          cudaGraph_t g;
+          const int64_t l0 = launches;
+          TC_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+          enqueue_iteration(st);
+          TC_CUDA(ctx, cudaStreamEndCapture(st, &g));
+          launches_per_iter = (int)(launches - l0);
+          launches = l0;
+          cudaError_t e = cudaGraphInstantiate(&graph, g, 0);
+          cudaGraphDestroy(g);
+          if (e != cudaSuccess) return ctx->cuda_fail(e, "cudaGraphInstantiate");
+        }
+        for (int i = 0; i < m; ++i) TC_CUDA(ctx, cudaGraphLaunch(graph, st));
+        launches += (int64_t)launches_per_iter * m;
+      } else {
+        for (int i = 0; i < m; ++i) TC_TRY(run_plain_iteration(st));
+      }
+      EsState h{};
+      TC_CUDA(ctx, cudaMemcpyAsync(&h, es.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+      TC_CUDA(ctx, cudaStreamSynchronize(st));
+      done += m;
+      best_iter = h.best_iter;
+      if (h.stopped) {
+        es_stopped = true;
+        done = h.stop_iter + 1 - iters_done;  // trees up to and including the stopping iteration
+      }
+    }
+    TC_CUDA(ctx, cudaEventRecord(ev1, st));
+    TC_CUDA(ctx, cudaGetLastError());
+    iters_done += done;
+    scores_dirty = true;
+    TC_CUDA(ctx, cudaEventSynchronize(ev1));
+    float ms = 0.0f;
+    TC_CUDA(ctx, cudaEventElapsedTime(&ms, ev0, ev1));
+    seconds += ms * 1e-3;
+    return TC_OK;
+  }
   if (prm.batched) {
     if (!graph) {
       cudaGraph_t g;
@@ -1843,6 +2073,29 @@ tc_status tc_trainer_stats(tc_trainer* tr, tc_train_stats* st) {
   st->hist_features_per_block = tr->cfg.W;
   st->hist_rows_per_chunk = tr->cfg.rows_fixed ? tr->cfg.rows_fixed : -tr->cfg.target_items;
   st->kernel_launches = tr->launches;
+  st->best_iteration = tr->cfg.nv > 0 ? tr->best_iter : -1;
+  st->stopped_early = tr->es_stopped ? 1 : 0;
+  return TC_OK;
+}
+
+tc_status tc_trainer_set_validation(tc_trainer* tr, const tc_dataset* valid, int32_t early_stopping_rounds) {
+  if (!tr || !valid) return TC_ERR_INVALID_ARG;
+  std::lock_guard<std::recursive_mutex> train_lock(tr->ctx->train_mu);
+  cudaSetDevice(tr->ctx->device);
+  return tr->set_validation(valid, early_stopping_rounds);
+}
+
+tc_status tc_trainer_valid_loss(tc_trainer* tr, double* out) {
+  if (!tr || !out) return TC_ERR_INVALID_ARG;
+  tc_ctx* ctx = tr->ctx;
+  std::lock_guard<std::recursive_mutex> train_lock(ctx->train_mu);
+  if (tr->cfg.nv == 0) return ctx->fail(TC_ERR_INVALID_ARG, "no validation set");
+  cudaSetDevice(ctx->device);
+  if (tr->iters_done > 0) {
+    TC_CUDA(ctx, cudaMemcpyAsync(out, tr->vloss.p, tr->iters_done * sizeof(double), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+    TC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
   return TC_OK;
 }
 

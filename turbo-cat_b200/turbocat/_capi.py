@@ -27,7 +27,7 @@ SYMBOLS = [
     "tc_ctx_create", "tc_ctx_destroy", "tc_last_error", "tc_ctx_memory", "tc_ctx_fail_next_allocs",
     "tc_ctx_synchronize", "tc_dataset_upload", "tc_dataset_destroy", "tc_quantize", "tc_dataset_bins",
     "tc_trainer_create", "tc_trainer_step", "tc_trainer_reset", "tc_trainer_stats", "tc_trainer_profile",
-    "tc_trainer_train_scores",
+    "tc_trainer_train_scores", "tc_trainer_set_validation", "tc_trainer_valid_loss",
     "tc_trainer_model", "tc_trainer_destroy", "tc_train", "tc_build_tree", "tc_histogram_root_noalloc",
     "tc_model_info_get", "tc_model_export",
     "tc_model_import", "tc_model_save_tcat", "tc_model_load_tcat", "tc_model_destroy", "tc_predict",
@@ -50,7 +50,8 @@ class TrainParams(C.Structure):
 class TrainStats(C.Structure):
     _fields_ = [("n_trees", C.c_int32), ("iterations_done", C.c_int32), ("base_prediction", C.c_float),
                 ("seconds", C.c_double), ("hist_features_per_block", C.c_int32),
-                ("hist_rows_per_chunk", C.c_int32), ("kernel_launches", C.c_int64)]
+                ("hist_rows_per_chunk", C.c_int32), ("kernel_launches", C.c_int64),
+                ("best_iteration", C.c_int32), ("stopped_early", C.c_int32)]
 
 
 class KernelTime(C.Structure):
@@ -211,6 +212,17 @@ class Trainer:
                for i in range(pr.n_kernels)}
         out["_hist_levels"] = [(pr.hist_level_ms[d], pr.hist_level_rows[d]) for d in range(16)]
         return out
+
+    def set_validation(self, vds, early_stopping_rounds=50):
+        """Validation set (a Dataset with labels, not necessarily quantized) and
+        early stopping; call before the first step."""
+        self.vds = vds  # must outlive the trainer
+        self.eng._chk(lib().tc_trainer_set_validation(self.h, vds.h, C.c_int32(early_stopping_rounds)))
+
+    def valid_loss(self):
+        out = np.zeros(max(1, self.stats().iterations_done), np.float64)
+        self.eng._chk(lib().tc_trainer_valid_loss(self.h, _p(out)))
+        return out[: self.stats().iterations_done]
 
     def scores(self, n):
         out = np.zeros((n, self.K), np.float32)
