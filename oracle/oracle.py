@@ -59,6 +59,9 @@ class FitParams(C.Structure):
         ("focal_gamma", C.c_float),
         ("focal_alpha", C.c_float),
         ("tree", TreeParams),
+        ("subsample", C.c_float),
+        ("colsample_bytree", C.c_float),
+        ("seed", C.c_uint64),
     ]
 
 
@@ -97,6 +100,9 @@ class Hyper:
     max_delta_step: float = 0.0
     focal_gamma: float = 2.0
     focal_alpha: float = 0.25
+    subsample: float = 1.0          # row sampling per iteration (BoostingConfig::subsample)
+    colsample_bytree: float = 1.0   # advances the random state only (symmetric trees ignore it)
+    seed: int = 42                  # Config::seed
 
     def tree(self) -> TreeParams:
         return TreeParams(self.max_depth, self.max_bins, self.min_samples_leaf, self.lambda_l2,
@@ -106,7 +112,7 @@ class Hyper:
     def fit(self) -> FitParams:
         return FitParams(LOSS_IDS[self.loss], self.n_classes if self.loss == "softmax" else 1,
                          self.n_estimators, self.learning_rate, self.focal_gamma,
-                         self.focal_alpha, self.tree())
+                         self.focal_alpha, self.tree(), self.subsample, self.colsample_bytree, self.seed)
 
     def ref(self) -> RefParams:
         return RefParams(LOSS_IDS[self.loss], self.n_classes if self.loss == "softmax" else 2,

@@ -310,6 +310,14 @@ int tco_build_tree(const uint8_t* bins, uint32_t n, uint32_t f, const float* edg
                    const uint16_t* n_edges, const float* g, const float* h,
                    const tco_tree_params* p, int32_t mode, tco_tree* out, float* leaf_values,
                    uint32_t* leaf_index, double* root_hist) {
+  return tco_build_tree_rows(bins, n, f, edges, n_edges, g, h, p, mode, NULL, n, out, leaf_values,
+                             leaf_index, root_hist);
+}
+
+int tco_build_tree_rows(const uint8_t* bins, uint32_t n, uint32_t f, const float* edges,
+                        const uint16_t* n_edges, const float* g, const float* h,
+                        const tco_tree_params* p, int32_t mode, const uint32_t* rows0, uint32_t n0,
+                        tco_tree* out, float* leaf_values, uint32_t* leaf_index, double* root_hist) {
   const int32_t D = p->max_depth;
   if (D < 0 || D > TCO_MAX_DEPTH) return -1;
   const uint32_t max_nodes = 1u << D;
@@ -346,13 +354,15 @@ int tco_build_tree(const uint8_t* bins, uint32_t n, uint32_t f, const float* edg
   int rc = 0;
   if (!rows_cur || !rows_nxt || !start || !cnt || (!H32 && !H64) || (!N32 && !N64)) { rc = -2; goto done; }
 
-  for (uint32_t i = 0; i < n; ++i) rows_cur[i] = i;
+  if (!rows0) n0 = n;
+  for (uint32_t i = 0; i < n0; ++i) rows_cur[i] = rows0 ? rows0[i] : i;
   start[0] = 0;
-  cnt[0] = n;
+  cnt[0] = n0;
   {
     float G = 0.0f, H = 0.0f;
     double G64 = 0.0, H64s = 0.0;
-    for (uint32_t i = 0; i < n; ++i) {
+    for (uint32_t q = 0; q < n0; ++q) {
+      const uint32_t i = rows_cur[q];
       G += g[i]; H += h[i];
       G64 += (double)g[i]; H64s += (double)h[i];
     }
@@ -373,8 +383,8 @@ int tco_build_tree(const uint8_t* bins, uint32_t n, uint32_t f, const float* edg
     if (stop) break;
 
     if (d == 0) {
-      if (mode == TCO_REF32) hist32(bins, n, f, g, h, rows_cur, n, H32);
-      else hist64(bins, n, f, g, h, rows_cur, n, H64);
+      if (mode == TCO_REF32) hist32(bins, n, f, g, h, rows_cur, n0, H32);
+      else hist64(bins, n, f, g, h, rows_cur, n0, H64);
       if (root_hist) {
         for (size_t q = 0; q < hsz; ++q) {
           root_hist[2 * q] = mode == TCO_REF32 ? (double)H32[q].g : H64[q].g;
@@ -611,7 +621,15 @@ int tco_fit(const uint8_t* bins, uint32_t n, uint32_t f, const float* edges,
   double min_margin = 1e300;
   int rc = 0;
   size_t t = 0;
+  uint64_t rng = p->seed;
+  const int sampling = p->subsample < 1.0f;
+  uint32_t* sample = sampling ? (uint32_t*)malloc((size_t)(n ? n : 1) * sizeof(uint32_t)) : NULL;
   for (int32_t it = 0; it < p->n_estimators; ++it) {
+    /* sample selection (booster.cpp:198-228): rows, then one draw for the
+     * feature subset, which the symmetric build does not use */
+    uint32_t n_sample = n;
+    if (sampling) n_sample = tco_random_subsample(n, p->subsample, tco_next_random(&rng), sample);
+    if (p->colsample_bytree < 1.0f) (void)tco_next_random(&rng);
     if (p->loss == TCO_LOSS_LOGLOSS) tco_grad_logloss(y, pred, gg, hh, n);
     else if (p->loss == TCO_LOSS_MSE) tco_grad_mse(y, pred, gg, hh, n);
     else if (p->loss == TCO_LOSS_FOCAL) tco_grad_focal(y, pred, gg, hh, n, p->focal_gamma, p->focal_alpha);
@@ -627,8 +645,21 @@ int tco_fit(const uint8_t* bins, uint32_t n, uint32_t f, const float* edges,
       }
       tco_tree tr;
       memset(lv, 0, (size_t)L * sizeof(float));
-      rc = tco_build_tree(bins, n, f, edges, n_edges, gsrc, hsrc, &p->tree, mode, &tr, lv, li, NULL);
+      rc = tco_build_tree_rows(bins, n, f, edges, n_edges, gsrc, hsrc, &p->tree, mode, sample, n_sample, &tr, lv,
+                               li, NULL);
       if (rc) goto done;
+      if (sampling) {
+        /* every row's leaf (SymmetricTree::predict_batch on the bins,
+         * src/tree/symmetric_tree.cpp:813-840): bin != 255 && bin > t goes right */
+        for (uint32_t i = 0; i < n; ++i) {
+          uint32_t idx = 0;
+          for (int32_t d = 0; d < tr.depth; ++d) {
+            const uint8_t b = bins[(size_t)tr.feature[d] * n + i];
+            idx = (idx << 1) | (uint32_t)(b != TCO_NAN_BIN && b > tr.bin[d]);
+          }
+          li[i] = idx;
+        }
+      }
       depth[t] = tr.depth;
       for (int32_t d = 0; d < D; ++d) {
         feature[t * D + d] = d < tr.depth ? tr.feature[d] : 0;
@@ -652,7 +683,7 @@ int tco_fit(const uint8_t* bins, uint32_t n, uint32_t f, const float* edges,
   if (train_pred) memcpy(train_pred, pred, (size_t)n * K * sizeof(float));
   if (min_margin_out) *min_margin_out = min_margin;
 done:
-  free(pred); free(gg); free(hh); free(gk); free(hk); free(li); free(lv);
+  free(pred); free(gg); free(hh); free(gk); free(hk); free(li); free(lv); free(sample);
   return rc;
 }
 

@@ -80,6 +80,12 @@ int tco_build_tree(const uint8_t* bins, uint32_t n, uint32_t f, const float* edg
                    const uint16_t* n_edges, const float* g, const float* h,
                    const tco_tree_params* p, int32_t mode, tco_tree* out, float* leaf_values,
                    uint32_t* leaf_index, double* root_hist);
+/* The same over the rows of `rows0` (n0 of them, in that order: FP32 sums
+ * follow the list order); rows0 = NULL: all rows. */
+int tco_build_tree_rows(const uint8_t* bins, uint32_t n, uint32_t f, const float* edges,
+                        const uint16_t* n_edges, const float* g, const float* h,
+                        const tco_tree_params* p, int32_t mode, const uint32_t* rows0, uint32_t n0,
+                        tco_tree* out, float* leaf_values, uint32_t* leaf_index, double* root_hist);
 
 /* FP64 level histograms for an arbitrary node assignment: out[node][f][256][2]. */
 void tco_histogram(const uint8_t* bins, uint32_t n, uint32_t f, const float* g, const float* h,
@@ -100,7 +106,20 @@ typedef struct {
   float focal_gamma;
   float focal_alpha;
   tco_tree_params tree;
+  /* row sampling (src/boosting/booster.cpp:198-228): subsample < 1 builds
+   * each iteration's trees on the rows random_subsample picks (in its
+   * order); colsample_bytree < 1 only advances the random state (the
+   * symmetric build ignores the feature subset); seed = Config::seed. */
+  float subsample;
+  float colsample_bytree;
+  uint64_t seed;
 } tco_fit_params;
+
+/* xorshift64* step (src/boosting/booster.cpp:1219-1225). */
+uint64_t tco_next_random(uint64_t* state);
+/* src/core/dataset.cpp:552-562: writes the first (uint32)(n * ratio)
+ * shuffled row ids to out, returns their count. */
+uint32_t tco_random_subsample(uint32_t n, float ratio, uint64_t seed, uint32_t* out);
 
 int tco_fit(const uint8_t* bins, uint32_t n, uint32_t f, const float* edges,
             const uint16_t* n_edges, const float* y, const tco_fit_params* p, int32_t mode,

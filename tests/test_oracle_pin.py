@@ -147,3 +147,45 @@ def test_early_stopping_replay_matches_reference():
     losses, stop, best = O.early_stopping(e, Xv, yv, "logloss", 200, 10, 0.3)
     assert stop >= 50 and best < stop  # the rule fired after the minimum iterations
     assert ref_trees == stop + 1
+
+
+_SS_SCRIPT = r"""
+import sys, os, tempfile
+sys.path[:0] = [sys.argv[1], sys.argv[2]]
+import _turbocat as ref
+from datagen import binary_c1
+X, y = binary_c1(20000, 12, seed=91)
+m = ref.TurboCatClassifier(n_estimators=6, learning_rate=0.1, max_depth=5, max_bins=255, subsample=0.8,
+                           colsample_bytree=0.8, min_child_weight=1.0, lambda_l2=1.0, loss="logloss",
+                           mode="large", verbosity=0, seed=42)
+m.fit(X, y)
+path = os.path.join(tempfile.mkdtemp(), "m.tcat")
+m.save(path)
+sys.stdout.write(path)
+"""
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference build (oracle/_ref) not present")
+def test_row_sampling_matches_reference():
+    """subsample = colsample_bytree = 0.8 (the facade's defaults), seed 42:
+    the oracle's row sampling (xorshift64* draws, std::shuffle with
+    std::mt19937_64, trees built over the sampled rows in their shuffled
+    order) reproduces the reference's fit bit for bit."""
+    import os
+    import subprocess
+    import sys
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    out = subprocess.run([sys.executable, "-c", _SS_SCRIPT, here, os.path.join(O.HERE, "_ref")],
+                         capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr
+    r = O.parse_tcat(open(out.stdout.strip().splitlines()[-1], "rb").read())
+    X, y = binary_c1(20000, 12, seed=91)
+    hp = O.Hyper(loss="logloss", n_estimators=6, learning_rate=0.1, max_depth=5, lambda_l2=1.0, subsample=0.8,
+                 colsample_bytree=0.8, seed=42)
+    e = O.fit(O.quantize(X), y, hp, mode=0)
+    assert np.array_equal(r.feature, e.feature) and np.array_equal(r.bin, e.bin)
+    assert np.array_equal(_u32(r.leaves), _u32(e.leaves))
+    full = O.fit(O.quantize(X), y, O.Hyper(loss="logloss", n_estimators=6, learning_rate=0.1, max_depth=5,
+                                           lambda_l2=1.0), mode=0)
+    assert not np.array_equal(full.leaves, e.leaves)  # sampling changed the trees
