@@ -119,6 +119,16 @@ typedef struct {
                                host synchronisation per level */
   int32_t hist_features_per_block; /* 0 = autotune; else 32 or 64 (other values: 32) */
   int32_t hist_rows_per_chunk;     /* 0 = autotune */
+  /* Row sampling, Booster::train's sample selection (src/boosting/booster.cpp:198-228):
+   * with 0 < subsample < 1 every iteration's trees are built on the first
+   * (uint32)(n * subsample) rows of a std::shuffle (std::mt19937_64 seeded by
+   * an xorshift64* draw from `seed`, src/core/dataset.cpp:552-562) and
+   * applied to all rows; with 0 < colsample_bytree < 1 one more draw per
+   * iteration (the reference's feature subset, which its symmetric trees do
+   * not use).  0 or >= 1: no sampling / no draw. */
+  float subsample;
+  float colsample_bytree;
+  uint64_t seed;                    /* Config::seed (default 42 in the reference) */
 } tc_train_params;
 
 typedef struct {

@@ -230,12 +230,15 @@ class TurboCatClassifier {
     p_.min_child_weight = min_child_weight;
     p_.lambda_l2 = lambda_l2;
     (void)goss_top_rate; (void)goss_other_rate; (void)use_symmetric; (void)grow_policy;
+    p_.subsample = subsample;
+    p_.colsample_bytree = colsample_bytree;
+    p_.seed = (uint64_t)(int64_t)seed;
     es_rounds_ = early_stopping_rounds;
     if (early_stopping_metric != "loss" && early_stopping_metric != "logloss")
       warn("early_stopping_metric '" + early_stopping_metric + "' is not on the device path; the validation "
            "loss is used (the reference's fallback for metrics it does not know)");
     (void)cat_encoding; (void)max_interactions;
-    (void)interaction_method; (void)n_threads; (void)seed;
+    (void)interaction_method; (void)n_threads;
   }
 
   void fit(FArray X, FArray y, FArray X_val, FArray y_val, std::vector<int> cat_features) {
@@ -245,7 +248,7 @@ class TurboCatClassifier {
     const uint16_t f = (uint16_t)X.shape(1);
     if ((size_t)y.shape(0) != n) throw std::runtime_error("X and y have different numbers of rows");
     if (mode_ == "small") warn("mode='small' (regular trees) is not on the device path; building symmetric trees");
-    if (subsample_ < 1.0f || use_goss_) warn("row sampling is not on the device path; every iteration uses all rows");
+    if (use_goss_) warn("GOSS sampling is not on the device path; random subsampling (subsample) is used");
     if (colsample_ < 1.0f && verbosity_ > 1) warn("colsample_bytree has no effect on symmetric trees");
     if (use_gradtree_ || use_ordered_ || auto_interactions_)
       warn("use_gradtree / use_ordered_boosting / auto_interactions are not on the device path and are ignored");
@@ -417,8 +420,11 @@ class TurboCatRegressor {
     p_.min_child_weight = min_child_weight;
     if (!(loss == "mse" || loss == "l2"))
       throw std::invalid_argument("loss '" + loss + "' is not on the device path (mse)");
-    (void)colsample_bytree; (void)goss_top_rate; (void)goss_other_rate; (void)early_stopping_rounds;
-    (void)max_leaves; (void)grow_policy; (void)n_threads; (void)seed;
+    p_.subsample = subsample;
+    p_.colsample_bytree = colsample_bytree;
+    p_.seed = (uint64_t)(int64_t)seed;
+    (void)goss_top_rate; (void)goss_other_rate; (void)early_stopping_rounds;
+    (void)max_leaves; (void)grow_policy; (void)n_threads;
   }
 
   void fit(FArray X, FArray y) {
@@ -427,7 +433,7 @@ class TurboCatRegressor {
     const uint16_t f = (uint16_t)X.shape(1);
     if ((size_t)y.size() != n) throw std::runtime_error("X and y have different numbers of rows");
     if (mode_ == "small") warn("mode='small' (regular trees) is not on the device path; building symmetric trees");
-    if (subsample_ < 1.0f || use_goss_) warn("row sampling is not on the device path; every iteration uses all rows");
+    if (use_goss_) warn("GOSS sampling is not on the device path; random subsampling (subsample) is used");
     {
       py::gil_scoped_release nogil;
       booster_.reset(new GpuBooster());

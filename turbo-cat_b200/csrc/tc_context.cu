@@ -114,10 +114,13 @@ tc_status tc_ctx_fail_next_allocs(tc_ctx* ctx, int count) {
 // stuck device turns into TC_ERR_TIMEOUT rather than a hung caller.
 tc_status tc_ctx_synchronize(tc_ctx* ctx, int timeout_ms) {
   if (!ctx) return TC_ERR_INVALID_ARG;
+  // not while another thread's training call may be capturing the stream
+  std::lock_guard<std::recursive_mutex> train_lock(ctx->train_mu);
   cudaSetDevice(ctx->device);
   const auto t0 = std::chrono::steady_clock::now();
   for (;;) {
     cudaError_t e = cudaStreamQuery(ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamQuery(ctx->pred_stream);
     if (e == cudaSuccess) return TC_OK;
     if (e != cudaErrorNotReady) return ctx->cuda_fail(e, "stream");
     const auto dt = std::chrono::duration_cast<std::chrono::milliseconds>(

@@ -37,7 +37,11 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <numeric>
+#include <random>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "tc_internal.h"
 
@@ -101,6 +105,7 @@ struct DevCfg {
   uint32_t nv;                   // validation rows (0: no validation set)
   int32_t es_rounds;             // early_stopping_rounds (< 0: never stop)
   int32_t es_min_iter;           // first iteration the stopping rule may fire at
+  int32_t sampled;               // 1: only the rows of smask grow this iteration's trees
 };
 
 struct DevPtrs {
@@ -151,7 +156,12 @@ struct DevPtrs {
   double* vpart;                 // [VALID_BLOCKS] partial loss sums
   double* vloss;                 // [n_estimators] validation loss per iteration
   EsState* es;
+  const uint32_t* smask;         // [ceil(n/32)] rows sampled this iteration (bit per row)
 };
+
+__device__ __forceinline__ bool row_sampled(const DevCfg& c, const DevPtrs& P, uint32_t i) {
+  return !c.sampled || ((P.smask[i >> 5] >> (i & 31)) & 1u);
+}
 
 __device__ __forceinline__ size_t hist_index(const DevCfg& c, int k, int node, int f, int b) {
   return (((size_t)k * (1u << (c.D > 0 ? c.D - 1 : 0)) + node) * c.f + f) * kSlots + b;
@@ -246,9 +256,17 @@ __global__ void __launch_bounds__(512) k_grad(DevCfg c, DevPtrs P, int use_given
         loss_grad(c.loss, P.pred[i], P.y[i], i, n_vec, c.gamma, c.alpha, g, h);
         P.gh[i] = make_float2(g, h);
       }
+      // rows outside this iteration's sample add nothing to any sum
+      if (!row_sampled(c, P, i))
+        for (int k = 0; k < K; ++k) P.gh[(size_t)k * c.n + i] = make_float2(0.0f, 0.0f);
     }
     for (int k = 0; k < K; ++k) P.leaf[(size_t)k * c.n + i] = 0;
   }
+  __shared__ uint32_t sCnt[16];
+  uint32_t my_cnt = 0;
+  for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) my_cnt += row_sampled(c, P, i) ? 1u : 0u;
+  for (int o = 16; o; o >>= 1) my_cnt += __shfl_down_sync(0xffffffffu, my_cnt, o);
+  if ((threadIdx.x & 31) == 0) sCnt[threadIdx.x >> 5] = my_cnt;
   // root sums per class: thread-local in row order, then a fixed-order block reduction
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int k = 0; k < K; ++k) {
@@ -268,8 +286,10 @@ __global__ void __launch_bounds__(512) k_grad(DevCfg c, DevPtrs P, int use_given
       double tg = 0.0, th = 0.0;
       for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { tg += sG[w]; th += sH[w]; }
       const size_t o = ((size_t)k * c.PB + blockIdx.x) * L;
+      uint32_t cnt = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) cnt += sCnt[w];
       P.psum[o] = make_double2(tg, th);
-      P.pcnt[o] = r1 > r0 ? r1 - r0 : 0;
+      P.pcnt[o] = cnt;
     }
     __syncthreads();
   }
@@ -947,6 +967,7 @@ __global__ void __launch_bounds__(PART_THREADS) k_partition(DevCfg c, DevPtrs P,
         nl = (int)(((uint32_t)lf[u] << 1) | right);
         leaf[i] = (uint16_t)nl;
         w = v[u];
+        if (!row_sampled(c, P, i)) nl = -1;  // its leaf moves on; it is not counted
       }
       if (nch <= 4) {
         for (int cc = 0; cc < nch; ++cc) {
@@ -1277,7 +1298,7 @@ __global__ void __launch_bounds__(PART_THREADS) k_scatter(DevCfg c, DevPtrs P, i
     for (int u = 0; u < SCAT_UNROLL; ++u) {
       const uint32_t i = base + u * blockDim.x + threadIdx.x;
       key[u] = -1;
-      if (i < r1) {
+      if (i < r1 && row_sampled(c, P, i)) {
         const int ch = leaf[i];
         if (ch == s_small[ch >> 1]) key[u] = ch >> 1;
       }
@@ -1477,8 +1498,18 @@ struct tc_trainer {
   DevBuf<EsState> es;
   bool es_stopped = false;       // the host has seen the stopping rule fire
   int best_iter = -1;
+  // row sampling (optional): per-iteration bit masks made on the host
+  bool sampling = false;
+  uint64_t rng_state = 0;
+  DevBuf<uint32_t> smask;
+  uint32_t* h_mask = nullptr;    // pinned: 2 sets x SAMPLE_CHUNK masks
+  cudaEvent_t mask_ev[2] = {nullptr, nullptr};
+  int mask_set = 0;
 
   ~tc_trainer() {
+    for (cudaEvent_t e : mask_ev)
+      if (e) cudaEventDestroy(e);
+    if (h_mask) cudaFreeHost(h_mask);
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
     if (graph) cudaGraphExecDestroy(graph);
     if (ev0) cudaEventDestroy(ev0);
@@ -1513,6 +1544,9 @@ struct tc_trainer {
   tc_status init_predictions();
   tc_status init_validation();
   tc_status set_validation(const tc_dataset* v, int rounds);
+  tc_status enable_sampling();
+  void make_masks(int m, uint32_t* out);
+  tc_status launch_iterations(int m, cudaStream_t st);
   tc_status step(int iters, bool sync);
 };
 
@@ -1537,7 +1571,10 @@ tc_status tc_trainer::setup(int) {
   cfg.rows_min = 512;
   cfg.rows_fixed = prm.hist_rows_per_chunk > 0 ? prm.hist_rows_per_chunk : 0;
   // MSE's hessian is 2 for every row (src/boosting/loss.cpp:348-362)
-  cfg.hconst = (prm.loss == TC_LOSS_MSE && !given_gh) ? 2.0f : 0.0f;
+  // counted hessians need every listed row to carry h = 2; with row
+  // sampling the root lists all rows and the unsampled ones carry 0
+  cfg.hconst = (prm.loss == TC_LOSS_MSE && !given_gh && !(prm.subsample > 0.0f && prm.subsample < 1.0f))
+                   ? 2.0f : 0.0f;
 
   T_cap = prm.n_estimators * K;
   TC_TRY(pred.alloc(ctx, (size_t)K * n, "predictions"));
@@ -1874,7 +1911,64 @@ tc_status tc_trainer::init_predictions() {
   TC_CUDA(ctx, cudaStreamSynchronize(st));
   iters_done = 0;
   seconds = 0.0;
+  rng_state = prm.seed;  // Booster: rng_state_ = config_.seed (src/boosting/booster.cpp:35-41)
   if (cfg.nv > 0) TC_TRY(init_validation());
+  return TC_OK;
+}
+
+constexpr int SAMPLE_CHUNK = 8;  // iterations per host batch of sample masks / early-stopping look
+
+// Sample masks of the next m iterations, in iteration order: per iteration an
+// xorshift64* draw seeds the row shuffle (src/boosting/booster.cpp:213-217,
+// src/core/dataset.cpp:552-562: std::shuffle with std::mt19937_64, first
+// (uint32)(n * subsample) rows), then one draw for the feature subset when
+// colsample_bytree < 1 (booster.cpp:223-227; symmetric trees do not use it).
+// The shuffles run on host threads, one per iteration.
+void tc_trainer::make_masks(int m, uint32_t* out) {
+  auto next_random = [this]() {
+    uint64_t x = rng_state;
+    x ^= x >> 12;
+    x ^= x << 25;
+    x ^= x >> 27;
+    rng_state = x;
+    return x * 0x2545F4914F6CDD1DULL;
+  };
+  const uint32_t n = cfg.n;
+  const size_t words = (n + 31) / 32;
+  std::vector<uint64_t> seeds(m);
+  for (int i = 0; i < m; ++i) {
+    seeds[i] = next_random();
+    if (prm.colsample_bytree > 0.0f && prm.colsample_bytree < 1.0f) (void)next_random();
+  }
+  const float ratio = prm.subsample;
+  auto one = [n, words, ratio](uint64_t seed, uint32_t* w) {
+    const uint32_t keep = static_cast<uint32_t>(n * ratio);  // Index * Float, as the reference
+    std::vector<uint32_t> idx(n);
+    std::iota(idx.begin(), idx.end(), 0u);
+    std::mt19937_64 rng(seed);
+    std::shuffle(idx.begin(), idx.end(), rng);
+    std::memset(w, 0, words * sizeof(uint32_t));
+    for (uint32_t q = 0; q < keep; ++q) w[idx[q] >> 5] |= 1u << (idx[q] & 31);
+  };
+  std::vector<std::thread> th;
+  for (int i = 1; i < m; ++i) th.emplace_back(one, seeds[i], out + (size_t)i * words);
+  if (m > 0) one(seeds[0], out);
+  for (auto& t : th) t.join();
+}
+
+tc_status tc_trainer::enable_sampling() {
+  sampling = true;
+  const size_t words = (cfg.n + 31) / 32;
+  TC_TRY(smask.alloc(ctx, words, "row sample mask"));
+  TC_CUDA(ctx, cudaHostAlloc(reinterpret_cast<void**>(&h_mask), 2 * SAMPLE_CHUNK * words * sizeof(uint32_t),
+                             cudaHostAllocDefault));
+  for (cudaEvent_t& e : mask_ev) TC_CUDA(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  cfg.sampled = 1;
+  ptr.smask = smask.p;
+  if (graph) {
+    cudaGraphExecDestroy(graph);
+    graph = nullptr;
+  }
   return TC_OK;
 }
 
@@ -1922,6 +2016,48 @@ tc_status tc_trainer::set_validation(const tc_dataset* v, int rounds) {
   return init_validation();
 }
 
+// One or more iterations on the stream: the captured graph (or the plain
+// path); with row sampling each iteration is preceded by the copy of its
+// sample mask, the masks of a batch being made on the host while the
+// previous batch runs.
+tc_status tc_trainer::launch_iterations(int m, cudaStream_t st) {
+  if (prm.batched && !graph) {
+    cudaGraph_t g;
+    const int64_t l0 = launches;
+    TC_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    enqueue_iteration(st);
+    TC_CUDA(ctx, cudaStreamEndCapture(st, &g));
+    launches_per_iter = (int)(launches - l0);
+    launches = l0;
+    cudaError_t e = cudaGraphInstantiate(&graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return ctx->cuda_fail(e, "cudaGraphInstantiate");
+  }
+  const size_t words = (cfg.n + 31) / 32;
+  uint32_t* set = nullptr;
+  if (sampling) {
+    TC_CUDA(ctx, cudaEventSynchronize(mask_ev[mask_set]));  // the set's previous copies are done
+    set = h_mask + (size_t)mask_set * SAMPLE_CHUNK * words;
+    make_masks(m, set);
+  }
+  for (int i = 0; i < m; ++i) {
+    if (sampling)
+      TC_CUDA(ctx, cudaMemcpyAsync(smask.p, set + (size_t)i * words, words * sizeof(uint32_t),
+                                   cudaMemcpyHostToDevice, st));
+    if (prm.batched) {
+      TC_CUDA(ctx, cudaGraphLaunch(graph, st));
+      launches += launches_per_iter;
+    } else {
+      TC_TRY(run_plain_iteration(st));
+    }
+  }
+  if (sampling) {
+    TC_CUDA(ctx, cudaEventRecord(mask_ev[mask_set], st));
+    mask_set ^= 1;
+  }
+  return TC_OK;
+}
+
 tc_status tc_trainer::step(int iters, bool sync) {
   cudaStream_t st = ctx->stream;
   if (iters < 0 || iters_done + iters > prm.n_estimators)
@@ -1929,72 +2065,33 @@ tc_status tc_trainer::step(int iters, bool sync) {
                      prm.n_estimators, iters_done);
   if (iters == 0 || es_stopped) return TC_OK;
   TC_CUDA(ctx, cudaEventRecord(ev0, st));
-  if (cfg.nv > 0) {
-    // with a validation set: chunks of iterations, then a look at the
-    // stopping state; iterations launched past the stop grow no tree
-    const int chunk = 8;
-    int done = 0;
-    while (done < iters && !es_stopped) {
-      const int m = std::min(chunk, iters - done);
-      if (prm.batched) {
-        if (!graph) {
-          cudaGraph_t g;
-          const int64_t l0 = launches;
-          TC_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-          enqueue_iteration(st);
-          TC_CUDA(ctx, cudaStreamEndCapture(st, &g));
-          launches_per_iter = (int)(launches - l0);
-          launches = l0;
-          cudaError_t e = cudaGraphInstantiate(&graph, g, 0);
-          cudaGraphDestroy(g);
-          if (e != cudaSuccess) return ctx->cuda_fail(e, "cudaGraphInstantiate");
-        }
-        for (int i = 0; i < m; ++i) TC_CUDA(ctx, cudaGraphLaunch(graph, st));
-        launches += (int64_t)launches_per_iter * m;
-      } else {
-        for (int i = 0; i < m; ++i) TC_TRY(run_plain_iteration(st));
-      }
-      EsState h{};
-      TC_CUDA(ctx, cudaMemcpyAsync(&h, es.p, sizeof(h), cudaMemcpyDeviceToHost, st));
-      TC_CUDA(ctx, cudaStreamSynchronize(st));
-      done += m;
-      best_iter = h.best_iter;
-      if (h.stopped) {
-        es_stopped = true;
-        done = h.stop_iter + 1 - iters_done;  // trees up to and including the stopping iteration
-      }
-    }
-    TC_CUDA(ctx, cudaEventRecord(ev1, st));
-    TC_CUDA(ctx, cudaGetLastError());
-    iters_done += done;
-    scores_dirty = true;
-    TC_CUDA(ctx, cudaEventSynchronize(ev1));
-    float ms = 0.0f;
-    TC_CUDA(ctx, cudaEventElapsedTime(&ms, ev0, ev1));
-    seconds += ms * 1e-3;
-    return TC_OK;
-  }
-  if (prm.batched) {
-    if (!graph) {
-      cudaGraph_t g;
-      const int64_t l0 = launches;
-      TC_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-      enqueue_iteration(st);
-      TC_CUDA(ctx, cudaStreamEndCapture(st, &g));
-      launches_per_iter = (int)(launches - l0);
-      launches = l0;
-      cudaError_t e = cudaGraphInstantiate(&graph, g, 0);
-      cudaGraphDestroy(g);
-      if (e != cudaSuccess) return ctx->cuda_fail(e, "cudaGraphInstantiate");
-    }
-    for (int i = 0; i < iters; ++i) TC_CUDA(ctx, cudaGraphLaunch(graph, st));
-    launches += (int64_t)launches_per_iter * iters;
+  int done = 0;
+  if (cfg.nv == 0 && !sampling) {
+    TC_TRY(launch_iterations(iters, st));
+    done = iters;
   } else {
-    for (int i = 0; i < iters; ++i) TC_TRY(run_plain_iteration(st));
+    // batches of iterations; with a validation set a look at the stopping
+    // state after each (iterations launched past the stop grow no tree)
+    while (done < iters && !es_stopped) {
+      const int m = std::min(SAMPLE_CHUNK, iters - done);
+      TC_TRY(launch_iterations(m, st));
+      done += m;
+      if (cfg.nv > 0) {
+        EsState h{};
+        TC_CUDA(ctx, cudaMemcpyAsync(&h, es.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+        TC_CUDA(ctx, cudaStreamSynchronize(st));
+        best_iter = h.best_iter;
+        if (h.stopped) {
+          es_stopped = true;
+          done = h.stop_iter + 1 - iters_done;  // trees up to and including the stopping iteration
+        }
+      }
+    }
+    sync = true;
   }
   TC_CUDA(ctx, cudaEventRecord(ev1, st));
   TC_CUDA(ctx, cudaGetLastError());
-  iters_done += iters;
+  iters_done += done;
   scores_dirty = true;
   if (sync) {
     TC_CUDA(ctx, cudaEventSynchronize(ev1));
@@ -2042,6 +2139,8 @@ tc_status tc_trainer_create(tc_ctx* ctx, tc_dataset* ds, const tc_train_params* 
   if (s == TC_OK) s = tr->init_predictions();
   // tuning runs up to three throw-away iterations: it needs that many tree slots
   if (s == TC_OK && p->hist_features_per_block == 0 && p->n_estimators >= 3) s = tr->autotune();
+  // row sampling starts after tuning (the tuner's trial iterations use every row)
+  if (s == TC_OK && p->subsample > 0.0f && p->subsample < 1.0f) s = tr->enable_sampling();
   if (s != TC_OK) {
     delete tr;
     return s;
@@ -2110,7 +2209,14 @@ tc_status tc_trainer_profile(tc_trainer* tr, int32_t iterations, tc_profile* out
   std::vector<tc_trainer::ProfRec> recs;
   tr->prof = &recs;
   tr->ev_used = 0;
+  std::vector<uint32_t> mask;
+  if (tr->sampling) mask.resize((tr->cfg.n + 31) / 32);
   for (int i = 0; i < iterations; ++i) {
+    if (tr->sampling) {  // this iteration's row sample, as step() would use
+      tr->make_masks(1, mask.data());
+      TC_CUDA(ctx, cudaMemcpyAsync(tr->smask.p, mask.data(), mask.size() * sizeof(uint32_t),
+                                   cudaMemcpyHostToDevice, st));
+    }
     tr->enqueue_iteration(st);
     // harvest every iteration so that the event pool stays small
     cudaError_t e = cudaStreamSynchronize(st);
@@ -2228,6 +2334,8 @@ tc_status tc_trainer_model(tc_trainer* tr, tc_model** out) {
 
 void tc_trainer_destroy(tc_trainer* tr) {
   if (!tr) return;
+  // serialised with the context's training calls: the stream may be capturing in another thread
+  std::lock_guard<std::recursive_mutex> train_lock(tr->ctx->train_mu);
   cudaSetDevice(tr->ctx->device);
   cudaStreamSynchronize(tr->ctx->stream);
   delete tr;

@@ -43,7 +43,8 @@ class TrainParams(C.Structure):
         ("lambda_l2", C.c_float), ("lambda_l1", C.c_float), ("min_child_weight", C.c_float),
         ("min_split_gain", C.c_float), ("max_delta_step", C.c_float), ("focal_gamma", C.c_float),
         ("focal_alpha", C.c_float), ("batched", C.c_int32), ("hist_features_per_block", C.c_int32),
-        ("hist_rows_per_chunk", C.c_int32),
+        ("hist_rows_per_chunk", C.c_int32), ("subsample", C.c_float), ("colsample_bytree", C.c_float),
+        ("seed", C.c_uint64),
     ]
 
 
@@ -107,11 +108,11 @@ def _p(a):
 def params(loss="logloss", n_classes=1, n_estimators=10, max_depth=6, max_bins=255, min_samples_leaf=1,
            learning_rate=0.1, lambda_l2=1.0, lambda_l1=0.0, min_child_weight=1.0, min_split_gain=0.0,
            max_delta_step=0.0, focal_gamma=2.0, focal_alpha=0.25, batched=1, hist_features_per_block=0,
-           hist_rows_per_chunk=0) -> TrainParams:
+           hist_rows_per_chunk=0, subsample=1.0, colsample_bytree=1.0, seed=42) -> TrainParams:
     return TrainParams(LOSS[loss] if isinstance(loss, str) else loss, n_classes, n_estimators, max_depth, max_bins,
                        min_samples_leaf, learning_rate, lambda_l2, lambda_l1, min_child_weight, min_split_gain,
                        max_delta_step, focal_gamma, focal_alpha, batched, hist_features_per_block,
-                       hist_rows_per_chunk)
+                       hist_rows_per_chunk, subsample, colsample_bytree, seed)
 
 
 class Model:
