@@ -1724,9 +1724,9 @@ tc_status tc_trainer::autotune() {
   return TC_OK;
 }
 
-enum { KC_GRAD, KC_HIST, KC_MERGE, KC_SCAN, KC_PICK, KC_PART, KC_REDUCE, KC_PLAN, KC_SCATTER, KC_OTHER, KC_N };
-static const char* kKernelNames[KC_N] = {"grad", "hist", "merge", "scan_pick", "pick", "partition",
-                                         "reduce_plan", "plan", "scatter", "other"};
+enum { KC_GRAD, KC_HIST, KC_MERGE, KC_SCAN, KC_PART, KC_REDUCE, KC_SCATTER, KC_OTHER, KC_N };
+static const char* kKernelNames[KC_N] = {"grad", "hist", "merge", "scan_pick", "partition",
+                                         "reduce_plan", "scatter", "other"};
 
 void tc_trainer::mark_begin(int cls, cudaStream_t st) {
   ++launches;
