@@ -244,6 +244,7 @@ def run_ours(args):
     tr.reset()
     prof = tr.profile(3)
     prof.pop("_hist_levels", None)
+    prof.pop("_part_levels", None)
     hl, hms, hbytes = prof["hist"]
     peak, peak_kind = load_peaks()
     achieved = hbytes / (hms * 1e-3) / 1e9 if hms > 0 else None
@@ -505,6 +506,7 @@ def suite_c5(eng, _capi, trees=20):
     per_tree = (tr.stats().seconds - s0) / trees
     prof = tr.profile(3)
     prof.pop("_hist_levels", None)
+    prof.pop("_part_levels", None)
     hl, hms, hbytes = prof["hist"]
     peak, kind = load_peaks()
     return {"config": "imbalanced 10M x 200, focal, depth 8 (1000 trees in the config)",

@@ -158,6 +158,7 @@ typedef struct {
   tc_kernel_time k[12];
   double hist_level_ms[16];     /* histogram kernel time per tree level */
   double hist_level_rows[16];   /* rows histogrammed per tree level */
+  double part_level_ms[16];     /* partition kernel time per tree level */
 } tc_profile;
 
 /* Stateful boosting loop over a quantized dataset.  Replaces

@@ -339,6 +339,8 @@ def test_autotuner_and_profile(engine, capi):
     tr.step(4)
     prof = tr.profile(3)
     levels = prof.pop("_hist_levels")
+    part_levels = prof.pop("_part_levels")
+    assert all(part_levels[d] > 0 for d in range(6))  # depth 6: a partition launch per level
     assert prof["hist"][0] == 3 * 6 and prof["hist"][1] > 0 and prof["hist"][2] > 0
     assert levels[0][1] == 3 * 30_000  # root rows histogrammed per profiled iteration
     assert tr.stats().iterations_done == 7

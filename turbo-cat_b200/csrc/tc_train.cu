@@ -921,10 +921,13 @@ __device__ void pick_body(const DevCfg& c, const DevPtrs& P, int d, int f, int k
 // (2*leaf + right, right = bin != 255 && bin > t) and every block sums its
 // rows' (grad, hess) and counts per child: FP32 within the block (rows in a
 // fixed order inside each warp), FP64 across blocks in the reduce kernel.
-// A warp's rows are first combined per distinct child (ballots for up to 4
-// children, a match over the warp beyond), so a child gets one shared
-// atomic per warp; four rows per thread are loaded before any is used.
+// With 2 or 4 children (8 when a thread has many rows) every thread sums its
+// rows per child in registers and the block's warps reduce them once at the
+// end; otherwise a warp's rows are combined per distinct child (a match over
+// the warp) first, so a child gets one shared atomic per warp.  Four rows per
+// thread are loaded before any is used.
 constexpr int PART_UNROLL = 4;
+template <int NCH>  // 2, 4, 8 children: per-thread register sums; 0: per-warp child groups
 __global__ void __launch_bounds__(PART_THREADS) k_partition(DevCfg c, DevPtrs P, int d) {
   extern __shared__ unsigned char smraw[];
   __shared__ float2 s_wv[PART_THREADS / 32][32];
@@ -944,6 +947,11 @@ __global__ void __launch_bounds__(PART_THREADS) k_partition(DevCfg c, DevPtrs P,
   const float2* gh = P.gh + (size_t)k * c.n;
   const uint8_t t = (uint8_t)cs.b;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NR = NCH > 0 ? NCH : 1;
+  float ag[NR], ah[NR];
+  uint32_t ac[NR];
+#pragma unroll
+  for (int cc = 0; cc < NR; ++cc) { ag[cc] = 0.0f; ah[cc] = 0.0f; ac[cc] = 0; }
   for (uint32_t base = r0; base < r1; base += blockDim.x * PART_UNROLL) {
     uint8_t bb[PART_UNROLL];
     uint16_t lf[PART_UNROLL];
@@ -969,20 +977,14 @@ __global__ void __launch_bounds__(PART_THREADS) k_partition(DevCfg c, DevPtrs P,
         w = v[u];
         if (!row_sampled(c, P, i)) nl = -1;  // its leaf moves on; it is not counted
       }
-      if (nch <= 4) {
-        for (int cc = 0; cc < nch; ++cc) {
-          float g = nl == cc ? w.x : 0.0f, h = nl == cc ? w.y : 0.0f;
-          const uint32_t cnt = __popc(__ballot_sync(0xffffffffu, nl == cc));
-          for (int o = 16; o; o >>= 1) {
-            g += __shfl_xor_sync(0xffffffffu, g, o);
-            h += __shfl_xor_sync(0xffffffffu, h, o);
+      if (NCH > 0) {
+#pragma unroll
+        for (int cc = 0; cc < NR; ++cc)
+          if (nl == cc) {
+            ag[cc] += w.x;
+            ah[cc] += w.y;
+            ac[cc] += 1u;
           }
-          if (lane == 0 && cnt) {
-            atomicAdd(&sG[cc], g);
-            atomicAdd(&sH[cc], h);
-            atomicAdd(&sC[cc], cnt);
-          }
-        }
       } else {
         // the first lane of each child's group sums the group in lane order
         const unsigned m = __match_any_sync(0xffffffffu, nl);
@@ -1000,6 +1002,23 @@ __global__ void __launch_bounds__(PART_THREADS) k_partition(DevCfg c, DevPtrs P,
           atomicAdd(&sC[nl], (uint32_t)__popc(m));
         }
         __syncwarp();
+      }
+    }
+  }
+  if (NCH > 0) {
+    // the thread sums, reduced across the warp (fixed tree), one atomic per warp and child
+#pragma unroll
+    for (int cc = 0; cc < NR; ++cc) {
+      float g = ag[cc], h = ah[cc];
+      for (int o = 16; o; o >>= 1) {
+        g += __shfl_xor_sync(0xffffffffu, g, o);
+        h += __shfl_xor_sync(0xffffffffu, h, o);
+      }
+      const uint32_t cnt = __reduce_add_sync(0xffffffffu, ac[cc]);
+      if (lane == 0 && cnt) {
+        atomicAdd(&sG[cc], g);
+        atomicAdd(&sH[cc], h);
+        atomicAdd(&sC[cc], cnt);
       }
     }
   }
@@ -1627,7 +1646,7 @@ tc_status tc_trainer::setup(int) {
   cudaFuncSetAttribute(k_hist<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape<2>::smem);
   cudaFuncSetAttribute(k_hist<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape<1>::smem);
   cudaFuncSetAttribute(k_hist<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape<2>::smem);
-  cudaFuncSetAttribute(k_partition, cudaFuncAttributeMaxDynamicSharedMemorySize, 12 * L);
+  cudaFuncSetAttribute(k_partition<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 12 * L);
   TC_CUDA(ctx, cudaEventCreate(&ev0));
   TC_CUDA(ctx, cudaEventCreate(&ev1));
   int J0 = prm.hist_features_per_block / 32;
@@ -1801,8 +1820,20 @@ void tc_trainer::launch_level(const DevCfg& c, const DevPtrs& P, int d, cudaStre
   k_scan<<<dim3(c.f, ng, K), SCAN_WARPS * 32, 0, st>>>(c, P, d);  // + pick
   mark_end(st);
   mark_begin(KC_PART, st);
-  k_partition<<<dim3(c.PB, K), PART_THREADS, 12 * (2 << d), st>>>(c, P, d);
+  {
+    const dim3 pg(c.PB, K);
+    const size_t psm = 12 * (2 << d);
+    // register sums pay a fixed per-warp reduction at the end: for 8 children
+    // they win only with enough rows per thread (measured: 4M rows 41 -> 13 us,
+    // 1M rows 15 -> 19 us)
+    const bool many_rows = c.n / (uint32_t)c.PB >= 16u * PART_THREADS;
+    if (d == 0) k_partition<2><<<pg, PART_THREADS, psm, st>>>(c, P, d);
+    else if (d == 1) k_partition<4><<<pg, PART_THREADS, psm, st>>>(c, P, d);
+    else if (d == 2 && many_rows) k_partition<8><<<pg, PART_THREADS, psm, st>>>(c, P, d);
+    else k_partition<0><<<pg, PART_THREADS, psm, st>>>(c, P, d);
+  }
   mark_end(st, (double)c.n * K * (1 + 2 + 2 + 8));
+  if (prof) prof->back().level = d;
   mark_begin(KC_REDUCE, st);
   k_node_reduce<true><<<dim3(1 << d, K), 512, 0, st>>>(c, P, d);  // + plan of level d + 1
   mark_end(st);
@@ -2234,10 +2265,11 @@ tc_status tc_trainer_profile(tc_trainer* tr, int32_t iterations, tc_profile* out
       k.launches += 1;
       k.ms += ms;
       k.alg_bytes += r.bytes;
-      if (r.level >= 0 && r.level < 16) {
+      if (r.level >= 0 && r.level < 16 && r.cls == KC_HIST) {
         out->hist_level_ms[r.level] += ms;
         out->hist_level_rows[r.level] += r.rows;
       }
+      if (r.level >= 0 && r.level < 16 && r.cls == KC_PART) out->part_level_ms[r.level] += ms;
     }
     recs.clear();
     tr->ev_used = 0;

@@ -61,7 +61,7 @@ class KernelTime(C.Structure):
 
 class Profile(C.Structure):
     _fields_ = [("n_kernels", C.c_int32), ("k", KernelTime * 12), ("hist_level_ms", C.c_double * 16),
-                ("hist_level_rows", C.c_double * 16)]
+                ("hist_level_rows", C.c_double * 16), ("part_level_ms", C.c_double * 16)]
 
 
 class ModelInfo(C.Structure):
@@ -212,6 +212,7 @@ class Trainer:
         out = {pr.k[i].name.decode(): (pr.k[i].launches, pr.k[i].ms, pr.k[i].alg_bytes)
                for i in range(pr.n_kernels)}
         out["_hist_levels"] = [(pr.hist_level_ms[d], pr.hist_level_rows[d]) for d in range(16)]
+        out["_part_levels"] = [pr.part_level_ms[d] for d in range(16)]
         return out
 
     def set_validation(self, vds, early_stopping_rounds=50):
