@@ -69,6 +69,8 @@ struct ClassState {
   int32_t done;        // 0 growing, 1 stopped (leaves pending), 2 finalized
   int32_t depth;       // accepted splits
   int32_t f, b;        // split of the current level
+  int32_t skew;        // one node of the current level holds more than 1/8 of the rows
+  int32_t pad;
 };
 
 // Early-stopping state of a validation set (device).
@@ -927,7 +929,9 @@ __device__ void pick_body(const DevCfg& c, const DevPtrs& P, int d, int f, int k
 // the warp) first, so a child gets one shared atomic per warp.  Four rows per
 // thread are loaded before any is used.
 constexpr int PART_UNROLL = 4;
-template <int NCH>  // 2, 4, 8 children: per-thread register sums; 0: per-warp child groups
+template <int NCH>  // 2, 4, 8 children: per-thread register sums; 0: per-warp child groups;
+                    // -1: per-lane atomics into per-warp copies of the child sums, or the
+                    // groups when one node holds most rows (the lanes would hit one address)
 __global__ void __launch_bounds__(PART_THREADS) k_partition(DevCfg c, DevPtrs P, int d) {
   extern __shared__ unsigned char smraw[];
   __shared__ float2 s_wv[PART_THREADS / 32][32];
@@ -935,10 +939,11 @@ __global__ void __launch_bounds__(PART_THREADS) k_partition(DevCfg c, DevPtrs P,
   const ClassState cs = P.cs[k];
   if (cs.done || cs.depth != d + 1) return;
   const int nch = 1 << (d + 1);
+  const int ncopy = NCH < 0 ? PART_THREADS / 32 : 1;  // copies of the child sums (one per warp)
   float* sG = reinterpret_cast<float*>(smraw);
-  float* sH = sG + nch;
-  uint32_t* sC = reinterpret_cast<uint32_t*>(sH + nch);
-  for (int q = threadIdx.x; q < nch; q += blockDim.x) { sG[q] = 0.0f; sH[q] = 0.0f; sC[q] = 0; }
+  float* sH = sG + nch * ncopy;
+  uint32_t* sC = reinterpret_cast<uint32_t*>(sH + nch * ncopy);
+  for (int q = threadIdx.x; q < nch * ncopy; q += blockDim.x) { sG[q] = 0.0f; sH[q] = 0.0f; sC[q] = 0; }
   __syncthreads();
   const uint32_t rpb = (c.n + gridDim.x - 1) / gridDim.x;
   const uint32_t r0 = blockIdx.x * rpb, r1 = min(c.n, r0 + rpb);
@@ -985,6 +990,13 @@ __global__ void __launch_bounds__(PART_THREADS) k_partition(DevCfg c, DevPtrs P,
             ah[cc] += w.y;
             ac[cc] += 1u;
           }
+      } else if (NCH < 0 && !cs.skew) {
+        if (nl >= 0) {
+          const int o = warp * nch + nl;
+          atomicAdd(&sG[o], w.x);
+          atomicAdd(&sH[o], w.y);
+          atomicAdd(&sC[o], 1u);
+        }
       } else {
         // the first lane of each child's group sums the group in lane order
         const unsigned m = __match_any_sync(0xffffffffu, nl);
@@ -1026,8 +1038,15 @@ __global__ void __launch_bounds__(PART_THREADS) k_partition(DevCfg c, DevPtrs P,
   const int L = 1 << c.D;
   for (int q = threadIdx.x; q < nch; q += blockDim.x) {
     const size_t o = ((size_t)k * c.PB + blockIdx.x) * L + q;
-    P.psum[o] = make_double2((double)sG[q], (double)sH[q]);
-    P.pcnt[o] = sC[q];
+    float g = 0.0f, h = 0.0f;
+    uint32_t cn = 0;
+    for (int w = 0; w < ncopy; ++w) {  // the warps' copies in a fixed order
+      g += sG[w * nch + q];
+      h += sH[w * nch + q];
+      cn += sC[w * nch + q];
+    }
+    P.psum[o] = make_double2((double)g, (double)h);
+    P.pcnt[o] = cn;
   }
 }
 
@@ -1111,6 +1130,7 @@ __device__ __forceinline__ void node_reduce_body(const DevCfg& c, const DevPtrs&
 // items.
 __device__ __forceinline__ void plan_body(const DevCfg& c, const DevPtrs& P, int d) {
   __shared__ int s_go;
+  __shared__ uint32_t s_maxcnt;
   __shared__ long long s_rows;
   __shared__ int s_warp[PLAN_THREADS / 32];
   __shared__ int s_carry;
@@ -1127,12 +1147,21 @@ __device__ __forceinline__ void plan_body(const DevCfg& c, const DevPtrs& P, int
     }
     __syncthreads();
     const bool alive = !cs.done && (d == 0 || cs.depth == d) && d < c.D;
+    if (tid == 0) s_maxcnt = 0;
+    __syncthreads();
     if (alive) {
       const NodeStat* ns = P.nstat + ((size_t)k * (c.D + 1) + d) * L;
-      for (int q = tid; q < (1 << d); q += blockDim.x)
+      for (int q = tid; q < (1 << d); q += blockDim.x) {
         if (ns[q].cnt >= (uint32_t)c.msl * 2u && (float)ns[q].H >= c.mcw * 2.0f) s_go = 1;
+        atomicMax(&s_maxcnt, ns[q].cnt);
+      }
     }
     __syncthreads();
+    if (tid == 0 && alive) {
+      uint32_t tot = 0;  // rows of the level (the root's count)
+      tot = P.nstat[((size_t)k * (c.D + 1)) * L].cnt;
+      cs.skew = (uint64_t)s_maxcnt * 8u > (uint64_t)tot ? 1 : 0;
+    }
     if (tid == 0 && !cs.done && !(alive && s_go)) cs.done = 1;
     __syncthreads();
     if (cs.done == 1) {
@@ -1647,6 +1676,7 @@ tc_status tc_trainer::setup(int) {
   cudaFuncSetAttribute(k_hist<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape<1>::smem);
   cudaFuncSetAttribute(k_hist<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape<2>::smem);
   cudaFuncSetAttribute(k_partition<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 12 * L);
+  cudaFuncSetAttribute(k_partition<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 12 * 256 * (PART_THREADS / 32));
   TC_CUDA(ctx, cudaEventCreate(&ev0));
   TC_CUDA(ctx, cudaEventCreate(&ev1));
   int J0 = prm.hist_features_per_block / 32;
@@ -1830,6 +1860,8 @@ void tc_trainer::launch_level(const DevCfg& c, const DevPtrs& P, int d, cudaStre
     if (d == 0) k_partition<2><<<pg, PART_THREADS, psm, st>>>(c, P, d);
     else if (d == 1) k_partition<4><<<pg, PART_THREADS, psm, st>>>(c, P, d);
     else if (d == 2 && many_rows) k_partition<8><<<pg, PART_THREADS, psm, st>>>(c, P, d);
+    else if (d >= 3 && (2 << d) <= 256)
+      k_partition<-1><<<pg, PART_THREADS, psm * (PART_THREADS / 32), st>>>(c, P, d);
     else k_partition<0><<<pg, PART_THREADS, psm, st>>>(c, P, d);
   }
   mark_end(st, (double)c.n * K * (1 + 2 + 2 + 8));
