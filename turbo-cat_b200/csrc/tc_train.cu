@@ -681,7 +681,8 @@ __global__ void k_merge(DevCfg c, DevPtrs P, int d) {
 
 // ------------------------------------------------------------------ scan --
 
-__device__ void pick_body(const DevCfg& c, const DevPtrs& P, int d, int f, int k);
+__device__ void pick_body(const DevCfg& c, const DevPtrs& P, int d, int f, int k, bool direct, double s_in,
+                          uint8_t any_in);
 
 // grid (F, node groups, K), SCAN_WARPS warps.  A warp scores one node at a
 // time: lane l holds bins 8l .. 8l+7 (bin 255 = NaN rows, added to the left
@@ -763,17 +764,21 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(DevCfg c, DevPtrs P, i
     s_any[warp][lane * 8 + i] = (anyb >> i) & 1u;
   }
   __syncthreads();
-  for (int b = threadIdx.x; b < kSlots; b += blockDim.x) {
-    double s = 0.0;
-    uint8_t a = 0;
-    for (int w = 0; w < SCAN_WARPS; ++w) {
-      s += s_acc[w][b];
-      a |= s_any[w][b];
-    }
-    const size_t o = (((size_t)k * c.f + f) * c.n_scan_groups_max + ng) * kSlots + b;
-    P.gpart[o] = s;
-    P.gany[o] = a;
+  // blockDim.x == kSlots: thread b sums bin b over the warps
+  const int b = threadIdx.x;
+  double sb = 0.0;
+  uint8_t ab = 0;
+  for (int w = 0; w < SCAN_WARPS; ++w) {
+    sb += s_acc[w][b];
+    ab |= s_any[w][b];
   }
+  if (gridDim.y == 1) {  // the only block of its feature: its sums go straight to the pick
+    pick_body(c, P, d, f, k, true, sb, ab);
+    return;
+  }
+  const size_t o = (((size_t)k * c.f + f) * c.n_scan_groups_max + ng) * kSlots + b;
+  P.gpart[o] = sb;
+  P.gany[o] = ab;
   // the last node-group block of feature f (completion counter; nobody
   // waits) picks the feature's best bin, and the class's last feature its split
   __shared__ bool s_fdone;
@@ -787,7 +792,7 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(DevCfg c, DevPtrs P, i
   if (!s_fdone) return;
   __threadfence();
   if (threadIdx.x == 0) P.fcnt[(size_t)k * c.f + f] = 0;  // re-armed for the next level / graph replay
-  pick_body(c, P, d, f, k);
+  pick_body(c, P, d, f, k, false, 0.0, 0);
 }
 
 // ------------------------------------------------------------------ pick --
@@ -798,28 +803,29 @@ __device__ __forceinline__ bool better(double ga, int fa, int ba, double gb, int
   return ba < bb;
 }
 
-// grid (F, K), 256 threads = bins.  Sums the node-group partials of every
-// bin of one feature, keeps the best bin (lowest bin on equal gain) and the
-// runner-up; the last block of a class to finish (completion counter, no
-// waiting) reduces the features in ascending order -- the reference keeps
-// the first strictly greater gain, i.e. lowest feature then lowest bin --
-// applies the stop rule and records the split.
-// Best bin of feature f of class k over the level's node groups, then, in the
-// last feature block of the class (completion counter), the level's split.
-// Called by the 256 threads of a scan block once its feature is complete.
-__device__ void pick_body(const DevCfg& c, const DevPtrs& P, int d, int f, int k) {
+// Called by the 256 threads (= bins) of the scan block that completes feature
+// f of class k: sums the node-group partials of every bin (or takes the
+// block's own sums, `direct`), keeps the best bin (lowest bin on equal gain)
+// and the runner-up; the last feature block of the class (completion
+// counter, no waiting) reduces the features in ascending order -- the
+// reference keeps the first strictly greater gain, i.e. lowest feature then
+// lowest bin -- applies the stop rule and records the split.
+__device__ void pick_body(const DevCfg& c, const DevPtrs& P, int d, int f, int k, bool direct, double s_in,
+                          uint8_t any_in) {
   __shared__ double s_g[256], s_2[256];
   __shared__ int s_b[256];
   __shared__ bool s_last;
   ClassState& cs = P.cs[k];
   const int b = threadIdx.x;
   const int ngroups = ((1 << d) + SCAN_NODES - 1) / SCAN_NODES;
-  double s = 0.0;
-  uint8_t any = 0;
-  const size_t o = ((size_t)k * c.f + f) * c.n_scan_groups_max * kSlots + b;
-  for (int g = 0; g < ngroups; ++g) {
-    s += P.gpart[o + (size_t)g * kSlots];
-    any |= P.gany[o + (size_t)g * kSlots];
+  double s = s_in;
+  uint8_t any = any_in;
+  if (!direct) {
+    const size_t o = ((size_t)k * c.f + f) * c.n_scan_groups_max * kSlots + b;
+    for (int g = 0; g < ngroups; ++g) {
+      s += P.gpart[o + (size_t)g * kSlots];
+      any |= P.gany[o + (size_t)g * kSlots];
+    }
   }
   const bool cand = b < c.nb_scan && (d > 0 || any);
   s_g[b] = cand ? s : -1e300;
