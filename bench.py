@@ -25,6 +25,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -72,8 +73,10 @@ class Clocks:
     """nvidia-smi clock sampling during the timed region."""
 
     def __init__(self, gpu):
-        self.path = os.path.join(ROOT, "gpurun_out", f"bench_clocks_{gpu}.csv")
-        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        # raw samples: $BENCH_CLOCKS_DIR if set (kept as evidence), else the temp directory
+        out = os.environ.get("BENCH_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(out, f"bench_clocks_{gpu}_{os.getpid()}.csv")
+        os.makedirs(out, exist_ok=True)
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -380,31 +383,11 @@ def _train_serving_models(eng, _capi):
     return models
 
 
-def suite_c4(eng, _capi, seconds=3.0, rate=20_000.0, ref_ok=False):
+def _device_predict(models, f):
+    """Device-resident prediction throughput of every model: 1M rows, kernel
+    only (CUDA events on the launching stream, L2 flushed between launches)."""
     import torch
 
-    models = _train_serving_models(eng, _capi)
-    f = 100
-    rng = np.random.default_rng(44)
-    pool = torch.empty((65536 + 65536, f), dtype=torch.float32, pin_memory=True).numpy()
-    pool[:] = rng.standard_normal(pool.shape).astype(np.float32)
-    res = {"config": "serving: 4 resident models (1000xd6, 200xd4, 500xd8, 2000xd10) on 100 features; "
-                     f"Poisson {rate:.0f} req/s for {seconds:.1f} s, rows log-uniform [1, 65536]"}
-    # fixed-batch latency of the 1000 x depth-6 model (host buffers, H2D + kernel + D2H)
-    lat = {}
-    for rows in (1, 64, 4096, 65536):
-        Xb = pool[:rows]
-        for _ in range(3):
-            models[0].predict(Xb, "sigmoid")
-        ts = []
-        for _ in range(30):
-            t0 = time.perf_counter()
-            models[0].predict(Xb, "sigmoid")
-            ts.append(time.perf_counter() - t0)
-        lat[str(rows)] = {"p50_us": _pct(ts, 50) * 1e6, "p99_us": _pct(ts, 99) * 1e6,
-                          "rows_per_s": rows / _pct(ts, 50)}
-    res["fixed_batch_1000xd6"] = lat
-    # device-resident throughput of every model (kernel only, CUDA events on the launching stream)
     n_dev = 1 << 20
     Xd = torch.randn((n_dev, f), dtype=torch.float32, device="cuda")
     od = torch.empty((n_dev, 1), dtype=torch.float32, device="cuda")
@@ -432,12 +415,37 @@ def suite_c4(eng, _capi, seconds=3.0, rate=20_000.0, ref_ok=False):
         dev_tp[f"{info.n_trees}xd{info.max_depth}"] = {
             "rows": n_dev, "ms": t * 1e3, "rows_per_s": n_dev / t, "gcompare_per_s": compares / t / 1e9,
             "input_gbs": n_dev * f * 4 / t / 1e9}
-    res["device_predict_1M_rows"] = dev_tp
     del Xd, od, flush
+    return dev_tp
+
+
+def suite_c4(eng, _capi, seconds=3.0, rate=20_000.0, ref_ok=False):
+    import torch
+
+    models = _train_serving_models(eng, _capi)
+    f = 100
+    rng = np.random.default_rng(44)
+    pool = torch.empty((65536 + 65536, f), dtype=torch.float32, pin_memory=True).numpy()
+    pool[:] = rng.standard_normal(pool.shape).astype(np.float32)
+    res = {"config": "serving: 4 resident models (1000xd6, 200xd4, 500xd8, 2000xd10) on 100 features; "
+                     f"Poisson {rate:.0f} req/s for {seconds:.1f} s, rows log-uniform [1, 65536]"}
+    # fixed-batch latency of the 1000 x depth-6 model (host buffers, H2D + kernel + D2H)
+    lat = {}
+    for rows in (1, 64, 4096, 65536):
+        Xb = pool[:rows]
+        for _ in range(3):
+            models[0].predict(Xb, "sigmoid")
+        ts = []
+        for _ in range(30):
+            t0 = time.perf_counter()
+            models[0].predict(Xb, "sigmoid")
+            ts.append(time.perf_counter() - t0)
+        lat[str(rows)] = {"p50_us": _pct(ts, 50) * 1e6, "p99_us": _pct(ts, 99) * 1e6,
+                          "rows_per_s": rows / _pct(ts, 50)}
+    res["fixed_batch_1000xd6"] = lat
+    res["device_predict_1M_rows"] = _device_predict(models, f)
     if ref_ok:
         sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
-        import tempfile
-
         import _turbocat as ref
 
         path = os.path.join(tempfile.mkdtemp(), "m.tcat")
@@ -532,6 +540,9 @@ def run_suite(args):
             r = suite_c3(eng, _capi)
         elif name == "c4":
             r = suite_c4(eng, _capi, ref_ok=ref_ok)
+        elif name == "c4dev":  # the four serving models' device-resident prediction only
+            r = {"config": "serving models (1000xd6, 200xd4, 500xd8, 2000xd10) on 100 features, 1M resident rows",
+                 "device_predict_1M_rows": _device_predict(_train_serving_models(eng, _capi), 100)}
         elif name == "c5":
             r = suite_c5(eng, _capi)
         else:

@@ -129,6 +129,20 @@ typedef struct {
   float subsample;
   float colsample_bytree;
   uint64_t seed;                    /* Config::seed (default 42 in the reference) */
+  /* Gradient-based one-side sampling, Dataset::goss_subsample
+   * (src/core/dataset.cpp:494-549), selected over subsample as in
+   * Booster::train (src/boosting/booster.cpp:200-219): with use_goss != 0
+   * every iteration's trees are built on the (uint32)(n * goss_top_rate) rows
+   * of largest |gradient| (softmax: the largest |gradient| over the classes,
+   * src/boosting/booster.cpp:1327-1348) plus (uint32)(n * goss_other_rate)
+   * rows drawn from the rest by a partial Fisher-Yates shuffle
+   * (std::mt19937_64 seeded by one xorshift64* draw).  The selection runs
+   * on the host from the iteration's gradients (std::nth_element's
+   * arrangement decides which rows the draws reach), so every such
+   * iteration synchronises with the host.  Rates in [0, 1]. */
+  int32_t use_goss;
+  float goss_top_rate;              /* reference default 0.2 */
+  float goss_other_rate;            /* reference default 0.1 */
 } tc_train_params;
 
 typedef struct {
@@ -177,6 +191,10 @@ tc_status tc_trainer_stats(tc_trainer* tr, tc_train_stats* st);
 tc_status tc_trainer_profile(tc_trainer* tr, int32_t iterations, tc_profile* out);
 /* Raw training-set scores [n][K] (base included) after the trees so far. */
 tc_status tc_trainer_train_scores(tc_trainer* tr, float* out);
+/* Rows the last iteration's trees were built on, one bit per row
+ * (row i: bit i % 32 of word i / 32; ceil(n / 32) words, bits past n are 0).
+ * Every row when neither subsample nor GOSS is on. */
+tc_status tc_trainer_sample_mask(tc_trainer* tr, uint32_t* out);
 /* Snapshot of the ensemble trained so far as an immutable model. */
 tc_status tc_trainer_model(tc_trainer* tr, tc_model** out);
 /* Validation set and early stopping, Booster::train's valid_data branch

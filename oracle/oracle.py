@@ -62,6 +62,9 @@ class FitParams(C.Structure):
         ("subsample", C.c_float),
         ("colsample_bytree", C.c_float),
         ("seed", C.c_uint64),
+        ("use_goss", C.c_int32),
+        ("goss_top_rate", C.c_float),
+        ("goss_other_rate", C.c_float),
     ]
 
 
@@ -103,6 +106,9 @@ class Hyper:
     subsample: float = 1.0          # row sampling per iteration (BoostingConfig::subsample)
     colsample_bytree: float = 1.0   # advances the random state only (symmetric trees ignore it)
     seed: int = 42                  # Config::seed
+    use_goss: bool = False          # GOSS row sampling (chosen over subsample)
+    goss_top_rate: float = 0.2
+    goss_other_rate: float = 0.1
 
     def tree(self) -> TreeParams:
         return TreeParams(self.max_depth, self.max_bins, self.min_samples_leaf, self.lambda_l2,
@@ -112,7 +118,8 @@ class Hyper:
     def fit(self) -> FitParams:
         return FitParams(LOSS_IDS[self.loss], self.n_classes if self.loss == "softmax" else 1,
                          self.n_estimators, self.learning_rate, self.focal_gamma,
-                         self.focal_alpha, self.tree(), self.subsample, self.colsample_bytree, self.seed)
+                         self.focal_alpha, self.tree(), self.subsample, self.colsample_bytree, self.seed,
+                         1 if self.use_goss else 0, self.goss_top_rate, self.goss_other_rate)
 
     def ref(self) -> RefParams:
         return RefParams(LOSS_IDS[self.loss], self.n_classes if self.loss == "softmax" else 2,
@@ -194,6 +201,25 @@ def gradients(loss: str, y, pred, K: int = 1, gamma=2.0, alpha=0.25):
     else:
         raise ValueError(loss)
     return g, h
+
+
+def next_random(state: int):
+    """One xorshift64* draw (src/boosting/booster.cpp:1219-1225): (new state, output)."""
+    st = C.c_uint64(state)
+    lib().tco_next_random.restype = C.c_uint64
+    out = lib().tco_next_random(C.byref(st))
+    return st.value, out
+
+
+def goss_subsample(absg, top_rate: float, other_rate: float, seed: int) -> np.ndarray:
+    """Rows of one GOSS selection (src/core/dataset.cpp:494-549) over per-row |g|, in the reference's order."""
+    absg = np.ascontiguousarray(absg, np.float32)
+    n = len(absg)
+    out = np.zeros(max(1, n), np.uint32)
+    lib().tco_goss_subsample.restype = C.c_uint32
+    m = lib().tco_goss_subsample(C.c_uint32(n), _ptr(absg), C.c_float(top_rate), C.c_float(other_rate),
+                                 C.c_uint64(seed), _ptr(out))
+    return out[:m]
 
 
 def init_prediction(loss: str, y) -> float:

@@ -622,18 +622,33 @@ int tco_fit(const uint8_t* bins, uint32_t n, uint32_t f, const float* edges,
   int rc = 0;
   size_t t = 0;
   uint64_t rng = p->seed;
-  const int sampling = p->subsample < 1.0f;
+  const int goss = p->use_goss != 0;
+  const int sampling = goss || p->subsample < 1.0f;
   uint32_t* sample = sampling ? (uint32_t*)malloc((size_t)(n ? n : 1) * sizeof(uint32_t)) : NULL;
+  float* absg = goss ? (float*)malloc((size_t)(n ? n : 1) * sizeof(float)) : NULL;
   for (int32_t it = 0; it < p->n_estimators; ++it) {
-    /* sample selection (booster.cpp:198-228): rows, then one draw for the
-     * feature subset, which the symmetric build does not use */
-    uint32_t n_sample = n;
-    if (sampling) n_sample = tco_random_subsample(n, p->subsample, tco_next_random(&rng), sample);
-    if (p->colsample_bytree < 1.0f) (void)tco_next_random(&rng);
     if (p->loss == TCO_LOSS_LOGLOSS) tco_grad_logloss(y, pred, gg, hh, n);
     else if (p->loss == TCO_LOSS_MSE) tco_grad_mse(y, pred, gg, hh, n);
     else if (p->loss == TCO_LOSS_FOCAL) tco_grad_focal(y, pred, gg, hh, n, p->focal_gamma, p->focal_alpha);
     else tco_grad_softmax(y, pred, gg, hh, n, K);
+    /* sample selection after the gradients (booster.cpp:198-228): GOSS or
+     * the random subsample, then one draw for the feature subset, which the
+     * symmetric build does not use */
+    uint32_t n_sample = n;
+    if (goss) {
+      for (uint32_t i = 0; i < n; ++i) {
+        float m = 0.0f; /* max |g| over the classes, from 0 (booster.cpp:1333-1339) */
+        for (uint32_t k = 0; k < K; ++k) {
+          const float a = fabsf(gg[(size_t)i * K + k]);
+          m = a > m ? a : m;
+        }
+        absg[i] = m;
+      }
+      n_sample = tco_goss_subsample(n, absg, p->goss_top_rate, p->goss_other_rate, tco_next_random(&rng), sample);
+    } else if (sampling) {
+      n_sample = tco_random_subsample(n, p->subsample, tco_next_random(&rng), sample);
+    }
+    if (p->colsample_bytree < 1.0f) (void)tco_next_random(&rng);
     if (grad_trace) memcpy(grad_trace + (size_t)it * n * K, gg, (size_t)n * K * sizeof(float));
     if (hess_trace) memcpy(hess_trace + (size_t)it * n * K, hh, (size_t)n * K * sizeof(float));
     for (uint32_t k = 0; k < K; ++k, ++t) {
@@ -683,7 +698,7 @@ int tco_fit(const uint8_t* bins, uint32_t n, uint32_t f, const float* edges,
   if (train_pred) memcpy(train_pred, pred, (size_t)n * K * sizeof(float));
   if (min_margin_out) *min_margin_out = min_margin;
 done:
-  free(pred); free(gg); free(hh); free(gk); free(hk); free(li); free(lv); free(sample);
+  free(pred); free(gg); free(hh); free(gk); free(hk); free(li); free(lv); free(sample); free(absg);
   return rc;
 }
 

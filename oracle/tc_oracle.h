@@ -113,6 +113,13 @@ typedef struct {
   float subsample;
   float colsample_bytree;
   uint64_t seed;
+  /* GOSS (Dataset::goss_subsample, src/core/dataset.cpp:494-549), chosen
+   * over subsample (booster.cpp:200-219): each iteration's rows from its
+   * gradients (softmax: the largest |g| over the classes,
+   * booster.cpp:1327-1348) and one next_random() draw. */
+  int32_t use_goss;
+  float goss_top_rate;
+  float goss_other_rate;
 } tco_fit_params;
 
 /* xorshift64* step (src/boosting/booster.cpp:1219-1225). */
@@ -120,6 +127,10 @@ uint64_t tco_next_random(uint64_t* state);
 /* src/core/dataset.cpp:552-562: writes the first (uint32)(n * ratio)
  * shuffled row ids to out, returns their count. */
 uint32_t tco_random_subsample(uint32_t n, float ratio, uint64_t seed, uint32_t* out);
+/* src/core/dataset.cpp:494-549 over per-row |g| values: writes the sampled
+ * row ids in the reference's order, returns their count. */
+uint32_t tco_goss_subsample(uint32_t n, const float* absg, float top_rate, float other_rate, uint64_t seed,
+                            uint32_t* out);
 
 int tco_fit(const uint8_t* bins, uint32_t n, uint32_t f, const float* edges,
             const uint16_t* n_edges, const float* y, const tco_fit_params* p, int32_t mode,

@@ -189,3 +189,66 @@ def test_row_sampling_matches_reference():
     full = O.fit(O.quantize(X), y, O.Hyper(loss="logloss", n_estimators=6, learning_rate=0.1, max_depth=5,
                                            lambda_l2=1.0), mode=0)
     assert not np.array_equal(full.leaves, e.leaves)  # sampling changed the trees
+
+
+_GOSS_SCRIPT = r"""
+import sys, os, tempfile
+sys.path[:0] = [sys.argv[1], sys.argv[2]]
+import _turbocat as ref
+from datagen import binary_c1
+X, y = binary_c1(20000, 12, seed=91)
+m = ref.TurboCatClassifier(n_estimators=6, learning_rate=0.1, max_depth=5, max_bins=255, subsample=1.0,
+                           colsample_bytree=0.8, min_child_weight=1.0, lambda_l2=1.0, loss="logloss",
+                           mode="large", verbosity=0, seed=42, use_goss=True, goss_top_rate=0.2,
+                           goss_other_rate=0.1)
+m.fit(X, y)
+path = os.path.join(tempfile.mkdtemp(), "m.tcat")
+m.save(path)
+sys.stdout.write(path)
+"""
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference build (oracle/_ref) not present")
+def test_goss_matches_reference():
+    """use_goss with the facade's rates (top 0.2, other 0.1), colsample_bytree
+    0.8, seed 42: the oracle's GOSS (std::nth_element over (|g|, row), a
+    partial Fisher-Yates shuffle of the rest with std::mt19937_64, trees
+    built over the sampled rows in that order) reproduces the reference's
+    fit bit for bit."""
+    import os
+    import subprocess
+    import sys
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    out = subprocess.run([sys.executable, "-c", _GOSS_SCRIPT, here, os.path.join(O.HERE, "_ref")],
+                         capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr
+    r = O.parse_tcat(open(out.stdout.strip().splitlines()[-1], "rb").read())
+    X, y = binary_c1(20000, 12, seed=91)
+    hp = O.Hyper(loss="logloss", n_estimators=6, learning_rate=0.1, max_depth=5, lambda_l2=1.0,
+                 colsample_bytree=0.8, seed=42, use_goss=True, goss_top_rate=0.2, goss_other_rate=0.1)
+    e = O.fit(O.quantize(X), y, hp, mode=0)
+    assert np.array_equal(r.feature, e.feature) and np.array_equal(r.bin, e.bin)
+    assert np.array_equal(_u32(r.leaves), _u32(e.leaves))
+    full = O.fit(O.quantize(X), y, O.Hyper(loss="logloss", n_estimators=6, learning_rate=0.1, max_depth=5,
+                                           lambda_l2=1.0), mode=0)
+    assert not np.array_equal(full.leaves, e.leaves)  # the sample changed the trees
+
+
+def test_goss_selection_properties():
+    """The oracle's GOSS selection: the top rows are the largest |g| (ties
+    aside), the other rows come from the rest, counts as the reference
+    computes them (uint32)(n * rate), and the same seed gives the same rows."""
+    rng = np.random.default_rng(5)
+    n = 10_007
+    absg = np.abs(rng.standard_normal(n)).astype(np.float32)
+    rows = O.goss_subsample(absg, 0.2, 0.1, 1234)
+    top_n, other_n = int(np.float32(n) * np.float32(0.2)), int(np.float32(n) * np.float32(0.1))
+    assert len(rows) == top_n + other_n and len(np.unique(rows)) == len(rows)
+    thr = np.sort(absg)[::-1][top_n - 1]
+    assert np.all(absg[rows[:top_n]] >= thr) and np.all(absg[rows[top_n:]] <= thr)
+    assert np.array_equal(rows, O.goss_subsample(absg, 0.2, 0.1, 1234))
+    assert not np.array_equal(rows[top_n:], O.goss_subsample(absg, 0.2, 0.1, 1235)[top_n:])
+    assert len(O.goss_subsample(absg, 0.0, 0.0, 1)) == 0
+    assert len(O.goss_subsample(absg, 1.0, 0.5, 1)) == n  # all rows on top, nothing else to draw
+    assert len(O.goss_subsample(absg, 0.0, 0.3, 1)) == int(np.float32(n) * np.float32(0.3))

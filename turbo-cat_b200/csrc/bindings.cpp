@@ -229,7 +229,10 @@ class TurboCatClassifier {
     p_.max_bins = max_bins;
     p_.min_child_weight = min_child_weight;
     p_.lambda_l2 = lambda_l2;
-    (void)goss_top_rate; (void)goss_other_rate; (void)use_symmetric; (void)grow_policy;
+    (void)use_symmetric; (void)grow_policy;
+    p_.use_goss = use_goss ? 1 : 0;  // python/bindings.cpp:76-78
+    p_.goss_top_rate = goss_top_rate;
+    p_.goss_other_rate = goss_other_rate;
     p_.subsample = subsample;
     p_.colsample_bytree = colsample_bytree;
     p_.seed = (uint64_t)(int64_t)seed;
@@ -248,7 +251,6 @@ class TurboCatClassifier {
     const uint16_t f = (uint16_t)X.shape(1);
     if ((size_t)y.shape(0) != n) throw std::runtime_error("X and y have different numbers of rows");
     if (mode_ == "small") warn("mode='small' (regular trees) is not on the device path; building symmetric trees");
-    if (use_goss_) warn("GOSS sampling is not on the device path; random subsampling (subsample) is used");
     if (colsample_ < 1.0f && verbosity_ > 1) warn("colsample_bytree has no effect on symmetric trees");
     if (use_gradtree_ || use_ordered_ || auto_interactions_)
       warn("use_gradtree / use_ordered_boosting / auto_interactions are not on the device path and are ignored");
@@ -423,7 +425,10 @@ class TurboCatRegressor {
     p_.subsample = subsample;
     p_.colsample_bytree = colsample_bytree;
     p_.seed = (uint64_t)(int64_t)seed;
-    (void)goss_top_rate; (void)goss_other_rate; (void)early_stopping_rounds;
+    p_.use_goss = use_goss ? 1 : 0;  // python/bindings.cpp:570-572
+    p_.goss_top_rate = goss_top_rate;
+    p_.goss_other_rate = goss_other_rate;
+    (void)early_stopping_rounds;
     (void)max_leaves; (void)grow_policy; (void)n_threads;
   }
 
@@ -433,7 +438,6 @@ class TurboCatRegressor {
     const uint16_t f = (uint16_t)X.shape(1);
     if ((size_t)y.size() != n) throw std::runtime_error("X and y have different numbers of rows");
     if (mode_ == "small") warn("mode='small' (regular trees) is not on the device path; building symmetric trees");
-    if (use_goss_) warn("GOSS sampling is not on the device path; random subsampling (subsample) is used");
     {
       py::gil_scoped_release nogil;
       booster_.reset(new GpuBooster());

@@ -221,8 +221,46 @@ __device__ __forceinline__ void loss_grad(int loss, float pred, float y, uint32_
 // (preds += lr * leaf, fused multiply-add as in src/boosting/booster.cpp:458-463),
 // computes the gradients and resets the leaf ids; then per-block root sums
 // (FP64, fixed order) go to psum[k][block][0] / pcnt.
-__global__ void __launch_bounds__(512) k_grad(DevCfg c, DevPtrs P, int use_given_gh) {
+// Root sums of the block's rows [r0, r1) per class (FP64, thread-local in
+// row order then a fixed-order block reduction) and their sampled count,
+// into the block's slot of the partition sums (the level -1 reduce reads them).
+__device__ void root_sums(const DevCfg& c, const DevPtrs& P, uint32_t r0, uint32_t r1) {
   __shared__ double sG[16], sH[16];
+  __shared__ uint32_t sCnt[16];
+  const int K = c.K;
+  const int L = 1 << c.D;
+  uint32_t my_cnt = 0;
+  for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) my_cnt += row_sampled(c, P, i) ? 1u : 0u;
+  for (int o = 16; o; o >>= 1) my_cnt += __shfl_down_sync(0xffffffffu, my_cnt, o);
+  if ((threadIdx.x & 31) == 0) sCnt[threadIdx.x >> 5] = my_cnt;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int k = 0; k < K; ++k) {
+    double g = 0.0, h = 0.0;
+    for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+      const float2 v = P.gh[(size_t)k * c.n + i];
+      g += (double)v.x;
+      h += (double)v.y;
+    }
+    for (int o = 16; o; o >>= 1) {
+      g += __shfl_down_sync(0xffffffffu, g, o);
+      h += __shfl_down_sync(0xffffffffu, h, o);
+    }
+    if (lane == 0) { sG[warp] = g; sH[warp] = h; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double tg = 0.0, th = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { tg += sG[w]; th += sH[w]; }
+      const size_t o = ((size_t)k * c.PB + blockIdx.x) * L;
+      uint32_t cnt = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) cnt += sCnt[w];
+      P.psum[o] = make_double2(tg, th);
+      P.pcnt[o] = cnt;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(512) k_grad(DevCfg c, DevPtrs P, int use_given_gh) {
   const int K = c.K;
   const int it = *P.iter;
   const uint32_t n_vec = (c.n / 8) * 8;
@@ -264,37 +302,22 @@ __global__ void __launch_bounds__(512) k_grad(DevCfg c, DevPtrs P, int use_given
     }
     for (int k = 0; k < K; ++k) P.leaf[(size_t)k * c.n + i] = 0;
   }
-  __shared__ uint32_t sCnt[16];
-  uint32_t my_cnt = 0;
-  for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) my_cnt += row_sampled(c, P, i) ? 1u : 0u;
-  for (int o = 16; o; o >>= 1) my_cnt += __shfl_down_sync(0xffffffffu, my_cnt, o);
-  if ((threadIdx.x & 31) == 0) sCnt[threadIdx.x >> 5] = my_cnt;
-  // root sums per class: thread-local in row order, then a fixed-order block reduction
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int k = 0; k < K; ++k) {
-    double g = 0.0, h = 0.0;
-    for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-      const float2 v = P.gh[(size_t)k * c.n + i];
-      g += (double)v.x;
-      h += (double)v.y;
-    }
-    for (int o = 16; o; o >>= 1) {
-      g += __shfl_down_sync(0xffffffffu, g, o);
-      h += __shfl_down_sync(0xffffffffu, h, o);
-    }
-    if (lane == 0) { sG[warp] = g; sH[warp] = h; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double tg = 0.0, th = 0.0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { tg += sG[w]; th += sH[w]; }
-      const size_t o = ((size_t)k * c.PB + blockIdx.x) * L;
-      uint32_t cnt = 0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) cnt += sCnt[w];
-      P.psum[o] = make_double2(tg, th);
-      P.pcnt[o] = cnt;
-    }
-    __syncthreads();
-  }
+  root_sums(c, P, r0, r1);
+}
+
+// GOSS iterations: the gradients of every row are in place (k_grad ran
+// without a sample); the host has since chosen the sample from them.  Rows
+// outside it get zero gradients for all classes, and the root sums and
+// counts are redone over the sample.
+__global__ void __launch_bounds__(512) k_goss_root(DevCfg c, DevPtrs P) {
+  const uint32_t rows_per_block = (c.n + gridDim.x - 1) / gridDim.x;
+  const uint32_t r0 = blockIdx.x * rows_per_block;
+  const uint32_t r1 = min(c.n, r0 + rows_per_block);
+  for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x)
+    if (!row_sampled(c, P, i))
+      for (int k = 0; k < c.K; ++k) P.gh[(size_t)k * c.n + i] = make_float2(0.0f, 0.0f);
+  __syncthreads();
+  root_sums(c, P, r0, r1);
 }
 
 // Applies the last tree's leaves to the predictions (end of training / before
@@ -753,7 +776,9 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(DevCfg c, DevPtrs P, i
       lh += hh[i];
       const int b = lane * 8 + i;
       if (b < c.nb_scan && lh >= 1e-10 && rsh[i] >= 1e-10) {
-        acc[i] += 0.5 * ((lg * lg) / (lh + lam) + (rsg[i] * rsg[i]) / (rsh[i] + lam) - pgain);
+        // GL^2/(HL+lam) + GR^2/(HR+lam) over one FP64 division
+        const double dl = lh + lam, dr = rsh[i] + lam;
+        acc[i] += 0.5 * ((lg * lg * dr + rsg[i] * rsg[i] * dl) / (dl * dr) - pgain);
         anyb |= 1u << i;
       }
     }
@@ -1520,7 +1545,13 @@ struct tc_trainer {
   bool base_known = false;       // base computed from the labels (they do not change)
   double seconds = 0.0;
   bool scores_dirty = false;
-  cudaGraphExec_t graph = nullptr;
+  cudaGraphExec_t graph = nullptr;       // one iteration (batched path)
+  cudaGraphExec_t graph_goss = nullptr;  // a GOSS iteration after its host-side selection
+  void drop_graphs() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (graph_goss) cudaGraphExecDestroy(graph_goss);
+    graph = graph_goss = nullptr;
+  }
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   DevBuf<float> pred;
   DevBuf<float2> gh, cgh;
@@ -1559,13 +1590,21 @@ struct tc_trainer {
   uint32_t* h_mask = nullptr;    // pinned: 2 sets x SAMPLE_CHUNK masks
   cudaEvent_t mask_ev[2] = {nullptr, nullptr};
   int mask_set = 0;
+  // GOSS (optional): the sample of an iteration is chosen on the host from
+  // its gradients
+  bool goss = false;
+  float2* h_gh = nullptr;        // pinned: the iteration's (grad, hess) of every row and class
+  uint32_t* h_gmask = nullptr;   // pinned: its sample mask
+  std::vector<std::pair<float, uint32_t>> goss_rank;
 
   ~tc_trainer() {
     for (cudaEvent_t e : mask_ev)
       if (e) cudaEventDestroy(e);
     if (h_mask) cudaFreeHost(h_mask);
+    if (h_gh) cudaFreeHost(h_gh);
+    if (h_gmask) cudaFreeHost(h_gmask);
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
-    if (graph) cudaGraphExecDestroy(graph);
+    drop_graphs();
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
   }
@@ -1594,7 +1633,12 @@ struct tc_trainer {
   tc_status autotune();
   void launch_level(const DevCfg& c, const DevPtrs& P, int d, cudaStream_t st);
   tc_status enqueue_iteration(cudaStream_t st);
-  tc_status run_plain_iteration(cudaStream_t st);
+  tc_status enqueue_rest(cudaStream_t st);
+  tc_status run_plain_iteration(cudaStream_t st, bool grad = true);
+  uint64_t next_random();
+  tc_status enable_goss();
+  void goss_select(uint64_t seed, uint32_t* words);
+  tc_status goss_iteration(cudaStream_t st);
   tc_status init_predictions();
   tc_status init_validation();
   tc_status set_validation(const tc_dataset* v, int rounds);
@@ -1627,7 +1671,8 @@ tc_status tc_trainer::setup(int) {
   // MSE's hessian is 2 for every row (src/boosting/loss.cpp:348-362)
   // counted hessians need every listed row to carry h = 2; with row
   // sampling the root lists all rows and the unsampled ones carry 0
-  cfg.hconst = (prm.loss == TC_LOSS_MSE && !given_gh && !(prm.subsample > 0.0f && prm.subsample < 1.0f))
+  cfg.hconst = (prm.loss == TC_LOSS_MSE && !given_gh && !(prm.subsample > 0.0f && prm.subsample < 1.0f) &&
+                !prm.use_goss)
                    ? 2.0f : 0.0f;
 
   T_cap = prm.n_estimators * K;
@@ -1714,10 +1759,7 @@ tc_status tc_trainer::configure(int J_, int waves) {
   TC_TRY(cum.alloc(ctx, (size_t)K * Pmax * G + 1, "chunk counts"));
   ptr.part = part.p;
   ptr.cum = cum.p;
-  if (graph) {
-    cudaGraphExecDestroy(graph);
-    graph = nullptr;
-  }
+  drop_graphs();
   return TC_OK;
 }
 
@@ -1884,10 +1926,16 @@ void tc_trainer::launch_level(const DevCfg& c, const DevPtrs& P, int d, cudaStre
 
 // The whole iteration as a fixed launch sequence (graph-capturable).
 tc_status tc_trainer::enqueue_iteration(cudaStream_t st) {
-  const int K = cfg.K, D = cfg.D;
   mark_begin(KC_GRAD, st);
   k_grad<<<cfg.PB, 512, 0, st>>>(cfg, ptr, 0);
-  mark_end(st, (double)cfg.n * K * (4 + 4 + 8 + 2 + 8) + (double)cfg.n * 4);
+  mark_end(st, (double)cfg.n * cfg.K * (4 + 4 + 8 + 2 + 8) + (double)cfg.n * 4);
+  return enqueue_rest(st);
+}
+
+// An iteration after its gradients: root reduce (+ plan of level 0), the
+// levels, the validation step and the iteration counter.
+tc_status tc_trainer::enqueue_rest(cudaStream_t st) {
+  const int K = cfg.K, D = cfg.D;
   mark_begin(KC_REDUCE, st);
   k_node_reduce<true><<<dim3(1, K), 512, 0, st>>>(cfg, ptr, -1);  // + plan of level 0
   mark_end(st);
@@ -1926,9 +1974,9 @@ static DevPtrs class_view(const DevCfg& c, const DevPtrs& P, int k, DevCfg* one)
 
 // The plain path: one class and one level per launch group, a host
 // synchronisation after every level (the host reads the stop flag), no graph.
-tc_status tc_trainer::run_plain_iteration(cudaStream_t st) {
+tc_status tc_trainer::run_plain_iteration(cudaStream_t st, bool grad) {
   const int K = cfg.K, D = cfg.D;
-  k_grad<<<cfg.PB, 512, 0, st>>>(cfg, ptr, 0);
+  if (grad) k_grad<<<cfg.PB, 512, 0, st>>>(cfg, ptr, 0);
   k_node_reduce<false><<<dim3(1, K), 512, 0, st>>>(cfg, ptr, -1);
   for (int k = 0; k < K; ++k) {
     DevCfg one;
@@ -1990,6 +2038,16 @@ tc_status tc_trainer::init_predictions() {
 
 constexpr int SAMPLE_CHUNK = 8;  // iterations per host batch of sample masks / early-stopping look
 
+// Booster::next_random (src/boosting/booster.cpp:1219-1225): xorshift64*.
+uint64_t tc_trainer::next_random() {
+  uint64_t x = rng_state;
+  x ^= x >> 12;
+  x ^= x << 25;
+  x ^= x >> 27;
+  rng_state = x;
+  return x * 0x2545F4914F6CDD1DULL;
+}
+
 // Sample masks of the next m iterations, in iteration order: per iteration an
 // xorshift64* draw seeds the row shuffle (src/boosting/booster.cpp:213-217,
 // src/core/dataset.cpp:552-562: std::shuffle with std::mt19937_64, first
@@ -1997,14 +2055,6 @@ constexpr int SAMPLE_CHUNK = 8;  // iterations per host batch of sample masks / 
 // colsample_bytree < 1 (booster.cpp:223-227; symmetric trees do not use it).
 // The shuffles run on host threads, one per iteration.
 void tc_trainer::make_masks(int m, uint32_t* out) {
-  auto next_random = [this]() {
-    uint64_t x = rng_state;
-    x ^= x >> 12;
-    x ^= x << 25;
-    x ^= x >> 27;
-    rng_state = x;
-    return x * 0x2545F4914F6CDD1DULL;
-  };
   const uint32_t n = cfg.n;
   const size_t words = (n + 31) / 32;
   std::vector<uint64_t> seeds(m);
@@ -2035,12 +2085,122 @@ tc_status tc_trainer::enable_sampling() {
   TC_CUDA(ctx, cudaHostAlloc(reinterpret_cast<void**>(&h_mask), 2 * SAMPLE_CHUNK * words * sizeof(uint32_t),
                              cudaHostAllocDefault));
   for (cudaEvent_t& e : mask_ev) TC_CUDA(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  TC_CUDA(ctx, cudaMemsetAsync(smask.p, 0xff, words * sizeof(uint32_t), ctx->stream));  // until the first sample
   cfg.sampled = 1;
   ptr.smask = smask.p;
-  if (graph) {
-    cudaGraphExecDestroy(graph);
-    graph = nullptr;
+  drop_graphs();
+  return TC_OK;
+}
+
+tc_status tc_trainer::enable_goss() {
+  goss = true;
+  const size_t words = (cfg.n + 31) / 32;
+  TC_TRY(smask.alloc(ctx, words, "row sample mask"));
+  TC_CUDA(ctx, cudaHostAlloc(reinterpret_cast<void**>(&h_gh), (size_t)cfg.K * cfg.n * sizeof(float2),
+                             cudaHostAllocDefault));
+  TC_CUDA(ctx, cudaHostAlloc(reinterpret_cast<void**>(&h_gmask), words * sizeof(uint32_t), cudaHostAllocDefault));
+  goss_rank.resize(cfg.n);
+  TC_CUDA(ctx, cudaMemsetAsync(smask.p, 0xff, words * sizeof(uint32_t), ctx->stream));  // until the first sample
+  cfg.sampled = 1;
+  ptr.smask = smask.p;
+  drop_graphs();
+  return TC_OK;
+}
+
+// The sample of one GOSS iteration from its gradients in h_gh, as
+// Dataset::goss_subsample (src/core/dataset.cpp:494-549): the
+// (uint32)(n * top_rate) rows of largest |g| (std::nth_element over
+// (|g|, row) pairs, descending), then (uint32)(n * other_rate) rows (at most
+// the rest) taken by a partial Fisher-Yates shuffle of the rest as
+// nth_element left it, std::uniform_int_distribution<uint32_t> over
+// std::mt19937_64 seeded by `seed`.  Softmax ranks rows by the largest |g|
+// over the classes (src/boosting/booster.cpp:1327-1348).  The draws reach
+// positions of nth_element's arrangement, so the same library calls are
+// made (libstdc++, as in the reference build); no other order would select
+// the same rows.
+void tc_trainer::goss_select(uint64_t seed, uint32_t* words) {
+  const uint32_t n = cfg.n;
+  const int K = cfg.K;
+  std::memset(words, 0, ((n + 31) / 32) * sizeof(uint32_t));
+  const uint32_t top_n = static_cast<uint32_t>(n * prm.goss_top_rate);  // Index * Float, as the reference
+  uint32_t other_n = static_cast<uint32_t>(n * prm.goss_other_rate);
+  if (top_n == 0 && other_n == 0) return;  // an empty sample: the trees are single leaves of 0
+  auto& a = goss_rank;
+  for (uint32_t i = 0; i < n; ++i) {
+    float m = 0.0f;
+    if (K == 1) {
+      m = std::abs(h_gh[i].x);
+    } else {
+      for (int k = 0; k < K; ++k) m = std::max(m, std::abs(h_gh[(size_t)k * n + i].x));
+    }
+    a[i] = {m, i};
   }
+  if (top_n > 0 && top_n < n)
+    std::nth_element(a.begin(), a.begin() + top_n, a.end(),
+                     [](const std::pair<float, uint32_t>& l, const std::pair<float, uint32_t>& r) {
+                       return l.first > r.first;
+                     });
+  auto keep = [words](uint32_t row) { words[row >> 5] |= 1u << (row & 31); };
+  for (uint32_t i = 0; i < top_n; ++i) keep(a[i].second);
+  if (other_n > 0 && top_n < n) {
+    const uint32_t rest = n - top_n;
+    other_n = std::min(other_n, rest);
+    std::mt19937_64 rng(seed);
+    for (uint32_t i = 0; i < other_n; ++i) {
+      std::uniform_int_distribution<uint32_t> pick(i, rest - 1);
+      const uint32_t j = pick(rng);
+      if (i != j) std::swap(a[top_n + i], a[top_n + j]);
+      keep(a[top_n + i].second);
+    }
+  }
+}
+
+// One GOSS iteration: the gradients of every row (k_grad without a sample),
+// copied to the host, which draws the iteration's random numbers (the GOSS
+// seed, then the feature-subset draw when colsample_bytree < 1) and picks the
+// sample; then the rest of the iteration (one graph on the batched path).
+tc_status tc_trainer::goss_iteration(cudaStream_t st) {
+  const uint32_t n = cfg.n;
+  const size_t words = (n + 31) / 32;
+  DevCfg all = cfg;
+  all.sampled = 0;
+  mark_begin(KC_GRAD, st);
+  k_grad<<<cfg.PB, 512, 0, st>>>(all, ptr, 0);
+  mark_end(st, (double)n * cfg.K * (4 + 4 + 8 + 2 + 8) + (double)n * 4);
+  TC_CUDA(ctx, cudaGetLastError());
+  TC_CUDA(ctx, cudaMemcpyAsync(h_gh, gh.p, (size_t)cfg.K * n * sizeof(float2), cudaMemcpyDeviceToHost, st));
+  TC_CUDA(ctx, cudaStreamSynchronize(st));
+  const uint64_t seed = next_random();
+  if (prm.colsample_bytree > 0.0f && prm.colsample_bytree < 1.0f) (void)next_random();
+  goss_select(seed, h_gmask);
+  TC_CUDA(ctx, cudaMemcpyAsync(smask.p, h_gmask, words * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+  if (prm.batched && !prof) {
+    if (!graph_goss) {
+      cudaGraph_t g;
+      const int64_t l0 = launches;
+      TC_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      k_goss_root<<<cfg.PB, 512, 0, st>>>(cfg, ptr);
+      ++launches;
+      enqueue_rest(st);
+      TC_CUDA(ctx, cudaStreamEndCapture(st, &g));
+      launches_per_iter = (int)(launches - l0);
+      launches = l0;
+      cudaError_t e = cudaGraphInstantiate(&graph_goss, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return ctx->cuda_fail(e, "cudaGraphInstantiate");
+    }
+    TC_CUDA(ctx, cudaGraphLaunch(graph_goss, st));
+    launches += launches_per_iter;
+  } else if (prm.batched) {  // profiled: launch by launch
+    mark_begin(KC_OTHER, st);
+    k_goss_root<<<cfg.PB, 512, 0, st>>>(cfg, ptr);
+    mark_end(st, (double)n * cfg.K * 8.0);
+    enqueue_rest(st);
+  } else {
+    k_goss_root<<<cfg.PB, 512, 0, st>>>(cfg, ptr);
+    TC_TRY(run_plain_iteration(st, false));
+  }
+  TC_CUDA(ctx, cudaGetLastError());
   return TC_OK;
 }
 
@@ -2081,10 +2241,7 @@ tc_status tc_trainer::set_validation(const tc_dataset* v, int rounds) {
   ptr.vpart = vpart.p;
   ptr.vloss = vloss.p;
   ptr.es = es.p;
-  if (graph) {
-    cudaGraphExecDestroy(graph);
-    graph = nullptr;
-  }
+  drop_graphs();
   return init_validation();
 }
 
@@ -2093,6 +2250,10 @@ tc_status tc_trainer::set_validation(const tc_dataset* v, int rounds) {
 // sample mask, the masks of a batch being made on the host while the
 // previous batch runs.
 tc_status tc_trainer::launch_iterations(int m, cudaStream_t st) {
+  if (goss) {
+    for (int i = 0; i < m; ++i) TC_TRY(goss_iteration(st));
+    return TC_OK;
+  }
   if (prm.batched && !graph) {
     cudaGraph_t g;
     const int64_t l0 = launches;
@@ -2138,7 +2299,7 @@ tc_status tc_trainer::step(int iters, bool sync) {
   if (iters == 0 || es_stopped) return TC_OK;
   TC_CUDA(ctx, cudaEventRecord(ev0, st));
   int done = 0;
-  if (cfg.nv == 0 && !sampling) {
+  if (cfg.nv == 0 && !sampling && !goss) {
     TC_TRY(launch_iterations(iters, st));
     done = iters;
   } else {
@@ -2189,6 +2350,9 @@ static tc_status validate(tc_ctx* ctx, const tc_dataset* ds, const tc_train_para
     return ctx->fail(TC_ERR_INVALID_ARG, "softmax needs 3 <= n_classes <= 16");
   if (p->n_estimators < 0) return ctx->fail(TC_ERR_INVALID_ARG, "n_estimators must be >= 0");
   if (ds->n == 0) return ctx->fail(TC_ERR_INVALID_ARG, "empty dataset");
+  if (p->use_goss && !(p->goss_top_rate >= 0.0f && p->goss_top_rate <= 1.0f && p->goss_other_rate >= 0.0f &&
+                       p->goss_other_rate <= 1.0f))
+    return ctx->fail(TC_ERR_INVALID_ARG, "goss_top_rate and goss_other_rate must be in [0, 1]");
   if (p->loss != TC_LOSS_SOFTMAX || true) {
     if (!ds->y.p) return ctx->fail(TC_ERR_INVALID_ARG, "dataset has no labels");
   }
@@ -2212,7 +2376,8 @@ tc_status tc_trainer_create(tc_ctx* ctx, tc_dataset* ds, const tc_train_params* 
   // tuning runs up to three throw-away iterations: it needs that many tree slots
   if (s == TC_OK && p->hist_features_per_block == 0 && p->n_estimators >= 3) s = tr->autotune();
   // row sampling starts after tuning (the tuner's trial iterations use every row)
-  if (s == TC_OK && p->subsample > 0.0f && p->subsample < 1.0f) s = tr->enable_sampling();
+  if (s == TC_OK && p->use_goss) s = tr->enable_goss();  // GOSS is chosen over subsample (booster.cpp:200-219)
+  else if (s == TC_OK && p->subsample > 0.0f && p->subsample < 1.0f) s = tr->enable_sampling();
   if (s != TC_OK) {
     delete tr;
     return s;
@@ -2289,7 +2454,15 @@ tc_status tc_trainer_profile(tc_trainer* tr, int32_t iterations, tc_profile* out
       TC_CUDA(ctx, cudaMemcpyAsync(tr->smask.p, mask.data(), mask.size() * sizeof(uint32_t),
                                    cudaMemcpyHostToDevice, st));
     }
-    tr->enqueue_iteration(st);
+    if (tr->goss) {
+      tc_status gs = tr->goss_iteration(st);
+      if (gs != TC_OK) {
+        tr->prof = nullptr;
+        return gs;
+      }
+    } else {
+      tr->enqueue_iteration(st);
+    }
     // harvest every iteration so that the event pool stays small
     cudaError_t e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
@@ -2319,6 +2492,23 @@ tc_status tc_trainer_profile(tc_trainer* tr, int32_t iterations, tc_profile* out
   for (int c = 0; c < KC_N; ++c) {
     std::strncpy(out->k[c].name, kKernelNames[c], sizeof(out->k[c].name) - 1);
   }
+  return TC_OK;
+}
+
+tc_status tc_trainer_sample_mask(tc_trainer* tr, uint32_t* out) {
+  if (!tr || !out) return TC_ERR_INVALID_ARG;
+  tc_ctx* ctx = tr->ctx;
+  std::lock_guard<std::recursive_mutex> train_lock(ctx->train_mu);
+  cudaSetDevice(ctx->device);
+  const uint32_t n = tr->cfg.n;
+  const size_t words = (n + 31) / 32;
+  if (tr->sampling || tr->goss) {
+    TC_CUDA(ctx, cudaMemcpyAsync(out, tr->smask.p, words * sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    TC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  } else {
+    std::fill(out, out + words, 0xffffffffu);
+  }
+  if (n % 32) out[words - 1] &= (1u << (n % 32)) - 1u;
   return TC_OK;
 }
 

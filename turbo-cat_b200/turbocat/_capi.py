@@ -27,7 +27,7 @@ SYMBOLS = [
     "tc_ctx_create", "tc_ctx_destroy", "tc_last_error", "tc_ctx_memory", "tc_ctx_fail_next_allocs",
     "tc_ctx_synchronize", "tc_dataset_upload", "tc_dataset_destroy", "tc_quantize", "tc_dataset_bins",
     "tc_trainer_create", "tc_trainer_step", "tc_trainer_reset", "tc_trainer_stats", "tc_trainer_profile",
-    "tc_trainer_train_scores", "tc_trainer_set_validation", "tc_trainer_valid_loss",
+    "tc_trainer_train_scores", "tc_trainer_sample_mask", "tc_trainer_set_validation", "tc_trainer_valid_loss",
     "tc_trainer_model", "tc_trainer_destroy", "tc_train", "tc_build_tree", "tc_histogram_root_noalloc",
     "tc_model_info_get", "tc_model_export",
     "tc_model_import", "tc_model_save_tcat", "tc_model_load_tcat", "tc_model_destroy", "tc_predict",
@@ -44,7 +44,8 @@ class TrainParams(C.Structure):
         ("min_split_gain", C.c_float), ("max_delta_step", C.c_float), ("focal_gamma", C.c_float),
         ("focal_alpha", C.c_float), ("batched", C.c_int32), ("hist_features_per_block", C.c_int32),
         ("hist_rows_per_chunk", C.c_int32), ("subsample", C.c_float), ("colsample_bytree", C.c_float),
-        ("seed", C.c_uint64),
+        ("seed", C.c_uint64), ("use_goss", C.c_int32), ("goss_top_rate", C.c_float),
+        ("goss_other_rate", C.c_float),
     ]
 
 
@@ -108,11 +109,13 @@ def _p(a):
 def params(loss="logloss", n_classes=1, n_estimators=10, max_depth=6, max_bins=255, min_samples_leaf=1,
            learning_rate=0.1, lambda_l2=1.0, lambda_l1=0.0, min_child_weight=1.0, min_split_gain=0.0,
            max_delta_step=0.0, focal_gamma=2.0, focal_alpha=0.25, batched=1, hist_features_per_block=0,
-           hist_rows_per_chunk=0, subsample=1.0, colsample_bytree=1.0, seed=42) -> TrainParams:
+           hist_rows_per_chunk=0, subsample=1.0, colsample_bytree=1.0, seed=42, use_goss=False,
+           goss_top_rate=0.2, goss_other_rate=0.1) -> TrainParams:
     return TrainParams(LOSS[loss] if isinstance(loss, str) else loss, n_classes, n_estimators, max_depth, max_bins,
                        min_samples_leaf, learning_rate, lambda_l2, lambda_l1, min_child_weight, min_split_gain,
                        max_delta_step, focal_gamma, focal_alpha, batched, hist_features_per_block,
-                       hist_rows_per_chunk, subsample, colsample_bytree, seed)
+                       hist_rows_per_chunk, subsample, colsample_bytree, seed, 1 if use_goss else 0,
+                       goss_top_rate, goss_other_rate)
 
 
 class Model:
@@ -230,6 +233,12 @@ class Trainer:
         out = np.zeros((n, self.K), np.float32)
         self.eng._chk(lib().tc_trainer_train_scores(self.h, _p(out)))
         return out
+
+    def sample_mask(self, n):
+        """Rows (bool [n]) the last iteration's trees were built on."""
+        words = np.zeros((n + 31) // 32, np.uint32)
+        self.eng._chk(lib().tc_trainer_sample_mask(self.h, _p(words)))
+        return np.unpackbits(words.view(np.uint8), bitorder="little")[:n].astype(bool)
 
     def model(self) -> Model:
         m = C.c_void_p()
