@@ -52,9 +52,21 @@ __device__ __forceinline__ void walk_full(const uint2* __restrict__ s_split, con
   constexpr int L = 1 << DD;
   uint2 q[NT][DD];
 #pragma unroll
-  for (int u = 0; u < NT; ++u)
+  for (int u = 0; u < NT; ++u) {
+    if constexpr (DD % 2 == 0) {
+      // a tree's splits start on a 16-byte boundary: two per 128-bit load
+      const uint4* sp = reinterpret_cast<const uint4*>(s_split + (t + u * TG) * DD);
 #pragma unroll
-    for (int d = 0; d < DD; ++d) q[u][d] = s_split[(t + u * TG) * DD + d];
+      for (int d = 0; d < DD / 2; ++d) {
+        const uint4 v = sp[d];
+        q[u][2 * d] = make_uint2(v.x, v.y);
+        q[u][2 * d + 1] = make_uint2(v.z, v.w);
+      }
+    } else {
+#pragma unroll
+      for (int d = 0; d < DD; ++d) q[u][d] = s_split[(t + u * TG) * DD + d];
+    }
+  }
   float xv[NT][DD];
 #pragma unroll
   for (int u = 0; u < NT; ++u)
@@ -64,7 +76,8 @@ __device__ __forceinline__ void walk_full(const uint2* __restrict__ s_split, con
   for (int u = 0; u < NT; ++u) {
     uint32_t idx = 0;
 #pragma unroll
-    for (int d = 0; d < DD; ++d) idx = (idx << 1) | (uint32_t)(xv[u][d] >= __uint_as_float(q[u][d].y));
+    for (int d = 0; d < DD; ++d)
+      if (xv[u][d] >= __uint_as_float(q[u][d].y)) idx |= 1u << (DD - 1 - d);  // false for NaN
     const float v = lv[(t + u * TG) * L + idx];
     if (u == 0) sum.x += v;
     else if (u == 1) sum.y += v;
@@ -132,8 +145,13 @@ __global__ void __launch_bounds__(PRED_THREADS) k_predict(JobTable jt) {
       for (int q = threadIdx.x; q < tn * L; q += blockDim.x) s_leaf[q] = md.leaves[(size_t)t0 * L + q];
     const float* lv = leaves_global ? md.leaves + (size_t)t0 * L : s_leaf;
     for (int q = threadIdx.x; q < tn * D; q += blockDim.x) s_split[q] = md.splits[(size_t)t0 * D + q];
-    for (int q = threadIdx.x; q < tn; q += blockDim.x) s_depth[q] = md.depth[t0 + q];
-    __syncthreads();
+    bool full_here = true;
+    for (int q = threadIdx.x; q < tn; q += blockDim.x) {
+      const int dq = md.depth[t0 + q];
+      s_depth[q] = dq;
+      full_here = full_here && dq == D;
+    }
+    const bool all_full = __syncthreads_and(full_here) != 0;  // every tree of the chunk has depth D
     if ((uint32_t)row < nr) {
       if (K == 1) {
         // full-depth trees in groups (depth <= 8: 4 at a time, 9-10: 2),
@@ -143,9 +161,11 @@ __global__ void __launch_bounds__(PRED_THREADS) k_predict(JobTable jt) {
         const int NT = D <= 8 ? 4 : 2;
         if (D <= 10) {
           for (; t + (NT - 1) * TG < tn; t += NT * TG) {
-            bool full = true;
-            for (int u = 0; u < NT; ++u) full = full && s_depth[t + u * TG] == D;
-            if (!full) break;
+            if (!all_full) {
+              bool full = true;
+              for (int u = 0; u < NT; ++u) full = full && s_depth[t + u * TG] == D;
+              if (!full) break;
+            }
             switch (D) {
               case 1: walk_full<4, 1>(s_split, xr, lv, t, TG, s4); break;
               case 2: walk_full<4, 2>(s_split, xr, lv, t, TG, s4); break;
