@@ -14,8 +14,9 @@
 // tile's rows are staged in shared memory (row stride f+1 words, so threads
 // reading the same feature of different rows hit different banks), trees are
 // streamed through shared memory in chunks of packed (feature, threshold)
-// pairs and weight-folded leaves, and every thread walks all trees for its
-// row.
+// pairs and weight-folded leaves, two chunks in flight (cp.async: the next
+// chunk lands while the current one is walked), and every thread walks all
+// trees for its row.
 #include <algorithm>
 #include <cstring>
 
@@ -26,8 +27,24 @@ namespace {
 
 constexpr int PRED_ROWS = 128;
 constexpr int PRED_THREADS = 512;                 // a row tile: up to 128 rows x 4 tree groups
-constexpr int PRED_LEAF_FLOATS = 8192;      // shared floats for one chunk of leaves (32 KB)
+constexpr int PRED_LEAF_FLOATS = 8192;      // shared floats for two chunks of leaves (2 x 16 KB)
+constexpr int PRED_LEAF_STAGE = PRED_LEAF_FLOATS / 2;
+constexpr int PRED_CHUNK = 128;             // trees per chunk at most (two chunks in flight)
 constexpr int PRED_MAX_K = 16;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void cp_async4(void* s, const void* g) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_addr(s)), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* s, const void* g) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_addr(s)), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* s, const void* g) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(s)), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 struct JobTable {
   const ReqDesc* reqs;         // nullptr: single job held inline
@@ -119,18 +136,40 @@ __global__ void __launch_bounds__(PRED_THREADS) k_predict(JobTable jt) {
   const int D = md.max_depth;
   const int L = 1 << D;
   // leaves of shallow trees are staged in shared memory with the splits;
-  // deep trees (more than 256 leaves) gather their leaf from global memory
-  // (L2), so a chunk still holds 256 trees' splits
-  const bool leaves_global = L > 256;
-  const int tchunk = leaves_global ? 256 : max(1, min(256, PRED_LEAF_FLOATS / L));
+  // deeper trees (256 leaves or more) gather their leaf from global memory
+  // (L2), so a chunk still holds PRED_CHUNK trees' splits
+  const bool leaves_global = L >= 256;
+  const int tchunk = leaves_global ? PRED_CHUNK : max(1, min(PRED_CHUNK, PRED_LEAF_STAGE / L));
+  const int Dmax = max(1, jt.max_depth);
   float* s_x = smp;                                  // [PRED_ROWS][f+1]
-  float* s_leaf = s_x + PRED_ROWS * (jt.max_f + 1);  // [tchunk][L]
-  uint2* s_split = reinterpret_cast<uint2*>(s_leaf + PRED_LEAF_FLOATS);  // [tchunk][D]
-  int* s_depth = reinterpret_cast<int*>(s_split + 256 * max(1, jt.max_depth));
+  float* s_leaf = s_x + PRED_ROWS * (jt.max_f + 1);  // 2 x [tchunk][L]
+  uint2* s_split = reinterpret_cast<uint2*>(s_leaf + PRED_LEAF_FLOATS);  // 2 x [tchunk][D]
+  int* s_depth = reinterpret_cast<int*>(s_split + 2 * PRED_CHUNK * Dmax);  // 2 x [tchunk]
+  // Every copy into shared memory is asynchronous (cp.async): the row tile
+  // and the first tree chunk, then chunk c + 1 while chunk c is walked.
   const float* Xt = rq.X + (size_t)r0 * f;
   // a warp copies whole rows (lane = feature), no division by f
   for (uint32_t i = threadIdx.x >> 5; i < nr; i += blockDim.x >> 5)
-    for (int j = threadIdx.x & 31; j < f; j += 32) s_x[i * fs + j] = Xt[(size_t)i * f + j];
+    for (int j = threadIdx.x & 31; j < f; j += 32) cp_async4(&s_x[i * fs + j], &Xt[(size_t)i * f + j]);
+  auto issue_chunk = [&](int t0, int buf) {
+    const int tn = min(tchunk, md.n_trees - t0);
+    if (!leaves_global) {
+      float* dl = s_leaf + buf * PRED_LEAF_STAGE;
+      const float* gl = md.leaves + (size_t)t0 * L;
+      const int cnt = tn * L;
+      if ((((size_t)t0 * L) & 3) == 0 && (cnt & 3) == 0) {
+        for (int q = threadIdx.x; q < cnt / 4; q += blockDim.x) cp_async16(dl + 4 * q, gl + 4 * q);
+      } else {
+        for (int q = threadIdx.x; q < cnt; q += blockDim.x) cp_async4(dl + q, gl + q);
+      }
+    }
+    uint2* ds = s_split + buf * PRED_CHUNK * Dmax;
+    for (int q = threadIdx.x; q < tn * D; q += blockDim.x) cp_async8(ds + q, md.splits + (size_t)t0 * D + q);
+    int* dd = s_depth + buf * PRED_CHUNK;
+    for (int q = threadIdx.x; q < tn; q += blockDim.x) cp_async4(dd + q, md.depth + t0 + q);
+  };
+  if (md.n_trees > 0) issue_chunk(0, 0);
+  cp_async_commit();
   const int K = md.n_classes;
   float acc[PRED_MAX_K];
 #pragma unroll
@@ -138,20 +177,18 @@ __global__ void __launch_bounds__(PRED_THREADS) k_predict(JobTable jt) {
   const int row = threadIdx.x % RT;
   const int tg = threadIdx.x / RT;
   const float* xr = s_x + row * fs;
-  for (int t0 = 0; t0 < md.n_trees; t0 += tchunk) {
+  for (int t0 = 0, buf = 0; t0 < md.n_trees; t0 += tchunk, buf ^= 1) {
     const int tn = min(tchunk, md.n_trees - t0);
-    __syncthreads();
-    if (!leaves_global)
-      for (int q = threadIdx.x; q < tn * L; q += blockDim.x) s_leaf[q] = md.leaves[(size_t)t0 * L + q];
-    const float* lv = leaves_global ? md.leaves + (size_t)t0 * L : s_leaf;
-    for (int q = threadIdx.x; q < tn * D; q += blockDim.x) s_split[q] = md.splits[(size_t)t0 * D + q];
+    if (t0 + tchunk < md.n_trees) issue_chunk(t0 + tchunk, buf ^ 1);
+    cp_async_commit();
+    cp_async_wait_prev();  // this thread's copies of the row tile and of chunk t0 have landed
+    const float* lv = leaves_global ? md.leaves + (size_t)t0 * L : s_leaf + buf * PRED_LEAF_STAGE;
+    const uint2* s_split_c = s_split + buf * PRED_CHUNK * Dmax;
+    const int* s_depth_c = s_depth + buf * PRED_CHUNK;
     bool full_here = true;
-    for (int q = threadIdx.x; q < tn; q += blockDim.x) {
-      const int dq = md.depth[t0 + q];
-      s_depth[q] = dq;
-      full_here = full_here && dq == D;
-    }
-    const bool all_full = __syncthreads_and(full_here) != 0;  // every tree of the chunk has depth D
+    for (int q = threadIdx.x; q < tn; q += blockDim.x) full_here = full_here && s_depth_c[q] == D;
+    // the barrier also publishes every thread's copies; every tree of the chunk has depth D?
+    const bool all_full = __syncthreads_and(full_here) != 0;
     if ((uint32_t)row < nr) {
       if (K == 1) {
         // full-depth trees in groups (depth <= 8: 4 at a time, 9-10: 2),
@@ -163,26 +200,26 @@ __global__ void __launch_bounds__(PRED_THREADS) k_predict(JobTable jt) {
           for (; t + (NT - 1) * TG < tn; t += NT * TG) {
             if (!all_full) {
               bool full = true;
-              for (int u = 0; u < NT; ++u) full = full && s_depth[t + u * TG] == D;
+              for (int u = 0; u < NT; ++u) full = full && s_depth_c[t + u * TG] == D;
               if (!full) break;
             }
             switch (D) {
-              case 1: walk_full<4, 1>(s_split, xr, lv, t, TG, s4); break;
-              case 2: walk_full<4, 2>(s_split, xr, lv, t, TG, s4); break;
-              case 3: walk_full<4, 3>(s_split, xr, lv, t, TG, s4); break;
-              case 4: walk_full<4, 4>(s_split, xr, lv, t, TG, s4); break;
-              case 5: walk_full<4, 5>(s_split, xr, lv, t, TG, s4); break;
-              case 6: walk_full<4, 6>(s_split, xr, lv, t, TG, s4); break;
-              case 7: walk_full<4, 7>(s_split, xr, lv, t, TG, s4); break;
-              case 8: walk_full<4, 8>(s_split, xr, lv, t, TG, s4); break;
-              case 9: walk_full<2, 9>(s_split, xr, lv, t, TG, s4); break;
-              default: walk_full<2, 10>(s_split, xr, lv, t, TG, s4); break;
+              case 1: walk_full<4, 1>(s_split_c, xr, lv, t, TG, s4); break;
+              case 2: walk_full<4, 2>(s_split_c, xr, lv, t, TG, s4); break;
+              case 3: walk_full<4, 3>(s_split_c, xr, lv, t, TG, s4); break;
+              case 4: walk_full<4, 4>(s_split_c, xr, lv, t, TG, s4); break;
+              case 5: walk_full<4, 5>(s_split_c, xr, lv, t, TG, s4); break;
+              case 6: walk_full<4, 6>(s_split_c, xr, lv, t, TG, s4); break;
+              case 7: walk_full<4, 7>(s_split_c, xr, lv, t, TG, s4); break;
+              case 8: walk_full<4, 8>(s_split_c, xr, lv, t, TG, s4); break;
+              case 9: walk_full<2, 9>(s_split_c, xr, lv, t, TG, s4); break;
+              default: walk_full<2, 10>(s_split_c, xr, lv, t, TG, s4); break;
             }
           }
         }
         for (; t < tn; t += TG) {
-          const int dep = s_depth[t];
-          const uint2* sp = s_split + t * D;
+          const int dep = s_depth_c[t];
+          const uint2* sp = s_split_c + t * D;
           uint32_t idx = 0;
           for (int d = 0; d < dep; ++d) {
             const uint2 q = sp[d];
@@ -193,8 +230,8 @@ __global__ void __launch_bounds__(PRED_THREADS) k_predict(JobTable jt) {
         acc[0] += (s4.x + s4.y) + (s4.z + s4.w);
       } else {
         for (int t = tg; t < tn; t += TG) {
-          const int dep = s_depth[t];
-          const uint2* sp = s_split + t * D;
+          const int dep = s_depth_c[t];
+          const uint2* sp = s_split_c + t * D;
           uint32_t idx = 0;
           for (int d = 0; d < dep; ++d) {
             const uint2 q = sp[d];
@@ -208,7 +245,9 @@ __global__ void __launch_bounds__(PRED_THREADS) k_predict(JobTable jt) {
         }
       }
     }
+    __syncthreads();  // chunk t0's buffers are refilled by the next iteration's copies
   }
+  cp_async_wait_all();
   // combine the thread groups' partial sums (pairwise, fixed order)
   __syncthreads();
   float* s_red = s_leaf;  // [TG][RT][K]: TG*RT = PRED_THREADS, 512*16 floats = PRED_LEAF_FLOATS
@@ -254,8 +293,8 @@ __global__ void __launch_bounds__(PRED_THREADS) k_predict(JobTable jt) {
 }
 
 size_t predict_smem(int max_f, int max_depth) {
-  return (size_t)PRED_ROWS * (max_f + 1) * 4 + PRED_LEAF_FLOATS * 4 + (size_t)256 * std::max(1, max_depth) * 8 +
-         256 * 4;
+  return (size_t)PRED_ROWS * (max_f + 1) * 4 + PRED_LEAF_FLOATS * 4 +
+         (size_t)2 * PRED_CHUNK * std::max(1, max_depth) * 8 + 2 * PRED_CHUNK * 4;
 }
 
 tc_status launch_predict(tc_ctx* ctx, const JobTable& jt, uint32_t n_tiles, cudaStream_t stream) {
