@@ -51,8 +51,10 @@ namespace {
 constexpr int HIST_THREADS = 512;
 constexpr int HIST_BATCH = 32;    // rows per warp batch (one per lane)
 constexpr int PART_THREADS = 512;
+constexpr int GRAD_UNROLL = 4;    // rows per thread with their loads in flight together (one class)
+constexpr int kSoftmaxMaxK = 16;  // softmax classes at most (checked when a trainer is created)
 constexpr int SCAN_WARPS = 8;     // warps per scan block
-constexpr int SCAN_NODES = 32;    // nodes per scan block (4 per warp)
+constexpr int SCAN_NODES = 16;    // nodes per scan block (2 per warp; measured: 32 per block 4% slower on 1M x 100 depth 8)
 static_assert(SCAN_WARPS * 32 == 256, "a scan block also runs the 256-thread pick");
 constexpr int MERGE_BB = 4;       // bins per merge block
 constexpr int PLAN_THREADS = 1024;
@@ -221,86 +223,162 @@ __device__ __forceinline__ void loss_grad(int loss, float pred, float y, uint32_
 // (preds += lr * leaf, fused multiply-add as in src/boosting/booster.cpp:458-463),
 // computes the gradients and resets the leaf ids; then per-block root sums
 // (FP64, fixed order) go to psum[k][block][0] / pcnt.
-// Root sums of the block's rows [r0, r1) per class (FP64, thread-local in
-// row order then a fixed-order block reduction) and their sampled count,
-// into the block's slot of the partition sums (the level -1 reduce reads them).
-__device__ void root_sums(const DevCfg& c, const DevPtrs& P, uint32_t r0, uint32_t r1) {
+// One class's root sums: per-thread FP64 partials (rows in increasing
+// order), reduced in a fixed order (warp shuffles, then the warps in order)
+// into the block's slot of the partition sums, which the level -1 reduce
+// reads; cnt = the thread's sampled rows.
+__device__ void store_root_partials(const DevCfg& c, const DevPtrs& P, int k, double g, double h, uint32_t cnt) {
   __shared__ double sG[16], sH[16];
   __shared__ uint32_t sCnt[16];
-  const int K = c.K;
-  const int L = 1 << c.D;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int o = 16; o; o >>= 1) {
+    g += __shfl_down_sync(0xffffffffu, g, o);
+    h += __shfl_down_sync(0xffffffffu, h, o);
+    cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+  }
+  if (lane == 0) { sG[warp] = g; sH[warp] = h; sCnt[warp] = cnt; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tg = 0.0, th = 0.0;
+    uint32_t tc = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { tg += sG[w]; th += sH[w]; tc += sCnt[w]; }
+    const size_t o = ((size_t)k * c.PB + blockIdx.x) * (1 << c.D);
+    P.psum[o] = make_double2(tg, th);
+    P.pcnt[o] = tc;
+  }
+  __syncthreads();
+}
+
+// Root sums of the block's rows [r0, r1) for every class, from P.gh.
+__device__ void root_sums(const DevCfg& c, const DevPtrs& P, uint32_t r0, uint32_t r1) {
   uint32_t my_cnt = 0;
   for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) my_cnt += row_sampled(c, P, i) ? 1u : 0u;
-  for (int o = 16; o; o >>= 1) my_cnt += __shfl_down_sync(0xffffffffu, my_cnt, o);
-  if ((threadIdx.x & 31) == 0) sCnt[threadIdx.x >> 5] = my_cnt;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int k = 0; k < K; ++k) {
+  for (int k = 0; k < c.K; ++k) {
     double g = 0.0, h = 0.0;
     for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
       const float2 v = P.gh[(size_t)k * c.n + i];
       g += (double)v.x;
       h += (double)v.y;
     }
-    for (int o = 16; o; o >>= 1) {
-      g += __shfl_down_sync(0xffffffffu, g, o);
-      h += __shfl_down_sync(0xffffffffu, h, o);
-    }
-    if (lane == 0) { sG[warp] = g; sH[warp] = h; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double tg = 0.0, th = 0.0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { tg += sG[w]; th += sH[w]; }
-      const size_t o = ((size_t)k * c.PB + blockIdx.x) * L;
-      uint32_t cnt = 0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) cnt += sCnt[w];
-      P.psum[o] = make_double2(tg, th);
-      P.pcnt[o] = cnt;
-    }
-    __syncthreads();
+    store_root_partials(c, P, k, g, h, my_cnt);
   }
 }
 
-__global__ void __launch_bounds__(512) k_grad(DevCfg c, DevPtrs P, int use_given_gh) {
-  const int K = c.K;
+// SOFTMAX: the K-class path (the row's classes loaded together); else one class.
+template <bool SOFTMAX>
+__global__ void __launch_bounds__(512, 2) k_grad(DevCfg c, DevPtrs P, int use_given_gh) {
+  const int K = SOFTMAX ? c.K : 1;
   const int it = *P.iter;
   const uint32_t n_vec = (c.n / 8) * 8;
   const uint32_t rows_per_block = (c.n + gridDim.x - 1) / gridDim.x;
   const uint32_t r0 = blockIdx.x * rows_per_block;
   const uint32_t r1 = min(c.n, r0 + rows_per_block);
   const int L = 1 << c.D;
+  if (!SOFTMAX) {
+    // one class: GRAD_UNROLL rows per thread with their loads issued first,
+    // and the root sums taken on the way (same rows, same order as root_sums)
+    const bool upd = it > 0 && !use_given_gh;
+    const size_t tl = upd ? ((size_t)(it - 1) * c.KT + c.k0) * L : 0;
+    double sg = 0.0, sh = 0.0;
+    uint32_t cnt = 0;
+    for (uint32_t base = r0 + threadIdx.x; base < r1; base += blockDim.x * GRAD_UNROLL) {
+      float pr[GRAD_UNROLL], yv[GRAD_UNROLL], lv[GRAD_UNROLL];
+      uint16_t lf[GRAD_UNROLL];
+      float2 given[GRAD_UNROLL];
+#pragma unroll
+      for (int u = 0; u < GRAD_UNROLL; ++u) {
+        const uint32_t i = base + u * blockDim.x;
+        if (i < r1) {
+          if (upd) lf[u] = P.leaf[i];
+          if (!use_given_gh) {
+            pr[u] = P.pred[i];
+            yv[u] = P.y[i];
+          } else {
+            given[u] = P.gh[i];
+          }
+        }
+      }
+      if (upd) {
+#pragma unroll
+        for (int u = 0; u < GRAD_UNROLL; ++u)
+          if (base + u * blockDim.x < r1) lv[u] = P.m_leaves[tl + lf[u]];
+      }
+#pragma unroll
+      for (int u = 0; u < GRAD_UNROLL; ++u) {
+        const uint32_t i = base + u * blockDim.x;
+        if (i >= r1) continue;
+        const bool in = row_sampled(c, P, i);
+        float2 v;
+        if (!use_given_gh) {
+          float p = pr[u];
+          if (upd) {
+            p = __fmaf_rn(c.lr, lv[u], p);
+            P.pred[i] = p;
+          }
+          float g, h;
+          loss_grad(c.loss, p, yv[u], i, n_vec, c.gamma, c.alpha, g, h);
+          // rows outside this iteration's sample add nothing to any sum
+          v = in ? make_float2(g, h) : make_float2(0.0f, 0.0f);
+          P.gh[i] = v;
+        } else {
+          v = given[u];
+        }
+        P.leaf[i] = 0;
+        sg += (double)v.x;
+        sh += (double)v.y;
+        cnt += in ? 1u : 0u;
+      }
+    }
+    store_root_partials(c, P, 0, sg, sh, cnt);
+    return;
+  }
+  // softmax (K classes, K <= 16): a row's K predictions and leaf ids are
+  // loaded together (unrolled over the class bound, guarded by K)
   for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+    float pr[kSoftmaxMaxK];
+#pragma unroll
+    for (int k = 0; k < kSoftmaxMaxK; ++k)
+      if (k < K) pr[k] = P.pred[(size_t)k * c.n + i];
     if (it > 0 && !use_given_gh) {
-      for (int k = 0; k < K; ++k) {
-        const size_t t = (size_t)(it - 1) * c.KT + c.k0 + k;
-        const float v = P.m_leaves[t * L + P.leaf[(size_t)k * c.n + i]];
-        float& pr = P.pred[(size_t)k * c.n + i];
-        pr = __fmaf_rn(c.lr, v, pr);
+      uint16_t lf[kSoftmaxMaxK];
+#pragma unroll
+      for (int k = 0; k < kSoftmaxMaxK; ++k)
+        if (k < K) lf[k] = P.leaf[(size_t)k * c.n + i];
+      const size_t t0 = (size_t)(it - 1) * c.KT + c.k0;
+#pragma unroll
+      for (int k = 0; k < kSoftmaxMaxK; ++k) {
+        if (k < K) {
+          pr[k] = __fmaf_rn(c.lr, P.m_leaves[(t0 + k) * L + lf[k]], pr[k]);
+          P.pred[(size_t)k * c.n + i] = pr[k];
+        }
       }
     }
     if (!use_given_gh) {
-      if (c.loss == TC_LOSS_SOFTMAX) {
-        // CrossEntropyLoss::compute_multiclass_gradients + softmax (src/boosting/loss.cpp:273-318)
-        float mx = P.pred[i];
-        for (int k = 1; k < K; ++k) mx = fmaxf(mx, P.pred[(size_t)k * c.n + i]);
-        float sum = 0.0f;
-        for (int k = 0; k < K; ++k) sum = __fadd_rn(sum, expf(__fsub_rn(P.pred[(size_t)k * c.n + i], mx)));
-        const int label = (int)P.y[i];
-        for (int k = 0; k < K; ++k) {
-          const float p = __fdiv_rn(expf(__fsub_rn(P.pred[(size_t)k * c.n + i], mx)), sum);
+      // CrossEntropyLoss::compute_multiclass_gradients + softmax (src/boosting/loss.cpp:273-318)
+      const bool in = row_sampled(c, P, i);
+      float mx = pr[0];
+#pragma unroll
+      for (int k = 1; k < kSoftmaxMaxK; ++k)
+        if (k < K) mx = fmaxf(mx, pr[k]);
+      float sum = 0.0f;
+#pragma unroll
+      for (int k = 0; k < kSoftmaxMaxK; ++k)
+        if (k < K) sum = __fadd_rn(sum, expf(__fsub_rn(pr[k], mx)));
+      const int label = (int)P.y[i];
+#pragma unroll
+      for (int k = 0; k < kSoftmaxMaxK; ++k) {
+        if (k < K) {
+          const float p = __fdiv_rn(expf(__fsub_rn(pr[k], mx)), sum);
           const float g = __fsub_rn(p, (k == label) ? 1.0f : 0.0f);
           const float h = fmaxf(__fmul_rn(p, __fsub_rn(1.0f, p)), 1e-6f);
-          P.gh[(size_t)k * c.n + i] = make_float2(g, h);
+          // rows outside this iteration's sample add nothing to any sum
+          P.gh[(size_t)k * c.n + i] = in ? make_float2(g, h) : make_float2(0.0f, 0.0f);
         }
-      } else {
-        float g, h;
-        loss_grad(c.loss, P.pred[i], P.y[i], i, n_vec, c.gamma, c.alpha, g, h);
-        P.gh[i] = make_float2(g, h);
       }
-      // rows outside this iteration's sample add nothing to any sum
-      if (!row_sampled(c, P, i))
-        for (int k = 0; k < K; ++k) P.gh[(size_t)k * c.n + i] = make_float2(0.0f, 0.0f);
     }
-    for (int k = 0; k < K; ++k) P.leaf[(size_t)k * c.n + i] = 0;
+#pragma unroll
+    for (int k = 0; k < kSoftmaxMaxK; ++k)
+      if (k < K) P.leaf[(size_t)k * c.n + i] = 0;
   }
   root_sums(c, P, r0, r1);
 }
@@ -1457,7 +1535,7 @@ __global__ void __launch_bounds__(256) k_valid(DevCfg c, DevPtrs P) {
   const int L = 1 << c.D;
   double part = 0.0;
   for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < c.nv; r += gridDim.x * blockDim.x) {
-    float pr[kMaxClasses];
+    float pr[kSoftmaxMaxK];
     const float* xr = P.xv + (size_t)r * c.f;
     for (int k = 0; k < c.K; ++k) {
       float vp = P.vpred[(size_t)k * c.nv + r];
@@ -1925,9 +2003,14 @@ void tc_trainer::launch_level(const DevCfg& c, const DevPtrs& P, int d, cudaStre
 }
 
 // The whole iteration as a fixed launch sequence (graph-capturable).
+static void launch_grad(const DevCfg& c, const DevPtrs& P, int use_given_gh, cudaStream_t st) {
+  if (c.K > 1) k_grad<true><<<c.PB, 512, 0, st>>>(c, P, use_given_gh);
+  else k_grad<false><<<c.PB, 512, 0, st>>>(c, P, use_given_gh);
+}
+
 tc_status tc_trainer::enqueue_iteration(cudaStream_t st) {
   mark_begin(KC_GRAD, st);
-  k_grad<<<cfg.PB, 512, 0, st>>>(cfg, ptr, 0);
+  launch_grad(cfg, ptr, 0, st);
   mark_end(st, (double)cfg.n * cfg.K * (4 + 4 + 8 + 2 + 8) + (double)cfg.n * 4);
   return enqueue_rest(st);
 }
@@ -1976,7 +2059,7 @@ static DevPtrs class_view(const DevCfg& c, const DevPtrs& P, int k, DevCfg* one)
 // synchronisation after every level (the host reads the stop flag), no graph.
 tc_status tc_trainer::run_plain_iteration(cudaStream_t st, bool grad) {
   const int K = cfg.K, D = cfg.D;
-  if (grad) k_grad<<<cfg.PB, 512, 0, st>>>(cfg, ptr, 0);
+  if (grad) launch_grad(cfg, ptr, 0, st);
   k_node_reduce<false><<<dim3(1, K), 512, 0, st>>>(cfg, ptr, -1);
   for (int k = 0; k < K; ++k) {
     DevCfg one;
@@ -2165,7 +2248,7 @@ tc_status tc_trainer::goss_iteration(cudaStream_t st) {
   DevCfg all = cfg;
   all.sampled = 0;
   mark_begin(KC_GRAD, st);
-  k_grad<<<cfg.PB, 512, 0, st>>>(all, ptr, 0);
+  launch_grad(all, ptr, 0, st);
   mark_end(st, (double)n * cfg.K * (4 + 4 + 8 + 2 + 8) + (double)n * 4);
   TC_CUDA(ctx, cudaGetLastError());
   TC_CUDA(ctx, cudaMemcpyAsync(h_gh, gh.p, (size_t)cfg.K * n * sizeof(float2), cudaMemcpyDeviceToHost, st));
@@ -2657,7 +2740,7 @@ tc_status tc_build_tree(tc_ctx* ctx, tc_dataset* ds, const float* grad, const fl
   }
   // one iteration with the given gradients
   const int D = tr->cfg.D;
-  k_grad<<<tr->cfg.PB, 512, 0, st>>>(tr->cfg, tr->ptr, 1);
+  launch_grad(tr->cfg, tr->ptr, 1, st);
   k_node_reduce<false><<<dim3(1, 1), 512, 0, st>>>(tr->cfg, tr->ptr, -1);
   k_plan<<<1, PLAN_THREADS, 0, st>>>(tr->cfg, tr->ptr, 0);
   for (int d = 0; d < D; ++d) {
