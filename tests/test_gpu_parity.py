@@ -168,6 +168,44 @@ def test_tree_parity_teacher_forced(engine, capi, case):
         assert abs(dev["gain"][d] - f64.gain_top[d]) <= 1e-4 * abs(f64.gain_top[d]) + 1e-9
 
 
+def test_partition_skewed_levels(engine, capi):
+    """Levels where one node holds more than 1/8 of the rows: the partition
+    sums that node's two children in registers and every other child with
+    per-warp shared atomics.  The data is checked to have such a level at
+    depth >= 3 in the device's own tree; the device's leaf values are checked
+    against FP64 sums over the device's own row leaf indices, whatever the
+    splits, and the tree against the FP64 oracle under the margin rule."""
+    rng = np.random.default_rng(48)
+    n, f = 80_000, 12
+    X = rng.standard_normal((n, f)).astype(np.float32)
+    # the label lives in rare tails: most rows stay in one node, level after level
+    y = (((X[:, 0] > 1.8) ^ (X[:, 1] > 2.0)) | (X[:, 2] > 2.2)).astype(np.float32)
+    hp = O.Hyper(loss="logloss", max_depth=7, min_child_weight=1e-3)
+    b = O.quantize(X)
+    pred = np.full(n, O.init_prediction(hp.loss, y), np.float32)
+    g, h = O.gradients(hp.loss, y, pred)
+    ds = engine.upload(X, y)
+    ds.quantize(255)
+    dev = engine.build_tree(ds, g, h, _params(capi, hp))
+    D = int(dev["depth"])
+    li = np.asarray(dev["leaf_index"]).astype(np.int64)
+    assert D >= 4
+    assert max(np.bincount(li >> (D - d)).max() / n for d in range(3, D)) > 1 / 8
+    L = 1 << D
+    lam = float(hp.lambda_l2)
+    G = np.bincount(li, weights=g.astype(np.float64), minlength=L)
+    H = np.bincount(li, weights=h.astype(np.float64), minlength=L)
+    absg = np.bincount(li, weights=np.abs(g.astype(np.float64)), minlength=L)
+    want = np.where(H >= 1e-10, -G / (H + lam), 0.0)
+    tol = REL * absg / (H + lam) + 1e-7
+    assert np.all(np.abs(dev["leaves"][:L].astype(np.float64) - want) <= tol)
+    ref = O.build_tree(b, g, h, hp, mode=0, want_rows=True)
+    f64 = O.build_tree(b, g, h, hp, mode=1, want_rows=True)
+    teacher = ref if np.array_equal(ref.feature, f64.feature) and np.array_equal(ref.bin, f64.bin) else f64
+    checked, _ = _check_tree(dev, teacher, f64, g, h, hp, lam)
+    assert checked >= 3
+
+
 # ----------------------------------------------------------------- full fit --
 
 def _fit_compare(engine, capi, X, y, hp, batched=1):

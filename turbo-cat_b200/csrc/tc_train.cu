@@ -72,7 +72,7 @@ struct ClassState {
   int32_t depth;       // accepted splits
   int32_t f, b;        // split of the current level
   int32_t skew;        // one node of the current level holds more than 1/8 of the rows
-  int32_t pad;
+  int32_t hot;         // with skew: that node (the largest; the lowest index on a tie)
 };
 
 // Early-stopping state of a validation set (device).
@@ -1039,8 +1039,9 @@ __device__ void pick_body(const DevCfg& c, const DevPtrs& P, int d, int f, int k
 // thread are loaded before any is used.
 constexpr int PART_UNROLL = 4;
 template <int NCH>  // 2, 4, 8 children: per-thread register sums; 0: per-warp child groups;
-                    // -1: per-lane atomics into per-warp copies of the child sums, or the
-                    // groups when one node holds most rows (the lanes would hit one address)
+                    // -1: per-lane atomics into per-warp copies of the child sums, except
+                    // that when one node holds more than 1/8 of the rows (its lanes would
+                    // hit one address) its two children are summed in registers
 __global__ void __launch_bounds__(PART_THREADS) k_partition(DevCfg c, DevPtrs P, int d) {
   extern __shared__ unsigned char smraw[];
   __shared__ float2 s_wv[PART_THREADS / 32][32];
@@ -1066,6 +1067,8 @@ __global__ void __launch_bounds__(PART_THREADS) k_partition(DevCfg c, DevPtrs P,
   uint32_t ac[NR];
 #pragma unroll
   for (int cc = 0; cc < NR; ++cc) { ag[cc] = 0.0f; ah[cc] = 0.0f; ac[cc] = 0; }
+  float hg[2] = {0.0f, 0.0f}, hh[2] = {0.0f, 0.0f};  // NCH < 0, skewed level: the largest node's children
+  uint32_t hc[2] = {0u, 0u};
   for (uint32_t base = r0; base < r1; base += blockDim.x * PART_UNROLL) {
     uint8_t bb[PART_UNROLL];
     uint16_t lf[PART_UNROLL];
@@ -1099,12 +1102,17 @@ __global__ void __launch_bounds__(PART_THREADS) k_partition(DevCfg c, DevPtrs P,
             ah[cc] += w.y;
             ac[cc] += 1u;
           }
-      } else if (NCH < 0 && !cs.skew) {
+      } else if (NCH < 0) {
         if (nl >= 0) {
-          const int o = warp * nch + nl;
-          atomicAdd(&sG[o], w.x);
-          atomicAdd(&sH[o], w.y);
-          atomicAdd(&sC[o], 1u);
+          if (cs.skew && (nl >> 1) == cs.hot) {
+            if (nl & 1) { hg[1] += w.x; hh[1] += w.y; hc[1] += 1u; }
+            else { hg[0] += w.x; hh[0] += w.y; hc[0] += 1u; }
+          } else {
+            const int o = warp * nch + nl;
+            atomicAdd(&sG[o], w.x);
+            atomicAdd(&sH[o], w.y);
+            atomicAdd(&sC[o], 1u);
+          }
         }
       } else {
         // the first lane of each child's group sums the group in lane order
@@ -1140,6 +1148,25 @@ __global__ void __launch_bounds__(PART_THREADS) k_partition(DevCfg c, DevPtrs P,
         atomicAdd(&sG[cc], g);
         atomicAdd(&sH[cc], h);
         atomicAdd(&sC[cc], cnt);
+      }
+    }
+  }
+  if (NCH < 0 && cs.skew) {
+    // the largest node's children: the thread sums, reduced across the warp
+    // (fixed tree), added to this warp's copy
+#pragma unroll
+    for (int cc = 0; cc < 2; ++cc) {
+      float g = hg[cc], h = hh[cc];
+      for (int o = 16; o; o >>= 1) {
+        g += __shfl_xor_sync(0xffffffffu, g, o);
+        h += __shfl_xor_sync(0xffffffffu, h, o);
+      }
+      const uint32_t cnt = __reduce_add_sync(0xffffffffu, hc[cc]);
+      if (lane == 0 && cnt) {
+        const int o = warp * nch + 2 * cs.hot + cc;
+        atomicAdd(&sG[o], g);
+        atomicAdd(&sH[o], h);
+        atomicAdd(&sC[o], cnt);
       }
     }
   }
@@ -1240,6 +1267,7 @@ __device__ __forceinline__ void node_reduce_body(const DevCfg& c, const DevPtrs&
 __device__ __forceinline__ void plan_body(const DevCfg& c, const DevPtrs& P, int d) {
   __shared__ int s_go;
   __shared__ uint32_t s_maxcnt;
+  __shared__ int s_hot;
   __shared__ long long s_rows;
   __shared__ int s_warp[PLAN_THREADS / 32];
   __shared__ int s_carry;
@@ -1265,11 +1293,19 @@ __device__ __forceinline__ void plan_body(const DevCfg& c, const DevPtrs& P, int
         atomicMax(&s_maxcnt, ns[q].cnt);
       }
     }
+    if (tid == 0) s_hot = INT32_MAX;
+    __syncthreads();
+    if (alive) {
+      const NodeStat* ns = P.nstat + ((size_t)k * (c.D + 1) + d) * L;
+      for (int q = tid; q < (1 << d); q += blockDim.x)
+        if (ns[q].cnt == s_maxcnt) atomicMin(&s_hot, q);
+    }
     __syncthreads();
     if (tid == 0 && alive) {
       uint32_t tot = 0;  // rows of the level (the root's count)
       tot = P.nstat[((size_t)k * (c.D + 1)) * L].cnt;
       cs.skew = (uint64_t)s_maxcnt * 8u > (uint64_t)tot ? 1 : 0;
+      cs.hot = s_hot == INT32_MAX ? 0 : s_hot;
     }
     if (tid == 0 && !cs.done && !(alive && s_go)) cs.done = 1;
     __syncthreads();
