@@ -6,7 +6,7 @@ Bars (from the task statement):
     than 1e-6 relative (the REF32 oracle is bit-identical to the reference);
   * float histograms, leaf values and predictions are within 1e-5 relative.
     "Relative" is taken against the natural scale of each sum, so that sums
-    that cancel to ~0 are judged by the magnitude of their terms:
+    that cancel to ~0 are measured against the magnitude of their terms:
       histogram bin:  |dev - fp64| <= 1e-5 * sum|g_i| over the bin's rows
       leaf value:     |dev - ref|  <= 1e-5 * sum|g_i| / (H + lambda)
       prediction:     |dev - fp64| <= 1e-5 * (|base| + sum_t |w_t * leaf_t(x)|)
@@ -163,7 +163,7 @@ def test_tree_parity_teacher_forced(engine, capi, case):
     assert checked >= 1
     # device FP64 gains vs the FP64 oracle
     for d in range(checked):
-        # gains are differences of larger terms: judged at 1e-4 relative (their
+        # gains are differences of larger terms: checked at 1e-4 relative (their
         # role is the argmax, checked above)
         assert abs(dev["gain"][d] - f64.gain_top[d]) <= 1e-4 * abs(f64.gain_top[d]) + 1e-9
 
