@@ -193,7 +193,9 @@ tc_status tc_trainer_profile(tc_trainer* tr, int32_t iterations, tc_profile* out
 tc_status tc_trainer_train_scores(tc_trainer* tr, float* out);
 /* Rows the last iteration's trees were built on, one bit per row
  * (row i: bit i % 32 of word i / 32; ceil(n / 32) words, bits past n are 0).
- * Every row when neither subsample nor GOSS is on. */
+ * Every row when neither subsample nor GOSS is on.  No counterpart in the
+ * reference, whose sample indices stay inside Booster::train
+ * (src/boosting/booster.cpp:198-232). */
 tc_status tc_trainer_sample_mask(tc_trainer* tr, uint32_t* out);
 /* Snapshot of the ensemble trained so far as an immutable model. */
 tc_status tc_trainer_model(tc_trainer* tr, tc_model** out);
