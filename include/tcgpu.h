@@ -245,10 +245,16 @@ tc_status tc_build_tree(tc_ctx* ctx, tc_dataset* ds, const float* grad, const fl
  * device array inside the library (every GPU that loads the library holds it
  * until the process exits); at most 8192 features, larger f is rejected with
  * TC_ERR_INVALID_ARG.  The first call on a device resolves that array's
- * device address, so make the first call before any stream capture.  Calls
- * share the array: calls that overlap on the GPU race (serialise them on one
- * stream).  Queued on `stream` (NULL = the context's stream); returns
- * without synchronising. */
+ * device address in the device's primary context (the one the CUDA runtime
+ * uses; a caller that drives its own driver-API context is not supported,
+ * and the address is not valid after cudaDeviceReset), so make the first
+ * call before any stream capture.  Calls share the array: calls that overlap
+ * on the GPU race (serialise them on one stream).  A block sums at most
+ * 16384 rows in FP32; larger inputs run as several passes merged into
+ * hist_out in FP64.  Queued on `stream` (NULL = the context's stream, in
+ * which case the call waits for any training call on the context to finish,
+ * so that it never joins the trainer's graph capture); returns without
+ * synchronising.  The calling thread's current device is left unchanged. */
 tc_status tc_histogram_root_noalloc(tc_ctx* ctx, const uint8_t* bins_rm, uint32_t n, uint16_t f,
                                     uint32_t row_stride, const float* grad, const float* hess,
                                     double* hist_out, void* stream);

@@ -1,7 +1,10 @@
 # Builds the reference implementation from its own sources (read in place
 # under REF) into oracle/_ref/ -- test infrastructure and CPU baseline only.
 #
-#   make -f oracle/ref.mk            (from the repository root)
+#   make -f oracle/ref.mk REF=<reference tree>     (from the repository root)
+#
+# REF defaults to $TURBOCAT_REFERENCE; with neither set the build stops with a
+# message (__graft_entry__.build passes REF explicitly).
 #
 # Outputs (git-ignored):
 #   oracle/_ref/libtcref.so                       probe harness (C entry points)
@@ -12,7 +15,10 @@
 # absent; GradTree is off the symmetric path); oracle/refshim supplies a
 # stand-in Eigen header for tree.hpp and throwing definitions of the symbols
 # whose sources are missing from the reference tree.
-REF      ?= /root/reference
+REF      ?= $(TURBOCAT_REFERENCE)
+ifeq ($(strip $(REF)),)
+$(error set REF=<reference source tree> or TURBOCAT_REFERENCE)
+endif
 OUT      := oracle/_ref
 PY       ?= python3
 CXX      := /usr/bin/g++

@@ -16,6 +16,7 @@ constexpr int NA_W = 64;                  // feature columns per block
 constexpr int NA_MAX_ITEMS = 128;         // (row chunk, feature group) partials held at once
 constexpr int NA_THREADS = 512;
 constexpr int NA_MAX_DEVICES = 64;
+constexpr uint32_t NA_CHUNK_ROWS = 16384; // rows summed in FP32 by one block, at most
 
 // 128 partials x 256 bins x 64 columns x (grad, hess) FP32 = 16 MiB per device.
 // Every GPU that loads this library holds it until the process exits.
@@ -24,11 +25,24 @@ static __device__ __align__(256) float2 tc_noalloc_scratch[NA_MAX_ITEMS * tc::kS
 std::mutex g_na_mu;
 float2* g_na_ptr[NA_MAX_DEVICES] = {};
 
-// grid (items); item = chunk * G + group.
+// Restores the calling thread's current device on every return path (the
+// entry point is meant to be embedded in another framework's process).
+struct DeviceGuard {
+  int prev = -1;
+  DeviceGuard() {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+// grid (items); item = chunk * G + group; the chunks of one pass start at row r_base.
 __global__ void __launch_bounds__(NA_THREADS) k_hist_root_na(const uint8_t* __restrict__ bins, uint32_t n,
                                                             uint32_t f, uint32_t fs, const float* __restrict__ g,
-                                                            const float* __restrict__ h, uint32_t rows_per_chunk,
-                                                            int G, float2* __restrict__ scratch) {
+                                                            const float* __restrict__ h, uint32_t r_base,
+                                                            uint32_t rows_per_chunk, int G,
+                                                            float2* __restrict__ scratch) {
   extern __shared__ float sm[];
   const int item = blockIdx.x;
   const int chunk = item / G, grp = item % G;
@@ -36,8 +50,8 @@ __global__ void __launch_bounds__(NA_THREADS) k_hist_root_na(const uint8_t* __re
   const int gsize = min(NA_W, (int)f - g0);
   for (int q = threadIdx.x; q < 2 * tc::kSlots * NA_W; q += blockDim.x) sm[q] = 0.0f;
   __syncthreads();
-  const uint32_t r0 = (uint32_t)chunk * rows_per_chunk;
-  const uint32_t r1 = min(n, r0 + rows_per_chunk);
+  const uint32_t r0 = r_base + (uint32_t)chunk * rows_per_chunk;
+  const uint32_t r1 = r0 < n ? min(n, r0 + rows_per_chunk) : r0;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (uint32_t r = r0 + warp; r < r1; r += nw) {
     const float gv = g[r], hv = h[r];
@@ -61,8 +75,9 @@ __global__ void __launch_bounds__(NA_THREADS) k_hist_root_na(const uint8_t* __re
   }
 }
 
-// grid (f), 256 threads = bins: FP64 sum of the chunks' partials, fixed order.
-__global__ void k_merge_root_na(const float2* __restrict__ scratch, int chunks, int G, uint32_t f,
+// grid (f), 256 threads = bins: FP64 sum of one pass's chunk partials in a
+// fixed order; the first pass stores, later passes add to hist_out.
+__global__ void k_merge_root_na(const float2* __restrict__ scratch, int chunks, int G, uint32_t f, int accumulate,
                                 double* __restrict__ out) {
   const int j = blockIdx.x, b = threadIdx.x;
   const int grp = j / NA_W, col = j % NA_W;
@@ -72,8 +87,13 @@ __global__ void k_merge_root_na(const float2* __restrict__ scratch, int chunks, 
     sg += (double)v.x;
     sh += (double)v.y;
   }
-  out[((size_t)j * tc::kSlots + b) * 2] = sg;
-  out[((size_t)j * tc::kSlots + b) * 2 + 1] = sh;
+  double* o = out + ((size_t)j * tc::kSlots + b) * 2;
+  if (accumulate) {
+    sg += o[0];
+    sh += o[1];
+  }
+  o[0] = sg;
+  o[1] = sh;
 }
 
 }  // namespace
@@ -90,11 +110,13 @@ extern "C" tc_status tc_histogram_root_noalloc(tc_ctx* ctx, const uint8_t* bins_
                      NA_MAX_ITEMS * NA_W);
   if (ctx->device < 0 || ctx->device >= NA_MAX_DEVICES)
     return ctx->fail(TC_ERR_INVALID_ARG, "device %d beyond the no-alloc device table", ctx->device);
+  DeviceGuard restore;
   if (cudaSetDevice(ctx->device) != cudaSuccess) return ctx->fail(TC_ERR_CUDA, "cudaSetDevice failed");
   float2* scratch = nullptr;
   {
     // once per device, with that device current: the host-side symbol is a
-    // stand-in, the kernel needs the array's device address
+    // stand-in, the kernel needs the array's device address (in the
+    // runtime's primary context of the device, which every call here uses)
     std::lock_guard<std::mutex> g(g_na_mu);
     if (!g_na_ptr[ctx->device]) {
       void* p = nullptr;
@@ -104,16 +126,33 @@ extern "C" tc_status tc_histogram_root_noalloc(tc_ctx* ctx, const uint8_t* bins_
     }
     scratch = g_na_ptr[ctx->device];
   }
+  // With no stream given the work goes on the context's stream, which the
+  // trainer captures into CUDA graphs while it holds the training lock; the
+  // enqueue takes the same lock so that it never lands inside a capture.
+  std::unique_lock<std::recursive_mutex> train_lock(ctx->train_mu, std::defer_lock);
+  if (!stream) train_lock.lock();
   cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
-  const int chunks = std::max(1, std::min(NA_MAX_ITEMS / G, (int)((n + 1023) / 1024)));
-  const uint32_t rows_per_chunk = (n + chunks - 1) / chunks;
+  // A pass holds at most NA_MAX_ITEMS / G chunks of at most NA_CHUNK_ROWS
+  // rows (a block never sums more rows than that in FP32); larger inputs
+  // take several passes, each merged into hist_out in FP64.
+  const int chunks_max = std::max(1, NA_MAX_ITEMS / G);
+  const uint32_t want = (uint32_t)std::max<uint64_t>(1, ((uint64_t)n + 1023) / 1024);
+  const uint32_t rows_per_chunk =
+      (uint32_t)std::min<uint64_t>(NA_CHUNK_ROWS, ((uint64_t)n + std::min<uint32_t>(want, chunks_max) - 1) /
+                                                      std::min<uint32_t>(want, chunks_max));
   const size_t smem = (size_t)2 * tc::kSlots * NA_W * sizeof(float);
   cudaError_t e = cudaFuncSetAttribute(k_hist_root_na, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return ctx->cuda_fail(e, "cudaFuncSetAttribute");
   if (n > 0) {
-    k_hist_root_na<<<chunks * G, NA_THREADS, smem, st>>>(bins_rm, n, f, row_stride, grad, hess,
-                                                        rows_per_chunk, G, scratch);
-    k_merge_root_na<<<f, tc::kSlots, 0, st>>>(scratch, chunks, G, f, hist_out);
+    const uint64_t rows_per_pass = (uint64_t)chunks_max * rows_per_chunk;
+    int pass = 0;
+    for (uint64_t r = 0; r < n; r += rows_per_pass, ++pass) {
+      const uint64_t left = n - r;
+      const int chunks = (int)std::min<uint64_t>(chunks_max, (left + rows_per_chunk - 1) / rows_per_chunk);
+      k_hist_root_na<<<chunks * G, NA_THREADS, smem, st>>>(bins_rm, n, f, row_stride, grad, hess, (uint32_t)r,
+                                                          rows_per_chunk, G, scratch);
+      k_merge_root_na<<<f, tc::kSlots, 0, st>>>(scratch, chunks, G, f, pass > 0 ? 1 : 0, hist_out);
+    }
   } else {
     e = cudaMemsetAsync(hist_out, 0, (size_t)f * tc::kSlots * 2 * sizeof(double), st);
     if (e != cudaSuccess) return ctx->cuda_fail(e, "cudaMemsetAsync");

@@ -278,6 +278,33 @@ tc_status tc_server_add_model(tc_server* s, const tc_model* m, int32_t* model_id
   return TC_OK;
 }
 
+static void release_slot(Slot& sl) {
+  sl.d_in.reset();
+  sl.d_out.reset();
+  sl.d_reqs.reset();
+  sl.d_tiles.reset();
+  if (sl.h_in) cudaFreeHost(sl.h_in);
+  if (sl.h_out) cudaFreeHost(sl.h_out);
+  if (sl.h_reqs) cudaFreeHost(sl.h_reqs);
+  if (sl.h_tiles) cudaFreeHost(sl.h_tiles);
+  sl.h_in = sl.h_out = nullptr;
+  sl.h_reqs = nullptr;
+  sl.h_tiles = nullptr;
+}
+
+static tc_status alloc_slot(tc_server* s, Slot& sl) {
+  tc_ctx* ctx = s->ctx;
+  TC_TRY(sl.d_in.alloc(ctx, (size_t)s->rows_cap * s->max_f, "server input staging"));
+  TC_TRY(sl.d_out.alloc(ctx, (size_t)s->rows_cap * 16, "server output staging"));
+  TC_TRY(sl.d_reqs.alloc(ctx, s->req_cap, "server request table"));
+  TC_TRY(sl.d_tiles.alloc(ctx, s->req_cap + 1, "server tile table"));
+  TC_CUDA(ctx, cudaMallocHost(&sl.h_in, (size_t)s->rows_cap * s->max_f * sizeof(float)));
+  TC_CUDA(ctx, cudaMallocHost(&sl.h_out, (size_t)s->rows_cap * 16 * sizeof(float)));
+  TC_CUDA(ctx, cudaMallocHost(&sl.h_reqs, s->req_cap * sizeof(ReqDesc)));
+  TC_CUDA(ctx, cudaMallocHost(&sl.h_tiles, (s->req_cap + 1) * sizeof(uint32_t)));
+  return TC_OK;
+}
+
 static tc_status ensure_started(tc_server* s) {
   if (s->worker.joinable()) return TC_OK;
   tc_ctx* ctx = s->ctx;
@@ -290,16 +317,16 @@ static tc_status ensure_started(tc_server* s) {
     if (rows_budget < 1) return ctx->fail(TC_ERR_OOM, "staging budget smaller than one row per slot");
     s->rows_cap = (int)std::min<size_t>(s->rows_cap, rows_budget);
   }
+  // a set-up that fails partway (budget, pinned memory) releases every
+  // slot's buffers, so that the retry of the next submit starts clean
+  tc_status st = TC_OK;
   for (auto& slp : s->slots) {
-    Slot& sl = *slp;
-    TC_TRY(sl.d_in.alloc(ctx, (size_t)s->rows_cap * s->max_f, "server input staging"));
-    TC_TRY(sl.d_out.alloc(ctx, (size_t)s->rows_cap * 16, "server output staging"));
-    TC_TRY(sl.d_reqs.alloc(ctx, s->req_cap, "server request table"));
-    TC_TRY(sl.d_tiles.alloc(ctx, s->req_cap + 1, "server tile table"));
-    TC_CUDA(ctx, cudaMallocHost(&sl.h_in, (size_t)s->rows_cap * s->max_f * sizeof(float)));
-    TC_CUDA(ctx, cudaMallocHost(&sl.h_out, (size_t)s->rows_cap * 16 * sizeof(float)));
-    TC_CUDA(ctx, cudaMallocHost(&sl.h_reqs, s->req_cap * sizeof(ReqDesc)));
-    TC_CUDA(ctx, cudaMallocHost(&sl.h_tiles, (s->req_cap + 1) * sizeof(uint32_t)));
+    st = alloc_slot(s, *slp);
+    if (st != TC_OK) break;
+  }
+  if (st != TC_OK) {
+    for (auto& slp : s->slots) release_slot(*slp);
+    return st;
   }
   s->worker = std::thread([s] { s->run(); });
   return TC_OK;
