@@ -1,20 +1,30 @@
-"""Benchmark: symmetric-tree training on the regression configuration.
+"""Benchmark: symmetric-tree training on the imbalanced focal-loss configuration.
 
 Workload (seeded synthetic data with the configuration's shapes and value
-distributions): 1,000,000 rows x 100 float32 features -- 60 N(0,1),
-30 U(-3,3), 10 Student-t(3) -- target sum_k sin(x_k) over 10 features +
-x2*x3 + N(0, 0.1); MSE ("RMSE" config), 500 symmetric trees, depth 8,
-learning rate 0.05, 255 bins, lambda_l2 0 (the facade default).
+distributions; no public dataset is involved): 10,000,000 rows x 200 float32
+features -- 100 N(0,1), 100 LogNormal(0,1) -- with about 1% positives from
+thresholding a sparse linear score (20 active features) plus N(0, 0.5);
+focal loss (gamma 2, alpha 0.25), 1000 symmetric trees, depth 8, learning
+rate 0.1, 255 bins, lambda_l2 1.  This is the largest configuration that fits
+one GPU.
 
 Metric: training seconds per 100 trees (lower is better).  A step is 100
-boosting iterations; --steps 5 therefore trains the configuration's 500
-trees.  `value` times the steps on device-resident data (CUDA events on the
-engine's stream, L2 flushed between steps); `e2e` times whole fits through
-the public API (turbocat.TurboCatRegressor.fit) from pinned host memory:
-upload, device binning, 500 trees, model download.
+boosting iterations of the configuration's 1000-tree fit; the fit restarts
+from the base prediction after every 10 steps (untimed), so no step trains a
+tree beyond the configuration.  `value` times the steps on device-resident
+data (CUDA events on the engine's stream, a 256 MiB L2 flush between steps;
+the 2 GB of bins are larger than L2 anyway).  `e2e` times whole fits through
+the public API (turbocat.TurboCatClassifier.fit) from pinned host memory:
+upload, device binning, 1000 trees, model download.  The line also carries
+the regression configuration (1M x 100, MSE, 500 trees, depth 8) as a
+secondary object, device-timed the same way.
 
---impl reference runs the reference's own CPU implementation (its pybind
-module built from source in oracle/_ref) on the same data on the host cores.
+--impl reference runs the reference's own CPU implementation (its sources
+compiled in oracle/_ref) on the same data on all host cores: Booster::train
+with the configuration's 1000 trees, stopped through its training callback
+after warm-up + timed trees; the full fit is extrapolated from the measured
+set-up and per-tree times (stated in the line).
+
 Multi-GPU: replicas only (one independent fit per rank, no collective on the
 data path); value aggregates over ranks.
 """
@@ -34,14 +44,18 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "turbo-cat_b200"))
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 
-N_ROWS, N_FEAT, DEPTH, LR, TREES = 1_000_000, 100, 8, 0.05, 500
+N_ROWS, N_FEAT, DEPTH, LR, TREES, L2 = 10_000_000, 200, 8, 0.1, 1000, 1.0
 TREES_PER_STEP = 100
+STEPS_PER_FIT = TREES // TREES_PER_STEP
 METRIC = "train_s_per_100_trees"
 UNIT = "s/100 trees"
-CONFIG = {"workload": "regression 1M x 100 float32 (60 N(0,1), 30 U(-3,3), 10 t(3)), MSE, 500 symmetric trees, "
-                      "depth 8, lr 0.05, 255 bins, lambda_l2 0",
+CONFIG = {"workload": "imbalanced classification 10M x 200 float32 (100 N(0,1), 100 LogNormal(0,1), ~1% positives), "
+                      "focal loss (gamma 2, alpha 0.25), 1000 symmetric trees, depth 8, lr 0.1, 255 bins, "
+                      "lambda_l2 1",
           "rows": N_ROWS, "features": N_FEAT, "trees": TREES, "depth": DEPTH, "bins": 255,
-          "step": "100 boosting iterations", "l2": "flushed between timed steps (256 MiB write)"}
+          "step": "100 boosting iterations of the 1000-tree fit (restarted from the base prediction every 10 steps)",
+          "l2": "inputs larger than L2 (2 GB of bins) plus a 256 MiB flush between timed steps"}
+C2 = dict(n=1_000_000, f=100, depth=8, lr=0.05, trees=500, l2=0.0)
 
 
 def log(*a):
@@ -57,9 +71,10 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-def hist_traffic_per_launch():
-    """dram bytes per histogram launch from the committed ncu summary (or None)."""
-    path = os.path.join(ROOT, "profiles", "k_hist_c2_regression.md")
+def profile_traffic(name):
+    """DRAM bytes per histogram launch recorded from an ncu capture in a
+    committed profile summary (a profile constant, not measured in this run)."""
+    path = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -145,60 +160,123 @@ def dist_barrier(ws):
 
 
 def make_data():
-    from datagen import regression_c2
+    from datagen import imbalanced_c5
 
-    return regression_c2(N_ROWS, N_FEAT, seed=2)
+    return imbalanced_c5(N_ROWS, N_FEAT, seed=5)
 
 
-def reference_sample(X, y, n_more=4):
-    """Reference CPU fit through its pybind module (oracle/_ref/_turbocat):
-    a 1-tree fit and a (1+n_more)-tree fit give setup and per-tree cost,
-    extrapolated to the configuration's 500 trees; returns s/100 trees."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
-    import _turbocat as ref  # the reference's own module, built from its sources
+def ref_hyper(n_estimators=TREES):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
 
-    def fit(T):
-        m = ref.TurboCatRegressor(n_estimators=T, learning_rate=LR, max_depth=DEPTH, loss="mse", mode="large",
-                                  subsample=1.0, colsample_bytree=1.0, lambda_l2=0.0, min_child_weight=1.0,
-                                  verbosity=0)
-        t0 = time.perf_counter()
-        m.fit(X, y)
-        return time.perf_counter() - t0
+    return O, O.Hyper(loss="focal", n_estimators=n_estimators, learning_rate=LR, max_depth=DEPTH, lambda_l2=L2,
+                      min_child_weight=1.0, focal_gamma=2.0, focal_alpha=0.25)
 
-    t1 = fit(1)
-    t2 = fit(1 + n_more)
-    per_tree = max(0.0, (t2 - t1) / n_more)
-    setup = max(0.0, t1 - per_tree)
-    full = setup + TREES * per_tree
-    return full / (TREES / TREES_PER_STEP), dict(setup_s=setup, per_tree_s=per_tree, fit1_s=t1,
-                                                  fit_more_s=t2, extra_trees=n_more)
+
+def reference_timed(X, y, warm_trees, timed_trees, max_seconds):
+    """The reference's own Booster::train (oracle/_ref, its sources compiled
+    with its own flags) on X, y with the configuration's 1000 trees, stopped
+    after warm_trees + timed_trees trees (or max_seconds).  Returns
+    (full-fit seconds extrapolated to 1000 trees, detail)."""
+    O, hp = ref_hyper()
+    setup, ends = O.ref_fit_timed(X, y, hp, warm_trees + timed_trees, max_seconds)
+    built = len(ends)
+    w = min(warm_trees, max(0, built - 2))
+    per_tree = (ends[-1] - ends[w - 1]) / (built - w) if w >= 1 else (ends[-1] - setup) / max(1, built)
+    full = ends[-1] + (TREES - built) * per_tree
+    steps_ms = [1e3 * (ends[i] - (ends[i - 1] if i else setup)) for i in range(w, built)]
+    return full, {"setup_s": setup, "first_tree_end_s": ends[0], "last_tree_end_s": ends[-1],
+                  "trees_built": built, "trees_timed": built - w,
+                  "per_tree_s": per_tree, "tree_ms": steps_ms,
+                  "extrapolation": "full fit = end of the last built tree + (1000 - built) x mean per-tree time "
+                                   "of the timed trees"}
 
 
 def run_reference(args):
     # rank 0 alone measures the host CPU; other ranks exit without work
     if int(os.environ.get("RANK", "0")) != 0:
         return
-    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref")):
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libtcref.so")):
         print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref not present"}))
         return
+    t0 = time.perf_counter()
     X, y = make_data()
+    log(f"reference arm: data in {time.perf_counter() - t0:.1f} s")
     cores = os.cpu_count()
-    for _ in range(args.warmup):
-        reference_sample(X, y, n_more=2)
-    vals = []
-    detail = None
-    for _ in range(args.steps):
-        v, detail = reference_sample(X, y, n_more=2)
-        vals.append(v)
-    value = float(np.mean(vals))
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": CONFIG, "impl": "reference",
+    full, detail = reference_timed(X, y, args.warmup, args.steps, args.reference_seconds)
+    value = full / STEPS_PER_FIT
+    detail["timed_region_s"] = float(np.sum(detail["tree_ms"]) / 1e3)
+    cfg = dict(CONFIG, step="one boosting iteration (tree) of the reference's 1000-tree fit; value is the "
+                            "extrapolated full fit (binning included) per 100 trees")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": detail["trees_timed"],
+            "warmup": detail["trees_built"] - detail["trees_timed"],
+            "ms_per_step": detail["per_tree_s"] * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg, "impl": "reference",
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
-                             "sample": "reference pybind fit of the 1M x 100 data with 1 and 3 trees per step; "
-                                       "setup + per-tree cost extrapolated to 500 trees", "detail": detail},
+                             "sample": f"reference Booster::train on the full 10M x 200 data, stopped after "
+                                       f"{detail['trees_built']} of 1000 trees ({detail['trees_timed']} timed); "
+                                       "set-up + per-tree time extrapolated to the 1000-tree fit",
+                             "detail": detail},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+def hist_roofline(prof, peak, peak_kind, traffic_file):
+    """Roofline of the histogram kernel from an in-graph profile."""
+    hl, hms, hbytes = prof["hist"]
+    achieved = hbytes / (hms * 1e-3) / 1e9 if hms > 0 else None
+    kern = {k: v for k, v in prof.items() if not k.startswith("_")}
+    dominant = max((v[1], k) for k, v in kern.items())[1]
+    iters = max(1, prof.get("_iters", 3))
+    return {"kernel": "k_hist (histogram)", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
+            "traffic": profile_traffic(traffic_file),
+            "traffic_source": f"profile constant: ncu dram bytes per launch recorded in profiles/{traffic_file}",
+            "alg_bytes_per_launch": hbytes / max(1, hl), "avg_launch_ms": hms / max(1, hl),
+            "timing": "CUDA events recorded as nodes of the replayed iteration graph" if prof["_in_graph"]
+                      else "CUDA events around launches outside a graph",
+            "dominant_kernel_by_time": dominant,
+            "kernel_ms_per_iter": {k: round(v[1] / iters, 4) for k, v in kern.items() if v[0]},
+            "kernels_sum_ms_per_iter": sum(v[1] for v in kern.values()) / iters,
+            "profiled_iteration_ms": prof["_iteration_ms"] / iters}
+
+
+def c2_secondary(eng, _capi, peak, peak_kind, steps):
+    """The regression configuration, device-timed like the headline."""
+    import torch
+
+    from datagen import regression_c2
+
+    X, y = regression_c2(C2["n"], C2["f"], seed=2)
+    ds = eng.upload(X, y)
+    ds.quantize(255)
+    p = _capi.params(loss="mse", n_estimators=C2["trees"], max_depth=C2["depth"], learning_rate=C2["lr"],
+                     lambda_l2=C2["l2"], max_bins=255)
+    tr = eng.trainer(ds, p)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    per_fit = C2["trees"] // TREES_PER_STEP
+    for _ in range(3):
+        tr.step(TREES_PER_STEP)
+    tr.reset()
+    step_s = []
+    for i in range(steps):
+        if i and i % per_fit == 0:
+            tr.reset()
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        s0 = tr.stats().seconds
+        tr.step(TREES_PER_STEP)
+        step_s.append(tr.stats().seconds - s0)
+    tr.reset()
+    prof = tr.profile(3)
+    prof["_iters"] = 3
+    out = {"workload": "regression 1M x 100 float32 (60 N(0,1), 30 U(-3,3), 10 t(3)), MSE, 500 symmetric trees, "
+                       "depth 8, lr 0.05, 255 bins, lambda_l2 0",
+           "value": float(np.mean(step_s)), "unit": UNIT, "steps": steps,
+           "roofline": hist_roofline(prof, peak, peak_kind, "k_hist_c2_regression.md")}
+    tr.close()
+    ds.close()
+    return out
 
 
 def run_ours(args):
@@ -211,30 +289,36 @@ def run_ours(args):
     from turbocat import _capi
 
     eng = _capi.Engine(local)
+    t0 = time.perf_counter()
     X, y = make_data()
+    log(f"data in {time.perf_counter() - t0:.1f} s")
     ds = eng.upload(X, y)
     ds.quantize(255)
-    iters_cap = TREES_PER_STEP * max(args.steps, args.warmup, 1) + 16
-    p = _capi.params(loss="mse", n_estimators=iters_cap, max_depth=DEPTH, learning_rate=LR, lambda_l2=0.0,
-                     max_bins=255)
+    p = _capi.params(loss="focal", n_estimators=TREES, max_depth=DEPTH, learning_rate=LR, lambda_l2=L2,
+                     max_bins=255, focal_gamma=2.0, focal_alpha=0.25)
     tr = eng.trainer(ds, p)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
 
-    # warm-up: W steps on a fresh model
+    def next_step(timed):
+        if tr.stats().iterations_done >= TREES:
+            tr.reset()  # the fit restarts: a step never trains a tree beyond the configuration
+        if not timed:
+            tr.step(TREES_PER_STEP)
+            return 0.0
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        s0 = tr.stats().seconds
+        tr.step(TREES_PER_STEP)  # synchronises; seconds from CUDA events on the engine stream
+        return tr.stats().seconds - s0
+
     for _ in range(args.warmup):
-        tr.step(TREES_PER_STEP)
+        next_step(False)
     tr.reset()
     torch.cuda.synchronize()
     dist_barrier(ws)
     clocks = Clocks(local)
     launches0 = tr.stats().kernel_launches
-    step_s = []
-    for _ in range(args.steps):
-        flush.fill_(1.0)
-        torch.cuda.synchronize()
-        s0 = tr.stats().seconds
-        tr.step(TREES_PER_STEP)  # synchronises; seconds from CUDA events on the engine stream
-        step_s.append(tr.stats().seconds - s0)
+    step_s = [next_step(True) for _ in range(args.steps)]
     torch.cuda.synchronize()
     clk = clocks.stop()
     launches = tr.stats().kernel_launches - launches0
@@ -243,21 +327,13 @@ def run_ours(args):
     # whole job: ws replicas x steps x 100 trees in `total` seconds
     value = total / (args.steps * ws)
 
-    # roofline of the dominant kernel (histogram) from event-timed launches
+    # roofline of the dominant kernel (histogram), timed inside the iteration graph
+    peak, peak_kind = load_peaks()
     tr.reset()
     prof = tr.profile(3)
-    prof.pop("_hist_levels", None)
-    prof.pop("_part_levels", None)
-    hl, hms, hbytes = prof["hist"]
-    peak, peak_kind = load_peaks()
-    achieved = hbytes / (hms * 1e-3) / 1e9 if hms > 0 else None
-    dominant = max((v[1], k) for k, v in prof.items())[1]
-    roofline = {"kernel": "k_hist (histogram)", "bound": "hbm", "achieved": achieved, "peak": peak,
-                "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                "traffic": hist_traffic_per_launch(), "peak_kind": peak_kind,
-                "alg_bytes_per_launch": hbytes / max(1, hl), "avg_launch_ms": hms / max(1, hl),
-                "dominant_kernel_by_time": dominant,
-                "kernel_ms_per_iter": {k: round(v[1] / 3, 4) for k, v in prof.items() if v[0]}}
+    prof["_iters"] = 3
+    roofline = hist_roofline(prof, peak, peak_kind, "k_hist_c5_focal.md")
+    tr.close()
 
     # end to end through the public API, pinned host inputs
     import turbocat
@@ -266,36 +342,51 @@ def run_ours(args):
     yp = torch.empty(N_ROWS, dtype=torch.float32, pin_memory=True).numpy()
     Xp[:] = X
     yp[:] = y
+    ds.close()
     e2e_s = []
     for i in range(1 + args.e2e_fits):
-        m = turbocat.TurboCatRegressor(n_estimators=TREES, learning_rate=LR, max_depth=DEPTH, loss="mse",
-                                       mode="large", subsample=1.0, colsample_bytree=1.0, lambda_l2=0.0,
-                                       verbosity=0)
+        m = turbocat.TurboCatClassifier(n_estimators=TREES, learning_rate=LR, max_depth=DEPTH, loss="focal",
+                                        mode="large", subsample=1.0, colsample_bytree=1.0, lambda_l2=L2,
+                                        min_child_weight=1.0, verbosity=0)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         m.fit(Xp, yp)
         dt = time.perf_counter() - t0
         if i > 0:
             e2e_s.append(dt)
-    e2e_fit = dist_max(float(np.median(e2e_s)), ws, dev)  # median: one fit can catch host noise
-    steps_per_fit = TREES / TREES_PER_STEP
+        del m
+    e2e_fit = dist_max(float(np.median(e2e_s)), ws, dev) if e2e_s else None
     model_bytes = TREES * (DEPTH * 11 + (1 << DEPTH) * 4 + 8)
-    e2e = {"value": e2e_fit / steps_per_fit / ws, "unit": UNIT,
-           "h2d_bytes_per_step": int((X.nbytes + y.nbytes) / steps_per_fit),
-           "d2h_bytes_per_step": int(model_bytes / steps_per_fit),
+    e2e = {"value": e2e_fit / STEPS_PER_FIT / ws if e2e_fit else None, "unit": UNIT,
+           "h2d_bytes_per_step": int((X.nbytes + y.nbytes) / STEPS_PER_FIT),
+           "d2h_bytes_per_step": int(model_bytes / STEPS_PER_FIT),
            "fit_seconds": e2e_fit, "fits_timed": args.e2e_fits, "fit_seconds_each": e2e_s,
-           "path": "turbocat.TurboCatRegressor.fit (pybind -> C ABI): upload, device binning, 500 trees, model"}
+           "path": "turbocat.TurboCatClassifier.fit (pybind -> C ABI): upload, device binning, 1000 trees, model"}
+    del Xp, yp
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
-            v, detail = reference_sample(X, y, n_more=2)
-            cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
-                   "sample": "reference pybind fit of the same 1M x 100 data with 1 and 3 trees; setup + "
-                             "per-tree cost extrapolated to 500 trees", "detail": detail}
+            sub = 1_000_000
+            full_sub, detail = reference_timed(np.ascontiguousarray(X[:sub]), np.ascontiguousarray(y[:sub]), 2, 6,
+                                               60.0)
+            scale = N_ROWS / sub
+            # per-tree work scales with the rows; binning sorts (n log n)
+            setup_full = detail["setup_s"] * scale * np.log(N_ROWS) / np.log(sub)
+            fit_full = setup_full + (detail["first_tree_end_s"] - detail["setup_s"]) * scale + \
+                (TREES - 1) * detail["per_tree_s"] * scale
+            cpu = {"value": fit_full / STEPS_PER_FIT, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": "reference Booster::train on the first 1M of the 10M rows (all 200 features), "
+                             f"{detail['trees_built']} trees built, {detail['trees_timed']} timed; per-tree time "
+                             "scaled by 10 (rows), binning by 10 x log(10M)/log(1M), extrapolated to 1000 trees",
+                   "detail": detail}
         except Exception as e:  # reference build absent
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"unavailable: {e}"}
+
+    secondary = None
+    if rank == 0 and ws == 1 and not args.no_c2:
+        secondary = c2_secondary(eng, _capi, peak, peak_kind, steps=5)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -303,7 +394,8 @@ def run_ours(args):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": CONFIG,
                 "parallelism": f"replicas x{ws}", "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "clocks": clk, "gpu_launches": int(launches),
-                "trees_per_s": args.steps * TREES_PER_STEP * ws / total}
+                "trees_per_s": args.steps * TREES_PER_STEP * ws / total,
+                "secondary": {"c2_regression": secondary} if secondary else None}
         print(json.dumps(line))
     if ws > 1:
         import torch.distributed as dist
@@ -496,34 +588,6 @@ def suite_c4(eng, _capi, seconds=3.0, rate=20_000.0, ref_ok=False):
     return res
 
 
-def suite_c5(eng, _capi, trees=20):
-    from datagen import imbalanced_c5
-
-    X, y = imbalanced_c5()
-    t0 = time.perf_counter()
-    ds = eng.upload(X, y)
-    up = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    ds.quantize(255)
-    qt = time.perf_counter() - t0
-    del X
-    tr = eng.trainer(ds, _capi.params(loss="focal", n_estimators=trees + 6, max_depth=8, learning_rate=0.1))
-    tr.step(3)
-    s0 = tr.stats().seconds
-    tr.step(trees)
-    per_tree = (tr.stats().seconds - s0) / trees
-    prof = tr.profile(3)
-    prof.pop("_hist_levels", None)
-    prof.pop("_part_levels", None)
-    hl, hms, hbytes = prof["hist"]
-    peak, kind = load_peaks()
-    return {"config": "imbalanced 10M x 200, focal, depth 8 (1000 trees in the config)",
-            "upload_s": up, "quantize_s": qt, "device_s_per_tree": per_tree,
-            "extrapolated_1000_trees_s": per_tree * 1000 + qt,
-            "hist_alg_gbs": hbytes / (hms * 1e-3) / 1e9, "hist_frac_of_hbm": hbytes / (hms * 1e-3) / 1e9 / peak,
-            "kernel_ms_per_iter": {k: round(v[1] / 3, 4) for k, v in prof.items() if v[0]}}
-
-
 def run_suite(args):
     import torch
 
@@ -543,8 +607,6 @@ def run_suite(args):
         elif name == "c4dev":  # the four serving models' device-resident prediction only
             r = {"config": "serving models (1000xd6, 200xd4, 500xd8, 2000xd10) on 100 features, 1M resident rows",
                  "device_predict_1M_rows": _device_predict(_train_serving_models(eng, _capi), 100)}
-        elif name == "c5":
-            r = suite_c5(eng, _capi)
         else:
             continue
         r["suite"] = name
@@ -555,12 +617,15 @@ def run_suite(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-fits", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--suite", default="", help="secondary configurations, e.g. c1,c3,c4,c5")
+    ap.add_argument("--no-c2", action="store_true", help="leave out the secondary regression configuration")
+    ap.add_argument("--reference-seconds", type=float, default=240.0,
+                    help="reference arm: stop building trees once this many seconds have passed")
+    ap.add_argument("--suite", default="", help="secondary configurations, e.g. c1,c3,c4")
     args = ap.parse_args()
     if args.suite:
         run_suite(args)

@@ -157,10 +157,15 @@ typedef struct {
   int32_t stopped_early;    /* validation set: 1 once the early-stopping rule has fired */
 } tc_train_stats;
 
-/* Per-kernel timing of profiled iterations (CUDA events on the launching
- * stream around every launch) with the algorithmic bytes each kernel class
- * moved: for the histogram kernel R*(F + 8) + R*4 (row ids, levels >= 1)
- * + built_nodes*F*256*8, R = rows histogrammed. */
+/* Per-kernel timing of profiled iterations with the algorithmic bytes each
+ * kernel class moved: for the histogram kernel R*(F + 8 + 1) +
+ * built_nodes*F*255*8, R = rows histogrammed (bin bytes, (grad, hess), node
+ * id per row; FP32 (grad, hess) sums per built node, feature and bin).  On
+ * the batched path (in_graph = 1) the iteration is captured as a CUDA graph
+ * with an event-record node around every launch and replayed, so the times
+ * are those of launches inside a graph; iteration_ms sums the replayed
+ * iterations from the first launch's start to the last one's end.  GOSS and
+ * the plain path are timed launch by launch (in_graph = 0). */
 typedef struct {
   char name[16];
   int64_t launches;
@@ -173,6 +178,8 @@ typedef struct {
   double hist_level_ms[16];     /* histogram kernel time per tree level */
   double hist_level_rows[16];   /* rows histogrammed per tree level */
   double part_level_ms[16];     /* partition kernel time per tree level */
+  int32_t in_graph;             /* 1: timed inside a replayed CUDA graph */
+  double iteration_ms;          /* profiled iterations, first launch start to last launch end */
 } tc_profile;
 
 /* Stateful boosting loop over a quantized dataset.  Replaces

@@ -393,6 +393,25 @@ def ref_fit(X, y, hp: Hyper, trace=False):
     return Binned(bins, edges, ne), data, gt, ht, tp
 
 
+
+def ref_fit_timed(X, y, hp: Hyper, max_trees: int, max_seconds: float = 1e30):
+    """Reference Booster::train (binary / regression) stopped through its
+    training callback after max_trees trees or max_seconds; returns
+    (seconds of from_dense + compute_bins, [seconds from the start to the end
+    of each tree built])."""
+    X = np.ascontiguousarray(X, np.float32)
+    y = np.ascontiguousarray(y, np.float32)
+    n, f = X.shape
+    setup = np.zeros(1)
+    ends = np.zeros(max(1, max_trees))
+    rp = hp.ref()
+    R = ref()
+    rc = R.tcref_fit_timed(_ptr(X), C.c_uint32(n), C.c_uint16(f), _ptr(y), C.byref(rp), C.c_int32(max_trees),
+                           C.c_double(max_seconds), _ptr(setup), _ptr(ends))
+    if rc < 0:
+        raise RuntimeError(R.tcref_last_error().decode())
+    return float(setup[0]), [float(v) for v in ends[:rc]]
+
 def ref_predict(model: bytes, X, proba=False) -> np.ndarray:
     X = np.ascontiguousarray(X, np.float32)
     n, f = X.shape

@@ -10,6 +10,7 @@
 //
 // Nothing here changes the reference's arithmetic: every number it returns is
 // computed by the reference's own code.
+#include <chrono>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
@@ -263,6 +264,39 @@ int tcref_fit_multiclass(const float* X, uint32_t n, uint16_t f, const float* y,
     }
     if (train_pred_out) std::memcpy(train_pred_out, preds.data(), preds.size() * sizeof(Float));
     return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
+// Timed reference fit for the CPU baseline: Dataset::from_dense +
+// compute_bins, then Booster::train with the configuration's n_estimators,
+// stopped through the training callback (which the reference's loop honours
+// with a break, src/boosting/booster.cpp:393-406) after `max_trees` trees or
+// once `max_seconds` have passed.  setup_s[0] = seconds of from_dense +
+// compute_bins; tree_end_s[i] = seconds from the start to the end of tree i
+// (Booster::train's own set-up falls inside tree 0).  Returns the number of
+// trees built.
+int tcref_fit_timed(const float* X, uint32_t n, uint16_t f, const float* y, const Params* p, int32_t max_trees,
+                    double max_seconds, double* setup_s, double* tree_end_s) {
+  try {
+    using clk = std::chrono::steady_clock;
+    const auto t0 = clk::now();
+    Config cfg = make_config(*p);
+    Dataset ds;
+    ds.from_dense(X, n, f, y);
+    ds.compute_bins(cfg);
+    setup_s[0] = std::chrono::duration<double>(clk::now() - t0).count();
+    Booster booster(cfg);
+    int32_t done = 0;
+    TrainingCallback cb = [&](const TrainingInfo&) {
+      const double t = std::chrono::duration<double>(clk::now() - t0).count();
+      if (done < max_trees) tree_end_s[done] = t;
+      ++done;
+      return done < max_trees && t < max_seconds;
+    };
+    booster.train(ds, nullptr, cb);
+    return done < max_trees ? done : max_trees;
   } catch (const std::exception& e) {
     return fail(e);
   }

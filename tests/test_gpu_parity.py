@@ -378,6 +378,11 @@ def test_autotuner_and_profile(engine, capi):
     prof = tr.profile(3)
     levels = prof.pop("_hist_levels")
     part_levels = prof.pop("_part_levels")
+    # timed inside the replayed graph: the kernels fill most of the iteration
+    assert prof.pop("_in_graph")
+    it_ms = prof.pop("_iteration_ms")
+    kern_ms = sum(v[1] for v in prof.values())
+    assert 0.5 * it_ms <= kern_ms <= it_ms * 1.001 + 1e-3
     assert all(part_levels[d] > 0 for d in range(6))  # depth 6: a partition launch per level
     assert prof["hist"][0] == 3 * 6 and prof["hist"][1] > 0 and prof["hist"][2] > 0
     assert levels[0][1] == 3 * 30_000  # root rows histogrammed per profiled iteration

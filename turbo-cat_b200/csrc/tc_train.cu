@@ -153,6 +153,8 @@ struct DevPtrs {
   double* m_second;              // [T][D]
   float* m_leaves;               // [T][2^D]
   double* root_hist_out;         // optional [F][256][2]
+  uint64_t* lvl_rows;            // [16] rows histogrammed at level d (all classes), written by the plan
+  uint32_t* lvl_nodes;           // [16] nodes histogrammed at level d (all classes)
   // validation set
   const float* xv;               // [nv][f] raw features
   const float* yv;               // [nv] labels
@@ -1269,12 +1271,13 @@ __device__ __forceinline__ void plan_body(const DevCfg& c, const DevPtrs& P, int
   __shared__ uint32_t s_maxcnt;
   __shared__ int s_hot;
   __shared__ long long s_rows;
+  __shared__ int s_nodes;
   __shared__ int s_warp[PLAN_THREADS / 32];
   __shared__ int s_carry;
   const int Pmax = 1 << (c.D - 1);
   const int L = 1 << c.D;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  if (tid == 0) s_rows = 0;
+  if (tid == 0) { s_rows = 0; s_nodes = 0; }
   for (int k = 0; k < c.K; ++k) {
     ClassState& cs = P.cs[k];
     if (tid == 0) {
@@ -1355,7 +1358,7 @@ __device__ __forceinline__ void plan_body(const DevCfg& c, const DevPtrs& P, int
         if (tid == blockDim.x - 1) s_carry = before + x;
         __syncthreads();
       }
-      if (tid == 0) s_rows += s_carry;
+      if (tid == 0) { s_rows += s_carry; s_nodes += np2; }
     }
     __syncthreads();
   }
@@ -1429,6 +1432,10 @@ __device__ __forceinline__ void plan_body(const DevCfg& c, const DevPtrs& P, int
   if (tid == 0) {
     P.cum[nsg] = min(s_carry, c.item_cap);
     *P.hist_ctr = 0;
+    if (d < 16) {
+      P.lvl_rows[d] = (uint64_t)s_rows;
+      P.lvl_nodes[d] = (uint32_t)s_nodes;
+    }
   }
 }
 
@@ -1690,6 +1697,8 @@ struct tc_trainer {
   DevBuf<float> m_thr, m_leaves;
   DevBuf<double> m_gain, m_second;
   DevBuf<double> root_hist;
+  DevBuf<uint64_t> lvl_rows;     // per-level build-set rows / nodes (profiling)
+  DevBuf<uint32_t> lvl_nodes;
   // validation set and early stopping (optional)
   const tc_dataset* vds = nullptr;
   DevBuf<float> vpred;
@@ -1737,6 +1746,7 @@ struct tc_trainer {
     double rows;
   };
   std::vector<ProfRec>* prof = nullptr;
+  bool prof_capture = false;     // profiling events become external event-record nodes of a graph
   std::vector<cudaEvent_t> ev_pool;
   size_t ev_used = 0;
   int cur_cls = -1;
@@ -1822,6 +1832,10 @@ tc_status tc_trainer::setup(int) {
   TC_TRY(m_gain.alloc(ctx, (size_t)T_cap * D, "model"));
   TC_TRY(m_second.alloc(ctx, (size_t)T_cap * D, "model"));
   TC_TRY(m_leaves.alloc(ctx, (size_t)T_cap * L, "model"));
+  TC_TRY(lvl_rows.alloc(ctx, 16, "level rows"));
+  TC_TRY(lvl_nodes.alloc(ctx, 16, "level nodes"));
+  TC_CUDA(ctx, cudaMemset(lvl_rows.p, 0, lvl_rows.bytes()));
+  TC_CUDA(ctx, cudaMemset(lvl_nodes.p, 0, lvl_nodes.bytes()));
   TC_CUDA(ctx, cudaMemset(counters.p, 0, counters.bytes()));
   TC_CUDA(ctx, cudaMemset(red_ctr.p, 0, red_ctr.bytes()));
   TC_CUDA(ctx, cudaMemset(fcnt.p, 0, fcnt.bytes()));
@@ -1835,6 +1849,7 @@ tc_status tc_trainer::setup(int) {
   ptr.fbest = fbest.p; ptr.counters = counters.p; ptr.hist_ctr = hist_ctr.p; ptr.red_ctr = red_ctr.p; ptr.fcnt = fcnt.p; ptr.cs = cs.p; ptr.iter = iter.p;
   ptr.m_depth = m_depth.p; ptr.m_feat = m_feat.p; ptr.m_bin = m_bin.p; ptr.m_thr = m_thr.p; ptr.m_gain = m_gain.p;
   ptr.m_second = m_second.p; ptr.m_leaves = m_leaves.p; ptr.root_hist_out = nullptr;
+  ptr.lvl_rows = lvl_rows.p; ptr.lvl_nodes = lvl_nodes.p;
 
   cudaFuncSetAttribute(k_hist<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape<1>::smem);
   cudaFuncSetAttribute(k_hist<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape<2>::smem);
@@ -1954,21 +1969,30 @@ void tc_trainer::mark_begin(int cls, cudaStream_t st) {
   }
   ProfRec r{cls, ev_pool[ev_used], ev_pool[ev_used + 1], 0.0, -1, 0.0};
   ev_used += 2;
-  cudaEventRecord(r.a, st);
+  if (prof_capture) cudaEventRecordWithFlags(r.a, st, cudaEventRecordExternal);
+  else cudaEventRecord(r.a, st);
   prof->push_back(r);
 }
 
 void tc_trainer::mark_end(cudaStream_t st, double bytes) {
   if (!prof) return;
-  cudaEventRecord(prof->back().b, st);
+  if (prof_capture) cudaEventRecordWithFlags(prof->back().b, st, cudaEventRecordExternal);
+  else cudaEventRecord(prof->back().b, st);
   prof->back().bytes = bytes;
+}
+
+// Algorithmic bytes of a histogram launch over `rows` listed rows and `nodes`
+// built nodes: rows x (F bin bytes + 8 bytes of (grad, hess) + 1 byte of node
+// id) + nodes x F x 255 bins x 8 bytes of (grad, hess) sums.
+static double hist_alg_bytes(double rows, double nodes, uint32_t f) {
+  return rows * ((double)f + 9.0) + nodes * (double)f * 255.0 * 8.0;
 }
 
 // All launches of level d for the classes of view (c, P).
 void tc_trainer::launch_level(const DevCfg& c, const DevPtrs& P, int d, cudaStream_t st) {
   const int K = c.K, D = c.D;
   double hist_bytes = 0.0, hist_rows = 0.0;
-  if (prof) {
+  if (prof && !prof_capture) {
     // algorithmic bytes: rows histogrammed at this level (device counts)
     TC_CUDA_VOID(cudaStreamSynchronize(st));
     std::vector<ClassState> h(K);
@@ -1987,7 +2011,7 @@ void tc_trainer::launch_level(const DevCfg& c, const DevPtrs& P, int d, cudaStre
         nodes += (double)sl.size();
       }
     }
-    hist_bytes = rows * (c.f + 8.0) + (d > 0 ? rows * 4.0 : 0.0) + nodes * c.f * kSlots * 8.0;
+    hist_bytes = hist_alg_bytes(rows, nodes, c.f);
     hist_rows = rows;
   }
   mark_begin(KC_HIST, st);
@@ -2554,6 +2578,37 @@ tc_status tc_trainer_valid_loss(tc_trainer* tr, double* out) {
   return TC_OK;
 }
 
+// Harvests one profiled iteration's events into `out`; histogram launches
+// get their algorithmic bytes from the level's build set when `lvl` is given
+// (the in-graph path records it on the device).
+static void harvest_profile(const std::vector<tc_trainer::ProfRec>& recs, const uint64_t* lvl_rows,
+                            const uint32_t* lvl_nodes, uint32_t f, tc_profile* out) {
+  for (const auto& r : recs) {
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, r.a, r.b);
+    tc_kernel_time& k = out->k[r.cls];
+    double bytes = r.bytes;
+    double rows = r.rows;
+    if (lvl_rows && r.cls == KC_HIST && r.level >= 0 && r.level < 16) {
+      rows = (double)lvl_rows[r.level];
+      bytes = hist_alg_bytes(rows, (double)lvl_nodes[r.level], f);
+    }
+    k.launches += 1;
+    k.ms += ms;
+    k.alg_bytes += bytes;
+    if (r.level >= 0 && r.level < 16 && r.cls == KC_HIST) {
+      out->hist_level_ms[r.level] += ms;
+      out->hist_level_rows[r.level] += rows;
+    }
+    if (r.level >= 0 && r.level < 16 && r.cls == KC_PART) out->part_level_ms[r.level] += ms;
+  }
+  if (!recs.empty()) {
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, recs.front().a, recs.back().b);
+    out->iteration_ms += ms;
+  }
+}
+
 tc_status tc_trainer_profile(tc_trainer* tr, int32_t iterations, tc_profile* out) {
   if (!tr || !out || iterations < 0) return TC_ERR_INVALID_ARG;
   std::lock_guard<std::recursive_mutex> train_lock(tr->ctx->train_mu);
@@ -2563,48 +2618,91 @@ tc_status tc_trainer_profile(tc_trainer* tr, int32_t iterations, tc_profile* out
     return ctx->fail(TC_ERR_INVALID_ARG, "profile(%d) exceeds n_estimators", iterations);
   cudaStream_t st = ctx->stream;
   std::vector<tc_trainer::ProfRec> recs;
-  tr->prof = &recs;
-  tr->ev_used = 0;
   std::vector<uint32_t> mask;
   if (tr->sampling) mask.resize((tr->cfg.n + 31) / 32);
-  for (int i = 0; i < iterations; ++i) {
+  auto copy_mask = [&]() -> tc_status {
     if (tr->sampling) {  // this iteration's row sample, as step() would use
       tr->make_masks(1, mask.data());
       TC_CUDA(ctx, cudaMemcpyAsync(tr->smask.p, mask.data(), mask.size() * sizeof(uint32_t),
                                    cudaMemcpyHostToDevice, st));
     }
-    if (tr->goss) {
-      tc_status gs = tr->goss_iteration(st);
-      if (gs != TC_OK) {
-        tr->prof = nullptr;
-        return gs;
-      }
-    } else {
-      tr->enqueue_iteration(st);
-    }
-    // harvest every iteration so that the event pool stays small
-    cudaError_t e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) {
-      tr->prof = nullptr;
-      return ctx->cuda_fail(e, "profiled iteration");
-    }
-    for (const auto& r : recs) {
-      float ms = 0.0f;
-      cudaEventElapsedTime(&ms, r.a, r.b);
-      tc_kernel_time& k = out->k[r.cls];
-      k.launches += 1;
-      k.ms += ms;
-      k.alg_bytes += r.bytes;
-      if (r.level >= 0 && r.level < 16 && r.cls == KC_HIST) {
-        out->hist_level_ms[r.level] += ms;
-        out->hist_level_rows[r.level] += r.rows;
-      }
-      if (r.level >= 0 && r.level < 16 && r.cls == KC_PART) out->part_level_ms[r.level] += ms;
-    }
-    recs.clear();
+    return TC_OK;
+  };
+  // The batched path is timed inside the graph it replays: the iteration is
+  // captured once more with an event-record node around every launch, and
+  // that graph is replayed per profiled iteration (the events of one replay
+  // are read before the next).  GOSS iterations and the plain path, which
+  // synchronise with the host inside an iteration, are timed launch by launch.
+  const bool in_graph = tr->prm.batched && !tr->goss;
+  out->in_graph = in_graph ? 1 : 0;
+  if (in_graph) {
+    tr->prof = &recs;
+    tr->prof_capture = true;
     tr->ev_used = 0;
+    const int64_t l0 = tr->launches;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      tr->enqueue_iteration(st);
+      e = cudaStreamEndCapture(st, &g);
+    }
+    tr->prof = nullptr;
+    tr->prof_capture = false;
+    const int64_t per_iter = tr->launches - l0;
+    tr->launches = l0;
+    if (e != cudaSuccess) return ctx->cuda_fail(e, "profiled iteration capture");
+    cudaGraphExec_t gx = nullptr;
+    e = cudaGraphInstantiate(&gx, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return ctx->cuda_fail(e, "profiled iteration instantiate");
+    uint64_t lr[16];
+    uint32_t ln[16];
+    for (int i = 0; i < iterations; ++i) {
+      tc_status ms = copy_mask();
+      if (ms == TC_OK) {
+        e = cudaGraphLaunch(gx, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e == cudaSuccess) e = cudaMemcpy(lr, tr->lvl_rows.p, sizeof(lr), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(ln, tr->lvl_nodes.p, sizeof(ln), cudaMemcpyDeviceToHost);
+      }
+      if (ms != TC_OK || e != cudaSuccess) {
+        cudaGraphExecDestroy(gx);
+        return ms != TC_OK ? ms : ctx->cuda_fail(e, "profiled iteration");
+      }
+      harvest_profile(recs, lr, ln, tr->cfg.f, out);
+      tr->launches += per_iter;
+    }
+    cudaGraphExecDestroy(gx);
+  } else {
+    tr->prof = &recs;
+    tr->ev_used = 0;
+    for (int i = 0; i < iterations; ++i) {
+      tc_status ms = copy_mask();
+      if (ms != TC_OK) {
+        tr->prof = nullptr;
+        return ms;
+      }
+      if (tr->goss) {
+        tc_status gs = tr->goss_iteration(st);
+        if (gs != TC_OK) {
+          tr->prof = nullptr;
+          return gs;
+        }
+      } else {
+        tr->enqueue_iteration(st);
+      }
+      // harvest every iteration so that the event pool stays small
+      cudaError_t e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) {
+        tr->prof = nullptr;
+        return ctx->cuda_fail(e, "profiled iteration");
+      }
+      harvest_profile(recs, nullptr, nullptr, tr->cfg.f, out);
+      recs.clear();
+      tr->ev_used = 0;
+    }
+    tr->prof = nullptr;
   }
-  tr->prof = nullptr;
   tr->iters_done += iterations;
   tr->scores_dirty = true;
   out->n_kernels = KC_N;

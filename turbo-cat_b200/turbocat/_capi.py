@@ -62,7 +62,8 @@ class KernelTime(C.Structure):
 
 class Profile(C.Structure):
     _fields_ = [("n_kernels", C.c_int32), ("k", KernelTime * 12), ("hist_level_ms", C.c_double * 16),
-                ("hist_level_rows", C.c_double * 16), ("part_level_ms", C.c_double * 16)]
+                ("hist_level_rows", C.c_double * 16), ("part_level_ms", C.c_double * 16),
+                ("in_graph", C.c_int32), ("iteration_ms", C.c_double)]
 
 
 class ModelInfo(C.Structure):
@@ -209,13 +210,17 @@ class Trainer:
         return st
 
     def profile(self, iters):
-        """Runs `iters` iterations launch by launch; returns {kernel: (launches, ms, alg_bytes)}."""
+        """Runs `iters` profiled iterations (inside a replayed CUDA graph on the
+        batched path); returns {kernel: (launches, ms, alg_bytes)} plus
+        "_hist_levels", "_part_levels", "_in_graph" and "_iteration_ms"."""
         pr = Profile()
         self.eng._chk(lib().tc_trainer_profile(self.h, C.c_int32(iters), C.byref(pr)))
         out = {pr.k[i].name.decode(): (pr.k[i].launches, pr.k[i].ms, pr.k[i].alg_bytes)
                for i in range(pr.n_kernels)}
         out["_hist_levels"] = [(pr.hist_level_ms[d], pr.hist_level_rows[d]) for d in range(16)]
         out["_part_levels"] = [pr.part_level_ms[d] for d in range(16)]
+        out["_in_graph"] = bool(pr.in_graph)
+        out["_iteration_ms"] = pr.iteration_ms
         return out
 
     def set_validation(self, vds, early_stopping_rounds=50):
