@@ -74,11 +74,25 @@ def test_results_same_alone_and_in_the_mix(engine, capi, coalesce, pinned):
     if not coalesce:
         assert launches == len(reqs)
     srv.close()
-    # and the single-call predictor matches the FP64 oracle
-    e = O.Ensemble(0.3, 1, 6, a1["depth"], a1["feature"], np.zeros((300, 6), np.uint8), a1["threshold"],
-                   a1["leaves"], a1["weights"])
-    p64 = O.predict(e, reqs[3])[:, 0]  # request 3 went to model 1 with the sigmoid
-    assert np.max(np.abs(alone[3][:, 0] - 1 / (1 + np.exp(-p64)))) < 1e-5
+    # every request's result (served in the mix, equal to alone above) against
+    # the FP64 oracle's prediction of its model with the request's transform
+    ens = []
+    for (T, D, K), a in zip(((300, 6, 1), (40, 10, 1), (50, 5, 4)), (a1, a2, a3)):
+        ens.append(O.Ensemble(0.3, K, D, a["depth"], a["feature"], np.zeros((T, D), np.uint8), a["threshold"],
+                              a["leaves"], a["weights"]))
+    for i, X in enumerate(reqs):
+        raw = O.predict(ens[i % 3], X)
+        if transforms[i % 3] == "sigmoid":
+            want = 1.0 / (1.0 + np.exp(-raw))
+        elif transforms[i % 3] == "softmax":
+            z = np.exp(raw - raw.max(1, keepdims=True))
+            want = z / z.sum(1, keepdims=True)
+        else:
+            want = raw
+        a = (a1, a2, a3)[i % 3]
+        scale = 0.3 + (np.abs(a["leaves"]).max(1) * a["weights"]).sum()  # |base| + sum |w * leaf|
+        tol = 1e-5 * (scale if transforms[i % 3] == "raw" else 1.0)
+        assert np.max(np.abs(outs[i] - want)) <= tol, (i, transforms[i % 3])
 
 
 def test_coalescing_happens_under_a_burst(engine, capi):

@@ -10,6 +10,7 @@
 #include <pybind11/pybind11.h>
 #include <pybind11/stl.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -18,6 +19,7 @@
 #include <fstream>
 #include <memory>
 #include <mutex>
+#include <set>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -150,6 +152,45 @@ class GpuBooster {
     float s2 = 0.0f;
     for (float v : gain) s2 += v;
     if (s2 > 0) for (size_t i = 0; i < nf; ++i) norm[i] = gain[i] / s2;
+  }
+
+  // Per-tree summary (python/bindings.cpp:804-830): node and leaf counts,
+  // the FP32 sum of the leaf values in leaf order and whether the tree is a
+  // single leaf.  A symmetric tree of depth d has 2^d - 1 split nodes and 2^d
+  // leaves.
+  py::list tree_info() const {
+    py::list trees;
+    if (!model) return trees;
+    const int T = info.n_trees, D = info.max_depth, L = 1 << D;
+    std::vector<int32_t> depth(T);
+    std::vector<float> lv((size_t)T * L);
+    tc_model_export(model->m, depth.data(), nullptr, nullptr, nullptr, nullptr, lv.data(), nullptr, nullptr,
+                    nullptr);
+    for (int t = 0; t < T; ++t) {
+      const int nl = 1 << depth[t];
+      float sum = 0.0f;
+      for (int l = 0; l < nl; ++l) sum += lv[(size_t)t * L + l];
+      py::dict d;
+      d["n_nodes"] = (size_t)(2 * nl - 1);
+      d["n_leaves"] = (size_t)nl;
+      d["leaf_sum"] = sum;
+      d["is_single_leaf"] = depth[t] == 0;
+      trees.append(d);
+    }
+    return trees;
+  }
+
+  // The model's bin edges (the training set's), for Dataset::apply_bins-style
+  // host binning: bin = number of edges <= x (std::upper_bound), NaN -> 255
+  // (src/core/dataset.cpp:336-379).
+  void edges(std::vector<float>& e, std::vector<uint16_t>& ne) const {
+    e.assign((size_t)info.n_features * 255, 0.0f);
+    ne.assign(info.n_features, 0);
+    tc_model_export(model->m, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, e.data(), ne.data());
+  }
+  static int host_bin(float x, const float* e, int m) {
+    if (std::isnan(x)) return 255;
+    return (int)(std::upper_bound(e, e + m, x) - e);
   }
 
   py::list dump() const {
@@ -445,8 +486,123 @@ class TurboCatRegressor {
     }
     n_features_ = f;
     is_fitted_ = true;
+    train_X_ = X;  // a reference, not a copy: debug_predict compares against the training rows
     if (verbosity_ > 0)
       py::print("[TurboCat-B200] trained", booster_->info.n_trees, "trees in", booster_->stats.seconds, "s (device)");
+  }
+
+  py::list tree_info() const { return booster_ ? booster_->tree_info() : py::list(); }
+
+  // Diagnostics of python/bindings.cpp:832-964 for the symmetric path: the
+  // bins of the first rows of X under the training edges, the first tree's
+  // path for the first samples (level by level: the level-order node index,
+  // split, the sample's bin and the direction, right = bin != 255 && bin >
+  // split bin), the bins of the first training rows and the value ranges of
+  // the first features in the training set and in X.  Without the training
+  // rows (a loaded model) the training entries are empty.
+  py::dict debug_predict(FArray X) const {
+    if (!is_fitted_ || !booster_) throw std::runtime_error("Model not fitted");
+    check_2d(X, "X");
+    const int64_t n = X.shape(0);
+    const int f = (int)X.shape(1);
+    if (f != booster_->info.n_features)
+      throw std::runtime_error("X has " + std::to_string(f) + " features, the model " +
+                               std::to_string(booster_->info.n_features));
+    std::vector<float> e;
+    std::vector<uint16_t> ne;
+    booster_->edges(e, ne);
+    const float* x = X.data();
+    auto bin_of = [&](const float* rows, int64_t i, int j) {
+      return GpuBooster::host_bin(rows[i * f + j], e.data() + (size_t)j * 255, ne[j]);
+    };
+    py::dict result;
+    py::list bin_variance;
+    for (int j = 0; j < std::min(f, 10); ++j) {
+      std::set<int> uniq;
+      for (int64_t i = 0; i < std::min<int64_t>(n, 100); ++i) uniq.insert(bin_of(x, i, j));
+      py::list sample_bins;
+      for (int64_t i = 0; i < std::min<int64_t>(n, 10); ++i) sample_bins.append(bin_of(x, i, j));
+      py::dict fi;
+      fi["feature"] = j;
+      fi["unique_bins"] = uniq.size();
+      fi["sample_bins"] = sample_bins;
+      bin_variance.append(fi);
+    }
+    result["bin_variance"] = bin_variance;
+    py::list traces;
+    const tc_model_info& inf = booster_->info;
+    if (inf.n_trees > 0) {
+      const int D = inf.max_depth, L = 1 << D;
+      std::vector<int32_t> depth(inf.n_trees);
+      std::vector<uint16_t> feat((size_t)inf.n_trees * D);
+      std::vector<uint8_t> sbin((size_t)inf.n_trees * D);
+      std::vector<float> lv((size_t)inf.n_trees * L);
+      tc_model_export(booster_->model->m, depth.data(), feat.data(), sbin.data(), nullptr, nullptr, lv.data(),
+                      nullptr, nullptr, nullptr);
+      for (int64_t row = 0; row < std::min<int64_t>(n, 5); ++row) {
+        py::dict tr;
+        tr["sample_idx"] = row;
+        py::list path;
+        uint32_t idx = 0;
+        for (int k = 0; k < depth[0]; ++k) {
+          const int fj = feat[k], b = bin_of(x, row, fj);
+          const bool right = b != 255 && b > (int)sbin[k];
+          py::dict step;
+          step["node_idx"] = (int)((1u << k) - 1 + idx);
+          step["split_feature"] = fj;
+          step["split_bin"] = (int)sbin[k];
+          step["sample_bin"] = b;
+          step["go_right"] = right;
+          path.append(step);
+          idx = (idx << 1) | (right ? 1u : 0u);
+        }
+        tr["path"] = path;
+        tr["leaf_idx"] = (int)idx;
+        tr["leaf_value"] = lv[idx];
+        traces.append(tr);
+      }
+    }
+    result["sample_traces"] = traces;
+    py::list train_bins, raw_compare;
+    const bool have_train = train_X_.size() > 0 && train_X_.ndim() == 2 && train_X_.shape(1) == f;
+    const int64_t nt = have_train ? train_X_.shape(0) : 0;
+    const float* xt = have_train ? train_X_.data() : nullptr;
+    if (have_train) {
+      for (int j = 0; j < std::min(f, 10); ++j) {
+        std::set<int> uniq;
+        for (int64_t i = 0; i < std::min<int64_t>(nt, 100); ++i) uniq.insert(bin_of(xt, i, j));
+        py::dict fi;
+        fi["feature"] = j;
+        fi["unique_bins"] = uniq.size();
+        train_bins.append(fi);
+      }
+    }
+    for (int j = 0; j < std::min(f, 5); ++j) {
+      auto range = [&](const float* rows, int64_t m, float& lo, float& hi) {
+        lo = 1e30f;
+        hi = -1e30f;
+        for (int64_t i = 0; i < m; ++i) {
+          const float v = rows[i * f + j];
+          if (!std::isnan(v)) { lo = std::min(lo, v); hi = std::max(hi, v); }
+        }
+      };
+      py::dict cmp;
+      cmp["feature"] = j;
+      if (have_train) {
+        float lo, hi;
+        range(xt, nt, lo, hi);
+        cmp["train_min"] = lo;
+        cmp["train_max"] = hi;
+      }
+      float lo, hi;
+      range(x, n, lo, hi);
+      cmp["test_min"] = lo;
+      cmp["test_max"] = hi;
+      raw_compare.append(cmp);
+    }
+    result["train_bin_variance"] = train_bins;
+    result["raw_value_comparison"] = raw_compare;
+    return result;
   }
 
   std::vector<float> predict(FArray X, bool timing) {
@@ -478,6 +634,7 @@ class TurboCatRegressor {
     booster_->load(path);
     n_features_ = booster_->info.n_features;
     is_fitted_ = true;
+    train_X_ = FArray();
   }
   py::list get_booster_dump() const {
     if (!is_fitted_) throw std::runtime_error("Model not fitted");
@@ -512,6 +669,7 @@ class TurboCatRegressor {
   bool use_goss_;
   int verbosity_;
   std::unique_ptr<GpuBooster> booster_;
+  FArray train_X_;
   int n_features_ = 0;
   bool is_fitted_ = false;
 };
@@ -521,6 +679,52 @@ void print_info() {
 }
 
 }  // namespace
+
+// ------------------------------------------------------------------- metrics
+// The `metrics` submodule (python/bindings.cpp:1139-1224) over the formulas
+// that include/turbocat/metrics.hpp:363-470 defines: FP32 sums in row order,
+// a row is positive when y_true > 0.5 and predicted positive when
+// y_pred >= threshold.  roc_auc, pr_auc and find_optimal_threshold have no
+// source in the reference tree (src/metrics/metrics.cpp is missing), so they
+// raise.
+enum class MetricType : uint8_t { LogLoss = 0, Accuracy, Precision, Recall, F1, ROC_AUC, PR_AUC, MSE, MAE, RMSE };
+
+struct Confusion {
+  uint32_t tp = 0, tn = 0, fp = 0, fn = 0;
+};
+
+Confusion confusion(const FArray& yt, const FArray& yp, float thr) {
+  if (yt.size() != yp.size()) throw std::runtime_error("y_true and y_pred have different lengths");
+  Confusion c;
+  const float* t = yt.data();
+  const float* p = yp.data();
+  for (py::ssize_t i = 0; i < yt.size(); ++i) {
+    const bool actual = t[i] > 0.5f, pred = p[i] >= thr;
+    if (actual && pred) ++c.tp;
+    else if (!actual && !pred) ++c.tn;
+    else if (!actual && pred) ++c.fp;
+    else ++c.fn;
+  }
+  return c;
+}
+float precision_of(const Confusion& c) { return c.tp + c.fp > 0 ? (float)c.tp / (float)(c.tp + c.fp) : 0.0f; }
+float recall_of(const Confusion& c) { return c.tp + c.fn > 0 ? (float)c.tp / (float)(c.tp + c.fn) : 0.0f; }
+
+float metric_mse(const FArray& yt, const FArray& yp) {
+  if (yt.size() != yp.size()) throw std::runtime_error("y_true and y_pred have different lengths");
+  float sum = 0.0f;
+  for (py::ssize_t i = 0; i < yt.size(); ++i) {
+    const float d = yt.data()[i] - yp.data()[i];
+    sum += d * d;
+  }
+  return sum / (float)yt.size();
+}
+
+[[noreturn]] void metric_unavailable(const char* name) {
+  throw std::runtime_error(std::string(name) +
+                           " is unavailable: the reference declares it but ships no source for it "
+                           "(src/metrics/metrics.cpp is missing)");
+}
 
 PYBIND11_MODULE(_turbocat, m) {
   m.doc() = "TurboCat symmetric-tree path on NVIDIA B200 (sm_100a)";
@@ -571,6 +775,8 @@ PYBIND11_MODULE(_turbocat, m) {
       .def("predict_nobinning", &TurboCatRegressor::predict, py::arg("X"), py::arg("timing") = false)
       .def("predict_nobinning_fast", &TurboCatRegressor::predict, py::arg("X"), py::arg("timing") = false)
       .def("debug_info", &TurboCatRegressor::debug_info)
+      .def("tree_info", &TurboCatRegressor::tree_info)
+      .def("debug_predict", &TurboCatRegressor::debug_predict)
       .def("feature_importance", &TurboCatRegressor::feature_importance)
       .def("save", &TurboCatRegressor::save)
       .def("load", &TurboCatRegressor::load)
@@ -581,4 +787,75 @@ PYBIND11_MODULE(_turbocat, m) {
       .def_property_readonly("train_seconds", &TurboCatRegressor::train_seconds);
 
   m.def("print_info", &print_info, "Print TurboCat library information");
+
+  auto metrics = m.def_submodule("metrics", "Evaluation metrics for TurboCat");
+  py::enum_<MetricType>(metrics, "MetricType")
+      .value("LogLoss", MetricType::LogLoss)
+      .value("Accuracy", MetricType::Accuracy)
+      .value("Precision", MetricType::Precision)
+      .value("Recall", MetricType::Recall)
+      .value("F1", MetricType::F1)
+      .value("ROC_AUC", MetricType::ROC_AUC)
+      .value("PR_AUC", MetricType::PR_AUC)
+      .value("MSE", MetricType::MSE)
+      .value("MAE", MetricType::MAE)
+      .value("RMSE", MetricType::RMSE)
+      .export_values();
+  metrics.def("roc_auc", [](FArray, FArray) -> float { metric_unavailable("roc_auc"); }, "Compute ROC-AUC score",
+              py::arg("y_true"), py::arg("y_pred"));
+  metrics.def("pr_auc", [](FArray, FArray) -> float { metric_unavailable("pr_auc"); }, "Compute PR-AUC score",
+              py::arg("y_true"), py::arg("y_pred"));
+  metrics.def(
+      "log_loss",
+      [](FArray yt, FArray yp, float eps) {
+        if (yt.size() != yp.size()) throw std::runtime_error("y_true and y_pred have different lengths");
+        float loss = 0.0f;
+        for (py::ssize_t i = 0; i < yt.size(); ++i) {
+          const float p = std::max(eps, std::min(1.0f - eps, yp.data()[i]));
+          const float y = yt.data()[i];
+          loss -= y * std::log(p) + (1.0f - y) * std::log(1.0f - p);
+        }
+        return loss / (float)yt.size();
+      },
+      "Compute log loss", py::arg("y_true"), py::arg("y_pred"), py::arg("eps") = 1e-15f);
+  metrics.def(
+      "accuracy",
+      [](FArray yt, FArray yp, float thr) {
+        const Confusion c = confusion(yt, yp, thr);
+        const uint32_t total = c.tp + c.tn + c.fp + c.fn;
+        return total > 0 ? (float)(c.tp + c.tn) / (float)total : 0.0f;
+      },
+      "Compute accuracy", py::arg("y_true"), py::arg("y_pred"), py::arg("threshold") = 0.5f);
+  metrics.def(
+      "precision", [](FArray yt, FArray yp, float thr) { return precision_of(confusion(yt, yp, thr)); },
+      "Compute precision", py::arg("y_true"), py::arg("y_pred"), py::arg("threshold") = 0.5f);
+  metrics.def(
+      "recall", [](FArray yt, FArray yp, float thr) { return recall_of(confusion(yt, yp, thr)); },
+      "Compute recall", py::arg("y_true"), py::arg("y_pred"), py::arg("threshold") = 0.5f);
+  metrics.def(
+      "f1_score",
+      [](FArray yt, FArray yp, float thr) {
+        const Confusion c = confusion(yt, yp, thr);
+        const float p = precision_of(c), r = recall_of(c);
+        return p + r > 0 ? 2.0f * p * r / (p + r) : 0.0f;
+      },
+      "Compute F1 score", py::arg("y_true"), py::arg("y_pred"), py::arg("threshold") = 0.5f);
+  metrics.def(
+      "find_optimal_threshold",
+      [](FArray, FArray, MetricType, int) -> float { metric_unavailable("find_optimal_threshold"); },
+      "Find optimal threshold for a metric", py::arg("y_true"), py::arg("y_pred"),
+      py::arg("metric") = MetricType::F1, py::arg("n_thresholds") = 100);
+  metrics.def("mse", &metric_mse, "Compute mean squared error", py::arg("y_true"), py::arg("y_pred"));
+  metrics.def(
+      "mae",
+      [](FArray yt, FArray yp) {
+        if (yt.size() != yp.size()) throw std::runtime_error("y_true and y_pred have different lengths");
+        float sum = 0.0f;
+        for (py::ssize_t i = 0; i < yt.size(); ++i) sum += std::abs(yt.data()[i] - yp.data()[i]);
+        return sum / (float)yt.size();
+      },
+      "Compute mean absolute error", py::arg("y_true"), py::arg("y_pred"));
+  metrics.def(
+      "rmse", [](FArray yt, FArray yp) { return std::sqrt(metric_mse(yt, yp)); },
+      "Compute root mean squared error", py::arg("y_true"), py::arg("y_pred"));
 }

@@ -154,6 +154,15 @@ class TurboCatRegressor:
         info["params"] = self._params
         return info
 
+    def tree_info(self):
+        """Per tree: node and leaf counts, leaf sum, single-leaf flag."""
+        return self._model.tree_info()
+
+    def debug_predict(self, X):
+        """Bins of the first rows under the training edges, the first tree's
+        path for the first samples, and train/test value ranges."""
+        return self._model.debug_predict(_f32(X))
+
     @property
     def n_trees(self):
         return self._model.n_trees
