@@ -58,7 +58,6 @@ constexpr int SCAN_NODES = 16;    // nodes per scan block (2 per warp; measured:
 static_assert(SCAN_WARPS * 32 == 256, "a scan block also runs the 256-thread pick");
 constexpr int MERGE_BB = 4;       // bins per merge block
 constexpr int PLAN_THREADS = 1024;
-constexpr int kHistRowsMax = (1 << 24) - 1;  // rows of a histogram item: its row count field has 24 bits
 constexpr int VALID_BLOCKS = 296;  // blocks of the validation kernel (fixed: its partial sums have a fixed order)
 
 struct NodeStat {
@@ -126,8 +125,7 @@ struct DevPtrs {
   uint16_t* leaf;                // [K][n]
   uint32_t* rows;                // [K][n]
   double2* hist[2];              // [K][2^(D-1)][F][256]
-  uint64_t* part;                // [item_cap][256][W] packed fixed-point partials of the histogram items
-  int2* part_exp;                // [item_cap] their (grad, hess) exponents
+  float2* part;                  // [item_cap][256][W]
   int32_t* cum;                  // [K*2^(D-1) + 1] cumulative item counts per segment (chunk-major)
   int32_t* rchunk;               // [1] rows per chunk at the current level
   int32_t* seg_start;            // [K][2^(D-1)]
@@ -439,7 +437,7 @@ struct HistShape {
   static constexpr int W = 32 * J;                      // histogram columns of a block
   static constexpr int WARPS = HIST_THREADS / 32;
   static constexpr int S = 2;                           // staging depth per warp (batches in flight)
-  static constexpr size_t hist_bytes = (size_t)kSlots * W * 8;
+  static constexpr size_t hist_bytes = (size_t)2 * kSlots * W * 4;
   static constexpr size_t warp_bytes = (size_t)S * HIST_BATCH * (W + 8);   // bins + (grad, hess)
   static constexpr size_t smem = hist_bytes + WARPS * warp_bytes;
 };
@@ -470,59 +468,11 @@ __device__ __forceinline__ HistCol hist_col(const DevPtrs& P, int f, int nf) {
   return {span, P.nan_any[f] ? 1 : min(HIST_THREADS / 32, max(1, 255 / span))};
 }
 
-__device__ __forceinline__ void red_add_u64(uint32_t a, uint64_t v) {
-  asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(a), "l"(v) : "memory");
+__device__ __forceinline__ void red_add_f32(uint32_t a, float v) {
+  asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
 }
-
-// Fixed-point packing of a row's (grad, hess) for the shared histogram.
-//
-// A work item accumulates one 64-bit integer per (bin slot, column) with one
-// shared atomic per (row, feature) pair: integer sums are exact and do not
-// depend on the order of the atomics, and one 8-byte atomic costs the
-// shared-memory banks half of the FP32 grad + hess (or grad + count) pair of
-// atomics it replaces.
-//   general   bits 63..32: grad * 2^eg (signed), bits 31..0: hess * 2^eh
-//   CNT       bits 63..24: grad * 2^eg (signed), bits 23..0: row count
-//             (every row's hessian is the same constant, MSE: h = 2, so
-//             hess = count * h exactly)
-// The scales are powers of two chosen per item from the item's own sums
-// S = sum |grad| and sum hess over its rows (FP64): with rounding to nearest,
-// |sum over any bin of round(g * 2^e)| <= 2^e * S + rows / 2, and e is the
-// largest value that keeps this below 2^31 (general grad), 2^32 (hess) or
-// 2^39 (CNT grad), so no field of any bin can overflow into its neighbour.
-// A row's grad is then represented to within 2^-(e+1) ~ S * 2^-32 (2^-40
-// for CNT): relative to the item's total |grad|, finer than an FP32 running
-// sum over its rows.  The partial of an item holds these integers; the merge
-// converts them to FP64 with the item's exponents (exactly) and sums items
-// in a fixed order.
-struct HistScale {
-  float sg, sh;    // 2^eg, 2^eh as multipliers (exact)
-  int32_t eg, eh;
-};
-
-__device__ __forceinline__ int hist_exponent(double S, double rows, double limit) {
-  if (!(S > 0.0)) return 0;
-  // a relative margin for the rounding of the FP64 sum S itself
-  const double room = limit * (1.0 - 0x1p-20) - 0.5 * rows;
-  if (!(room > 0.0)) return -126;
-  int e = ilogb(room / S);
-  // ilogb(x) = floor(log2 x); the product 2^e * S <= room holds, but check
-  // once more against rounding of the division
-  if (ldexp(S, e) > room) --e;
-  return max(-126, min(64, e));
-}
-
-__device__ __forceinline__ float exp2i(int e) { return __int_as_float((e + 127) << 23); }
-
-template <bool CNT>
-__device__ __forceinline__ uint64_t hist_pack(float g, float h, const HistScale& sc) {
-  if (CNT) {
-    const long long gi = __float2ll_rn(g * sc.sg);  // exact product: sc.sg is a power of two
-    return ((uint64_t)gi << 24) + 1ull;
-  }
-  const int gi = __float2int_rn(g * sc.sg);
-  const unsigned hi = __float2uint_rn(h * sc.sh);
-  return ((uint64_t)(uint32_t)gi << 32) | (uint64_t)hi;
+__device__ __forceinline__ void red_add_u32(uint32_t a, uint32_t v) {
+  asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(a), "r"(v) : "memory");
 }
 
 // Persistent blocks over work items; an item is one chunk of one segment's
@@ -531,38 +481,40 @@ __device__ __forceinline__ uint64_t hist_pack(float g, float h, const HistScale&
 // together read the same rows and the L2 serves a row's bytes and its
 // (grad, hess) to every group.
 //
-// An item starts with a pass over its rows' (grad, hess) (contiguous in list
-// order) for the sums that fix its fixed-point scales (above).  Then every
-// warp runs its own copy pipeline: lane l stages row l of a 32-row batch (its
-// group slice and its (grad, hess)) by cp.async into the warp's private
-// buffers, one batch ahead of the updates, with the row ids of gathered rows
-// fetched a further batch ahead; no block barrier is taken until the item is
-// done.
+// Every warp runs its own copy pipeline: lane l stages row l of a 32-row
+// batch (its group slice and its (grad, hess)) by cp.async into the warp's
+// private buffers, one batch ahead of the updates, with the row ids of
+// gathered rows fetched a further batch ahead; no block barrier is taken
+// until the item is done.
 //
 // Shared histogram layout: column fastest, so a column always hits the same
-// bank pair: uint64 hist[slot * W + column].  A wide group is updated four
-// rows at a time: lane (r = l/8, c = l%8) loads the 4 bins of columns
-// 4c..4c+3 of row r of the quad as one word and, in step s, updates column
-// 4c + (s + r) % 4, so the 32 lanes of every step hit 32 different columns.
-// A group of at most 16 features is packed: with p2 = next power of two >=
-// its width, the 32 columns hold 32/p2 private copies and one warp
-// instruction updates 32/p2 rows; the copies are summed when the partial is
-// written.  Columns past a group's width (padding bytes, all bin 0: one hot
-// address) are not updated.  Each lane keeps the shared address of (its
-// warp's copy of) every column it updates, so an update is a byte permute, an
-// add and one 64-bit atomic.
+// bank: float hist[(2*slot + {0 grad, 1 hess}) * W + column].  A wide group
+// is updated four rows at a time: lane (r = l/8, c = l%8) loads the 4 bins
+// of columns 4c..4c+3 of row r of the quad as one word and, in step s,
+// updates column 4c + (s + r) % 4, so the 32 lanes of every step hit 32
+// different columns (banks).  A group of at most 16 features is packed: with
+// p2 = next power of two >= its width, the 32 columns hold 32/p2 private
+// copies and one warp instruction updates 32/p2 rows; the copies are summed
+// when the partial is written.  Columns past a group's width (padding bytes,
+// all bin 0: one hot address) are not updated.  Each lane keeps the shared
+// address of (its warp's copy of) every column it updates, so an update is a
+// byte permute, an add and the atomics.
+//
+// CNT: every row's hessian is the same constant (MSE: h = 2); rows are
+// counted with 32-bit integer shared atomics (2.7x the throughput of FP32
+// shared atomics on this part) and hess = count * h is exact.
 template <int J, bool CNT>
 __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs P, int d) {
   using S_ = HistShape<J>;
   constexpr int W = S_::W, S = S_::S, B = HIST_BATCH;
-  constexpr uint32_t BIN_BYTES = 8 * W;   // one slot: W 64-bit accumulators
+  constexpr uint32_t BIN_BYTES = 8 * W;   // grad and hess rows of one slot
   extern __shared__ __align__(16) unsigned char smraw[];
-  uint64_t* hist = reinterpret_cast<uint64_t*>(smraw);
+  float* hist = reinterpret_cast<float*>(smraw);
+  uint32_t* histu = reinterpret_cast<uint32_t*>(smraw);
   const uint32_t hbase = (uint32_t)__cvta_generic_to_shared(hist);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   uint8_t* w_bins = smraw + S_::hist_bytes + (size_t)warp * S_::warp_bytes;        // [S][B][W]
   float2* w_gh = reinterpret_cast<float2*>(w_bins + (size_t)S * B * W);            // [S][B]
-  __shared__ double s_sum[2][HIST_THREADS / 32];
   const int P2 = pairs_at(d);
   const int nseg = c.K * P2;
   const int n_items = P.cum[nseg];
@@ -574,7 +526,7 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
   uint32_t sel[4];
 #pragma unroll
   for (int s = 0; s < 4; ++s) sel[s] = 0x4404u | ((uint32_t)((s + qr) & 3) << 4);
-  for (int q = threadIdx.x; q < kSlots * W; q += blockDim.x) hist[q] = 0ull;
+  for (int q = threadIdx.x; q < 2 * kSlots * W; q += blockDim.x) hist[q] = 0.0f;
   __syncthreads();
   // Items are claimed from a counter (blocks that drew cheap items take
   // more), the next one while the current one runs.  Item ci*G + g is chunk
@@ -603,42 +555,6 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
     const int p2 = gsize <= 1 ? 1 : (gsize <= 2 ? 2 : (gsize <= 4 ? 4 : (gsize <= 8 ? 8 : (gsize <= 16 ? 16 : 32))));
     const bool narrow = p2 <= 16;
     const int nchunk16 = (gsize + 15) >> 4;  // 16-byte pieces of the slice that hold features
-    // the segment's ceil(len / R) chunks have equal sizes (within one row)
-    const int s0 = d == 0 ? 0 : P.seg_start[k * Pmax + p];
-    const int sl = d == 0 ? (int)c.n : P.seg_len[k * Pmax + p];
-    const int nch = (sl + R - 1) / R;
-    const int start = s0 + (int)((long long)sl * ch_idx / nch);
-    const int end = s0 + (int)((long long)sl * (ch_idx + 1) / nch);
-    const uint32_t* rows = P.rows + (size_t)k * c.n;
-    // (grad, hess) in list order: the root's rows are 0..n-1, a smaller
-    // child's were copied next to its row ids by the scatter kernel
-    const float2* gh = (d == 0 ? P.gh : P.cgh) + (size_t)k * c.n;
-    // this item's fixed-point scales: FP64 sums of |grad| and hess over its
-    // rows, every thread a fixed stride, the warps in a fixed order
-    HistScale sc;
-    {
-      double sa = 0.0, sb = 0.0;
-#pragma unroll 4
-      for (int r = start + threadIdx.x; r < end; r += blockDim.x) {
-        const float2 v = gh[r];
-        sa += (double)fabsf(v.x);
-        sb += (double)v.y;
-      }
-      for (int o = 16; o; o >>= 1) {
-        sa += __shfl_xor_sync(0xffffffffu, sa, o);
-        sb += __shfl_xor_sync(0xffffffffu, sb, o);
-      }
-      if (lane == 0) { s_sum[0][warp] = sa; s_sum[1][warp] = sb; }
-      __syncthreads();
-      sa = 0.0;
-      sb = 0.0;
-      for (int w = 0; w < nwarps; ++w) { sa += s_sum[0][w]; sb += s_sum[1][w]; }
-      const double rows_item = (double)(end - start);
-      sc.eg = hist_exponent(sa, rows_item, CNT ? 549755813887.0 : 2147483647.0);
-      sc.eh = CNT ? 0 : hist_exponent(sb, rows_item, 4294967295.0);
-      sc.sg = exp2i(sc.eg);
-      sc.sh = exp2i(sc.eh);
-    }
     // shared address of this warp's copy of each column the lane updates;
     // columns past the group's width are skipped (their padding bytes are
     // all bin 0, a single hot address)
@@ -650,9 +566,19 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
       for (int s = 0; s < 4; ++s) {
         const int col = 32 * j + 4 * c4 + ((s + qr) & 3);
         const HistCol hc = hist_col(P, g0 + col, (int)c.f);
-        ab[j][s] = hbase + BIN_BYTES * (uint32_t)((warp % hc.copies) * hc.span) + 8u * col;
+        ab[j][s] = hbase + BIN_BYTES * (uint32_t)((warp % hc.copies) * hc.span) + 4u * col;
         if (col < gsize) live |= 1u << (4 * j + s);
       }
+    // the segment's ceil(len / R) chunks have equal sizes (within one row)
+    const int s0 = d == 0 ? 0 : P.seg_start[k * Pmax + p];
+    const int sl = d == 0 ? (int)c.n : P.seg_len[k * Pmax + p];
+    const int nch = (sl + R - 1) / R;
+    const int start = s0 + (int)((long long)sl * ch_idx / nch);
+    const int end = s0 + (int)((long long)sl * (ch_idx + 1) / nch);
+    const uint32_t* rows = P.rows + (size_t)k * c.n;
+    // (grad, hess) in list order: the root's rows are 0..n-1, a smaller
+    // child's were copied next to its row ids by the scatter kernel
+    const float2* gh = (d == 0 ? P.gh : P.cgh) + (size_t)k * c.n;
     const uint8_t* bsrc = P.bins_rm + g0;
     const int nb = (end - start + B - 1) / B;   // batches in the item; warp w takes w, w+nwarps, ...
     uint32_t rid_next = 0;
@@ -686,16 +612,17 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
       const uint8_t* sb = w_bins + (size_t)st * B * W;
       const float2* sv = w_gh + st * B;
       if (!narrow) {
-        // the batch's bins and packed (grad, hess) go to registers first, so
-        // the loads are not ordered behind the updates (they share the memory space)
+        // the batch's bins and (grad, hess) go to registers first, so the
+        // loads are not ordered behind the updates (they share the memory space)
         const uint32_t* sw = reinterpret_cast<const uint32_t*>(sb);
         uint32_t wd[B / 4][J];
-        uint64_t pv[B / 4];
+        float vx[B / 4], vy[B / 4];
 #pragma unroll
         for (int qd = 0; qd < B / 4; ++qd) {
           const int row = 4 * qd + qr;
           const float2 v = sv[row];
-          pv[qd] = hist_pack<CNT>(v.x, v.y, sc);
+          vx[qd] = v.x;
+          vy[qd] = v.y;
 #pragma unroll
           for (int j = 0; j < J; ++j) wd[qd][j] = sw[row * (W / 4) + 8 * j + c4];
         }
@@ -709,7 +636,11 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
                 for (int s = 0; s < 4; ++s) {
                   // __byte_perm gives bin * 256; a slot is BIN_BYTES = 256 * J bytes
                   const uint32_t a = ab[j][s] + __byte_perm(wd[qd][j], 0u, sel[s]) * J;
-                  if (live & (1u << (4 * j + s))) red_add_u64(a, pv[qd]);
+                  if (live & (1u << (4 * j + s))) {
+                    red_add_f32(a, vx[qd]);
+                    if (CNT) red_add_u32(a + 4 * W, 1u);
+                    else red_add_f32(a + 4 * W, vy[qd]);
+                  }
                 }
               }
             }
@@ -721,20 +652,26 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
         const int rpi = 32 / p2;
         const int my_row = lane / p2, my_col = lane - my_row * p2;
         const HistCol hc = hist_col(P, g0 + my_col, (int)c.f);
-        const uint32_t abn = hbase + BIN_BYTES * (uint32_t)((warp % hc.copies) * hc.span) + 8u * lane;
+        const uint32_t abn = hbase + BIN_BYTES * (uint32_t)((warp % hc.copies) * hc.span) + 4u * lane;
         for (int i0 = 0; i0 < B; i0 += 4 * rpi) {
           uint32_t bb[4];
-          uint64_t pv[4];
+          float gx[4], gy[4];
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
             const int row = min(i0 + u * rpi + my_row, B - 1);
             const float2 v = sv[row];
-            pv[u] = hist_pack<CNT>(v.x, v.y, sc);
+            gx[u] = v.x;
+            gy[u] = v.y;
             bb[u] = sb[row * W + my_col];
           }
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
-            if (i0 + u * rpi + my_row < nvalid && my_col < gsize) red_add_u64(abn + BIN_BYTES * bb[u], pv[u]);
+            if (i0 + u * rpi + my_row < nvalid && my_col < gsize) {
+              const uint32_t a = abn + BIN_BYTES * bb[u];
+              red_add_f32(a, gx[u]);
+              if (CNT) red_add_u32(a + 4 * W, 1u);
+              else red_add_f32(a + 4 * W, gy[u]);
+            }
           }
         }
       }
@@ -744,9 +681,8 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
 #undef TC_ISSUE
     cp_async_wait<0>();
     __syncthreads();
-    uint64_t* out = P.part + (size_t)item * kSlots * W;
-    if (threadIdx.x == 0) P.part_exp[item] = make_int2(sc.eg, sc.eh);
-    // write the partial (copies summed; integer sums are exact) and clear the
+    float2* out = P.part + (size_t)item * kSlots * W;
+    // write the partial (copies summed in a fixed order) and clear the
     // histogram for the next item; a thread clears exactly the slots it reads
     const int ncp = narrow ? 32 / p2 : 1;     // packed copies of a narrow group
     // blockDim.x is a multiple of W: a thread's column is the same on every pass
@@ -754,23 +690,30 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
     const HistCol fc = hist_col(P, g0 + col, (int)c.f);
     for (int q = threadIdx.x; q < kSlots * W; q += blockDim.x) {
       const int b = q / W;
-      uint64_t acc = 0ull;
+      float sgv = 0.0f, shv = 0.0f;
+      uint32_t cnt = 0;
       if (!narrow || col < p2) {
         const int kc = b == kNanBin ? 1 : (b < fc.span ? fc.copies : 0);
         for (int cc = 0; cc < kc; ++cc) {
           const int slot = b == kNanBin ? kNanBin : cc * fc.span + b;
           for (int cp = 0; cp < ncp; ++cp) {
-            const int o = slot * W + cp * p2 * (narrow ? 1 : 0) + col;
-            acc += hist[o];
-            if (!narrow) hist[o] = 0ull;
+            const int o = 2 * slot * W + cp * p2 * (narrow ? 1 : 0) + col;
+            sgv += hist[o];
+            if (CNT) cnt += histu[o + W];
+            else shv += hist[o + W];
+            if (!narrow) {
+              hist[o] = 0.0f;
+              hist[o + W] = 0.0f;
+            }
           }
         }
+        if (CNT) shv = c.hconst * (float)cnt;
       }
-      out[q] = acc;
+      out[q] = make_float2(sgv, shv);
     }
     if (narrow) {
       __syncthreads();
-      for (int q = threadIdx.x; q < kSlots * 32; q += blockDim.x) hist[(q >> 5) * W + (q & 31)] = 0ull;
+      for (int q = threadIdx.x; q < 2 * kSlots * 32; q += blockDim.x) hist[(q >> 5) * W + (q & 31)] = 0.0f;
     }
     __syncthreads();
     item = s_item[it & 1];
@@ -779,23 +722,9 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
 
 // ----------------------------------------------------------------- merge --
 
-// Exact FP64 value of a packed partial (grad, hess) with the item's exponents.
-template <bool CNT>
-__device__ __forceinline__ double2 hist_unpack(uint64_t v, int2 e, float hconst) {
-  if (CNT) {
-    const long long g = (long long)v >> 24;
-    const uint32_t cnt = (uint32_t)(v & 0xffffffull);
-    return make_double2(ldexp((double)g, -e.x), (double)hconst * (double)cnt);
-  }
-  const long long g = (long long)v >> 32;
-  const uint32_t h = (uint32_t)v;
-  return make_double2(ldexp((double)g, -e.x), ldexp((double)h, -e.y));
-}
-
 // grid (256/MERGE_BB, segments, groups).  FP64 sum of a segment's partials
-// (each converted exactly from its fixed-point integers; fixed chunk order),
-// then larger = parent - smaller (FP64).
-template <int J, bool CNT>
+// (fixed chunk order), then larger = parent - smaller (FP64).
+template <int J>
 __global__ void k_merge(DevCfg c, DevPtrs P, int d) {
   constexpr int W = 32 * J;
   __shared__ double2 tile[MERGE_BB][W];
@@ -814,28 +743,21 @@ __global__ void k_merge(DevCfg c, DevPtrs P, int d) {
     double sg_ = 0.0, sh = 0.0;
     if (col < gsize) {
       // four partials loaded ahead of their (in-order) FP64 adds
-      const uint64_t* src = P.part + ((size_t)ib * kSlots + b0 + bl) * W + col;
+      const float2* src = P.part + ((size_t)ib * kSlots + b0 + bl) * W + col;
       const size_t step = (size_t)c.G * kSlots * W;
       int ch = 0;
       for (; ch + 4 <= nch; ch += 4) {
-        uint64_t v[4];
-        int2 e[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          v[u] = src[(size_t)(ch + u) * step];
-          e[u] = P.part_exp[ib + (ch + u) * c.G];
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const double2 x = hist_unpack<CNT>(v[u], e[u], c.hconst);
-          sg_ += x.x;
-          sh += x.y;
-        }
+        const float2 v0 = src[(size_t)ch * step], v1 = src[(size_t)(ch + 1) * step];
+        const float2 v2 = src[(size_t)(ch + 2) * step], v3 = src[(size_t)(ch + 3) * step];
+        sg_ += (double)v0.x; sh += (double)v0.y;
+        sg_ += (double)v1.x; sh += (double)v1.y;
+        sg_ += (double)v2.x; sh += (double)v2.y;
+        sg_ += (double)v3.x; sh += (double)v3.y;
       }
       for (; ch < nch; ++ch) {
-        const double2 x = hist_unpack<CNT>(src[(size_t)ch * step], P.part_exp[ib + ch * c.G], c.hconst);
-        sg_ += x.x;
-        sh += x.y;
+        const float2 v = src[(size_t)ch * step];
+        sg_ += (double)v.x;
+        sh += (double)v.y;
       }
     }
     tile[bl][col] = make_double2(sg_, sh);
@@ -1452,7 +1374,7 @@ __device__ __forceinline__ void plan_body(const DevCfg& c, const DevPtrs& P, int
   if (tid == 0) {
     int R = c.rows_fixed;
     if (R <= 0) R = (int)max((long long)c.rows_min, (s_rows * gw + c.target_items - 1) / c.target_items);
-    s_R = min(R, kHistRowsMax);
+    s_R = R;
   }
   __syncthreads();
   for (int round = 0; c.rows_fixed <= 0 && round < 16; ++round) {
@@ -1473,7 +1395,7 @@ __device__ __forceinline__ void plan_body(const DevCfg& c, const DevPtrs& P, int
     const long long items = s_cnt * gw;
     __syncthreads();
     if (items <= c.target_items) break;
-    if (tid == 0) s_R = (int)min((long long)kHistRowsMax, (long long)Rt * items / c.target_items + 1);
+    if (tid == 0) s_R = (int)min((long long)INT32_MAX / 2, (long long)Rt * items / c.target_items + 1);
     __syncthreads();
   }
   if (tid == 0) {
@@ -1757,8 +1679,7 @@ struct tc_trainer {
   DevBuf<uint16_t> leaf;
   DevBuf<uint32_t> rows;
   DevBuf<double2> hist0, hist1;
-  DevBuf<uint64_t> part;
-  DevBuf<int2> part_exp;
+  DevBuf<float2> part;
   DevBuf<int32_t> cum, rchunk, seg_start, seg_len, small, iter;
   DevBuf<FeatBest> fbest;
   DevBuf<uint32_t> counters;
@@ -1958,17 +1879,14 @@ tc_status tc_trainer::configure(int J_, int waves) {
   hist_waves = waves;
   long long cap = (long long)waves * hist_grid + (long long)K * Pmax * G + 1;
   if (cfg.rows_fixed) cap += (long long)K * G * ((cfg.n + cfg.rows_fixed - 1) / cfg.rows_fixed + 1);
-  cap += (long long)K * G * (cfg.n / kHistRowsMax + 1);  // chunks capped at kHistRowsMax rows
   cfg.G = G;
   cfg.W = W;
   cfg.hist_grid = hist_grid;
   cfg.target_items = waves * hist_grid;
   cfg.item_cap = (int)cap;
   TC_TRY(part.alloc(ctx, (size_t)cap * kSlots * W, "histogram partials"));
-  TC_TRY(part_exp.alloc(ctx, (size_t)cap, "histogram partial exponents"));
   TC_TRY(cum.alloc(ctx, (size_t)K * Pmax * G + 1, "chunk counts"));
   ptr.part = part.p;
-  ptr.part_exp = part_exp.p;
   ptr.cum = cum.p;
   drop_graphs();
   return TC_OK;
@@ -2110,10 +2028,8 @@ void tc_trainer::launch_level(const DevCfg& c, const DevPtrs& P, int d, cudaStre
   const int P2 = d == 0 ? 1 : (1 << (d - 1));
   dim3 mg(kSlots / MERGE_BB, K * P2, c.G);
   mark_begin(KC_MERGE, st);
-  if (J == 1 && cnt) k_merge<1, true><<<mg, MERGE_BB * 32, 0, st>>>(c, P, d);
-  else if (J == 1) k_merge<1, false><<<mg, MERGE_BB * 32, 0, st>>>(c, P, d);
-  else if (cnt) k_merge<2, true><<<mg, MERGE_BB * 64, 0, st>>>(c, P, d);
-  else k_merge<2, false><<<mg, MERGE_BB * 64, 0, st>>>(c, P, d);
+  if (J == 1) k_merge<1><<<mg, MERGE_BB * 32, 0, st>>>(c, P, d);
+  else k_merge<2><<<mg, MERGE_BB * 64, 0, st>>>(c, P, d);
   mark_end(st);
   const int ng = ((1 << d) + SCAN_NODES - 1) / SCAN_NODES;
   mark_begin(KC_SCAN, st);
