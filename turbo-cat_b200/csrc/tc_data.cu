@@ -12,8 +12,11 @@
 //      in the reference-compatible mode (the reference truncates U to
 //      uint8, src/core/dataset.cpp:308);
 //   4. bin = number of edges <= x (std::upper_bound), NaN -> bin 255,
-//      written both row-major [n][fs] (histogram kernels) and column-major
-//      [f][np] (partition kernels, export).
+//      written both as feature-group tiles (histogram kernels: group g of 32
+//      features is one contiguous [rows][32] block, so a row's slice of a
+//      group is one aligned 32-byte sector and a run of rows is one
+//      contiguous range; the last group's block is only 4, 8, 16 or 32
+//      bytes wide) and column-major [f][np] (partition kernels, export).
 #include <algorithm>
 
 #include "tc_internal.h"
@@ -234,10 +237,11 @@ __global__ void k_edge_meta(const uint32_t* __restrict__ U_, uint32_t f, int max
 constexpr int AB_ROWS = 256;
 
 // bin = #edges <= x (upper_bound), NaN -> 255; writes both bin layouts.
+// Block (row tile, group): 256 rows of the 32 features of group blockIdx.y.
 __global__ void k_assign_bins(const float* __restrict__ X, uint32_t n, uint32_t f,
                               const float* __restrict__ edges, const uint16_t* __restrict__ n_edges,
-                              uint8_t* __restrict__ bins_rm, uint32_t fs, uint8_t* __restrict__ bins_cm,
-                              uint32_t np, uint32_t* __restrict__ nan_any) {
+                              uint8_t* __restrict__ bins_t, uint64_t gstride, uint32_t nt, uint32_t wlast,
+                              uint8_t* __restrict__ bins_cm, uint32_t np, uint32_t* __restrict__ nan_any) {
   __shared__ float s_e[32][kSlots + 1];
   __shared__ int s_ne[32];
   __shared__ uint8_t s_b[32][AB_ROWS + 4];
@@ -281,11 +285,13 @@ __global__ void k_assign_bins(const float* __restrict__ X, uint32_t n, uint32_t 
     const uint32_t r = r0 + i;
     if (j0 + jj < f && r < np) bins_cm[(size_t)(j0 + jj) * np + r] = (r < n) ? s_b[jj][i] : (uint8_t)0;
   }
-  // row-major slices
+  // the group's tile block: rows r0.. at a stride of the group's width
+  const uint32_t w = (blockIdx.y == gridDim.y - 1) ? wlast : 32u;
+  uint8_t* blk = bins_t + (uint64_t)blockIdx.y * gstride;
   for (int q = tid; q < 32 * AB_ROWS; q += blockDim.x) {
     const int i = q / 32, jj = q % 32;
     const uint32_t r = r0 + i;
-    if (r < n && j0 + jj < fs) bins_rm[(size_t)r * fs + j0 + jj] = (j0 + jj < f) ? s_b[jj][i] : (uint8_t)0;
+    if (r < nt && (uint32_t)jj < w) blk[(size_t)r * w + jj] = (r < n && j0 + jj < f) ? s_b[jj][i] : (uint8_t)0;
   }
 }
 
@@ -306,7 +312,8 @@ tc_status quantize(tc_dataset* ds, int max_bins, int compat_u8) {
   TC_TRY(ds->n_edges.alloc(ctx, f, "edge counts"));
   TC_TRY(ds->nan_any.alloc(ctx, f, "NaN flags"));
   TC_CUDA(ctx, cudaMemsetAsync(ds->nan_any.p, 0, ds->nan_any.bytes(), st));
-  TC_TRY(ds->bins_rm.alloc(ctx, (size_t)n * ds->fs, "row-major bins"));
+  TC_TRY(ds->bins_t.alloc(ctx, (size_t)(ds->groups - 1) * ds->gstride + (size_t)ds->wlast * ds->nt,
+                          "feature-group bin tiles"));
   TC_TRY(ds->bins_cm.alloc(ctx, (size_t)f * ds->np, "column-major bins"));
   TC_CUDA(ctx, cudaMemsetAsync(ds->edges.p, 0, ds->edges.bytes(), st));
 
@@ -329,11 +336,11 @@ tc_status quantize(tc_dataset* ds, int max_bins, int compat_u8) {
     TC_CUDA(ctx, cudaMemsetAsync(U.p, 0, U.bytes(), st));
   }
   k_edge_meta<<<(f + 127) / 128, 128, 0, st>>>(U.p, f, max_bins, compat_u8, ds->edges.p, ds->n_edges.p);
-  TC_CUDA(ctx, cudaMemsetAsync(ds->bins_rm.p, 0, ds->bins_rm.bytes(), st));
+  TC_CUDA(ctx, cudaMemsetAsync(ds->bins_t.p, 0, ds->bins_t.bytes(), st));
   if (n > 0) {
-    dim3 ag((n + AB_ROWS - 1) / AB_ROWS, (ds->fs + 31) / 32);
-    k_assign_bins<<<ag, 256, 0, st>>>(ds->X.p, n, f, ds->edges.p, ds->n_edges.p, ds->bins_rm.p, ds->fs,
-                                      ds->bins_cm.p, ds->np, ds->nan_any.p);
+    dim3 ag((n + AB_ROWS - 1) / AB_ROWS, ds->groups);
+    k_assign_bins<<<ag, 256, 0, st>>>(ds->X.p, n, f, ds->edges.p, ds->n_edges.p, ds->bins_t.p, ds->gstride,
+                                      ds->nt, ds->wlast, ds->bins_cm.p, ds->np, ds->nan_any.p);
   }
   TC_CUDA(ctx, cudaGetLastError());
   // host copy of the edges for model export / thresholds
@@ -365,7 +372,13 @@ tc_status tc_dataset_upload(tc_ctx* ctx, const float* X, uint32_t n, uint16_t f,
   ds->ctx = ctx;
   ds->n = n;
   ds->f = f;
-  ds->fs = (uint32_t)tc::round_up(f, 32);
+  ds->groups = (f + 31) / 32;
+  ds->nt = (uint32_t)tc::round_up(n > 0 ? n : 1, 32);
+  {
+    const uint32_t last = f - 32 * (ds->groups - 1);  // features in the last group, 1 .. 32
+    ds->wlast = last <= 4 ? 4 : (last <= 8 ? 8 : (last <= 16 ? 16 : 32));
+  }
+  ds->gstride = (uint64_t)32 * ds->nt;
   ds->np = (uint32_t)tc::round_up(n > 0 ? n : 1, 16);
   tc_status s = ds->X.alloc(ctx, (size_t)n * f, "training matrix");
   if (s == TC_OK && y) s = ds->y.alloc(ctx, n, "labels");

@@ -106,14 +106,16 @@ struct tc_dataset {
   tc_ctx* ctx = nullptr;
   uint32_t n = 0;
   uint32_t f = 0;
-  uint32_t fs = 0;           // row stride of the row-major bin matrix (f rounded up to 32:
-                             // a 32-feature group of a row is one 32-byte sector)
+  uint32_t groups = 0;       // 32-feature groups of the tiled bin matrix
+  uint32_t nt = 0;           // rows of a tile block (n rounded up to 32)
+  uint32_t wlast = 0;        // bytes per row of the last group's block: 4, 8, 16 or 32
+  uint64_t gstride = 0;      // bytes of one full group block (32 x nt)
   uint32_t np = 0;           // column stride of the column-major bin matrix (n rounded up to 16)
   bool quantized = false;
   int max_bins = 255;
   DevBuf<float> X;           // [n][f] row-major input
   DevBuf<float> y;           // [n] labels (may be empty)
-  DevBuf<uint8_t> bins_rm;   // [n][fs]
+  DevBuf<uint8_t> bins_t;    // feature-group tiles: group g is a [nt][32] block (the last [nt][wlast])
   DevBuf<uint8_t> bins_cm;   // [f][np]
   DevBuf<float> edges;       // [f][256]
   DevBuf<uint16_t> n_edges;  // [f]

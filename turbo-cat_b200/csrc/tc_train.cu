@@ -56,7 +56,6 @@ constexpr int kSoftmaxMaxK = 16;  // softmax classes at most (checked when a tra
 constexpr int SCAN_WARPS = 8;     // warps per scan block
 constexpr int SCAN_NODES = 16;    // nodes per scan block (2 per warp; measured: 32 per block 4% slower on 1M x 100 depth 8)
 static_assert(SCAN_WARPS * 32 == 256, "a scan block also runs the 256-thread pick");
-constexpr int MERGE_BB = 4;       // bins per merge block
 constexpr int PLAN_THREADS = 1024;
 constexpr int VALID_BLOCKS = 296;  // blocks of the validation kernel (fixed: its partial sums have a fixed order)
 
@@ -92,7 +91,9 @@ struct FeatBest {
 };
 
 struct DevCfg {
-  uint32_t n, f, fs, np;
+  uint32_t n, f, np;
+  uint32_t groups, wlast;        // 32-feature groups of the bin tiles; bytes per row of the last one
+  uint64_t gstride;              // bytes of one full group block
   int32_t K, D, nb_scan, loss;
   int32_t KT, k0;                // classes in the model; first class of this launch view
   int32_t msl;
@@ -113,7 +114,7 @@ struct DevCfg {
 };
 
 struct DevPtrs {
-  const uint8_t* bins_rm;
+  const uint8_t* bins_t;         // feature-group tiles (tc_dataset::bins_t)
   const uint8_t* bins_cm;
   const float* edges;            // [f][256]
   const uint16_t* n_edges;
@@ -125,7 +126,8 @@ struct DevPtrs {
   uint16_t* leaf;                // [K][n]
   uint32_t* rows;                // [K][n]
   double2* hist[2];              // [K][2^(D-1)][F][256]
-  float2* part;                  // [item_cap][256][W]
+  double2* acc;                  // [K][2^(D-1)][F][256] FP64 sums of the level's smaller children (the
+                                 // root at level 0), added by the histogram items; the scan reads and re-zeroes them
   int32_t* cum;                  // [K*2^(D-1) + 1] cumulative item counts per segment (chunk-major)
   int32_t* rchunk;               // [1] rows per chunk at the current level
   int32_t* seg_start;            // [K][2^(D-1)]
@@ -429,6 +431,10 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
@@ -554,7 +560,6 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
     const int gsize = min(W, (int)c.f - g0);
     const int p2 = gsize <= 1 ? 1 : (gsize <= 2 ? 2 : (gsize <= 4 ? 4 : (gsize <= 8 ? 8 : (gsize <= 16 ? 16 : 32))));
     const bool narrow = p2 <= 16;
-    const int nchunk16 = (gsize + 15) >> 4;  // 16-byte pieces of the slice that hold features
     // shared address of this warp's copy of each column the lane updates;
     // columns past the group's width are skipped (their padding bytes are
     // all bin 0, a single hot address)
@@ -579,7 +584,18 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
     // (grad, hess) in list order: the root's rows are 0..n-1, a smaller
     // child's were copied next to its row ids by the scatter kernel
     const float2* gh = (d == 0 ? P.gh : P.cgh) + (size_t)k * c.n;
-    const uint8_t* bsrc = P.bins_rm + g0;
+    // 16-byte pieces of a row's slice: piece u comes from 32-feature group
+    // J*g + u/2 of the tiles; a narrow last group copies only its width
+    uint32_t pw[2 * J];
+    const uint8_t* psrc[2 * J];
+#pragma unroll
+    for (int u = 0; u < 2 * J; ++u) {
+      const uint32_t gg = (uint32_t)(J * g + (u >> 1));
+      const uint32_t w = gg + 1 == c.groups ? c.wlast : 32u;
+      pw[u] = gg < c.groups ? (uint32_t)max(0, min(16, (int)w - 16 * (u & 1))) : 0u;
+      psrc[u] = P.bins_t + (uint64_t)gg * c.gstride + 16 * (u & 1);
+      pw[u] |= w << 8;  // the group's row stride in the high byte
+    }
     const int nb = (end - start + B - 1) / B;   // batches in the item; warp w takes w, w+nwarps, ...
     uint32_t rid_next = 0;
 #define TC_FETCH_ID(bi)                                                                      \
@@ -590,10 +606,14 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
 #define TC_ISSUE(bi, st_)                                                                    \
     {                                                                                        \
       if ((bi) < nb && start + (bi) * B + lane < end) {                                      \
-        const uint8_t* src_ = bsrc + (size_t)rid_next * c.fs;                                \
         uint8_t* dst_ = w_bins + ((size_t)(st_) * B + lane) * W;                             \
-        _Pragma("unroll") for (int u = 0; u < 2 * J; ++u)                                    \
-          if (u < nchunk16) cp_async16(dst_ + 16 * u, src_ + 16 * u);                        \
+        _Pragma("unroll") for (int u = 0; u < 2 * J; ++u) {                                  \
+          const uint32_t sz_ = pw[u] & 0xffu;                                                \
+          const uint8_t* src_ = psrc[u] + (size_t)rid_next * (pw[u] >> 8);                   \
+          if (sz_ == 16) cp_async16(dst_ + 16 * u, src_);                                    \
+          else if (sz_ == 8) cp_async8(dst_ + 16 * u, src_);                                 \
+          else if (sz_ == 4) cp_async4(dst_ + 16 * u, src_);                                 \
+        }                                                                                    \
         cp_async8(w_gh + (st_) * B + lane, gh + start + (bi) * B + lane);                     \
       }                                                                                      \
       cp_async_commit();                                                                     \
@@ -681,9 +701,10 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
 #undef TC_ISSUE
     cp_async_wait<0>();
     __syncthreads();
-    float2* out = P.part + (size_t)item * kSlots * W;
-    // write the partial (copies summed in a fixed order) and clear the
+    // add the block's FP32 sums to the segment's FP64 accumulator (copies
+    // summed in a fixed order first; zero sums are not sent) and clear the
     // histogram for the next item; a thread clears exactly the slots it reads
+    double2* dst = P.acc + (((size_t)k * Pmax + p) * c.f + g0) * kSlots;
     const int ncp = narrow ? 32 / p2 : 1;     // packed copies of a narrow group
     // blockDim.x is a multiple of W: a thread's column is the same on every pass
     const int col = threadIdx.x % W;
@@ -709,7 +730,11 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
         }
         if (CNT) shv = c.hconst * (float)cnt;
       }
-      out[q] = make_float2(sgv, shv);
+      if (col < gsize) {
+        double2* o = dst + (size_t)col * kSlots + b;
+        if (sgv != 0.0f) atomicAdd(&o->x, (double)sgv);
+        if (shv != 0.0f) atomicAdd(&o->y, (double)shv);
+      }
     }
     if (narrow) {
       __syncthreads();
@@ -717,68 +742,6 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
     }
     __syncthreads();
     item = s_item[it & 1];
-  }
-}
-
-// ----------------------------------------------------------------- merge --
-
-// grid (256/MERGE_BB, segments, groups).  FP64 sum of a segment's partials
-// (fixed chunk order), then larger = parent - smaller (FP64).
-template <int J>
-__global__ void k_merge(DevCfg c, DevPtrs P, int d) {
-  constexpr int W = 32 * J;
-  __shared__ double2 tile[MERGE_BB][W];
-  const int P2 = pairs_at(d);
-  const int seg = blockIdx.y;
-  const int k = seg / P2, p = seg % P2, g = blockIdx.z;
-  if (P.cs[k].done) return;
-  const int Pmax = 1 << (c.D - 1);
-  const int g0 = g * W;
-  const int gsize = min(W, (int)c.f - g0);
-  const int b0 = blockIdx.x * MERGE_BB;
-  const int ib = P.cum[seg] + g;                        // chunk-major: chunk ch is item ib + ch*G
-  const int nch = (P.cum[seg + 1] - P.cum[seg]) / c.G;
-  for (int q = threadIdx.x; q < MERGE_BB * W; q += blockDim.x) {
-    const int bl = q / W, col = q % W;
-    double sg_ = 0.0, sh = 0.0;
-    if (col < gsize) {
-      // four partials loaded ahead of their (in-order) FP64 adds
-      const float2* src = P.part + ((size_t)ib * kSlots + b0 + bl) * W + col;
-      const size_t step = (size_t)c.G * kSlots * W;
-      int ch = 0;
-      for (; ch + 4 <= nch; ch += 4) {
-        const float2 v0 = src[(size_t)ch * step], v1 = src[(size_t)(ch + 1) * step];
-        const float2 v2 = src[(size_t)(ch + 2) * step], v3 = src[(size_t)(ch + 3) * step];
-        sg_ += (double)v0.x; sh += (double)v0.y;
-        sg_ += (double)v1.x; sh += (double)v1.y;
-        sg_ += (double)v2.x; sh += (double)v2.y;
-        sg_ += (double)v3.x; sh += (double)v3.y;
-      }
-      for (; ch < nch; ++ch) {
-        const float2 v = src[(size_t)ch * step];
-        sg_ += (double)v.x;
-        sh += (double)v.y;
-      }
-    }
-    tile[bl][col] = make_double2(sg_, sh);
-  }
-  __syncthreads();
-  double2* cur = P.hist[d & 1];
-  const double2* par = P.hist[(d & 1) ^ 1];
-  for (int q = threadIdx.x; q < MERGE_BB * W; q += blockDim.x) {
-    const int col = q / MERGE_BB, bl = q % MERGE_BB;
-    if (col >= gsize) continue;
-    const int f = g0 + col, b = b0 + bl;
-    const double2 s = tile[bl][col];
-    if (d == 0) {
-      cur[hist_index(c, k, 0, f, b)] = s;
-    } else {
-      const int sn = P.small[k * Pmax + p];
-      const int ln = sn ^ 1;
-      const double2 pv = par[hist_index(c, k, p, f, b)];
-      cur[hist_index(c, k, sn, f, b)] = s;
-      cur[hist_index(c, k, ln, f, b)] = make_double2(pv.x - s.x, pv.y - s.y);
-    }
   }
 }
 
@@ -801,7 +764,12 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(DevCfg c, DevPtrs P, i
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nn = 1 << d;
   const double lam = (double)c.lam;
-  const double2* cur = P.hist[d & 1];
+  double2* cur = P.hist[d & 1];
+  const double2* par = P.hist[(d & 1) ^ 1];
+  const int Pmax = 1 << (c.D - 1);
+  // the next level reads this level's histograms as parents (the root's is
+  // also the tree builder's root-histogram output)
+  const bool keep = d == 0 || d + 1 < c.D;
   const NodeStat* ns = P.nstat + ((size_t)k * (c.D + 1) + d) * (1 << c.D);
   double acc[8];
   uint32_t anyb = 0;
@@ -811,13 +779,30 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(DevCfg c, DevPtrs P, i
   for (int node = n0 + warp; node < n1; node += SCAN_WARPS) {
     const NodeStat st = ns[node];
     if (st.cnt == 0) continue;
-    const double2* hp = cur + hist_index(c, k, node, f, 0) + lane * 8;
+    // the smaller child of a pair (and the root) is the items' FP64 sum; the
+    // larger one is parent - smaller (FP64)
+    const int pr = d == 0 ? 0 : node >> 1;
+    const double2* ap = P.acc + (((size_t)k * Pmax + pr) * c.f + f) * kSlots + lane * 8;
     double hg[8], hh[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      const double2 v = hp[i];
+      const double2 v = ap[i];
       hg[i] = v.x;
       hh[i] = v.y;
+    }
+    if (d > 0 && node != P.small[k * Pmax + pr]) {
+      const double2* pp = par + hist_index(c, k, pr, f, 0) + lane * 8;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const double2 v = pp[i];
+        hg[i] = v.x - hg[i];
+        hh[i] = v.y - hh[i];
+      }
+    }
+    if (keep) {
+      double2* hp = cur + hist_index(c, k, node, f, 0) + lane * 8;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) hp[i] = make_double2(hg[i], hh[i]);
     }
     const double nan_g = __shfl_sync(0xffffffffu, hg[7], 31);
     const double nan_h = __shfl_sync(0xffffffffu, hh[7], 31);
@@ -871,6 +856,9 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(DevCfg c, DevPtrs P, i
   __syncthreads();
   // blockDim.x == kSlots: thread b sums bin b over the warps
   const int b = threadIdx.x;
+  // the accumulators of this block's pairs (this feature) start the next level at zero
+  for (int pr = (d == 0 ? 0 : n0 >> 1); pr < (d == 0 ? 1 : (n1 + 1) >> 1); ++pr)
+    P.acc[(((size_t)k * Pmax + pr) * c.f + f) * kSlots + b] = make_double2(0.0, 0.0);
   double sb = 0.0;
   uint8_t ab = 0;
   for (int w = 0; w < SCAN_WARPS; ++w) {
@@ -1679,7 +1667,7 @@ struct tc_trainer {
   DevBuf<uint16_t> leaf;
   DevBuf<uint32_t> rows;
   DevBuf<double2> hist0, hist1;
-  DevBuf<float2> part;
+  DevBuf<double2> acc;
   DevBuf<int32_t> cum, rchunk, seg_start, seg_len, small, iter;
   DevBuf<FeatBest> fbest;
   DevBuf<uint32_t> counters;
@@ -1783,7 +1771,8 @@ tc_status tc_trainer::setup(int) {
   const int ngroups_max = (L / 2 + SCAN_NODES - 1) / SCAN_NODES;
   const int G = 1, W = 32;  // placeholders until configure()
 
-  cfg.n = n; cfg.f = f; cfg.fs = ds->fs; cfg.np = ds->np;
+  cfg.n = n; cfg.f = f; cfg.np = ds->np;
+  cfg.groups = ds->groups; cfg.wlast = ds->wlast; cfg.gstride = ds->gstride;
   cfg.K = K; cfg.KT = K; cfg.k0 = 0; cfg.D = D; cfg.nb_scan = (int)(uint8_t)prm.max_bins - 1; cfg.loss = prm.loss;
   cfg.msl = prm.min_samples_leaf; cfg.lr = prm.learning_rate; cfg.lam = prm.lambda_l2; cfg.l1 = prm.lambda_l1;
   cfg.mcw = prm.min_child_weight; cfg.msg = prm.min_split_gain; cfg.mds = prm.max_delta_step;
@@ -1808,6 +1797,8 @@ tc_status tc_trainer::setup(int) {
   const size_t hsz = (size_t)K * Pmax * f * kSlots;
   TC_TRY(hist0.alloc(ctx, hsz, "level histograms"));
   TC_TRY(hist1.alloc(ctx, hsz, "level histograms"));
+  TC_TRY(acc.alloc(ctx, hsz, "histogram accumulators"));
+  TC_CUDA(ctx, cudaMemset(acc.p, 0, acc.bytes()));
   TC_TRY(rchunk.alloc(ctx, 1, "chunk rows"));
   TC_TRY(seg_start.alloc(ctx, (size_t)K * Pmax, "segments"));
   TC_TRY(seg_len.alloc(ctx, (size_t)K * Pmax, "segments"));
@@ -1840,10 +1831,10 @@ tc_status tc_trainer::setup(int) {
   TC_CUDA(ctx, cudaMemset(red_ctr.p, 0, red_ctr.bytes()));
   TC_CUDA(ctx, cudaMemset(fcnt.p, 0, fcnt.bytes()));
 
-  ptr.bins_rm = ds->bins_rm.p; ptr.bins_cm = ds->bins_cm.p; ptr.edges = ds->edges.p; ptr.n_edges = ds->n_edges.p;
+  ptr.bins_t = ds->bins_t.p; ptr.bins_cm = ds->bins_cm.p; ptr.edges = ds->edges.p; ptr.n_edges = ds->n_edges.p;
   ptr.nan_any = ds->nan_any.p;
   ptr.y = ds->y.p; ptr.pred = pred.p; ptr.gh = gh.p; ptr.cgh = cgh.p; ptr.leaf = leaf.p; ptr.rows = rows.p;
-  ptr.hist[0] = hist0.p; ptr.hist[1] = hist1.p; ptr.rchunk = rchunk.p;
+  ptr.hist[0] = hist0.p; ptr.hist[1] = hist1.p; ptr.acc = acc.p; ptr.rchunk = rchunk.p;
   ptr.seg_start = seg_start.p; ptr.seg_len = seg_len.p; ptr.small = small.p; ptr.nstat = nstat.p;
   ptr.pcnt = pcnt.p; ptr.psum = psum.p; ptr.blk_off = blk_off.p; ptr.gpart = gpart.p; ptr.gany = gany.p;
   ptr.fbest = fbest.p; ptr.counters = counters.p; ptr.hist_ctr = hist_ctr.p; ptr.red_ctr = red_ctr.p; ptr.fcnt = fcnt.p; ptr.cs = cs.p; ptr.iter = iter.p;
@@ -1884,9 +1875,8 @@ tc_status tc_trainer::configure(int J_, int waves) {
   cfg.hist_grid = hist_grid;
   cfg.target_items = waves * hist_grid;
   cfg.item_cap = (int)cap;
-  TC_TRY(part.alloc(ctx, (size_t)cap * kSlots * W, "histogram partials"));
+
   TC_TRY(cum.alloc(ctx, (size_t)K * Pmax * G + 1, "chunk counts"));
-  ptr.part = part.p;
   ptr.cum = cum.p;
   drop_graphs();
   return TC_OK;
@@ -2025,12 +2015,6 @@ void tc_trainer::launch_level(const DevCfg& c, const DevPtrs& P, int d, cudaStre
     prof->back().level = d;
     prof->back().rows = hist_rows;
   }
-  const int P2 = d == 0 ? 1 : (1 << (d - 1));
-  dim3 mg(kSlots / MERGE_BB, K * P2, c.G);
-  mark_begin(KC_MERGE, st);
-  if (J == 1) k_merge<1><<<mg, MERGE_BB * 32, 0, st>>>(c, P, d);
-  else k_merge<2><<<mg, MERGE_BB * 64, 0, st>>>(c, P, d);
-  mark_end(st);
   const int ng = ((1 << d) + SCAN_NODES - 1) / SCAN_NODES;
   mark_begin(KC_SCAN, st);
   k_scan<<<dim3(c.f, ng, K), SCAN_WARPS * 32, 0, st>>>(c, P, d);  // + pick
@@ -2105,6 +2089,7 @@ static DevPtrs class_view(const DevCfg& c, const DevPtrs& P, int k, DevCfg* one)
   pk.pred += k * n; pk.gh += k * n; pk.cgh += k * n; pk.leaf += k * n; pk.rows += k * n;
   pk.hist[0] += (size_t)k * Pmax * c.f * kSlots;
   pk.hist[1] += (size_t)k * Pmax * c.f * kSlots;
+  pk.acc += (size_t)k * Pmax * c.f * kSlots;
   pk.seg_start += k * Pmax; pk.seg_len += k * Pmax;
   pk.small += k * Pmax; pk.nstat += (size_t)k * (c.D + 1) * L;
   pk.fbest += (size_t)k * c.f; pk.counters += k; pk.fcnt += (size_t)k * c.f;
