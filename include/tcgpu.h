@@ -117,7 +117,7 @@ typedef struct {
   int32_t batched;          /* 1: all classes and nodes of a level per launch, one CUDA graph per
                                iteration; 0: the plain path, one tree and one level at a time with a
                                host synchronisation per level */
-  int32_t hist_features_per_block; /* 0 = autotune; else 32 or 64 (other values: 32) */
+  int32_t hist_features_per_block; /* feature-group width of the histogram kernel: 32 (any value) */
   int32_t hist_rows_per_chunk;     /* 0 = autotune */
   /* Row sampling, Booster::train's sample selection (src/boosting/booster.cpp:198-228):
    * with 0 < subsample < 1 every iteration's trees are built on the first

@@ -48,7 +48,7 @@
 namespace tc {
 namespace {
 
-constexpr int HIST_THREADS = 512;
+constexpr int HIST_THREADS = 1024;  // one histogram block per SM (its accumulators take 128 KB)
 constexpr int HIST_BATCH = 32;    // rows per warp batch (one per lane)
 constexpr int PART_THREADS = 512;
 constexpr int GRAD_UNROLL = 4;    // rows per thread with their loads in flight together (one class)
@@ -57,6 +57,7 @@ constexpr int SCAN_WARPS = 8;     // warps per scan block
 constexpr int SCAN_NODES = 16;    // nodes per scan block (2 per warp; measured: 32 per block 4% slower on 1M x 100 depth 8)
 static_assert(SCAN_WARPS * 32 == 256, "a scan block also runs the 256-thread pick");
 constexpr int PLAN_THREADS = 1024;
+constexpr int kHistRowsMax = 65535;  // rows of a histogram item: its 16-bit low fields sum without overflow
 constexpr int VALID_BLOCKS = 296;  // blocks of the validation kernel (fixed: its partial sums have a fixed order)
 
 struct NodeStat {
@@ -438,15 +439,16 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-template <int J>
 struct HistShape {
-  static constexpr int W = 32 * J;                      // histogram columns of a block
+  static constexpr int W = 32;                          // histogram columns (features) of an item
   static constexpr int WARPS = HIST_THREADS / 32;
   static constexpr int S = 2;                           // staging depth per warp (batches in flight)
-  static constexpr size_t hist_bytes = (size_t)2 * kSlots * W * 4;
+  static constexpr int FIELDS = 4;                      // u32 accumulators per (slot, column)
+  static constexpr size_t hist_bytes = (size_t)kSlots * FIELDS * W * 4;    // 128 KB
   static constexpr size_t warp_bytes = (size_t)S * HIST_BATCH * (W + 8);   // bins + (grad, hess)
   static constexpr size_t smem = hist_bytes + WARPS * warp_bytes;
 };
+static_assert(HistShape::smem <= 227 * 1024 - 1024, "histogram shared memory");
 
 // Work item -> segment (class, pair) through the cumulative item counts.
 __device__ __forceinline__ int find_seg(const int32_t* cum, int nseg, int item) {
@@ -463,8 +465,8 @@ __device__ __forceinline__ int find_seg(const int32_t* cum, int nseg, int item) 
 // its span are free.  A feature without NaN rows keeps private copies of its
 // column there for different warps (copy c of bin b in slot c*span + b, at
 // most 255/span copies, so bin + offset never reaches 255), which spreads the
-// updates of few-bin features over more addresses: concurrent atomics on one
-// shared address serialise.  A feature with NaN rows keeps one copy.
+// updates of few-bin features over more addresses.  A feature with NaN rows
+// keeps one copy.
 struct HistCol {
   int span, copies;
 };
@@ -474,53 +476,92 @@ __device__ __forceinline__ HistCol hist_col(const DevPtrs& P, int f, int nf) {
   return {span, P.nan_any[f] ? 1 : min(HIST_THREADS / 32, max(1, 255 / span))};
 }
 
-__device__ __forceinline__ void red_add_f32(uint32_t a, float v) {
-  asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
-}
 __device__ __forceinline__ void red_add_u32(uint32_t a, uint32_t v) {
   asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(a), "r"(v) : "memory");
 }
 
-// Persistent blocks over work items; an item is one chunk of one segment's
-// rows (the root at d = 0, a smaller child after) for one feature group, and
-// the items of a chunk's groups are adjacent (chunk-major), so blocks that run
-// together read the same rows and the L2 serves a row's bytes and its
+// Exact fixed-point accumulation.
+//
+// Each row's grad (and hess) becomes the integer v = round(x * 2^e), with a
+// power of two 2^e chosen per work item from the item's own sum S of |x|
+// over its rows (FP64): e is the largest value with 2^e * S + rows / 2
+// below 2^46, so every partial sum of any bin has |sum v| < 2^46.  v is kept
+// as two unsigned 32-bit shared accumulators, hi = v >> 16 (arithmetic, so
+// |sum hi| < 2^31) and lo = v & 0xffff (an item has at most 65535 rows, so
+// sum lo < 2^32): integer sums are exact, independent of the order of the
+// atomics, and 32-bit shared integer atomics run at about twice the rate of
+// FP32 shared atomics on this part (measured, and unlike FP32 they do not
+// slow down when many lanes hit few addresses).  A row is represented to
+// within 2^-(e+1) <= S * 2^-46 ... 2^-47: relative to the item's total |x|,
+// about 1e-14; the sum of a bin is exact on top of that.
+// Accumulators per (slot, column): 0 grad hi, 1 grad lo, 2 hess hi (CNT: the
+// row count; every row's hessian is the same constant, MSE: h = 2), 3 hess lo.
+constexpr double kFixLimit = 70368744177664.0;  // 2^46
+
+__device__ __forceinline__ int fix_exponent(double S, double rows) {
+  if (!(S > 0.0)) return 0;
+  // a relative margin for the rounding of the FP64 sum S itself
+  const double room = kFixLimit * (1.0 - 0x1p-20) - 0.5 * rows;
+  int e = ilogb(room / S);      // floor(log2(room / S))
+  if (ldexp(S, e) > room) --e;  // against rounding of the division
+  return max(-126, min(100, e));
+}
+__device__ __forceinline__ float exp2i(int e) { return __int_as_float((e + 127) << 23); }
+
+struct FixRow {
+  uint32_t ghi, glo, hhi, hlo;
+};
+__device__ __forceinline__ FixRow fix_row(float g, float h, float sg, float sh) {
+  FixRow r;
+  const long long vg = __float2ll_rn(g * sg);  // exact product: sg is a power of two
+  r.ghi = (uint32_t)(vg >> 16);
+  r.glo = (uint32_t)vg & 0xffffu;
+  const long long vh = __float2ll_rn(h * sh);
+  r.hhi = (uint32_t)(vh >> 16);
+  r.hlo = (uint32_t)vh & 0xffffu;
+  return r;
+}
+
+// Persistent blocks (one per SM) over work items; an item is one chunk of one
+// segment's rows (the root at d = 0, a smaller child after) for one group of
+// 32 features, and the items of a chunk's groups are adjacent (chunk-major),
+// so blocks that run together read the same rows and the L2 serves a row's
 // (grad, hess) to every group.
 //
-// Every warp runs its own copy pipeline: lane l stages row l of a 32-row
-// batch (its group slice and its (grad, hess)) by cp.async into the warp's
-// private buffers, one batch ahead of the updates, with the row ids of
+// An item starts with a pass over its rows' (grad, hess) (contiguous in list
+// order) for the sums that fix its scales.  Then every warp runs its own copy
+// pipeline: lane l stages row l of a 32-row batch (its 32-byte group slice
+// from the feature-group tiles, and its (grad, hess)) by cp.async into the
+// warp's private buffers, one batch ahead of the updates, with the row ids of
 // gathered rows fetched a further batch ahead; no block barrier is taken
-// until the item is done.
+// until the item is done.  The item ends by adding its exact sums, converted
+// to FP64, to the segment's FP64 accumulator in global memory.
 //
 // Shared histogram layout: column fastest, so a column always hits the same
-// bank: float hist[(2*slot + {0 grad, 1 hess}) * W + column].  A wide group
-// is updated four rows at a time: lane (r = l/8, c = l%8) loads the 4 bins
-// of columns 4c..4c+3 of row r of the quad as one word and, in step s,
-// updates column 4c + (s + r) % 4, so the 32 lanes of every step hit 32
-// different columns (banks).  A group of at most 16 features is packed: with
-// p2 = next power of two >= its width, the 32 columns hold 32/p2 private
-// copies and one warp instruction updates 32/p2 rows; the copies are summed
-// when the partial is written.  Columns past a group's width (padding bytes,
-// all bin 0: one hot address) are not updated.  Each lane keeps the shared
-// address of (its warp's copy of) every column it updates, so an update is a
-// byte permute, an add and the atomics.
-//
-// CNT: every row's hessian is the same constant (MSE: h = 2); rows are
-// counted with 32-bit integer shared atomics (2.7x the throughput of FP32
-// shared atomics on this part) and hess = count * h is exact.
-template <int J, bool CNT>
-__global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs P, int d) {
-  using S_ = HistShape<J>;
+// bank: uint32 hist[(4 * slot + field) * 32 + column].  A wide group is
+// updated four rows at a time: lane (r = l/8, c = l%8) loads the 4 bins of
+// columns 4c..4c+3 of row r of the quad as one word and, in step s, updates
+// column 4c + (s + r) % 4, so the 32 lanes of every step hit 32 different
+// banks.  A group of at most 16 features is packed: with p2 = next power of
+// two >= its width, the 32 columns hold 32/p2 private copies and one warp
+// instruction updates 32/p2 rows; the copies are summed when the item ends.
+// Columns past a group's width (padding bytes, all bin 0: one hot address)
+// are not updated.  Each lane keeps the shared address of (its warp's copy of)
+// every column it updates, so an update is a byte permute, an add and the
+// integer atomics.
+template <bool CNT>
+__global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(DevCfg c, DevPtrs P, int d) {
+  using S_ = HistShape;
   constexpr int W = S_::W, S = S_::S, B = HIST_BATCH;
-  constexpr uint32_t BIN_BYTES = 8 * W;   // grad and hess rows of one slot
+  constexpr uint32_t SLOT_BYTES = 4 * S_::FIELDS * W;   // 512: the 4 fields of one slot
+  constexpr uint32_t FB = 4 * W;                         // bytes between two fields of a slot
   extern __shared__ __align__(16) unsigned char smraw[];
-  float* hist = reinterpret_cast<float*>(smraw);
-  uint32_t* histu = reinterpret_cast<uint32_t*>(smraw);
+  uint32_t* hist = reinterpret_cast<uint32_t*>(smraw);
   const uint32_t hbase = (uint32_t)__cvta_generic_to_shared(hist);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   uint8_t* w_bins = smraw + S_::hist_bytes + (size_t)warp * S_::warp_bytes;        // [S][B][W]
   float2* w_gh = reinterpret_cast<float2*>(w_bins + (size_t)S * B * W);            // [S][B]
+  __shared__ double s_sum[2][HIST_THREADS / 32];
   const int P2 = pairs_at(d);
   const int nseg = c.K * P2;
   const int n_items = P.cum[nseg];
@@ -532,7 +573,7 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
   uint32_t sel[4];
 #pragma unroll
   for (int s = 0; s < 4; ++s) sel[s] = 0x4404u | ((uint32_t)((s + qr) & 3) << 4);
-  for (int q = threadIdx.x; q < 2 * kSlots * W; q += blockDim.x) hist[q] = 0.0f;
+  for (int q = threadIdx.x; q < kSlots * S_::FIELDS * W; q += blockDim.x) hist[q] = 0u;
   __syncthreads();
   // Items are claimed from a counter (blocks that drew cheap items take
   // more), the next one while the current one runs.  Item ci*G + g is chunk
@@ -560,20 +601,6 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
     const int gsize = min(W, (int)c.f - g0);
     const int p2 = gsize <= 1 ? 1 : (gsize <= 2 ? 2 : (gsize <= 4 ? 4 : (gsize <= 8 ? 8 : (gsize <= 16 ? 16 : 32))));
     const bool narrow = p2 <= 16;
-    // shared address of this warp's copy of each column the lane updates;
-    // columns past the group's width are skipped (their padding bytes are
-    // all bin 0, a single hot address)
-    uint32_t ab[J][4];
-    uint32_t live = 0;
-#pragma unroll
-    for (int j = 0; j < J; ++j)
-#pragma unroll
-      for (int s = 0; s < 4; ++s) {
-        const int col = 32 * j + 4 * c4 + ((s + qr) & 3);
-        const HistCol hc = hist_col(P, g0 + col, (int)c.f);
-        ab[j][s] = hbase + BIN_BYTES * (uint32_t)((warp % hc.copies) * hc.span) + 4u * col;
-        if (col < gsize) live |= 1u << (4 * j + s);
-      }
     // the segment's ceil(len / R) chunks have equal sizes (within one row)
     const int s0 = d == 0 ? 0 : P.seg_start[k * Pmax + p];
     const int sl = d == 0 ? (int)c.n : P.seg_len[k * Pmax + p];
@@ -584,18 +611,48 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
     // (grad, hess) in list order: the root's rows are 0..n-1, a smaller
     // child's were copied next to its row ids by the scatter kernel
     const float2* gh = (d == 0 ? P.gh : P.cgh) + (size_t)k * c.n;
-    // 16-byte pieces of a row's slice: piece u comes from 32-feature group
-    // J*g + u/2 of the tiles; a narrow last group copies only its width
-    uint32_t pw[2 * J];
-    const uint8_t* psrc[2 * J];
-#pragma unroll
-    for (int u = 0; u < 2 * J; ++u) {
-      const uint32_t gg = (uint32_t)(J * g + (u >> 1));
-      const uint32_t w = gg + 1 == c.groups ? c.wlast : 32u;
-      pw[u] = gg < c.groups ? (uint32_t)max(0, min(16, (int)w - 16 * (u & 1))) : 0u;
-      psrc[u] = P.bins_t + (uint64_t)gg * c.gstride + 16 * (u & 1);
-      pw[u] |= w << 8;  // the group's row stride in the high byte
+    // the item's scales: FP64 sums of |grad| and |hess| over its rows (every
+    // thread a fixed stride, the warps in a fixed order)
+    int eg, eh;
+    float sg, sh;
+    {
+      double sa = 0.0, sb = 0.0;
+#pragma unroll 4
+      for (int r = start + threadIdx.x; r < end; r += blockDim.x) {
+        const float2 v = gh[r];
+        sa += (double)fabsf(v.x);
+        sb += (double)fabsf(v.y);
+      }
+      for (int o = 16; o; o >>= 1) {
+        sa += __shfl_xor_sync(0xffffffffu, sa, o);
+        sb += __shfl_xor_sync(0xffffffffu, sb, o);
+      }
+      if (lane == 0) { s_sum[0][warp] = sa; s_sum[1][warp] = sb; }
+      __syncthreads();
+      sa = 0.0;
+      sb = 0.0;
+      for (int w = 0; w < nwarps; ++w) { sa += s_sum[0][w]; sb += s_sum[1][w]; }
+      eg = fix_exponent(sa, (double)(end - start));
+      eh = CNT ? 0 : fix_exponent(sb, (double)(end - start));
+      sg = exp2i(eg);
+      sh = exp2i(eh);
     }
+    // shared address of this warp's copy of each column the lane updates;
+    // columns past the group's width are skipped (their padding bytes are
+    // all bin 0, a single hot address)
+    uint32_t ab[4];
+    uint32_t live = 0;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      const int col = 4 * c4 + ((s + qr) & 3);
+      const HistCol hc = hist_col(P, g0 + col, (int)c.f);
+      ab[s] = hbase + SLOT_BYTES * (uint32_t)((warp % hc.copies) * hc.span) + 4u * col;
+      if (col < gsize) live |= 1u << s;
+    }
+    // the two 16-byte pieces of a row's group slice in the feature-group
+    // tiles; the last group's narrower block copies only its width
+    const uint32_t gwid = (uint32_t)g + 1 == c.groups ? c.wlast : 32u;
+    const uint8_t* tile = P.bins_t + (uint64_t)g * c.gstride;
     const int nb = (end - start + B - 1) / B;   // batches in the item; warp w takes w, w+nwarps, ...
     uint32_t rid_next = 0;
 #define TC_FETCH_ID(bi)                                                                      \
@@ -607,12 +664,16 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
     {                                                                                        \
       if ((bi) < nb && start + (bi) * B + lane < end) {                                      \
         uint8_t* dst_ = w_bins + ((size_t)(st_) * B + lane) * W;                             \
-        _Pragma("unroll") for (int u = 0; u < 2 * J; ++u) {                                  \
-          const uint32_t sz_ = pw[u] & 0xffu;                                                \
-          const uint8_t* src_ = psrc[u] + (size_t)rid_next * (pw[u] >> 8);                   \
-          if (sz_ == 16) cp_async16(dst_ + 16 * u, src_);                                    \
-          else if (sz_ == 8) cp_async8(dst_ + 16 * u, src_);                                 \
-          else if (sz_ == 4) cp_async4(dst_ + 16 * u, src_);                                 \
+        const uint8_t* src_ = tile + (size_t)rid_next * gwid;                                \
+        if (gwid == 32) {                                                                    \
+          cp_async16(dst_, src_);                                                            \
+          cp_async16(dst_ + 16, src_ + 16);                                                  \
+        } else if (gwid == 16) {                                                             \
+          cp_async16(dst_, src_);                                                            \
+        } else if (gwid == 8) {                                                              \
+          cp_async8(dst_, src_);                                                             \
+        } else {                                                                             \
+          cp_async4(dst_, src_);                                                             \
         }                                                                                    \
         cp_async8(w_gh + (st_) * B + lane, gh + start + (bi) * B + lane);                     \
       }                                                                                      \
@@ -635,7 +696,7 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
         // the batch's bins and (grad, hess) go to registers first, so the
         // loads are not ordered behind the updates (they share the memory space)
         const uint32_t* sw = reinterpret_cast<const uint32_t*>(sb);
-        uint32_t wd[B / 4][J];
+        uint32_t wd[B / 4];
         float vx[B / 4], vy[B / 4];
 #pragma unroll
         for (int qd = 0; qd < B / 4; ++qd) {
@@ -643,24 +704,24 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
           const float2 v = sv[row];
           vx[qd] = v.x;
           vy[qd] = v.y;
-#pragma unroll
-          for (int j = 0; j < J; ++j) wd[qd][j] = sw[row * (W / 4) + 8 * j + c4];
+          wd[qd] = sw[row * (W / 4) + c4];
         }
 #pragma unroll
         for (int qd = 0; qd < B / 4; ++qd) {
           if (4 * qd + qr < nvalid) {
+            const FixRow fr = fix_row(vx[qd], vy[qd], sg, sh);
 #pragma unroll
-            for (int j = 0; j < J; ++j) {
-              if (32 * j < gsize) {
-#pragma unroll
-                for (int s = 0; s < 4; ++s) {
-                  // __byte_perm gives bin * 256; a slot is BIN_BYTES = 256 * J bytes
-                  const uint32_t a = ab[j][s] + __byte_perm(wd[qd][j], 0u, sel[s]) * J;
-                  if (live & (1u << (4 * j + s))) {
-                    red_add_f32(a, vx[qd]);
-                    if (CNT) red_add_u32(a + 4 * W, 1u);
-                    else red_add_f32(a + 4 * W, vy[qd]);
-                  }
+            for (int s = 0; s < 4; ++s) {
+              // __byte_perm gives bin * 256; a slot is SLOT_BYTES = 512 bytes
+              const uint32_t a = ab[s] + 2u * __byte_perm(wd[qd], 0u, sel[s]);
+              if (live & (1u << s)) {
+                red_add_u32(a, fr.ghi);
+                red_add_u32(a + FB, fr.glo);
+                if (CNT) {
+                  red_add_u32(a + 2 * FB, 1u);
+                } else {
+                  red_add_u32(a + 2 * FB, fr.hhi);
+                  red_add_u32(a + 3 * FB, fr.hlo);
                 }
               }
             }
@@ -672,7 +733,7 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
         const int rpi = 32 / p2;
         const int my_row = lane / p2, my_col = lane - my_row * p2;
         const HistCol hc = hist_col(P, g0 + my_col, (int)c.f);
-        const uint32_t abn = hbase + BIN_BYTES * (uint32_t)((warp % hc.copies) * hc.span) + 4u * lane;
+        const uint32_t abn = hbase + SLOT_BYTES * (uint32_t)((warp % hc.copies) * hc.span) + 4u * lane;
         for (int i0 = 0; i0 < B; i0 += 4 * rpi) {
           uint32_t bb[4];
           float gx[4], gy[4];
@@ -687,10 +748,16 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
             if (i0 + u * rpi + my_row < nvalid && my_col < gsize) {
-              const uint32_t a = abn + BIN_BYTES * bb[u];
-              red_add_f32(a, gx[u]);
-              if (CNT) red_add_u32(a + 4 * W, 1u);
-              else red_add_f32(a + 4 * W, gy[u]);
+              const FixRow fr = fix_row(gx[u], gy[u], sg, sh);
+              const uint32_t a = abn + SLOT_BYTES * bb[u];
+              red_add_u32(a, fr.ghi);
+              red_add_u32(a + FB, fr.glo);
+              if (CNT) {
+                red_add_u32(a + 2 * FB, 1u);
+              } else {
+                red_add_u32(a + 2 * FB, fr.hhi);
+                red_add_u32(a + 3 * FB, fr.hlo);
+              }
             }
           }
         }
@@ -701,9 +768,10 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
 #undef TC_ISSUE
     cp_async_wait<0>();
     __syncthreads();
-    // add the block's FP32 sums to the segment's FP64 accumulator (copies
-    // summed in a fixed order first; zero sums are not sent) and clear the
-    // histogram for the next item; a thread clears exactly the slots it reads
+    // add the item's exact sums (copies summed as integers), converted to
+    // FP64, to the segment's FP64 accumulator (zero sums are not sent), and
+    // clear the histogram for the next item; a thread clears exactly the
+    // slots it reads
     double2* dst = P.acc + (((size_t)k * Pmax + p) * c.f + g0) * kSlots;
     const int ncp = narrow ? 32 / p2 : 1;     // packed copies of a narrow group
     // blockDim.x is a multiple of W: a thread's column is the same on every pass
@@ -711,34 +779,36 @@ __global__ void __launch_bounds__(HIST_THREADS, 3 - J) k_hist(DevCfg c, DevPtrs 
     const HistCol fc = hist_col(P, g0 + col, (int)c.f);
     for (int q = threadIdx.x; q < kSlots * W; q += blockDim.x) {
       const int b = q / W;
-      float sgv = 0.0f, shv = 0.0f;
-      uint32_t cnt = 0;
+      long long G = 0, H = 0;
       if (!narrow || col < p2) {
         const int kc = b == kNanBin ? 1 : (b < fc.span ? fc.copies : 0);
         for (int cc = 0; cc < kc; ++cc) {
           const int slot = b == kNanBin ? kNanBin : cc * fc.span + b;
           for (int cp = 0; cp < ncp; ++cp) {
-            const int o = 2 * slot * W + cp * p2 * (narrow ? 1 : 0) + col;
-            sgv += hist[o];
-            if (CNT) cnt += histu[o + W];
-            else shv += hist[o + W];
+            uint32_t* o = hist + 4 * slot * W + cp * p2 * (narrow ? 1 : 0) + col;
+            G += (long long)(int32_t)o[0] * 65536 + (long long)o[W];
+            if (CNT) H += (long long)o[2 * W];
+            else H += (long long)(int32_t)o[2 * W] * 65536 + (long long)o[3 * W];
             if (!narrow) {
-              hist[o] = 0.0f;
-              hist[o + W] = 0.0f;
+              o[0] = 0u;
+              o[W] = 0u;
+              o[2 * W] = 0u;
+              o[3 * W] = 0u;
             }
           }
         }
-        if (CNT) shv = c.hconst * (float)cnt;
       }
       if (col < gsize) {
+        const double gd = ldexp((double)G, -eg);
+        const double hd = CNT ? (double)c.hconst * (double)H : ldexp((double)H, -eh);
         double2* o = dst + (size_t)col * kSlots + b;
-        if (sgv != 0.0f) atomicAdd(&o->x, (double)sgv);
-        if (shv != 0.0f) atomicAdd(&o->y, (double)shv);
+        if (gd != 0.0) atomicAdd(&o->x, gd);
+        if (hd != 0.0) atomicAdd(&o->y, hd);
       }
     }
     if (narrow) {
       __syncthreads();
-      for (int q = threadIdx.x; q < 2 * kSlots * 32; q += blockDim.x) hist[(q >> 5) * W + (q & 31)] = 0.0f;
+      for (int q = threadIdx.x; q < kSlots * S_::FIELDS * 32; q += blockDim.x) hist[q] = 0u;
     }
     __syncthreads();
     item = s_item[it & 1];
@@ -1362,7 +1432,7 @@ __device__ __forceinline__ void plan_body(const DevCfg& c, const DevPtrs& P, int
   if (tid == 0) {
     int R = c.rows_fixed;
     if (R <= 0) R = (int)max((long long)c.rows_min, (s_rows * gw + c.target_items - 1) / c.target_items);
-    s_R = R;
+    s_R = min(R, kHistRowsMax);
   }
   __syncthreads();
   for (int round = 0; c.rows_fixed <= 0 && round < 16; ++round) {
@@ -1383,7 +1453,7 @@ __device__ __forceinline__ void plan_body(const DevCfg& c, const DevPtrs& P, int
     const long long items = s_cnt * gw;
     __syncthreads();
     if (items <= c.target_items) break;
-    if (tid == 0) s_R = (int)min((long long)INT32_MAX / 2, (long long)Rt * items / c.target_items + 1);
+    if (tid == 0) s_R = (int)min((long long)kHistRowsMax, (long long)Rt * items / c.target_items + 1);
     __syncthreads();
   }
   if (tid == 0) {
@@ -1780,7 +1850,7 @@ tc_status tc_trainer::setup(int) {
   cfg.G = G; cfg.W = W; cfg.PB = PB;
   cfg.n_scan_groups_max = std::max(1, ngroups_max);
   cfg.rows_min = 512;
-  cfg.rows_fixed = prm.hist_rows_per_chunk > 0 ? prm.hist_rows_per_chunk : 0;
+  cfg.rows_fixed = prm.hist_rows_per_chunk > 0 ? std::min(prm.hist_rows_per_chunk, kHistRowsMax) : 0;
   // MSE's hessian is 2 for every row (src/boosting/loss.cpp:348-362)
   // counted hessians need every listed row to carry h = 2; with row
   // sampling the root lists all rows and the unsampled ones carry 0
@@ -1842,17 +1912,13 @@ tc_status tc_trainer::setup(int) {
   ptr.m_second = m_second.p; ptr.m_leaves = m_leaves.p; ptr.root_hist_out = nullptr;
   ptr.lvl_rows = lvl_rows.p; ptr.lvl_nodes = lvl_nodes.p;
 
-  cudaFuncSetAttribute(k_hist<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape<1>::smem);
-  cudaFuncSetAttribute(k_hist<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape<2>::smem);
-  cudaFuncSetAttribute(k_hist<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape<1>::smem);
-  cudaFuncSetAttribute(k_hist<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape<2>::smem);
+  cudaFuncSetAttribute(k_hist<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape::smem);
+  cudaFuncSetAttribute(k_hist<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape::smem);
   cudaFuncSetAttribute(k_partition<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 12 * L);
   cudaFuncSetAttribute(k_partition<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 12 * 256 * (PART_THREADS / 32));
   TC_CUDA(ctx, cudaEventCreate(&ev0));
   TC_CUDA(ctx, cudaEventCreate(&ev1));
-  int J0 = prm.hist_features_per_block / 32;
-  if (J0 < 1 || J0 > 2) J0 = 1;  // default before tuning: 32-column groups
-  return configure(J0, 2);
+  return configure(1, 2);  // 32-column feature groups (the only width), 2 waves before tuning
 }
 
 // Feature-group width (32*J columns) and work items per histogram launch
@@ -1864,12 +1930,11 @@ tc_status tc_trainer::configure(int J_, int waves) {
   J = J_;
   const int W = 32 * J;
   const int G = (int)((f + W - 1) / W);
-  const size_t hsm = J == 1 ? HistShape<1>::smem : HistShape<2>::smem;
-  const int blocks_per_sm = std::max<int>(1, (int)((227 * 1024) / (hsm + 1024)));
-  hist_grid = ctx->sm_count * std::min(blocks_per_sm, 4);
+  hist_grid = ctx->sm_count;  // one 1024-thread block per SM
   hist_waves = waves;
   long long cap = (long long)waves * hist_grid + (long long)K * Pmax * G + 1;
   if (cfg.rows_fixed) cap += (long long)K * G * ((cfg.n + cfg.rows_fixed - 1) / cfg.rows_fixed + 1);
+  cap += (long long)K * G * (cfg.n / kHistRowsMax + 1);  // chunks of at most kHistRowsMax rows
   cfg.G = G;
   cfg.W = W;
   cfg.hist_grid = hist_grid;
@@ -2005,11 +2070,8 @@ void tc_trainer::launch_level(const DevCfg& c, const DevPtrs& P, int d, cudaStre
     hist_rows = rows;
   }
   mark_begin(KC_HIST, st);
-  const bool cnt = c.hconst > 0.0f;
-  if (J == 1 && cnt) k_hist<1, true><<<hist_grid, HIST_THREADS, HistShape<1>::smem, st>>>(c, P, d);
-  else if (J == 1) k_hist<1, false><<<hist_grid, HIST_THREADS, HistShape<1>::smem, st>>>(c, P, d);
-  else if (cnt) k_hist<2, true><<<hist_grid, HIST_THREADS, HistShape<2>::smem, st>>>(c, P, d);
-  else k_hist<2, false><<<hist_grid, HIST_THREADS, HistShape<2>::smem, st>>>(c, P, d);
+  if (c.hconst > 0.0f) k_hist<true><<<hist_grid, HIST_THREADS, HistShape::smem, st>>>(c, P, d);
+  else k_hist<false><<<hist_grid, HIST_THREADS, HistShape::smem, st>>>(c, P, d);
   mark_end(st, hist_bytes);
   if (prof) {
     prof->back().level = d;
