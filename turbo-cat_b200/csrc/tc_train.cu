@@ -889,9 +889,14 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(DevCfg c, DevPtrs P, i
       if (lane >= o) { pg += ug; ph += uh; }
       if (lane + o < 32) { sg += dg; sh += dh; }
     }
+    // the node's totals from its own histogram (lane 31's inclusive prefix
+    // plus the NaN slot: one value for the whole warp), so that the parent
+    // term of every bin's gain is consistent with its left and right sums
+    const double Gn = __shfl_sync(0xffffffffu, pg, 31) + nan_g;
+    const double Hn = __shfl_sync(0xffffffffu, ph, 31) + nan_h;
     pg -= tg; ph -= th;  // exclusive prefix
     sg -= tg; sh -= th;  // exclusive suffix
-    const double pgain = (st.H > 1e-10) ? (st.G * st.G) / (st.H + lam) : 0.0;
+    const double pgain = (Hn > 1e-10) ? (Gn * Gn) / (Hn + lam) : 0.0;
     // right side of bin 8l+i: this lane's bins above i plus all lanes above
     double rsg[8], rsh[8];
     {
