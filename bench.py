@@ -652,7 +652,15 @@ def main():
     ap.add_argument("--reference-seconds", type=float, default=240.0,
                     help="reference arm: stop building trees once this many seconds have passed")
     ap.add_argument("--suite", default="", help="secondary configurations, e.g. c1,c3,c4")
+    ap.add_argument("--rows", type=int, default=0,
+                    help="rows of the workload (default: the configuration's 10M); a smaller case of the same "
+                         "workload for profiler captures")
     args = ap.parse_args()
+    if args.rows > 0:
+        global N_ROWS
+        N_ROWS = args.rows
+        CONFIG["rows"] = N_ROWS
+        CONFIG["workload"] = CONFIG["workload"].replace("10M x 200", f"{N_ROWS:,} x 200")
     if args.suite:
         run_suite(args)
         return
