@@ -71,13 +71,14 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-def profile_traffic(name):
-    """DRAM bytes per histogram launch recorded from an ncu capture in a
-    committed profile summary (a profile constant, not measured in this run)."""
+def profile_traffic_ratio(name):
+    """DRAM bytes over algorithmic bytes of the histogram kernel, recorded from
+    an ncu capture in a committed profile summary (a profile constant, not
+    measured in this run)."""
     path = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(path):
-            if line.startswith("traffic_bytes_per_launch:"):
+            if line.startswith("dram_over_algorithmic:"):
                 return float(line.split(":")[1])
     except OSError:
         pass
@@ -256,10 +257,12 @@ def hist_roofline(prof, peak, peak_kind, traffic_file):
     kern = {k: v for k, v in prof.items() if not k.startswith("_")}
     dominant = max((v[1], k) for k, v in kern.items())[1]
     iters = max(1, prof.get("_iters", 3))
+    ratio = profile_traffic_ratio(traffic_file)
     return {"kernel": "k_hist (histogram)", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
-            "traffic": profile_traffic(traffic_file),
-            "traffic_source": f"profile constant: ncu dram bytes per launch recorded in profiles/{traffic_file}",
+            "traffic": ratio * hbytes / max(1, hl) if ratio else None,
+            "traffic_source": f"per launch: algorithmic bytes x the DRAM/algorithmic ratio {ratio} of an ncu "
+                              f"capture of a smaller case (profiles/{traffic_file}); a profile constant",
             "alg_bytes_per_launch": hbytes / max(1, hl), "avg_launch_ms": hms / max(1, hl),
             "timing": "CUDA events recorded as nodes of the replayed iteration graph" if prof["_in_graph"]
                       else "CUDA events around launches outside a graph",
@@ -630,6 +633,9 @@ def run_suite(args):
             r = suite_c3(eng, _capi)
         elif name == "c4":
             r = suite_c4(eng, _capi, ref_ok=ref_ok)
+        elif name == "c2":  # the regression configuration alone, device-timed like the headline
+            peak, kind = load_peaks()
+            r = c2_secondary(eng, _capi, peak, kind, steps=5)
         elif name == "c4dev":  # the four serving models' device-resident prediction only
             r = {"config": "serving models (1000xd6, 200xd4, 500xd8, 2000xd10) on 100 features, 1M resident rows",
                  "device_predict_1M_rows": _device_predict(_train_serving_models(eng, _capi), 100)}
@@ -651,7 +657,7 @@ def main():
     ap.add_argument("--no-c2", action="store_true", help="leave out the secondary regression configuration")
     ap.add_argument("--reference-seconds", type=float, default=240.0,
                     help="reference arm: stop building trees once this many seconds have passed")
-    ap.add_argument("--suite", default="", help="secondary configurations, e.g. c1,c3,c4")
+    ap.add_argument("--suite", default="", help="secondary configurations, e.g. c1,c2,c3,c4")
     ap.add_argument("--rows", type=int, default=0,
                     help="rows of the workload (default: the configuration's 10M); a smaller case of the same "
                          "workload for profiler captures")
