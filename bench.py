@@ -564,6 +564,27 @@ def suite_c4(eng, _capi, seconds=3.0, rate=20_000.0, ref_ok=False):
         lat[str(rows)] = {"p50_us": _pct(ts, 50) * 1e6, "p99_us": _pct(ts, 99) * 1e6,
                           "rows_per_s": rows / _pct(ts, 50)}
     res["fixed_batch_1000xd6"] = lat
+    # the same through the reference-shaped facade: TurboCatClassifier.predict_proba
+    # on host (pageable) buffers, the model loaded from its TCAT file
+    import turbocat
+
+    path = os.path.join(tempfile.mkdtemp(), "m.tcat")
+    with open(path, "wb") as fh:
+        fh.write(models[0].tcat())
+    clf = turbocat.TurboCatClassifier(verbosity=0).load(path)
+    flat = {}
+    for rows in (1, 64, 4096, 65536):
+        Xb = np.ascontiguousarray(pool[:rows])
+        for _ in range(3):
+            clf.predict_proba(Xb)
+        ts = []
+        for _ in range(100 if rows <= 64 else 30):
+            t0 = time.perf_counter()
+            clf.predict_proba(Xb)
+            ts.append(time.perf_counter() - t0)
+        flat[str(rows)] = {"p50_us": _pct(ts, 50) * 1e6, "p99_us": _pct(ts, 99) * 1e6,
+                           "rows_per_s": rows / _pct(ts, 50)}
+    res["facade_predict_proba_1000xd6"] = flat
     res["device_predict_1M_rows"] = _device_predict(models, f)
     if ref_ok:
         sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
@@ -579,7 +600,7 @@ def suite_c4(eng, _capi, seconds=3.0, rate=20_000.0, ref_ok=False):
             Xb = np.ascontiguousarray(pool[:rows])
             rm.predict_proba(Xb)
             ts = []
-            for _ in range(30):
+            for _ in range(100 if rows <= 64 else 30):
                 t0 = time.perf_counter()
                 rm.predict_proba(Xb)
                 ts.append(time.perf_counter() - t0)

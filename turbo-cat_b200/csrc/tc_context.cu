@@ -86,6 +86,7 @@ void tc_ctx_destroy(tc_ctx* ctx) {
   cudaStreamSynchronize(ctx->pred_stream);
   for (auto& kv : ctx->allocs) cudaFree(kv.first);
   ctx->allocs.clear();
+  if (ctx->pin_io) cudaFreeHost(ctx->pin_io);
   cudaStreamDestroy(ctx->stream);
   cudaStreamDestroy(ctx->pred_stream);
   delete ctx;

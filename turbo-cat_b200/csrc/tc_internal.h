@@ -43,6 +43,14 @@ struct tc_ctx {
   std::mutex pred_mu;
   void* pred_scratch = nullptr;
   size_t pred_scratch_bytes = 0;
+  // small predictions: pinned host staging mapped into the device's address
+  // space (inputs read and outputs written by the kernel in place), and
+  // device partial sums with a completion counter
+  float* pin_io = nullptr;           // [pin_floats] inputs, then outputs
+  float* pin_io_dev = nullptr;       // its device alias
+  size_t pin_floats = 0;
+  void* small_scratch = nullptr;     // partials [blocks][rows][K] + counter
+  size_t small_scratch_bytes = 0;
 
   tc_status fail(tc_status code, const char* fmt, ...) {
     char buf[512];

@@ -293,6 +293,110 @@ __global__ void __launch_bounds__(PRED_THREADS) k_predict(JobTable jt) {
   }
 }
 
+// Small requests (at most SMALL_ROWS rows): the trees are split over the
+// blocks of one launch instead of streamed through one block.  Block b walks
+// trees [b*T/NB, (b+1)*T/NB) for every row of the request (row slot =
+// thread % RT, tree lane = thread / RT, trees in order within a lane), sums
+// its lanes pairwise in a fixed order and stores one partial per (row,
+// class); the last block to finish (completion counter; nobody waits) adds
+// the blocks' partials in block order, adds the base and applies the
+// transform.  Inputs may sit in pinned host memory mapped into the device
+// (a few rows are read in place), outputs may be written straight into it.
+constexpr int SMALL_ROWS = 64;
+constexpr int SMALL_THREADS = 256;
+constexpr int SMALL_TREES_PER_BLOCK = 32;
+constexpr int SMALL_MAX_F = 512;   // features of a small request (its rows fit in shared memory)
+
+__global__ void __launch_bounds__(SMALL_THREADS) k_predict_small(ModelDesc md, const float* __restrict__ X, uint32_t n,
+                                                                  int transform, float* __restrict__ partial,
+                                                                  uint32_t* __restrict__ counter,
+                                                                  float* __restrict__ out) {
+  extern __shared__ float sm_small[];
+  const int f = md.n_features, fs = f + 1;
+  const int K = md.n_classes, D = md.max_depth, L = 1 << D;
+  float* s_x = sm_small;                         // [n][f+1]
+  float* s_red = s_x + n * fs;                   // [SMALL_THREADS][K]
+  for (uint32_t i = threadIdx.x >> 5; i < n; i += blockDim.x >> 5)
+    for (int j = threadIdx.x & 31; j < f; j += 32) s_x[i * fs + j] = X[(size_t)i * f + j];
+  __syncthreads();
+  int RT = SMALL_ROWS;
+  while (RT > 1 && (uint32_t)(RT >> 1) >= n) RT >>= 1;
+  const int TG = blockDim.x / RT;
+  const int row = threadIdx.x % RT, tg = threadIdx.x / RT;
+  const int T = md.n_trees, NB = gridDim.x;
+  const int t0 = (int)((long long)T * blockIdx.x / NB), t1 = (int)((long long)T * (blockIdx.x + 1) / NB);
+  float acc[PRED_MAX_K];
+#pragma unroll
+  for (int k = 0; k < PRED_MAX_K; ++k) acc[k] = 0.0f;
+  if ((uint32_t)row < n) {
+    const float* xr = s_x + row * fs;
+    for (int t = t0 + tg; t < t1; t += TG) {
+      const int dep = md.depth[t];
+      const uint2* sp = md.splits + (size_t)t * D;
+      uint32_t idx = 0;
+      for (int d = 0; d < dep; ++d) {
+        const uint2 q = sp[d];
+        idx = (idx << 1) | (uint32_t)(xr[q.x] >= __uint_as_float(q.y));  // false for NaN
+      }
+      const float v = md.leaves[(size_t)t * L + idx];
+      const int cls = K == 1 ? 0 : t % K;
+#pragma unroll
+      for (int k = 0; k < PRED_MAX_K; ++k)
+        if (k == cls) acc[k] += v;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < PRED_MAX_K; ++k)
+    if (k < K) s_red[threadIdx.x * K + k] = acc[k];
+  __syncthreads();
+  for (int h = TG >> 1; h > 0; h >>= 1) {  // lanes pairwise, fixed order
+    if (tg < h)
+      for (int k = 0; k < K; ++k) s_red[threadIdx.x * K + k] += s_red[(threadIdx.x + h * RT) * K + k];
+    __syncthreads();
+  }
+  if (tg == 0 && (uint32_t)row < n)
+    for (int k = 0; k < K; ++k) partial[((size_t)blockIdx.x * n + row) * K + k] = s_red[row * K + k];
+  __shared__ bool s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(counter, 1u) == (uint32_t)NB - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  for (uint32_t r = threadIdx.x; r < n; r += blockDim.x) {
+    float v[PRED_MAX_K];
+#pragma unroll
+    for (int k = 0; k < PRED_MAX_K; ++k) v[k] = 0.0f;
+    for (int b = 0; b < NB; ++b)
+#pragma unroll
+      for (int k = 0; k < PRED_MAX_K; ++k)
+        if (k < K) v[k] += __ldcg(&partial[((size_t)b * n + r) * K + k]);
+    float* o = out + (size_t)r * K;
+    if (transform == TC_TRANSFORM_SOFTMAX && K > 1) {
+      float mx = -INFINITY;
+      for (int k = 0; k < K; ++k) mx = fmaxf(mx, v[k] + md.base);
+      float sum = 0.0f, e[PRED_MAX_K];
+#pragma unroll
+      for (int k = 0; k < PRED_MAX_K; ++k)
+        if (k < K) { e[k] = expf(v[k] + md.base - mx); sum += e[k]; }
+#pragma unroll
+      for (int k = 0; k < PRED_MAX_K; ++k)
+        if (k < K) o[k] = e[k] / sum;
+    } else {
+#pragma unroll
+      for (int k = 0; k < PRED_MAX_K; ++k) {
+        if (k < K) {
+          const float raw = v[k] + md.base;
+          o[k] = transform == TC_TRANSFORM_SIGMOID ? sigmoidf_ref(raw) : raw;
+        }
+      }
+    }
+  }
+  if (threadIdx.x == 0) *counter = 0u;  // re-armed for the next call
+}
+
 size_t predict_smem(int max_f, int max_depth) {
   return (size_t)PRED_ROWS * (max_f + 1) * 4 + PRED_LEAF_FLOATS * 4 +
          (size_t)2 * PRED_CHUNK * std::max(1, max_depth) * 8 + 2 * PRED_CHUNK * 4;
@@ -617,6 +721,57 @@ tc_status tc_model_load_tcat(tc_ctx* ctx, const uint8_t* buf, size_t len, tc_mod
 
 void tc_model_destroy(tc_model* m) { delete m; }
 
+// Small request (n <= SMALL_ROWS): inputs and outputs through the context's
+// pinned mapped staging, one launch of k_predict_small, one synchronisation.
+// The staging and the device partials are allocated once, at their largest
+// (SMALL_ROWS rows of SMALL_MAX_F features; one partial block per SM).
+static tc_status predict_small(tc_ctx* ctx, const tc_model* m, const float* X, uint32_t n, uint32_t f,
+                               int32_t transform, float* out) {
+  const int K = m->info.n_classes;
+  const int T = m->info.n_trees;
+  const int NB = std::max(1, std::min(ctx->sm_count, (T + SMALL_TREES_PER_BLOCK - 1) / SMALL_TREES_PER_BLOCK));
+  const size_t in_cap = (size_t)SMALL_ROWS * SMALL_MAX_F;         // floats
+  const size_t out_cap = (size_t)SMALL_ROWS * PRED_MAX_K;
+  if (!ctx->pin_io) {
+    TC_CUDA(ctx, cudaHostAlloc(reinterpret_cast<void**>(&ctx->pin_io), (in_cap + out_cap) * sizeof(float),
+                               cudaHostAllocMapped));
+    TC_CUDA(ctx, cudaHostGetDevicePointer(reinterpret_cast<void**>(&ctx->pin_io_dev), ctx->pin_io, 0));
+    ctx->pin_floats = in_cap + out_cap;
+  }
+  if (!ctx->small_scratch) {
+    // [256 B counter][partials: SMs x SMALL_ROWS x PRED_MAX_K][inputs: in_cap]
+    const size_t bytes = 256 + ((size_t)ctx->sm_count * SMALL_ROWS * PRED_MAX_K + in_cap) * sizeof(float);
+    TC_TRY(ctx->alloc(&ctx->small_scratch, bytes, "small predict partials"));
+    TC_CUDA(ctx, cudaMemset(ctx->small_scratch, 0, bytes));
+    ctx->small_scratch_bytes = bytes;
+  }
+  cudaStream_t st = ctx->pred_stream;
+  uint32_t* counter = static_cast<uint32_t*>(ctx->small_scratch);
+  float* partial = reinterpret_cast<float*>(static_cast<char*>(ctx->small_scratch) + 256);
+  float* dx = partial + (size_t)ctx->sm_count * SMALL_ROWS * PRED_MAX_K;
+  const size_t in_f = (size_t)n * f, out_f = (size_t)n * K;
+  std::memcpy(ctx->pin_io, X, in_f * sizeof(float));
+  // a few rows are read in place over the bus by every block; more rows go
+  // to device memory first in one copy
+  const float* xk = ctx->pin_io_dev;
+  if (in_f * sizeof(float) > 2048) {
+    TC_CUDA(ctx, cudaMemcpyAsync(dx, ctx->pin_io, in_f * sizeof(float), cudaMemcpyHostToDevice, st));
+    xk = dx;
+  }
+  const size_t smem = ((size_t)n * (f + 1) + (size_t)SMALL_THREADS * K) * sizeof(float);
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaFuncSetAttribute(k_predict_small, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_done = true;
+  }
+  k_predict_small<<<NB, SMALL_THREADS, smem, st>>>(model_desc(m), xk, n, transform, partial, counter,
+                                                   ctx->pin_io_dev + in_cap);
+  TC_CUDA(ctx, cudaGetLastError());
+  TC_CUDA(ctx, cudaStreamSynchronize(st));
+  std::memcpy(out, ctx->pin_io + in_cap, out_f * sizeof(float));
+  return TC_OK;
+}
+
 tc_status tc_predict(tc_ctx* ctx, const tc_model* m, const float* X, uint32_t n, uint16_t f, int32_t transform,
                      float* out) {
   if (!ctx || !m || (!X && n) || (!out && n)) return TC_ERR_INVALID_ARG;
@@ -625,6 +780,10 @@ tc_status tc_predict(tc_ctx* ctx, const tc_model* m, const float* X, uint32_t n,
   if (n == 0) return TC_OK;
   cudaSetDevice(ctx->device);
   const int K = m->info.n_classes;
+  if (n <= (uint32_t)SMALL_ROWS && K <= PRED_MAX_K && f <= SMALL_MAX_F && m->info.n_trees > 0) {
+    std::lock_guard<std::mutex> g(ctx->pred_mu);
+    return predict_small(ctx, m, X, n, f, transform, out);
+  }
   // input and output share one grow-only device buffer of the context, so a
   // call allocates nothing once the largest batch has been seen
   const size_t in_bytes = ((size_t)n * f * sizeof(float) + 255) / 256 * 256;
