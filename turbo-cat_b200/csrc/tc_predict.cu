@@ -18,6 +18,7 @@
 // chunk lands while the current one is walked), and every thread walks all
 // trees for its row.
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 
 #include "tc_internal.h"
@@ -294,30 +295,36 @@ __global__ void __launch_bounds__(PRED_THREADS) k_predict(JobTable jt) {
 }
 
 // Small requests (at most SMALL_ROWS rows): the trees are split over the
-// blocks of one launch instead of streamed through one block.  Block b walks
+// blocks of one launch instead of streamed through one block, as few blocks
+// as the (row, tree) walks need (one block for a single row).  Block b walks
 // trees [b*T/NB, (b+1)*T/NB) for every row of the request (row slot =
-// thread % RT, tree lane = thread / RT, trees in order within a lane), sums
-// its lanes pairwise in a fixed order and stores one partial per (row,
-// class); the last block to finish (completion counter; nobody waits) adds
-// the blocks' partials in block order, adds the base and applies the
-// transform.  Inputs may sit in pinned host memory mapped into the device
-// (a few rows are read in place), outputs may be written straight into it.
+// thread % RT, tree lane = thread / RT, trees in order within a lane) and
+// sums its lanes pairwise in a fixed order; with several blocks each stores
+// one partial per (row, class) and the last block to finish (completion
+// counter; nobody waits) adds them in block order.  The block that finishes
+// adds the base, applies the transform and writes the outputs (which may be
+// pinned host memory mapped into the device).  The rows come from device
+// memory or, for the smallest requests, from the launch parameters.
 constexpr int SMALL_ROWS = 64;
-constexpr int SMALL_THREADS = 256;
-constexpr int SMALL_TREES_PER_BLOCK = 32;
+constexpr int SMALL_INLINE = 928;  // floats of a request carried in the launch parameters (4 KB in all)
+struct SmallRows {
+  float v[SMALL_INLINE];
+};
+constexpr int SMALL_THREADS = 512;
+constexpr int SMALL_WALKS_PER_BLOCK = 4096;  // (row, tree) walks per block: one block for a single row
 constexpr int SMALL_MAX_F = 512;   // features of a small request (its rows fit in shared memory)
 
 __global__ void __launch_bounds__(SMALL_THREADS) k_predict_small(ModelDesc md, const float* __restrict__ X, uint32_t n,
                                                                   int transform, float* __restrict__ partial,
                                                                   uint32_t* __restrict__ counter,
-                                                                  float* __restrict__ out) {
+                                                                  float* __restrict__ out, SmallRows inl) {
   extern __shared__ float sm_small[];
   const int f = md.n_features, fs = f + 1;
   const int K = md.n_classes, D = md.max_depth, L = 1 << D;
   float* s_x = sm_small;                         // [n][f+1]
   float* s_red = s_x + n * fs;                   // [SMALL_THREADS][K]
   for (uint32_t i = threadIdx.x >> 5; i < n; i += blockDim.x >> 5)
-    for (int j = threadIdx.x & 31; j < f; j += 32) s_x[i * fs + j] = X[(size_t)i * f + j];
+    for (int j = threadIdx.x & 31; j < f; j += 32) s_x[i * fs + j] = X ? X[(size_t)i * f + j] : inl.v[i * f + j];
   __syncthreads();
   int RT = SMALL_ROWS;
   while (RT > 1 && (uint32_t)(RT >> 1) >= n) RT >>= 1;
@@ -331,13 +338,19 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_predict_small(ModelDesc md, c
   if ((uint32_t)row < n) {
     const float* xr = s_x + row * fs;
     for (int t = t0 + tg; t < t1; t += TG) {
-      const int dep = md.depth[t];
+      // the tree's depth and every split are loaded before any compare (one
+      // round trip to L2 instead of one per level); a shallower tree ignores
+      // its padding splits
       const uint2* sp = md.splits + (size_t)t * D;
+      uint2 q[kMaxDepth];
+#pragma unroll
+      for (int d = 0; d < kMaxDepth; ++d)
+        if (d < D) q[d] = sp[d];
+      const int dep = md.depth[t];
       uint32_t idx = 0;
-      for (int d = 0; d < dep; ++d) {
-        const uint2 q = sp[d];
-        idx = (idx << 1) | (uint32_t)(xr[q.x] >= __uint_as_float(q.y));  // false for NaN
-      }
+#pragma unroll
+      for (int d = 0; d < kMaxDepth; ++d)
+        if (d < dep) idx = (idx << 1) | (uint32_t)(xr[q[d].x] >= __uint_as_float(q[d].y));  // false for NaN
       const float v = md.leaves[(size_t)t * L + idx];
       const int cls = K == 1 ? 0 : t % K;
 #pragma unroll
@@ -354,22 +367,24 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_predict_small(ModelDesc md, c
       for (int k = 0; k < K; ++k) s_red[threadIdx.x * K + k] += s_red[(threadIdx.x + h * RT) * K + k];
     __syncthreads();
   }
-  if (tg == 0 && (uint32_t)row < n)
-    for (int k = 0; k < K; ++k) partial[((size_t)blockIdx.x * n + row) * K + k] = s_red[row * K + k];
-  __shared__ bool s_last;
-  __syncthreads();
-  if (threadIdx.x == 0) {
+  if (NB > 1) {
+    if (tg == 0 && (uint32_t)row < n)
+      for (int k = 0; k < K; ++k) partial[((size_t)blockIdx.x * n + row) * K + k] = s_red[row * K + k];
+    __shared__ bool s_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      s_last = atomicAdd(counter, 1u) == (uint32_t)NB - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
     __threadfence();
-    s_last = atomicAdd(counter, 1u) == (uint32_t)NB - 1;
   }
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
   for (uint32_t r = threadIdx.x; r < n; r += blockDim.x) {
     float v[PRED_MAX_K];
 #pragma unroll
-    for (int k = 0; k < PRED_MAX_K; ++k) v[k] = 0.0f;
-    for (int b = 0; b < NB; ++b)
+    for (int k = 0; k < PRED_MAX_K; ++k) v[k] = NB > 1 ? 0.0f : (k < K ? s_red[r * K + k] : 0.0f);
+    for (int b = 0; NB > 1 && b < NB; ++b)
 #pragma unroll
       for (int k = 0; k < PRED_MAX_K; ++k)
         if (k < K) v[k] += __ldcg(&partial[((size_t)b * n + r) * K + k]);
@@ -394,7 +409,7 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_predict_small(ModelDesc md, c
       }
     }
   }
-  if (threadIdx.x == 0) *counter = 0u;  // re-armed for the next call
+  if (NB > 1 && threadIdx.x == 0) *counter = 0u;  // re-armed for the next call
 }
 
 size_t predict_smem(int max_f, int max_depth) {
@@ -729,14 +744,19 @@ static tc_status predict_small(tc_ctx* ctx, const tc_model* m, const float* X, u
                                int32_t transform, float* out) {
   const int K = m->info.n_classes;
   const int T = m->info.n_trees;
-  const int NB = std::max(1, std::min(ctx->sm_count, (T + SMALL_TREES_PER_BLOCK - 1) / SMALL_TREES_PER_BLOCK));
+  const long long walks = (long long)n * T;
+  const int NB = (int)std::max<long long>(1, std::min<long long>(std::min(ctx->sm_count, T),
+                                                                  (walks + SMALL_WALKS_PER_BLOCK - 1) /
+                                                                      SMALL_WALKS_PER_BLOCK));
   const size_t in_cap = (size_t)SMALL_ROWS * SMALL_MAX_F;         // floats
   const size_t out_cap = (size_t)SMALL_ROWS * PRED_MAX_K;
   if (!ctx->pin_io) {
-    TC_CUDA(ctx, cudaHostAlloc(reinterpret_cast<void**>(&ctx->pin_io), (in_cap + out_cap) * sizeof(float),
+    // [inputs][outputs][the sequence word]
+    TC_CUDA(ctx, cudaHostAlloc(reinterpret_cast<void**>(&ctx->pin_io), (in_cap + out_cap + 16) * sizeof(float),
                                cudaHostAllocMapped));
+    std::memset(ctx->pin_io, 0, (in_cap + out_cap + 16) * sizeof(float));
     TC_CUDA(ctx, cudaHostGetDevicePointer(reinterpret_cast<void**>(&ctx->pin_io_dev), ctx->pin_io, 0));
-    ctx->pin_floats = in_cap + out_cap;
+    ctx->pin_floats = in_cap + out_cap + 16;
   }
   if (!ctx->small_scratch) {
     // [256 B counter][partials: SMs x SMALL_ROWS x PRED_MAX_K][inputs: in_cap]
@@ -750,11 +770,18 @@ static tc_status predict_small(tc_ctx* ctx, const tc_model* m, const float* X, u
   float* partial = reinterpret_cast<float*>(static_cast<char*>(ctx->small_scratch) + 256);
   float* dx = partial + (size_t)ctx->sm_count * SMALL_ROWS * PRED_MAX_K;
   const size_t in_f = (size_t)n * f, out_f = (size_t)n * K;
-  std::memcpy(ctx->pin_io, X, in_f * sizeof(float));
-  // a few rows are read in place over the bus by every block; more rows go
-  // to device memory first in one copy
-  const float* xk = ctx->pin_io_dev;
-  if (in_f * sizeof(float) > 2048) {
+  // A request of at most SMALL_INLINE floats travels in the launch's own
+  // parameters; larger ones go to device memory in one copy from the pinned
+  // buffer (measured: a kernel that reads its input over the bus in place
+  // takes ~6 us longer than the copy).  Outputs are written by the kernel
+  // straight into the mapped buffer.
+  thread_local SmallRows inl_buf;
+  SmallRows* inl = &inl_buf;
+  const float* xk = nullptr;
+  if (in_f <= (size_t)SMALL_INLINE) {
+    std::memcpy(inl->v, X, in_f * sizeof(float));
+  } else {
+    std::memcpy(ctx->pin_io, X, in_f * sizeof(float));
     TC_CUDA(ctx, cudaMemcpyAsync(dx, ctx->pin_io, in_f * sizeof(float), cudaMemcpyHostToDevice, st));
     xk = dx;
   }
@@ -765,7 +792,7 @@ static tc_status predict_small(tc_ctx* ctx, const tc_model* m, const float* X, u
     attr_done = true;
   }
   k_predict_small<<<NB, SMALL_THREADS, smem, st>>>(model_desc(m), xk, n, transform, partial, counter,
-                                                   ctx->pin_io_dev + in_cap);
+                                                   ctx->pin_io_dev + in_cap, *inl);
   TC_CUDA(ctx, cudaGetLastError());
   TC_CUDA(ctx, cudaStreamSynchronize(st));
   std::memcpy(out, ctx->pin_io + in_cap, out_f * sizeof(float));
