@@ -489,6 +489,30 @@ def suite_c3(eng, _capi, iters=10):
     return res
 
 
+def suite_goss(eng, _capi, iters=10):
+    """GOSS on the regression configuration's data (1M x 100, MSE, depth 8,
+    top 0.2, other 0.1): wall time per iteration (the host ranks the
+    iteration's gradients and draws the sample; the device waits) against
+    the device kernel time of such iterations."""
+    from datagen import regression_c2
+
+    X, y = regression_c2(C2["n"], C2["f"], seed=2)
+    ds = eng.upload(X, y)
+    ds.quantize(255)
+    p = _capi.params(loss="mse", n_estimators=3 + iters + 5, max_depth=C2["depth"], learning_rate=C2["lr"],
+                     lambda_l2=C2["l2"], use_goss=True, goss_top_rate=0.2, goss_other_rate=0.1)
+    tr = eng.trainer(ds, p)
+    tr.step(3)
+    t0 = time.perf_counter()
+    tr.step(iters)
+    wall = (time.perf_counter() - t0) / iters
+    prof = tr.profile(5)
+    dev = sum(v[1] for k, v in prof.items() if not k.startswith("_")) / 5 * 1e-3
+    return {"config": "GOSS (top 0.2, other 0.1) on regression 1M x 100, MSE, depth 8",
+            "wall_s_per_iter": wall, "device_kernel_s_per_iter": dev,
+            "host_selection_and_sync_s_per_iter": wall - dev}
+
+
 def _train_serving_models(eng, _capi):
     rng = np.random.default_rng(4)
     n, f = 200_000, 100
@@ -657,6 +681,8 @@ def run_suite(args):
         elif name == "c2":  # the regression configuration alone, device-timed like the headline
             peak, kind = load_peaks()
             r = c2_secondary(eng, _capi, peak, kind, steps=5)
+        elif name == "goss":
+            r = suite_goss(eng, _capi)
         elif name == "c4dev":  # the four serving models' device-resident prediction only
             r = {"config": "serving models (1000xd6, 200xd4, 500xd8, 2000xd10) on 100 features, 1M resident rows",
                  "device_predict_1M_rows": _device_predict(_train_serving_models(eng, _capi), 100)}

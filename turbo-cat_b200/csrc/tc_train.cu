@@ -1571,6 +1571,9 @@ __global__ void __launch_bounds__(PART_THREADS) k_scatter(DevCfg c, DevPtrs P, i
       if (key[u] >= 0) g[u] = gh[base + u * blockDim.x + threadIdx.x];
 #pragma unroll
     for (int u = 0; u < SCAT_UNROLL; ++u) {
+      // a group of 32 rows without a smaller-child row needs no slot (most
+      // groups on deep, skewed levels)
+      if (__ballot_sync(0xffffffffu, key[u] >= 0) == 0u) continue;
       // one shared atomic per distinct pair of the warp; lanes keep their order
       const unsigned m = __match_any_sync(0xffffffffu, key[u]);
       const int leader = __ffs(m) - 1;
