@@ -144,7 +144,6 @@ struct DevPtrs {
   uint32_t* counters;            // [K] completion counters of the pick blocks
   uint32_t* fcnt;                // [K][F] completion counters of a feature's scan blocks
   int32_t* hist_ctr;             // [1] next histogram work item (reset by the plan kernel)
-  uint32_t* dev_err;             // [1] nonzero: a bounded device wait gave up (checked by the host after a step)
   uint32_t* red_ctr;             // [1] completion counter of the fused reduce + plan kernel
   ClassState* cs;                // [K]
   int32_t* iter;                 // [1] boosting iteration (tree slot = iter*KT + k0 + k)
@@ -437,48 +436,6 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
   const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
 }
-// Bulk (TMA engine) copy of contiguous global bytes into this CTA's shared
-// memory, completed through an mbarrier; 16-byte aligned addresses and a
-// size that is a multiple of 16 bytes.
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"((uint32_t)__cvta_generic_to_shared(bar)), "r"(count)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
-                   (uint32_t)__cvta_generic_to_shared(bar)),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   (uint32_t)__cvta_generic_to_shared(dst)),
-               "l"(src), "r"(bytes), "r"((uint32_t)__cvta_generic_to_shared(bar))
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(ok)
-      : "r"((uint32_t)__cvta_generic_to_shared(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Waits (bounded) for phase `parity` of a bulk copy's mbarrier; on giving up
-// it raises the device error flag and returns (the host reports it).
-__device__ __forceinline__ void mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint32_t* err) {
-  for (uint32_t spin = 0; !mbar_try_wait(bar, parity); ++spin) {
-    if (spin > (1u << 22)) {
-      atomicExch(err, 1u);
-      return;
-    }
-  }
-}
-__device__ __forceinline__ void fence_proxy_async_smem() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
@@ -605,7 +562,6 @@ __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(DevCfg c, DevPtrs P, i
   uint8_t* w_bins = smraw + S_::hist_bytes + (size_t)warp * S_::warp_bytes;        // [S][B][W]
   float2* w_gh = reinterpret_cast<float2*>(w_bins + (size_t)S * B * W);            // [S][B]
   __shared__ double s_sum[2][HIST_THREADS / 32];
-  __shared__ __align__(8) uint64_t s_bar[HIST_THREADS / 32][S];  // a warp's bulk-copy barriers, one per stage
   const int P2 = pairs_at(d);
   const int nseg = c.K * P2;
   const int n_items = P.cum[nseg];
@@ -618,12 +574,7 @@ __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(DevCfg c, DevPtrs P, i
 #pragma unroll
   for (int s = 0; s < 4; ++s) sel[s] = 0x4404u | ((uint32_t)((s + qr) & 3) << 4);
   for (int q = threadIdx.x; q < kSlots * S_::FIELDS * W; q += blockDim.x) hist[q] = 0u;
-  if (lane == 0) {
-    for (int st = 0; st < S; ++st) mbar_init(&s_bar[warp][st], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");  // visible to the copy engine
-  }
   __syncthreads();
-  uint32_t bar_phase = 0;  // bit st: parity of stage st's next bulk-copy completion
   // Items are claimed from a counter (blocks that drew cheap items take
   // more), the next one while the current one runs.  Item ci*G + g is chunk
   // ci (over all segments) of group g; a narrow last group costs a fraction
@@ -703,9 +654,6 @@ __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(DevCfg c, DevPtrs P, i
     const uint32_t gwid = (uint32_t)g + 1 == c.groups ? c.wlast : 32u;
     const uint8_t* tile = P.bins_t + (uint64_t)g * c.gstride;
     const int nb = (end - start + B - 1) / B;   // batches in the item; warp w takes w, w+nwarps, ...
-    // the root's rows of a full-width group are one contiguous range of the
-    // tile block (32-byte rows: every batch starts on a 16-byte boundary)
-    const bool bulk = d == 0 && gwid == 32;
     uint32_t rid_next = 0;
 #define TC_FETCH_ID(bi)                                                                      \
     {                                                                                        \
@@ -714,18 +662,7 @@ __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(DevCfg c, DevPtrs P, i
     }
 #define TC_ISSUE(bi, st_)                                                                    \
     {                                                                                        \
-      if (bulk && (bi) < nb) {                                                               \
-        /* the batch's rows are contiguous: one bulk copy by lane 0 */                       \
-        if (lane == 0) {                                                                     \
-          const uint32_t nbytes_ = (uint32_t)min(B, end - (start + (bi) * B)) * 32u;         \
-          fence_proxy_async_smem();                                                          \
-          mbar_expect_tx(&s_bar[warp][st_], nbytes_);                                        \
-          bulk_g2s(w_bins + (size_t)(st_) * B * W, tile + (size_t)(start + (bi) * B) * 32,   \
-                   nbytes_, &s_bar[warp][st_]);                                              \
-        }                                                                                    \
-        if (start + (bi) * B + lane < end)                                                   \
-          cp_async8(w_gh + (st_) * B + lane, gh + start + (bi) * B + lane);                   \
-      } else if ((bi) < nb && start + (bi) * B + lane < end) {                               \
+      if ((bi) < nb && start + (bi) * B + lane < end) {                                      \
         uint8_t* dst_ = w_bins + ((size_t)(st_) * B + lane) * W;                             \
         const uint8_t* src_ = tile + (size_t)rid_next * gwid;                                \
         if (gwid == 32) {                                                                    \
@@ -751,10 +688,6 @@ __global__ void __launch_bounds__(HIST_THREADS, 1) k_hist(DevCfg c, DevPtrs P, i
       TC_ISSUE(bi + nwarps, st ^ 1);       // the next batch streams in while this one is counted
       TC_FETCH_ID(bi + 2 * nwarps);        // row ids for the batch after, behind this batch's updates
       cp_async_wait<1>();
-      if (bulk) {
-        mbar_wait_bounded(&s_bar[warp][st], (bar_phase >> st) & 1u, P.dev_err);
-        bar_phase ^= 1u << st;
-      }
       __syncwarp();
       const int nvalid = min(B, end - (start + bi * B));
       const uint8_t* sb = w_bins + (size_t)st * B * W;
@@ -1817,7 +1750,6 @@ struct tc_trainer {
   DevBuf<FeatBest> fbest;
   DevBuf<uint32_t> counters;
   DevBuf<int32_t> hist_ctr;
-  DevBuf<uint32_t> dev_err;
   DevBuf<uint32_t> red_ctr, fcnt;
   DevBuf<NodeStat> nstat;
   DevBuf<uint32_t> pcnt, blk_off;
@@ -1959,8 +1891,6 @@ tc_status tc_trainer::setup(int) {
   TC_TRY(fbest.alloc(ctx, (size_t)K * f, "feature bests"));
   TC_TRY(counters.alloc(ctx, K, "pick counters"));
   TC_TRY(hist_ctr.alloc(ctx, 1, "histogram item counter"));
-  TC_TRY(dev_err.alloc(ctx, 1, "device error flag"));
-  TC_CUDA(ctx, cudaMemset(dev_err.p, 0, dev_err.bytes()));
   TC_TRY(red_ctr.alloc(ctx, 1, "reduce completion counter"));
   TC_TRY(fcnt.alloc(ctx, (size_t)K * f, "scan completion counters"));
   TC_TRY(cs.alloc(ctx, K, "class state"));
@@ -1985,7 +1915,7 @@ tc_status tc_trainer::setup(int) {
   ptr.hist[0] = hist0.p; ptr.hist[1] = hist1.p; ptr.acc = acc.p; ptr.rchunk = rchunk.p;
   ptr.seg_start = seg_start.p; ptr.seg_len = seg_len.p; ptr.small = small.p; ptr.nstat = nstat.p;
   ptr.pcnt = pcnt.p; ptr.psum = psum.p; ptr.blk_off = blk_off.p; ptr.gpart = gpart.p; ptr.gany = gany.p;
-  ptr.fbest = fbest.p; ptr.counters = counters.p; ptr.hist_ctr = hist_ctr.p; ptr.dev_err = dev_err.p; ptr.red_ctr = red_ctr.p; ptr.fcnt = fcnt.p; ptr.cs = cs.p; ptr.iter = iter.p;
+  ptr.fbest = fbest.p; ptr.counters = counters.p; ptr.hist_ctr = hist_ctr.p; ptr.red_ctr = red_ctr.p; ptr.fcnt = fcnt.p; ptr.cs = cs.p; ptr.iter = iter.p;
   ptr.m_depth = m_depth.p; ptr.m_feat = m_feat.p; ptr.m_bin = m_bin.p; ptr.m_thr = m_thr.p; ptr.m_gain = m_gain.p;
   ptr.m_second = m_second.p; ptr.m_leaves = m_leaves.p; ptr.root_hist_out = nullptr;
   ptr.lvl_rows = lvl_rows.p; ptr.lvl_nodes = lvl_nodes.p;
@@ -2599,9 +2529,6 @@ tc_status tc_trainer::step(int iters, bool sync) {
     float ms = 0.0f;
     TC_CUDA(ctx, cudaEventElapsedTime(&ms, ev0, ev1));
     seconds += ms * 1e-3;
-    uint32_t derr = 0;
-    TC_CUDA(ctx, cudaMemcpy(&derr, dev_err.p, sizeof(derr), cudaMemcpyDeviceToHost));
-    if (derr) return ctx->fail(TC_ERR_TIMEOUT, "a bounded device wait gave up (histogram bulk copy)");
   }
   return TC_OK;
 }
