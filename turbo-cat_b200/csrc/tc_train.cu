@@ -837,9 +837,9 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(DevCfg c, DevPtrs P, i
   double2* cur = P.hist[d & 1];
   const double2* par = P.hist[(d & 1) ^ 1];
   const int Pmax = 1 << (c.D - 1);
-  // the next level reads this level's histograms as parents (the root's is
-  // also the tree builder's root-histogram output)
-  const bool keep = d == 0 || d + 1 < c.D;
+  // the next level reads this level's histograms as parents, the reduce
+  // kernel reads the split feature's row for the children's sums (and the
+  // root's is the tree builder's root-histogram output)
   const NodeStat* ns = P.nstat + ((size_t)k * (c.D + 1) + d) * (1 << c.D);
   double acc[8];
   uint32_t anyb = 0;
@@ -869,7 +869,7 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(DevCfg c, DevPtrs P, i
         hh[i] = v.y - hh[i];
       }
     }
-    if (keep) {
+    {
       double2* hp = cur + hist_index(c, k, node, f, 0) + lane * 8;
 #pragma unroll
       for (int i = 0; i < 8; ++i) hp[i] = make_double2(hg[i], hh[i]);
@@ -1088,166 +1088,98 @@ __device__ void pick_body(const DevCfg& c, const DevPtrs& P, int d, int f, int k
 
 // ------------------------------------------------------------- partition --
 
-// grid (PB, K).  Rows of block b: a contiguous range.  Updates leaf ids and
-// writes per-block child counts and sums (FP32 within the block, handed on
-// as FP64 for the cross-block merge).  With few children, a warp reduces
-// each child's contributions through shuffles first (one shared update per
-// warp and child) instead of letting every lane hit the same two addresses.
 // grid (PB, K).  Rows of the split level get their child leaf index
-// (2*leaf + right, right = bin != 255 && bin > t) and every block sums its
-// rows' (grad, hess) and counts per child: FP32 within the block (rows in a
-// fixed order inside each warp), FP64 across blocks in the reduce kernel.
-// With 2 or 4 children (8 when a thread has many rows) every thread sums its
-// rows per child in registers and the block's warps reduce them once at the
-// end; otherwise a warp's rows are combined per distinct child (a match over
-// the warp) first, so a child gets one shared atomic per warp.  Four rows per
-// thread are loaded before any is used.
+// (2*leaf + right, right = bin != 255 && bin > t) and every block counts its
+// sampled rows per child; the children's (grad, hess) sums come from their
+// parent's histogram (the reduce kernel), so no row's (grad, hess) is read
+// here.  With 2 or 4 children (8 when a thread has many rows) every thread
+// counts in registers and each warp reduces once at the end; with 16-256
+// children the lanes add into per-warp copies of the counts with shared
+// atomics, except that when one node holds more than 1/8 of the rows its two
+// children are counted in registers; beyond that a warp's rows are grouped
+// per distinct child (a match over the warp) first.  Four rows per thread are
+// loaded before any is used.
 constexpr int PART_UNROLL = 4;
-template <int NCH>  // 2, 4, 8 children: per-thread register sums; 0: per-warp child groups;
-                    // -1: per-lane atomics into per-warp copies of the child sums, except
-                    // that when one node holds more than 1/8 of the rows (its lanes would
-                    // hit one address) its two children are summed in registers
+template <int NCH>  // 2, 4, 8 children: per-thread register counts; 0: per-warp child groups;
+                    // -1: per-lane atomics into per-warp copies of the counts, the skewed
+                    // level's largest node counted in registers
 __global__ void __launch_bounds__(PART_THREADS) k_partition(DevCfg c, DevPtrs P, int d) {
   extern __shared__ unsigned char smraw[];
-  __shared__ float2 s_wv[PART_THREADS / 32][32];
   const int k = blockIdx.y;
   const ClassState cs = P.cs[k];
   if (cs.done || cs.depth != d + 1) return;
   const int nch = 1 << (d + 1);
-  const int ncopy = NCH < 0 ? PART_THREADS / 32 : 1;  // copies of the child sums (one per warp)
-  float* sG = reinterpret_cast<float*>(smraw);
-  float* sH = sG + nch * ncopy;
-  uint32_t* sC = reinterpret_cast<uint32_t*>(sH + nch * ncopy);
-  for (int q = threadIdx.x; q < nch * ncopy; q += blockDim.x) { sG[q] = 0.0f; sH[q] = 0.0f; sC[q] = 0; }
+  const int ncopy = NCH < 0 ? PART_THREADS / 32 : 1;  // copies of the counts (one per warp)
+  uint32_t* sC = reinterpret_cast<uint32_t*>(smraw);
+  for (int q = threadIdx.x; q < nch * ncopy; q += blockDim.x) sC[q] = 0;
   __syncthreads();
   const uint32_t rpb = (c.n + gridDim.x - 1) / gridDim.x;
   const uint32_t r0 = blockIdx.x * rpb, r1 = min(c.n, r0 + rpb);
   const uint8_t* col = P.bins_cm + (size_t)cs.f * c.np;
   uint16_t* leaf = P.leaf + (size_t)k * c.n;
-  const float2* gh = P.gh + (size_t)k * c.n;
   const uint8_t t = (uint8_t)cs.b;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int NR = NCH > 0 ? NCH : 1;
-  float ag[NR], ah[NR];
   uint32_t ac[NR];
 #pragma unroll
-  for (int cc = 0; cc < NR; ++cc) { ag[cc] = 0.0f; ah[cc] = 0.0f; ac[cc] = 0; }
-  float hg[2] = {0.0f, 0.0f}, hh[2] = {0.0f, 0.0f};  // NCH < 0, skewed level: the largest node's children
-  uint32_t hc[2] = {0u, 0u};
+  for (int cc = 0; cc < NR; ++cc) ac[cc] = 0;
+  uint32_t hc[2] = {0u, 0u};  // NCH < 0, skewed level: the largest node's children
   for (uint32_t base = r0; base < r1; base += blockDim.x * PART_UNROLL) {
     uint8_t bb[PART_UNROLL];
     uint16_t lf[PART_UNROLL];
-    float2 v[PART_UNROLL];
 #pragma unroll
     for (int u = 0; u < PART_UNROLL; ++u) {
       const uint32_t i = base + u * blockDim.x + threadIdx.x;
       if (i < r1) {
         bb[u] = col[i];
         lf[u] = leaf[i];
-        v[u] = gh[i];
       }
     }
 #pragma unroll
     for (int u = 0; u < PART_UNROLL; ++u) {
       const uint32_t i = base + u * blockDim.x + threadIdx.x;
       int nl = -1;
-      float2 w = make_float2(0.f, 0.f);
       if (i < r1) {
         const uint32_t right = (bb[u] != (uint8_t)kNanBin && bb[u] > t) ? 1u : 0u;
         nl = (int)(((uint32_t)lf[u] << 1) | right);
         leaf[i] = (uint16_t)nl;
-        w = v[u];
         if (!row_sampled(c, P, i)) nl = -1;  // its leaf moves on; it is not counted
       }
       if (NCH > 0) {
 #pragma unroll
-        for (int cc = 0; cc < NR; ++cc)
-          if (nl == cc) {
-            ag[cc] += w.x;
-            ah[cc] += w.y;
-            ac[cc] += 1u;
-          }
+        for (int cc = 0; cc < NR; ++cc) ac[cc] += nl == cc ? 1u : 0u;
       } else if (NCH < 0) {
         if (nl >= 0) {
-          if (cs.skew && (nl >> 1) == cs.hot) {
-            if (nl & 1) { hg[1] += w.x; hh[1] += w.y; hc[1] += 1u; }
-            else { hg[0] += w.x; hh[0] += w.y; hc[0] += 1u; }
-          } else {
-            const int o = warp * nch + nl;
-            atomicAdd(&sG[o], w.x);
-            atomicAdd(&sH[o], w.y);
-            atomicAdd(&sC[o], 1u);
-          }
+          if (cs.skew && (nl >> 1) == cs.hot) hc[nl & 1] += 1u;
+          else atomicAdd(&sC[warp * nch + nl], 1u);
         }
       } else {
-        // the first lane of each child's group sums the group in lane order
+        // the first lane of each child's group adds the group's size
         const unsigned m = __match_any_sync(0xffffffffu, nl);
-        s_wv[warp][lane] = w;
-        __syncwarp();
-        if (nl >= 0 && lane == __ffs(m) - 1) {
-          float g = 0.0f, h = 0.0f;
-          for (unsigned mm = m; mm; mm &= mm - 1) {
-            const float2 x = s_wv[warp][__ffs(mm) - 1];
-            g += x.x;
-            h += x.y;
-          }
-          atomicAdd(&sG[nl], g);
-          atomicAdd(&sH[nl], h);
-          atomicAdd(&sC[nl], (uint32_t)__popc(m));
-        }
-        __syncwarp();
+        if (nl >= 0 && lane == __ffs(m) - 1) atomicAdd(&sC[nl], (uint32_t)__popc(m));
       }
     }
   }
   if (NCH > 0) {
-    // the thread sums, reduced across the warp (fixed tree), one atomic per warp and child
 #pragma unroll
     for (int cc = 0; cc < NR; ++cc) {
-      float g = ag[cc], h = ah[cc];
-      for (int o = 16; o; o >>= 1) {
-        g += __shfl_xor_sync(0xffffffffu, g, o);
-        h += __shfl_xor_sync(0xffffffffu, h, o);
-      }
       const uint32_t cnt = __reduce_add_sync(0xffffffffu, ac[cc]);
-      if (lane == 0 && cnt) {
-        atomicAdd(&sG[cc], g);
-        atomicAdd(&sH[cc], h);
-        atomicAdd(&sC[cc], cnt);
-      }
+      if (lane == 0 && cnt) atomicAdd(&sC[cc], cnt);
     }
   }
   if (NCH < 0 && cs.skew) {
-    // the largest node's children: the thread sums, reduced across the warp
-    // (fixed tree), added to this warp's copy
 #pragma unroll
     for (int cc = 0; cc < 2; ++cc) {
-      float g = hg[cc], h = hh[cc];
-      for (int o = 16; o; o >>= 1) {
-        g += __shfl_xor_sync(0xffffffffu, g, o);
-        h += __shfl_xor_sync(0xffffffffu, h, o);
-      }
       const uint32_t cnt = __reduce_add_sync(0xffffffffu, hc[cc]);
-      if (lane == 0 && cnt) {
-        const int o = warp * nch + 2 * cs.hot + cc;
-        atomicAdd(&sG[o], g);
-        atomicAdd(&sH[o], h);
-        atomicAdd(&sC[o], cnt);
-      }
+      if (lane == 0 && cnt) atomicAdd(&sC[warp * nch + 2 * cs.hot + cc], cnt);
     }
   }
   __syncthreads();
   const int L = 1 << c.D;
   for (int q = threadIdx.x; q < nch; q += blockDim.x) {
-    const size_t o = ((size_t)k * c.PB + blockIdx.x) * L + q;
-    float g = 0.0f, h = 0.0f;
     uint32_t cn = 0;
-    for (int w = 0; w < ncopy; ++w) {  // the warps' copies in a fixed order
-      g += sG[w * nch + q];
-      h += sH[w * nch + q];
-      cn += sC[w * nch + q];
-    }
-    P.psum[o] = make_double2((double)g, (double)h);
-    P.pcnt[o] = cn;
+    for (int w = 0; w < ncopy; ++w) cn += sC[w * nch + q];  // the warps' copies
+    P.pcnt[((size_t)k * c.PB + blockIdx.x) * L + q] = cn;
   }
 }
 
@@ -1267,14 +1199,31 @@ __device__ __forceinline__ void node_reduce_body(const DevCfg& c, const DevPtrs&
   const int nkids = root ? 1 : 2;
   const int blk = threadIdx.x;
   uint32_t my_cnt[2] = {0, 0};
+  // row counts per child from the partition blocks; (G, H) of the root from
+  // the gradient pass's block sums, of two children from their parent's
+  // histogram row of the split feature: left = NaN slot + bins 0 .. b,
+  // right = bins b+1 .. 254 (exact sums of the level's histogram)
+  const double2* hrow = root ? nullptr : P.hist[d & 1] + hist_index(c, k, p, cs.f, 0);
   for (int kid = 0; kid < nkids; ++kid) {
     const int child = root ? 0 : 2 * p + kid;
     double g = 0.0, h = 0.0;
     uint32_t cn = 0;
     if (blk < c.PB) {
       const size_t o = ((size_t)k * c.PB + blk) * L + child;
-      const double2 v = P.psum[o];
-      g = v.x; h = v.y; cn = P.pcnt[o];
+      if (root) {
+        const double2 v = P.psum[o];
+        g = v.x;
+        h = v.y;
+      }
+      cn = P.pcnt[o];
+    }
+    if (!root && blk < kSlots) {
+      const bool left = blk == kNanBin || blk <= cs.b;
+      if (left == (kid == 0)) {
+        const double2 v = hrow[blk];
+        g = v.x;
+        h = v.y;
+      }
     }
     my_cnt[kid] = cn;
     s_g[kid][blk] = g; s_h[kid][blk] = h; s_c[kid][blk] = cn;
@@ -1300,8 +1249,10 @@ __device__ __forceinline__ void node_reduce_body(const DevCfg& c, const DevPtrs&
   const int sm = (cl <= cr) ? 0 : 1;
   const int Pmax = 1 << (c.D - 1);
   if (blk == 0) {
-    ns[2 * p] = NodeStat{s_g[0][0], s_h[0][0], cl, 0};
-    ns[2 * p + 1] = NodeStat{s_g[1][0], s_h[1][0], cr, 0};
+    // an empty child has zero sums (its parent's histogram row is not
+    // written when the parent itself is empty)
+    ns[2 * p] = cl ? NodeStat{s_g[0][0], s_h[0][0], cl, 0} : NodeStat{0.0, 0.0, 0u, 0};
+    ns[2 * p + 1] = cr ? NodeStat{s_g[1][0], s_h[1][0], cr, 0} : NodeStat{0.0, 0.0, 0u, 0};
     if (d + 1 < c.D) {
       P.small[k * Pmax + p] = 2 * p + sm;
       P.seg_len[k * Pmax + p] = (int)(sm ? cr : cl);
@@ -1922,8 +1873,8 @@ tc_status tc_trainer::setup(int) {
 
   cudaFuncSetAttribute(k_hist<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape::smem);
   cudaFuncSetAttribute(k_hist<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HistShape::smem);
-  cudaFuncSetAttribute(k_partition<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 12 * L);
-  cudaFuncSetAttribute(k_partition<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 12 * 256 * (PART_THREADS / 32));
+  cudaFuncSetAttribute(k_partition<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * L);
+  cudaFuncSetAttribute(k_partition<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * 256 * (PART_THREADS / 32));
   TC_CUDA(ctx, cudaEventCreate(&ev0));
   TC_CUDA(ctx, cudaEventCreate(&ev1));
   return configure(1, 2);  // 32-column feature groups (the only width), 2 waves before tuning
@@ -2092,10 +2043,9 @@ void tc_trainer::launch_level(const DevCfg& c, const DevPtrs& P, int d, cudaStre
   mark_begin(KC_PART, st);
   {
     const dim3 pg(c.PB, K);
-    const size_t psm = 12 * (2 << d);
-    // register sums pay a fixed per-warp reduction at the end: for 8 children
-    // they win only with enough rows per thread (measured: 4M rows 41 -> 13 us,
-    // 1M rows 15 -> 19 us)
+    const size_t psm = 4 * (2 << d);
+    // register counts pay a fixed per-warp reduction at the end: for 8
+    // children they win only with enough rows per thread
     const bool many_rows = c.n / (uint32_t)c.PB >= 16u * PART_THREADS;
     if (d == 0) k_partition<2><<<pg, PART_THREADS, psm, st>>>(c, P, d);
     else if (d == 1) k_partition<4><<<pg, PART_THREADS, psm, st>>>(c, P, d);
@@ -2104,7 +2054,7 @@ void tc_trainer::launch_level(const DevCfg& c, const DevPtrs& P, int d, cudaStre
       k_partition<-1><<<pg, PART_THREADS, psm * (PART_THREADS / 32), st>>>(c, P, d);
     else k_partition<0><<<pg, PART_THREADS, psm, st>>>(c, P, d);
   }
-  mark_end(st, (double)c.n * K * (1 + 2 + 2 + 8));
+  mark_end(st, (double)c.n * K * (1 + 2 + 2));
   if (prof) prof->back().level = d;
   mark_begin(KC_REDUCE, st);
   k_node_reduce<true><<<dim3(1 << d, K), 512, 0, st>>>(c, P, d);  // + plan of level d + 1
