@@ -336,6 +336,40 @@ def test_predict_nan_and_edges(engine):
         assert np.max(np.abs(p - fn(p64))) <= 1e-5 * (0.25 + np.abs(info_arrays["leaves"]).max(1).sum() * 0.1)
 
 
+@pytest.mark.parametrize("D,K,F", [(1, 1, 1), (4, 1, 9), (6, 1, 100), (7, 1, 1), (8, 3, 20), (10, 1, 13),
+                                   (11, 1, 7), (13, 2, 5)])
+def test_predict_tile_shapes(engine, D, K, F):
+    """Every walk of the predict kernels against FP64: trees of every depth up
+    to D (padded on the device), NaN inputs and thresholds, values on
+    thresholds, a feature with more than 127 distinct thresholds (two virtual
+    features of the binned form), request sizes around the tile (128 rows)
+    boundary, and the small-request path (at most 64 rows)."""
+    rng = np.random.default_rng(100 + D)
+    T = K * (3 if D >= 11 else 29)
+    depth = rng.integers(0, D + 1, T).astype(np.int32)
+    depth[0] = D
+    arrays = dict(depth=depth, feature=rng.integers(0, F, (T, D)).astype(np.uint16),
+                  threshold=rng.standard_normal((T, D)).astype(np.float32),
+                  leaves=rng.standard_normal((T, 1 << D)).astype(np.float32),
+                  weights=rng.uniform(0.05, 0.2, T).astype(np.float32))
+    arrays["threshold"][rng.random((T, D)) < 0.03] = np.nan  # x >= NaN is false
+    arrays["threshold"][0, 0] = 0.25
+    from turbocat import _capi
+    m = engine.import_model(_capi.ModelInfo(T, K, D, F, 1 if K > 1 else 0, -0.5, 0.1, 1.0), arrays)
+    e = O.Ensemble(-0.5, K, D, depth, arrays["feature"], np.zeros((T, D), np.uint8), arrays["threshold"],
+                   arrays["leaves"], arrays["weights"])
+    scale = 0.5 + (np.abs(arrays["leaves"]).max(1) * arrays["weights"]).sum() / K
+    X = rng.standard_normal((1000, F)).astype(np.float32)
+    X[rng.random(X.shape) < 0.08] = np.nan
+    X[1, arrays["feature"][0, 0]] = 0.25  # on a threshold: goes right
+    X[2, :] = -0.0
+    p64_all = O.predict(e, X)
+    for n in (1, 5, 32, 33, 64, 65, 127, 128, 129, 300, 1000):
+        p = m.predict(X[:n], "raw")
+        assert p.shape == (n, K)
+        assert np.max(np.abs(p - p64_all[:n])) <= 1e-5 * scale, n
+
+
 def test_bad_tcat_is_rejected(engine, capi):
     g = np.load(f"{O.HERE}/../tests/golden/c1_small.npz")
     data = g["tcat"].tobytes()

@@ -18,6 +18,7 @@ namespace tc {
 constexpr int kNanBin = 255;      // bin of NaN rows; always routed left
 constexpr int kSlots = 256;       // histogram slots per (node, feature): bins 0..254 + NaN
 constexpr int kMaxDepth = 12;     // deepest tree the trainer builds
+constexpr int kModelMaxDepth = 13;  // deepest tree a model may hold (import, TCAT, prediction)
 constexpr int kMaxClasses = 64;
 
 inline size_t round_up(size_t x, size_t m) { return (x + m - 1) / m * m; }
@@ -147,9 +148,12 @@ struct tc_model {
   std::vector<float> edges;         // [f][255]
   std::vector<uint16_t> n_edges;    // [f]
   // device copies used by the predict kernels
-  DevBuf<uint2> d_splits;           // [T][D] packed (feature | depth flags, threshold bits)
-  DevBuf<float> d_leaves;           // [T][2^D] (weights folded in)
-  DevBuf<int32_t> d_depth;          // [T]
+  DevBuf<uint2> d_splits;           // [T][D] (feature, threshold bits), padded to depth D
+  DevBuf<float> d_leaves;           // [T][2^D] (weights folded in, padded trees' leaves spread)
+  DevBuf<uint2> d_bsplits;          // binned form: [T][D] (virtual feature's column, byte-wise 128 - k)
+  DevBuf<float> d_bord;             // binned form: borders of every virtual feature, Eytzinger order
+  DevBuf<uint2> d_vdesc;            // binned form: (feature, border offset | search steps << 24)
+  int n_virtual = 0, n_bord = 0;
   tc_status upload();
 };
 
@@ -172,20 +176,32 @@ struct ReqDesc {
   int32_t transform;
 };
 struct ModelDesc {
-  const uint2* splits;
+  const uint2* splits;   // float form
   const float* leaves;
-  const int32_t* depth;
+  const uint2* bsplits;  // binned form (nullptr: the model has none)
+  const float* bord;
+  const uint2* vdesc;
   int32_t n_trees;
   int32_t max_depth;
   int32_t n_classes;
   int32_t n_features;
   float base;
-  int32_t pad[3];
+  int32_t n_virtual;
+  int32_t n_bord;
+  int32_t pad;
 };
 // Coalesced prediction over a request table: job j covers tiles
 // [tile_begin[j], tile_begin[j+1]) of PRED_ROWS rows each.
+// Launch shape of a batch: dynamic shared memory and stage sizes that fit
+// every model of the batch.
+struct PredictPlan {
+  size_t smem;
+  int leaf_stage;   // floats of one leaf stage
+  int split_stage;  // splits of one split stage
+};
+PredictPlan predict_plan(const tc_model* const* models, int n);
 tc_status predict_batched(tc_ctx* ctx, const ModelDesc* d_models, const ReqDesc* d_reqs, int n_reqs,
-                          const uint32_t* d_tile_begin, uint32_t n_tiles, int max_depth_all, int max_f,
+                          const uint32_t* d_tile_begin, uint32_t n_tiles, const PredictPlan& plan,
                           cudaStream_t stream);
 uint32_t predict_tiles(uint32_t n);
 ModelDesc model_desc(const tc_model* m);

@@ -9,16 +9,41 @@
 // sigmoid (include/turbocat/loss.hpp:99-101) or softmax
 // (src/boosting/loss.cpp:320-330) applied.
 //
-// Kernel layout: a block owns a tile of rows of one job (one request of a
-// coalesced serving batch, or the whole input of a single call).  The
-// tile's rows are staged in shared memory (row stride f+1 words, so threads
-// reading the same feature of different rows hit different banks), trees are
-// streamed through shared memory in chunks of packed (feature, threshold)
-// pairs and weight-folded leaves, two chunks in flight (cp.async: the next
-// chunk lands while the current one is walked), and every thread walks all
-// trees for its row.
+// Device model.  Every tree is padded to the model's depth D (a padding
+// split's bit is always 0; leaf l of a tree of depth d moves to l << (D - d))
+// and the tree weight is folded into the leaves.  Float form: splits are
+// (feature, threshold bits), the padding threshold NaN.  Binned form
+// (single-output models): per feature, the model's distinct thresholds sorted
+// and cut into virtual features of at most 127 borders; a row's bin on a
+// virtual feature is the number of its borders <= x (NaN: 0), and
+// x >= threshold  <=>  bin >= k, k the threshold's rank in its virtual
+// feature + 1 (the same float compare, so the leaf index is exact).  The
+// binarisation restates Dataset::apply_bins (src/core/dataset.cpp:346-379)
+// with the model's borders in place of the training edges.
+//
+// Kernel layout: a block owns a tile of 128 rows of one job (one request of a
+// coalesced serving batch, or the whole input of a single call); the tile's
+// rows are staged row-major in shared memory (odd row stride: threads reading
+// the same feature of different rows hit different banks).  Trees stream
+// through shared memory in chunks (splits and leaves, two chunks in flight:
+// cp.async, the next chunk lands while the current one is walked).
+//
+// Binned walk (models with a binned form): the tile is binarised once into a
+// byte per (virtual feature, row) (Eytzinger-ordered borders: the i-th step of
+// every search reads one of 2^i consecutive words), column-major, so the
+// 32-bit word l of a column holds rows 4l..4l+3.  Lane l of each warp owns
+// those rows; a split costs one 32-bit shared load and a byte-wise add
+// (b + 128 - k sets bit 7 exactly when b >= k: bins are at most 127) for all
+// four rows, and the level bits are gathered per byte with a shift and a mask.
+// The 8 warps walk every 8th tree (warp w: trees w, w + 8, ...) and their
+// sums are added in warp order.  Other models (multiclass, or no binned form)
+// split the block's threads as row slots x tree groups, one row per thread,
+// and add the groups' sums pairwise in a fixed order.  Which walk a tile
+// takes depends only on its model, so a request gives the same bits alone or
+// in a batch.
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstring>
 
 #include "tc_internal.h"
@@ -27,11 +52,18 @@ namespace tc {
 namespace {
 
 constexpr int PRED_ROWS = 128;
-constexpr int PRED_THREADS = 512;                 // a row tile: up to 128 rows x 4 tree groups
-constexpr int PRED_LEAF_FLOATS = 8192;      // shared floats for two chunks of leaves (2 x 16 KB)
-constexpr int PRED_LEAF_STAGE = PRED_LEAF_FLOATS / 2;
-constexpr int PRED_CHUNK = 128;             // trees per chunk at most (two chunks in flight)
+constexpr int PRED_THREADS = 256;
+constexpr int PRED_WARPS = PRED_THREADS / 32;
+constexpr int PRED_LEAF_STAGE_MIN = 4096;       // floats of one leaf stage at least (16 KB)
+constexpr int PRED_STAGED_MAX_DEPTH = 5;        // deeper trees gather their leaves from global memory (L2)
+constexpr int PRED_CHUNK = 128;                 // trees per chunk at most
 constexpr int PRED_MAX_K = 16;
+constexpr int BIN_MAX_BORDERS = 127;            // borders of one virtual feature (bins 0..127)
+constexpr int BIN_MAX_VIRTUAL = 512;            // virtual features of a binned model (column offset < 2^16)
+constexpr uint32_t kNaNBits = 0x7fc00000u;      // padding split threshold: x >= NaN is false
+
+__host__ __device__ constexpr int row_stride(int f) { return f | 1; }  // odd: conflict-free column reads
+__host__ __device__ constexpr size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void cp_async4(void* s, const void* g) {
@@ -52,60 +84,123 @@ struct JobTable {
   const ModelDesc* models;
   const uint32_t* tile_begin;  // [n_jobs + 1] first tile of each job
   int n_jobs;
-  int max_depth;               // largest model depth in the batch (shared sizing)
-  int max_f;                   // largest feature count in the batch
+  int leaf_stage;              // floats of one leaf stage
+  int split_stage;             // splits of one split stage
   ReqDesc one_req;
   ModelDesc one_model;
 };
 
 __device__ __forceinline__ float sigmoidf_ref(float x) { return 1.0f / (1.0f + expf(-x)); }
 
-// NT full-depth trees of depth DD walked together: every split is loaded
-// first, then every feature value, then the compares, so the shared-memory
-// loads of the NT trees are in flight together instead of one dependent
-// chain per level.
-template <int NT, int DD>
-__device__ __forceinline__ void walk_full(const uint2* __restrict__ s_split, const float* __restrict__ xr,
-                                          const float* __restrict__ lv, int t, int TG, float4& sum) {
-  constexpr int L = 1 << DD;
-  uint2 q[NT][DD];
+// Trees per chunk for a model of depth D (L leaves): bounded by both stages,
+// at least one tree per warp (the host sizes the stages for that).
+__device__ __forceinline__ int chunk_trees(int D, int L, int leaf_stage, int split_stage) {
+  int c = min(PRED_CHUNK, split_stage / max(1, D));
+  if (D <= PRED_STAGED_MAX_DEPTH) c = min(c, leaf_stage / L);
+  return c;
+}
+
+// 32-bit shared-memory loads (shared-window addresses: 32-bit address
+// arithmetic, no generic-to-shared conversion).
+__device__ __forceinline__ uint4 lds128(uint32_t a) {
+  uint4 v;
+  asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ uint2 lds64(uint32_t a) {
+  uint2 v;
+  asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];\n" : "=r"(v.x), "=r"(v.y) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ uint32_t lds32(uint32_t a) {
+  uint32_t v;
+  asm volatile("ld.shared.u32 %0, [%1];\n" : "=r"(v) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ float ldsf(uint32_t a) {
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1];\n" : "=f"(v) : "r"(a));
+  return v;
+}
+
+// NT binned trees (t, t + PRED_WARPS, ...) of depth D for the lane's 4 rows.
+// Splits are stored in processing order: levels 7..0, then D-1..8, so that
+// after the shifts byte i of `a` holds the first min(D, 8) levels of row i
+// with level 0 in bit 7, and byte i of `b` the levels from 8 on.  Addresses:
+// spc = the chunk's splits, sbl = this lane's word of bin column 0 (both in
+// shared memory); leaves in shared memory (lvs) or, for GL, global (lvg).
+template <int NT, int D, bool GL>
+__device__ __forceinline__ void walk_bins4(uint32_t spc, uint32_t sbl, uint32_t lvs, const float* __restrict__ lvg,
+                                           int t, float4& acc) {
+  constexpr int L = 1 << D;
+  uint2 q[NT][D];
 #pragma unroll
   for (int u = 0; u < NT; ++u) {
-    if constexpr (DD % 2 == 0) {
-      // a tree's splits start on a 16-byte boundary: two per 128-bit load
-      const uint4* sp = reinterpret_cast<const uint4*>(s_split + (t + u * TG) * DD);
+    const uint32_t sp = spc + (uint32_t)((t + u * PRED_WARPS) * D) * 8u;
+    if constexpr (D % 2 == 0) {
 #pragma unroll
-      for (int d = 0; d < DD / 2; ++d) {
-        const uint4 v = sp[d];
+      for (int d = 0; d < D / 2; ++d) {  // a tree's splits start on a 16-byte boundary
+        const uint4 v = lds128(sp + 16u * d);
         q[u][2 * d] = make_uint2(v.x, v.y);
         q[u][2 * d + 1] = make_uint2(v.z, v.w);
       }
     } else {
 #pragma unroll
-      for (int d = 0; d < DD; ++d) q[u][d] = s_split[(t + u * TG) * DD + d];
+      for (int d = 0; d < D; ++d) q[u][d] = lds64(sp + 8u * d);
     }
   }
-  float xv[NT][DD];
+  uint32_t w[NT][D];
 #pragma unroll
   for (int u = 0; u < NT; ++u)
 #pragma unroll
-    for (int d = 0; d < DD; ++d) xv[u][d] = xr[q[u][d].x];
+    for (int d = 0; d < D; ++d) w[u][d] = lds32(sbl + q[u][d].x);
 #pragma unroll
   for (int u = 0; u < NT; ++u) {
-    uint32_t idx = 0;
+    uint32_t a = 0, b = 0;
 #pragma unroll
-    for (int d = 0; d < DD; ++d)
-      if (xv[u][d] >= __uint_as_float(q[u][d].y)) idx |= 1u << (DD - 1 - d);  // false for NaN
-    const float v = lv[(t + u * TG) * L + idx];
-    if (u == 0) sum.x += v;
-    else if (u == 1) sum.y += v;
-    else if (u == 2) sum.z += v;
-    else sum.w += v;
+    for (int d = 0; d < D; ++d) {
+      const uint32_t s = w[u][d] + q[u][d].y;  // bit 7 of byte i: bin of row i >= k
+      if (d < 8) a = (a >> 1) | (s & 0x80808080u);
+      else b = (b >> 1) | (s & 0x80808080u);
+    }
+    uint32_t idx[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const uint32_t hi = (a >> (8 * i)) & 0xffu;
+      if constexpr (D <= 8) idx[i] = hi >> (8 - D);
+      else idx[i] = (hi << (D - 8)) | (((b >> (8 * i)) & 0xffu) >> (16 - D));
+    }
+    const int tt = t + u * PRED_WARPS;
+    float v[4];
+    if constexpr (GL) {
+      const float* lv = lvg + (size_t)tt * L;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) v[i] = __ldg(lv + idx[i]);
+    } else {
+      const uint32_t lv = lvs + (uint32_t)(tt * L) * 4u;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) v[i] = ldsf(lv + 4u * idx[i]);
+    }
+    acc.x += v[0];
+    acc.y += v[1];
+    acc.z += v[2];
+    acc.w += v[3];
   }
 }
 
-__global__ void __launch_bounds__(PRED_THREADS) k_predict(JobTable jt) {
-  extern __shared__ float smp[];
+// The chunk's trees of warp w: pairs while two remain (depth <= 10), then one
+// at a time; the sums go into acc in tree order either way.
+template <int D, bool GL>
+__device__ __forceinline__ void walk_chunk_bins4(uint32_t spc, uint32_t sbl, uint32_t lvs, const float* lvg, int w,
+                                                 int tn, float4& acc) {
+  int t = w;
+  if constexpr (D <= 10)
+    for (; t + PRED_WARPS < tn; t += 2 * PRED_WARPS) walk_bins4<2, D, GL>(spc, sbl, lvs, lvg, t, acc);
+  for (; t < tn; t += PRED_WARPS) walk_bins4<1, D, GL>(spc, sbl, lvs, lvg, t, acc);
+}
+
+__global__ void __launch_bounds__(PRED_THREADS, 2) k_predict(JobTable jt) {
+  extern __shared__ __align__(16) float smp[];
   ReqDesc rq;
   ModelDesc md;
   uint32_t tile;
@@ -126,133 +221,176 @@ __global__ void __launch_bounds__(PRED_THREADS) k_predict(JobTable jt) {
   }
   const uint32_t r0 = tile * PRED_ROWS;
   if (r0 >= rq.n) return;
-  const uint32_t nr = min((uint32_t)PRED_ROWS, rq.n - r0);
-  // row slots of this tile (a power of two >= nr); the block's other threads
-  // split the trees, so a small request still uses every thread
-  int RT = PRED_ROWS;
-  while (RT > 1 && (uint32_t)(RT >> 1) >= nr) RT >>= 1;
-  const int TG = PRED_THREADS / RT;
+  const int nr = (int)min((uint32_t)PRED_ROWS, rq.n - r0);
   const int f = md.n_features;
-  const int fs = f + 1;
+  // row stride: for the binned walk, rows of a feature count that is a
+  // multiple of 4 (16-byte aligned input) are staged densely by 16-byte
+  // copies; others by 4-byte copies at an odd stride (conflict-free column
+  // reads, which the float walk does once per split)
+  const bool dense = md.bsplits != nullptr && (f & 3) == 0 && (reinterpret_cast<uintptr_t>(rq.X) & 15) == 0;
+  const int fs = dense ? f : row_stride(f);
   const int D = md.max_depth;
   const int L = 1 << D;
-  // leaves of shallow trees are staged in shared memory with the splits;
-  // deeper trees (64 leaves or more) gather their leaf from global memory
-  // (L2), so a chunk still holds PRED_CHUNK trees' splits (measured on 1M
-  // rows: depth 6 is 6% faster from L2, depth 4 2% slower)
-  const bool leaves_global = L >= 64;
-  const int tchunk = leaves_global ? PRED_CHUNK : max(1, min(PRED_CHUNK, PRED_LEAF_STAGE / L));
-  const int Dmax = max(1, jt.max_depth);
-  float* s_x = smp;                                  // [PRED_ROWS][f+1]
-  float* s_leaf = s_x + PRED_ROWS * (jt.max_f + 1);  // 2 x [tchunk][L]
-  uint2* s_split = reinterpret_cast<uint2*>(s_leaf + PRED_LEAF_FLOATS);  // 2 x [tchunk][D]
-  int* s_depth = reinterpret_cast<int*>(s_split + 2 * PRED_CHUNK * Dmax);  // 2 x [tchunk]
-  // Every copy into shared memory is asynchronous (cp.async): the row tile
-  // and the first tree chunk, then chunk c + 1 while chunk c is walked.
-  const float* Xt = rq.X + (size_t)r0 * f;
-  // a warp copies whole rows (lane = feature), no division by f
-  for (uint32_t i = threadIdx.x >> 5; i < nr; i += blockDim.x >> 5)
-    for (int j = threadIdx.x & 31; j < f; j += 32) cp_async4(&s_x[i * fs + j], &Xt[(size_t)i * f + j]);
+  const int K = md.n_classes;
+  const int LS = jt.leaf_stage, SS = jt.split_stage;
+  const bool leaves_global = D > PRED_STAGED_MAX_DEPTH;
+  const int tchunk = chunk_trees(D, L, LS, SS);
+  const bool binned = md.bsplits != nullptr;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // Regions.  Binned: [bins V x 128 B][borders][virtual features][U]; the
+  // row tile lives in U until the tile is binarised, then U holds the
+  // stages.  Float: [row tile][stages].
+  char* base = reinterpret_cast<char*>(smp);
+  const int V = md.n_virtual;
+  uint8_t* s_bins = reinterpret_cast<uint8_t*>(base);
+  float* s_bord = reinterpret_cast<float*>(base + align16((size_t)V * PRED_ROWS));
+  uint2* s_vd = reinterpret_cast<uint2*>(reinterpret_cast<char*>(s_bord) + align16((size_t)md.n_bord * 4));
+  char* U = binned ? reinterpret_cast<char*>(s_vd) + align16((size_t)V * 8) : base;
+  float* s_x = reinterpret_cast<float*>(U);                      // [128][fs]
+  char* stages = binned ? U : U + align16((size_t)PRED_ROWS * fs * 4);
+  float* s_leaf = reinterpret_cast<float*>(stages);              // 2 x [LS]
+  uint2* s_split = reinterpret_cast<uint2*>(s_leaf + 2 * (size_t)LS);  // 2 x [SS]
+  // the tile's rows: one contiguous range of nr x f floats
+  {
+    const float* Xt = rq.X + (size_t)r0 * f;
+    if (dense) {
+      for (int q = threadIdx.x; q < nr * (f >> 2); q += PRED_THREADS) cp_async16(s_x + 4 * q, Xt + 4 * q);
+    } else {
+      for (int i = warp; i < nr; i += PRED_WARPS)  // a warp copies whole rows, lane = feature
+        for (int j = lane; j < f; j += 32) cp_async4(&s_x[i * fs + j], &Xt[(size_t)i * f + j]);
+    }
+  }
+  const uint2* gsplits = binned ? md.bsplits : md.splits;
   auto issue_chunk = [&](int t0, int buf) {
     const int tn = min(tchunk, md.n_trees - t0);
     if (!leaves_global) {
-      float* dl = s_leaf + buf * PRED_LEAF_STAGE;
+      float* dl = s_leaf + buf * LS;
       const float* gl = md.leaves + (size_t)t0 * L;
       const int cnt = tn * L;
-      if ((((size_t)t0 * L) & 3) == 0 && (cnt & 3) == 0) {
-        for (int q = threadIdx.x; q < cnt / 4; q += blockDim.x) cp_async16(dl + 4 * q, gl + 4 * q);
+      if (L >= 4) {
+        for (int q = threadIdx.x; q < cnt / 4; q += PRED_THREADS) cp_async16(dl + 4 * q, gl + 4 * q);
       } else {
-        for (int q = threadIdx.x; q < cnt; q += blockDim.x) cp_async4(dl + q, gl + q);
+        for (int q = threadIdx.x; q < cnt; q += PRED_THREADS) cp_async4(dl + q, gl + q);
       }
     }
-    uint2* ds = s_split + buf * PRED_CHUNK * Dmax;
-    for (int q = threadIdx.x; q < tn * D; q += blockDim.x) cp_async8(ds + q, md.splits + (size_t)t0 * D + q);
-    int* dd = s_depth + buf * PRED_CHUNK;
-    for (int q = threadIdx.x; q < tn; q += blockDim.x) cp_async4(dd + q, md.depth + t0 + q);
+    uint2* ds = s_split + buf * SS;
+    for (int q = threadIdx.x; q < tn * D; q += PRED_THREADS) cp_async8(ds + q, gsplits + (size_t)t0 * D + q);
   };
+  if (binned) {
+    // borders and virtual features (16-byte copies: both arrays are padded
+    // to whole 16-byte units on the device)
+    for (int q = threadIdx.x; q < (md.n_bord + 3) / 4; q += PRED_THREADS) cp_async16(s_bord + 4 * q, md.bord + 4 * q);
+    for (int q = threadIdx.x; q < (V + 1) / 2; q += PRED_THREADS) cp_async16(s_vd + 2 * q, md.vdesc + 2 * q);
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    // binarise: warp w takes virtual features w, w + 8, ...; lane l rows
+    // l, l + 32, l + 64, l + 96 (rows past the tile's last get bin 0)
+    for (int v = warp; v < V; v += PRED_WARPS) {
+      const uint2 vd = s_vd[v];
+      const float* bt = s_bord + (vd.y & 0xffffffu);
+      const int h = (int)(vd.y >> 24);
+      float x[4];
+      uint32_t nd[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int r = lane + 32 * i;
+        x[i] = r < nr ? s_x[r * fs + vd.x] : 0.0f;
+        nd[i] = 0;
+      }
+      for (int s = 0; s < h; ++s)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) nd[i] = 2 * nd[i] + 1 + (uint32_t)(bt[nd[i]] <= x[i]);  // NaN: false
+      const uint32_t first_leaf = (1u << h) - 1;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int r = lane + 32 * i;
+        s_bins[v * PRED_ROWS + r] = r < nr ? (uint8_t)(nd[i] - first_leaf) : (uint8_t)0;
+      }
+    }
+    __syncthreads();  // the bins are complete and the row tile's space is free for the stages
+  }
   if (md.n_trees > 0) issue_chunk(0, 0);
   cp_async_commit();
-  const int K = md.n_classes;
+  // binned walk state
+  float4 acc4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const uint32_t sbl = smem_addr(s_bins) + 4u * lane;
+  // per-row walk state: row slots (a power of two >= nr) x tree groups
+  int RT = PRED_ROWS;
+  while (RT > 1 && (RT >> 1) >= nr) RT >>= 1;
+  const int TG = PRED_THREADS / RT;
+  const int row = threadIdx.x % RT, tg = threadIdx.x / RT;
+  const float* xr = s_x + row * fs;
   float acc[PRED_MAX_K];
 #pragma unroll
   for (int k = 0; k < PRED_MAX_K; ++k) acc[k] = 0.0f;
-  const int row = threadIdx.x % RT;
-  const int tg = threadIdx.x / RT;
-  const float* xr = s_x + row * fs;
   for (int t0 = 0, buf = 0; t0 < md.n_trees; t0 += tchunk, buf ^= 1) {
     const int tn = min(tchunk, md.n_trees - t0);
     if (t0 + tchunk < md.n_trees) issue_chunk(t0 + tchunk, buf ^ 1);
     cp_async_commit();
-    cp_async_wait_prev();  // this thread's copies of the row tile and of chunk t0 have landed
-    const float* lv = leaves_global ? md.leaves + (size_t)t0 * L : s_leaf + buf * PRED_LEAF_STAGE;
-    const uint2* s_split_c = s_split + buf * PRED_CHUNK * Dmax;
-    const int* s_depth_c = s_depth + buf * PRED_CHUNK;
-    bool full_here = true;
-    for (int q = threadIdx.x; q < tn; q += blockDim.x) full_here = full_here && s_depth_c[q] == D;
-    // the barrier also publishes every thread's copies; every tree of the chunk has depth D?
-    const bool all_full = __syncthreads_and(full_here) != 0;
-    if ((uint32_t)row < nr) {
-      if (K == 1) {
-        // full-depth trees in groups (depth <= 8: 4 at a time, 9-10: 2),
-        // partial sums combined in a fixed order; other trees one by one
-        float4 s4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        int t = tg;
-        const int NT = D <= 8 ? 4 : 2;
-        if (D <= 10) {
-          for (; t + (NT - 1) * TG < tn; t += NT * TG) {
-            if (!all_full) {
-              bool full = true;
-              for (int u = 0; u < NT; ++u) full = full && s_depth_c[t + u * TG] == D;
-              if (!full) break;
-            }
-            switch (D) {
-              case 1: walk_full<4, 1>(s_split_c, xr, lv, t, TG, s4); break;
-              case 2: walk_full<4, 2>(s_split_c, xr, lv, t, TG, s4); break;
-              case 3: walk_full<4, 3>(s_split_c, xr, lv, t, TG, s4); break;
-              case 4: walk_full<4, 4>(s_split_c, xr, lv, t, TG, s4); break;
-              case 5: walk_full<4, 5>(s_split_c, xr, lv, t, TG, s4); break;
-              case 6: walk_full<4, 6>(s_split_c, xr, lv, t, TG, s4); break;
-              case 7: walk_full<4, 7>(s_split_c, xr, lv, t, TG, s4); break;
-              case 8: walk_full<4, 8>(s_split_c, xr, lv, t, TG, s4); break;
-              case 9: walk_full<2, 9>(s_split_c, xr, lv, t, TG, s4); break;
-              default: walk_full<2, 10>(s_split_c, xr, lv, t, TG, s4); break;
-            }
-          }
-        }
-        for (; t < tn; t += TG) {
-          const int dep = s_depth_c[t];
-          const uint2* sp = s_split_c + t * D;
-          uint32_t idx = 0;
-          for (int d = 0; d < dep; ++d) {
-            const uint2 q = sp[d];
-            idx = (idx << 1) | (uint32_t)(xr[q.x] >= __uint_as_float(q.y));  // false for NaN
-          }
-          s4.x += lv[t * L + idx];
-        }
-        acc[0] += (s4.x + s4.y) + (s4.z + s4.w);
-      } else {
-        for (int t = tg; t < tn; t += TG) {
-          const int dep = s_depth_c[t];
-          const uint2* sp = s_split_c + t * D;
-          uint32_t idx = 0;
-          for (int d = 0; d < dep; ++d) {
-            const uint2 q = sp[d];
-            idx = (idx << 1) | (uint32_t)(xr[q.x] >= __uint_as_float(q.y));
-          }
-          const int cls = (t0 + t) % K;
-          const float v = lv[t * L + idx];
+    cp_async_wait_prev();  // this thread's copies of the tile and of chunk t0 have landed
+    __syncthreads();       // ... and everybody's
+    const float* lvc = leaves_global ? md.leaves + (size_t)t0 * L : s_leaf + buf * LS;
+    const uint2* spc = s_split + buf * SS;
+    if (binned) {
+      const uint32_t spa = smem_addr(spc), lva = smem_addr(leaves_global ? s_leaf : lvc);
+      switch (D) {
+        case 1: walk_chunk_bins4<1, false>(spa, sbl, lva, lvc, warp, tn, acc4); break;
+        case 2: walk_chunk_bins4<2, false>(spa, sbl, lva, lvc, warp, tn, acc4); break;
+        case 3: walk_chunk_bins4<3, false>(spa, sbl, lva, lvc, warp, tn, acc4); break;
+        case 4: walk_chunk_bins4<4, false>(spa, sbl, lva, lvc, warp, tn, acc4); break;
+        case 5: walk_chunk_bins4<5, false>(spa, sbl, lva, lvc, warp, tn, acc4); break;
+        case 6: walk_chunk_bins4<6, true>(spa, sbl, lva, lvc, warp, tn, acc4); break;
+        case 7: walk_chunk_bins4<7, true>(spa, sbl, lva, lvc, warp, tn, acc4); break;
+        case 8: walk_chunk_bins4<8, true>(spa, sbl, lva, lvc, warp, tn, acc4); break;
+        case 9: walk_chunk_bins4<9, true>(spa, sbl, lva, lvc, warp, tn, acc4); break;
+        case 10: walk_chunk_bins4<10, true>(spa, sbl, lva, lvc, warp, tn, acc4); break;
+        case 11: walk_chunk_bins4<11, true>(spa, sbl, lva, lvc, warp, tn, acc4); break;
+        case 12: walk_chunk_bins4<12, true>(spa, sbl, lva, lvc, warp, tn, acc4); break;
+        default: walk_chunk_bins4<13, true>(spa, sbl, lva, lvc, warp, tn, acc4); break;
+      }
+    } else if (row < nr) {
+      for (int t = tg; t < tn; t += TG) {
+        const uint2* sp = spc + t * D;
+        uint2 q[kModelMaxDepth];
 #pragma unroll
-          for (int k = 0; k < PRED_MAX_K; ++k)
-            if (k == cls) acc[k] += v;
-        }
+        for (int d = 0; d < kModelMaxDepth; ++d)
+          if (d < D) q[d] = sp[d];
+        float xv[kModelMaxDepth];
+#pragma unroll
+        for (int d = 0; d < kModelMaxDepth; ++d)
+          if (d < D) xv[d] = xr[q[d].x];
+        uint32_t idx = 0;
+#pragma unroll
+        for (int d = 0; d < kModelMaxDepth; ++d)
+          if (d < D) idx = idx + idx + (uint32_t)(xv[d] >= __uint_as_float(q[d].y));  // false for NaN
+        const float v = lvc[(size_t)t * L + idx];
+        const int cls = K == 1 ? 0 : (t0 + t) % K;
+#pragma unroll
+        for (int k = 0; k < PRED_MAX_K; ++k)
+          if (k == cls) acc[k] += v;
       }
     }
     __syncthreads();  // chunk t0's buffers are refilled by the next iteration's copies
   }
   cp_async_wait_all();
-  // combine the thread groups' partial sums (pairwise, fixed order)
   __syncthreads();
-  float* s_red = s_leaf;  // [TG][RT][K]: TG*RT = PRED_THREADS, 512*16 floats = PRED_LEAF_FLOATS
+  float* s_red = s_leaf;  // at least 2 x 4096 floats
+  float* o = rq.out + (size_t)r0 * K;
+  if (binned) {
+    // [warp][128 rows]; row sums in warp order
+    *reinterpret_cast<float4*>(&s_red[warp * PRED_ROWS + 4 * lane]) = acc4;
+    __syncthreads();
+    if (threadIdx.x >= nr) return;
+    const int r = threadIdx.x;
+    float s = s_red[r];
+#pragma unroll
+    for (int w = 1; w < PRED_WARPS; ++w) s += s_red[w * PRED_ROWS + r];
+    const float raw = s + md.base;
+    o[r] = (rq.transform == TC_TRANSFORM_SIGMOID) ? sigmoidf_ref(raw) : raw;
+    return;
+  }
+  // [TG][RT][K] (TG*RT = PRED_THREADS, 256 x 16 floats <= one leaf stage)
 #pragma unroll
   for (int k = 0; k < PRED_MAX_K; ++k)
     if (k < K) s_red[(tg * RT + row) * K + k] = acc[k];
@@ -263,14 +401,16 @@ __global__ void __launch_bounds__(PRED_THREADS) k_predict(JobTable jt) {
     }
     __syncthreads();
   }
-  if (tg != 0 || (uint32_t)row >= nr) return;
+  if (tg != 0 || row >= nr) return;
 #pragma unroll
   for (int k = 0; k < PRED_MAX_K; ++k)
     if (k < K) acc[k] = s_red[row * K + k];
-  float* o = rq.out + (size_t)(r0 + row) * K;
+  o += (size_t)row * K;
   if (rq.transform == TC_TRANSFORM_SOFTMAX && K > 1) {
     float mx = -INFINITY;
-    for (int k = 0; k < K; ++k) mx = fmaxf(mx, acc[k] + md.base);
+#pragma unroll
+    for (int k = 0; k < PRED_MAX_K; ++k)
+      if (k < K) mx = fmaxf(mx, acc[k] + md.base);
     float sum = 0.0f;
     float e[PRED_MAX_K];
 #pragma unroll
@@ -338,19 +478,17 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_predict_small(ModelDesc md, c
   if ((uint32_t)row < n) {
     const float* xr = s_x + row * fs;
     for (int t = t0 + tg; t < t1; t += TG) {
-      // the tree's depth and every split are loaded before any compare (one
-      // round trip to L2 instead of one per level); a shallower tree ignores
-      // its padding splits
+      // every split is loaded before any compare (one round trip to L2
+      // instead of one per level); padding splits give 0 bits
       const uint2* sp = md.splits + (size_t)t * D;
-      uint2 q[kMaxDepth];
+      uint2 q[kModelMaxDepth];
 #pragma unroll
-      for (int d = 0; d < kMaxDepth; ++d)
+      for (int d = 0; d < kModelMaxDepth; ++d)
         if (d < D) q[d] = sp[d];
-      const int dep = md.depth[t];
       uint32_t idx = 0;
 #pragma unroll
-      for (int d = 0; d < kMaxDepth; ++d)
-        if (d < dep) idx = (idx << 1) | (uint32_t)(xr[q[d].x] >= __uint_as_float(q[d].y));  // false for NaN
+      for (int d = 0; d < kModelMaxDepth; ++d)
+        if (d < D) idx = idx + idx + (uint32_t)(xr[q[d].x] >= __uint_as_float(q[d].y));  // false for NaN
       const float v = md.leaves[(size_t)t * L + idx];
       const int cls = K == 1 ? 0 : t % K;
 #pragma unroll
@@ -391,7 +529,9 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_predict_small(ModelDesc md, c
     float* o = out + (size_t)r * K;
     if (transform == TC_TRANSFORM_SOFTMAX && K > 1) {
       float mx = -INFINITY;
-      for (int k = 0; k < K; ++k) mx = fmaxf(mx, v[k] + md.base);
+#pragma unroll
+      for (int k = 0; k < PRED_MAX_K; ++k)
+        if (k < K) mx = fmaxf(mx, v[k] + md.base);
       float sum = 0.0f, e[PRED_MAX_K];
 #pragma unroll
       for (int k = 0; k < PRED_MAX_K; ++k)
@@ -412,22 +552,49 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_predict_small(ModelDesc md, c
   if (NB > 1 && threadIdx.x == 0) *counter = 0u;  // re-armed for the next call
 }
 
-size_t predict_smem(int max_f, int max_depth) {
-  return (size_t)PRED_ROWS * (max_f + 1) * 4 + PRED_LEAF_FLOATS * 4 +
-         (size_t)2 * PRED_CHUNK * std::max(1, max_depth) * 8 + 2 * PRED_CHUNK * 4;
+// Stage sizes for a batch whose deepest model has depth max_depth: a leaf
+// stage holds at least one tree per warp (16 KB at least); a split stage
+// holds the splits of as many trees as the leaf stage takes, for every depth
+// up to max_depth.
+void stage_sizes(int max_depth, int* leaf_stage, int* split_stage) {
+  const int Ls = 1 << std::min(std::max(max_depth, 0), PRED_STAGED_MAX_DEPTH);
+  const int LS = std::max(PRED_LEAF_STAGE_MIN, PRED_WARPS * Ls);
+  int SS = PRED_WARPS;
+  for (int d = 1; d <= max_depth; ++d) {
+    const int trees = d <= PRED_STAGED_MAX_DEPTH ? std::min(PRED_CHUNK, LS >> d) : PRED_CHUNK;
+    SS = std::max(SS, trees * d);
+  }
+  *leaf_stage = LS;
+  *split_stage = (SS + 1) & ~1;  // whole 16-byte pairs
 }
 
-tc_status launch_predict(tc_ctx* ctx, const JobTable& jt, uint32_t n_tiles, cudaStream_t stream) {
+// Shared memory of one model's tiles (the larger of its two layouts).
+size_t model_smem(int n_features, int n_virtual, int n_bord, bool binned, int leaf_stage, int split_stage) {
+  const size_t S = (size_t)2 * leaf_stage * 4 + (size_t)2 * split_stage * 8;
+  const size_t T = align16((size_t)PRED_ROWS * row_stride(n_features) * 4);
+  size_t need = T + S;
+  if (binned) {
+    const size_t X = align16((size_t)n_virtual * PRED_ROWS) + align16((size_t)n_bord * 4) + align16((size_t)n_virtual * 8);
+    need = std::max(need, X + std::max(T, S));
+  }
+  return need;
+}
+
+constexpr size_t PRED_SMEM_MAX = 220 * 1024;
+
+tc_status launch_predict(tc_ctx* ctx, JobTable& jt, const PredictPlan& plan, uint32_t n_tiles, cudaStream_t stream) {
   if (n_tiles == 0) return TC_OK;
-  const size_t smem = predict_smem(jt.max_f, jt.max_depth);
+  jt.leaf_stage = plan.leaf_stage;
+  jt.split_stage = plan.split_stage;
   static bool attr_done = false;
   if (!attr_done) {
-    cudaFuncSetAttribute(k_predict, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_predict, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PRED_SMEM_MAX);
     attr_done = true;
   }
-  if (smem > 200 * 1024)
-    return ctx->fail(TC_ERR_INVALID_ARG, "too many features for the predict kernel (%d)", jt.max_f);
-  k_predict<<<n_tiles, PRED_THREADS, smem, stream>>>(jt);
+  if (plan.smem > PRED_SMEM_MAX)
+    return ctx->fail(TC_ERR_INVALID_ARG, "the model's features do not fit the predict kernel's row tile (%zu bytes)",
+                     plan.smem);
+  k_predict<<<n_tiles, PRED_THREADS, plan.smem, stream>>>(jt);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return ctx->cuda_fail(e, "k_predict");
   return TC_OK;
@@ -435,17 +602,28 @@ tc_status launch_predict(tc_ctx* ctx, const JobTable& jt, uint32_t n_tiles, cuda
 
 }  // namespace
 
+PredictPlan predict_plan(const tc_model* const* models, int n) {
+  int max_depth = 0;
+  for (int i = 0; i < n; ++i) max_depth = std::max(max_depth, models[i]->info.max_depth);
+  PredictPlan p{};
+  stage_sizes(max_depth, &p.leaf_stage, &p.split_stage);
+  for (int i = 0; i < n; ++i) {
+    const tc_model* m = models[i];
+    p.smem = std::max(p.smem, model_smem(m->info.n_features, m->n_virtual, m->n_bord, m->d_bsplits.p != nullptr,
+                                         p.leaf_stage, p.split_stage));
+  }
+  return p;
+}
+
 tc_status predict_batched(tc_ctx* ctx, const ModelDesc* d_models, const ReqDesc* d_reqs, int n_reqs,
-                          const uint32_t* d_tile_begin, uint32_t n_tiles, int max_depth_all, int max_f,
+                          const uint32_t* d_tile_begin, uint32_t n_tiles, const PredictPlan& plan,
                           cudaStream_t stream) {
   JobTable jt{};
   jt.reqs = d_reqs;
   jt.models = d_models;
   jt.tile_begin = d_tile_begin;
   jt.n_jobs = n_reqs;
-  jt.max_depth = max_depth_all;
-  jt.max_f = max_f;
-  return launch_predict(ctx, jt, n_tiles, stream);
+  return launch_predict(ctx, jt, plan, n_tiles, stream);
 }
 
 uint32_t predict_tiles(uint32_t n) { return (n + PRED_ROWS - 1) / PRED_ROWS; }
@@ -454,26 +632,118 @@ uint32_t predict_tiles(uint32_t n) { return (n + PRED_ROWS - 1) / PRED_ROWS; }
 
 using namespace tc;
 
-// Packs splits as (feature, threshold bits) and folds the tree weights into
-// the leaves (w * leaf in FP32, the product the reference forms per tree).
+namespace {
+
+// Fills t[0 .. n) (n = 2^h - 1) with vals in Eytzinger (breadth-first) order:
+// an in-order walk of the implicit tree visits vals in sorted order.
+void eytzinger_fill(const std::vector<float>& vals, std::vector<float>& t, size_t base, size_t n, size_t i,
+                    size_t& next) {
+  if (i >= n) return;
+  eytzinger_fill(vals, t, base, n, 2 * i + 1, next);
+  t[base + i] = next < vals.size() ? vals[next] : std::nanf("");
+  ++next;
+  eytzinger_fill(vals, t, base, n, 2 * i + 2, next);
+}
+
+}  // namespace
+
+// The device model: every tree padded to the model's depth (padding splits:
+// feature 0 against a NaN threshold, whose bit is always 0; leaf l of a tree
+// of depth d moves to l << (D - d)), the tree weights folded into the leaves
+// (w * leaf in FP32, the product the reference forms per tree), the float
+// splits (feature, threshold bits) and, for single-output models, the binned
+// form (virtual features, Eytzinger-ordered borders, binned splits).
 tc_status tc_model::upload() {
-  const int T = info.n_trees, D = info.max_depth, L = 1 << D;
+  const int T = info.n_trees, D = info.max_depth, L = 1 << D, F = info.n_features;
   std::vector<uint2> sp((size_t)std::max(1, T * D));
-  std::vector<float> lv((size_t)std::max(1, T * L));
+  std::vector<float> lv((size_t)std::max(1, T * L), 0.0f);
   for (int t = 0; t < T; ++t) {
+    const int dt = depth[t];
     for (int d = 0; d < D; ++d) {
-      uint32_t bits;
-      std::memcpy(&bits, &threshold[(size_t)t * D + d], 4);
-      sp[(size_t)t * D + d] = make_uint2(feature[(size_t)t * D + d], bits);
+      uint32_t bits = kNaNBits, j = 0;
+      if (d < dt) {
+        std::memcpy(&bits, &threshold[(size_t)t * D + d], 4);
+        j = feature[(size_t)t * D + d];
+      }
+      sp[(size_t)t * D + d] = make_uint2(j, bits);
     }
-    for (int l = 0; l < L; ++l) lv[(size_t)t * L + l] = weights[t] * leaves[(size_t)t * L + l];
+    for (int l = 0; l < (1 << dt); ++l) lv[(size_t)t * L + ((size_t)l << (D - dt))] = weights[t] * leaves[(size_t)t * L + l];
   }
   TC_TRY(d_splits.alloc(ctx, sp.size(), "model splits"));
   TC_TRY(d_leaves.alloc(ctx, lv.size(), "model leaves"));
-  TC_TRY(d_depth.alloc(ctx, std::max(1, T), "model depths"));
   TC_CUDA(ctx, cudaMemcpy(d_splits.p, sp.data(), sp.size() * sizeof(uint2), cudaMemcpyHostToDevice));
   TC_CUDA(ctx, cudaMemcpy(d_leaves.p, lv.data(), lv.size() * sizeof(float), cudaMemcpyHostToDevice));
-  if (T > 0) TC_CUDA(ctx, cudaMemcpy(d_depth.p, depth.data(), T * sizeof(int32_t), cudaMemcpyHostToDevice));
+  if (info.n_classes != 1 || D < 1) return TC_OK;
+  // binned form: distinct thresholds per feature (-0.0 and +0.0 are one)
+  std::vector<std::vector<float>> u((size_t)F);
+  for (int t = 0; t < T; ++t)
+    for (int d = 0; d < depth[t]; ++d) {
+      const float th = threshold[(size_t)t * D + d];
+      if (!std::isnan(th)) u[feature[(size_t)t * D + d]].push_back(th);
+    }
+  struct VF { int j, start, cnt; };
+  std::vector<VF> vf;
+  std::vector<int> first_v((size_t)F, -1);
+  for (int j = 0; j < F; ++j) {
+    auto& a = u[j];
+    std::sort(a.begin(), a.end());
+    a.erase(std::unique(a.begin(), a.end(), [](float x, float y) { return x == y; }), a.end());
+    for (int s0 = 0; s0 < (int)a.size(); s0 += BIN_MAX_BORDERS) {
+      if (first_v[j] < 0) first_v[j] = (int)vf.size();
+      vf.push_back({j, s0, std::min(BIN_MAX_BORDERS, (int)a.size() - s0)});
+    }
+  }
+  if (vf.empty()) vf.push_back({0, 0, 0});  // padding splits read virtual feature 0
+  if ((int)vf.size() > BIN_MAX_VIRTUAL) return TC_OK;  // served by the float walk
+  std::vector<float> bord;
+  std::vector<uint2> vd;
+  for (const VF& v : vf) {
+    int h = 0;
+    while ((1 << h) - 1 < v.cnt) ++h;
+    const size_t n = ((size_t)1 << h) - 1, off = bord.size();
+    if (off + n >= ((size_t)1 << 24)) return TC_OK;
+    bord.resize(off + n);
+    std::vector<float> vals;
+    if (v.cnt) vals.assign(u[v.j].begin() + v.start, u[v.j].begin() + v.start + v.cnt);
+    size_t next = 0;
+    eytzinger_fill(vals, bord, off, n, 0, next);
+    vd.push_back(make_uint2((uint32_t)v.j, (uint32_t)off | ((uint32_t)h << 24)));
+  }
+  const int V = (int)vd.size(), B = (int)bord.size();
+  {
+    int LS, SS;
+    stage_sizes(D, &LS, &SS);
+    if (model_smem(F, V, B, true, LS, SS) > PRED_SMEM_MAX) return TC_OK;  // served by the float walk
+  }
+  while (bord.size() % 4) bord.push_back(std::nanf(""));  // whole 16-byte copies
+  if (vd.size() % 2) vd.push_back(make_uint2(0, 0));
+  // binned splits in processing order: levels min(D,8)-1 .. 0, then D-1 .. 8
+  std::vector<uint2> bs((size_t)T * D);
+  for (int t = 0; t < T; ++t) {
+    for (int p = 0; p < D; ++p) {
+      const int lev = D <= 8 ? D - 1 - p : (p < 8 ? 7 - p : D - 1 - (p - 8));
+      uint2 q = make_uint2(0, 0);  // padding: k = 128, never reached by a bin
+      if (lev < depth[t]) {
+        const float th = threshold[(size_t)t * D + lev];
+        if (!std::isnan(th)) {
+          const int j = feature[(size_t)t * D + lev];
+          const int r = (int)(std::lower_bound(u[j].begin(), u[j].end(), th) - u[j].begin());
+          const int v = first_v[j] + r / BIN_MAX_BORDERS, k = r % BIN_MAX_BORDERS + 1;
+          q = make_uint2((uint32_t)v * PRED_ROWS, (uint32_t)(128 - k) * 0x01010101u);
+        }
+      }
+      bs[(size_t)t * D + p] = q;
+    }
+  }
+  TC_TRY(d_bsplits.alloc(ctx, std::max<size_t>(1, bs.size()), "binned model splits"));
+  TC_TRY(d_bord.alloc(ctx, bord.size(), "model borders"));
+  TC_TRY(d_vdesc.alloc(ctx, vd.size(), "model virtual features"));
+  if (!bs.empty())
+    TC_CUDA(ctx, cudaMemcpy(d_bsplits.p, bs.data(), bs.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+  TC_CUDA(ctx, cudaMemcpy(d_bord.p, bord.data(), bord.size() * sizeof(float), cudaMemcpyHostToDevice));
+  TC_CUDA(ctx, cudaMemcpy(d_vdesc.p, vd.data(), vd.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+  n_virtual = V;
+  n_bord = B;
   return TC_OK;
 }
 
@@ -483,7 +753,11 @@ ModelDesc model_desc(const tc_model* m) {
   ModelDesc d{};
   d.splits = m->d_splits.p;
   d.leaves = m->d_leaves.p;
-  d.depth = m->d_depth.p;
+  d.bsplits = m->d_bsplits.p;
+  d.bord = m->d_bord.p;
+  d.vdesc = m->d_vdesc.p;
+  d.n_virtual = m->n_virtual;
+  d.n_bord = m->n_bord;
   d.n_trees = m->info.n_trees;
   d.max_depth = m->info.max_depth;
   d.n_classes = m->info.n_classes;
@@ -495,14 +769,13 @@ ModelDesc model_desc(const tc_model* m) {
 tc_status predict_device(tc_ctx* ctx, const tc_model* m, const float* X, uint32_t n, uint32_t f, int transform,
                          float* out, cudaStream_t stream) {
   if (n == 0) return TC_OK;
+  (void)f;
   JobTable jt{};
   jt.reqs = nullptr;
   jt.n_jobs = 1;
-  jt.max_depth = m->info.max_depth;
-  jt.max_f = (int)f;
   jt.one_model = model_desc(m);
   jt.one_req = ReqDesc{X, out, n, 0, 0, transform};
-  return launch_predict(ctx, jt, predict_tiles(n), stream);
+  return launch_predict(ctx, jt, predict_plan(&m, 1), predict_tiles(n), stream);
 }
 
 }  // namespace tc
@@ -570,7 +843,7 @@ tc_status tc_model_import(tc_ctx* ctx, const tc_model_info* info, const int32_t*
   if (!ctx || !info || !out) return TC_ERR_INVALID_ARG;
   *out = nullptr;
   const int T = info->n_trees, D = info->max_depth, L = 1 << (D > 0 ? D : 0);
-  if (T < 0 || D < 0 || D > 13 || info->n_classes < 1 || info->n_classes > 16 || info->n_features < 1)
+  if (T < 0 || D < 0 || D > kModelMaxDepth || info->n_classes < 1 || info->n_classes > 16 || info->n_features < 1)
     return ctx->fail(TC_ERR_INVALID_ARG, "invalid model shape (trees %d, depth %d, classes %d, features %d)", T, D,
                      info->n_classes, info->n_features);
   if (T > 0 && (!depth || !feature || !threshold || !leaves))
@@ -689,7 +962,7 @@ tc_status tc_model_load_tcat(tc_ctx* ctx, const uint8_t* buf, size_t len, tc_mod
   const uint8_t sym = r.get<uint8_t>();
   if (!r.ok) return ctx->fail(TC_ERR_FORMAT, "truncated TCAT header");
   if (!sym) return ctx->fail(TC_ERR_FORMAT, "TCAT model holds regular trees; only symmetric trees are served");
-  if (info.max_depth > 16) return ctx->fail(TC_ERR_FORMAT, "TCAT max_depth %d too large", info.max_depth);
+  if (info.max_depth > kModelMaxDepth) return ctx->fail(TC_ERR_FORMAT, "TCAT max_depth %d too large", info.max_depth);
   info.n_classes = info.task == TC_TASK_MULTICLASS ? (int)ncls : 1;
   if (info.n_classes < 1 || info.n_classes > 16) return ctx->fail(TC_ERR_FORMAT, "TCAT class count %u", ncls);
   const uint64_t nf = r.get<uint64_t>();

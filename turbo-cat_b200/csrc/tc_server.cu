@@ -70,6 +70,7 @@ struct tc_server {
   int req_cap = 1024;
   int max_f = 0;
   int max_depth = 0;
+  PredictPlan plan{};
   std::vector<std::unique_ptr<Slot>> slots;
   std::vector<ModelDesc> models;
   std::vector<const tc_model*> model_ptrs;
@@ -120,7 +121,7 @@ bool tc_server::launch(Slot& s, std::vector<Request*>& batch) {
   s.h_tiles[j] = tile;
   cudaMemcpyAsync(s.d_reqs.p, s.h_reqs, j * sizeof(ReqDesc), cudaMemcpyHostToDevice, s.stream);
   cudaMemcpyAsync(s.d_tiles.p, s.h_tiles, (j + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, s.stream);
-  if (predict_batched(ctx, d_models.p, s.d_reqs.p, j, s.d_tiles.p, tile, max_depth, max_f, s.stream) != TC_OK)
+  if (predict_batched(ctx, d_models.p, s.d_reqs.p, j, s.d_tiles.p, tile, plan, s.stream) != TC_OK)
     return false;
   for (int q = 0; q < j; ++q) {
     Request* r = batch[q];
@@ -272,6 +273,7 @@ tc_status tc_server_add_model(tc_server* s, const tc_model* m, int32_t* model_id
   s->model_ptrs.push_back(m);
   s->max_f = std::max(s->max_f, m->info.n_features);
   s->max_depth = std::max(s->max_depth, m->info.max_depth);
+  s->plan = predict_plan(s->model_ptrs.data(), (int)s->model_ptrs.size());
   TC_CUDA(ctx, cudaMemcpy(s->d_models.p, s->models.data(), s->models.size() * sizeof(ModelDesc),
                           cudaMemcpyHostToDevice));
   *model_id = (int32_t)s->models.size() - 1;
