@@ -93,6 +93,12 @@ void tc_dataset_destroy(tc_dataset* ds);
  * optional host outputs. */
 tc_status tc_quantize(tc_dataset* ds, uint16_t max_bins, int compat_uint8_count, float* edges_out,
                       uint16_t* n_edges_out);
+/* Bins ds with the edges of ref (a quantized dataset of the same context and
+ * feature count): bin = number of ref's edges <= x, NaN -> 255, the same
+ * assignment tc_quantize makes; ds can then be trained on or exported like a
+ * quantized dataset.  Replaces Dataset::apply_bins (src/core/dataset.cpp:346-379)
+ * for numeric features. */
+tc_status tc_apply_bins(tc_dataset* ds, const tc_dataset* ref);
 /* Host copy of the binned matrix, column-major [f][n]
  * (BinnedData::column, include/turbocat/dataset.hpp:27-82). */
 tc_status tc_dataset_bins(const tc_dataset* ds, uint8_t* bins_out);

@@ -81,6 +81,34 @@ def test_quantize_all_nan_and_constant(engine):
     assert np.array_equal(ds.bins(), ob.bins)
 
 
+@pytest.mark.parametrize("n,f", [(1, 3), (1000, 17), (70_000, 40)])
+def test_apply_bins_with_training_edges(engine, n, f):
+    """A second matrix binned with the first one's edges
+    (Dataset::apply_bins, src/core/dataset.cpp:346-379): bin = number of edges
+    <= x (upper_bound), NaN -> 255, values outside the training range, +-0
+    and +-inf included; bit-exact against the oracle's edges."""
+    rng = np.random.default_rng(n + f)
+    Xtr = rng.standard_normal((5000, f)).astype(np.float32)
+    Xtr[:, 1] = np.round(Xtr[:, 1] * 2) / 2
+    ob = O.quantize(Xtr)
+    tr = engine.upload(Xtr)
+    tr.quantize(255)
+    X = (3.0 * rng.standard_normal((n, f))).astype(np.float32)
+    X[rng.random(X.shape) < 0.1] = np.nan
+    X[0, :] = ob.edges[np.arange(f), np.maximum(ob.n_edges.astype(np.int64) - 1, 0)]  # on an edge
+    if n > 4:
+        X[1:5, 0] = [-0.0, 0.0, np.inf, -np.inf]
+    ds = engine.upload(X)
+    ds.apply_bins(tr)
+    want = np.zeros((f, n), np.uint8)
+    for j in range(f):
+        e = ob.edges[j, :ob.n_edges[j]]
+        col = X[:, j]
+        b = np.searchsorted(e, col, side="right")
+        want[j] = np.where(np.isnan(col), 255, b).astype(np.uint8)
+    assert np.array_equal(ds.bins(), want)
+
+
 def test_quantize_full_size_c2_bins(engine):
     X, y = regression_c2()
     ds = engine.upload(X, y)

@@ -25,7 +25,8 @@ TRANSFORM = {"raw": 0, "sigmoid": 1, "softmax": 2}
 # every symbol include/tcgpu.h declares
 SYMBOLS = [
     "tc_ctx_create", "tc_ctx_destroy", "tc_last_error", "tc_ctx_memory", "tc_ctx_fail_next_allocs",
-    "tc_ctx_synchronize", "tc_dataset_upload", "tc_dataset_destroy", "tc_quantize", "tc_dataset_bins",
+    "tc_ctx_synchronize", "tc_dataset_upload", "tc_dataset_destroy", "tc_quantize", "tc_apply_bins",
+    "tc_dataset_bins",
     "tc_trainer_create", "tc_trainer_step", "tc_trainer_reset", "tc_trainer_stats", "tc_trainer_profile",
     "tc_trainer_train_scores", "tc_trainer_sample_mask", "tc_trainer_set_validation", "tc_trainer_valid_loss",
     "tc_trainer_model", "tc_trainer_destroy", "tc_train", "tc_build_tree", "tc_histogram_root_noalloc",
@@ -179,6 +180,10 @@ class Dataset:
         self.eng._chk(lib().tc_quantize(self.h, C.c_uint16(max_bins), C.c_int(1 if compat_u8 else 0), _p(edges),
                                         _p(ne)))
         return edges, ne
+
+    def apply_bins(self, ref: "Dataset"):
+        """Bins this dataset with ref's edges (Dataset::apply_bins)."""
+        self.eng._chk(lib().tc_apply_bins(self.h, ref.h))
 
     def bins(self):
         out = np.zeros((self.f, self.n), np.uint8)
