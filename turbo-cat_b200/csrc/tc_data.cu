@@ -358,6 +358,39 @@ tc_status quantize(tc_dataset* ds, int max_bins, int compat_u8) {
   return TC_OK;
 }
 
+tc_status apply_bins(tc_dataset* ds, const tc_dataset* ref) {
+  tc_ctx* ctx = ds->ctx;
+  if (ref->ctx != ctx) return ctx->fail(TC_ERR_INVALID_ARG, "the reference dataset belongs to another context");
+  if (!ref->quantized) return ctx->fail(TC_ERR_NOT_FITTED, "reference dataset not quantized");
+  if (ref->f != ds->f)
+    return ctx->fail(TC_ERR_INVALID_ARG, "feature counts differ (%u vs reference %u)", ds->f, ref->f);
+  if (ref == ds) return TC_OK;  // already binned with its own edges
+  cudaStream_t st = ctx->stream;
+  const uint32_t n = ds->n, f = ds->f;
+  TC_TRY(ds->edges.alloc(ctx, (size_t)f * kSlots, "bin edges"));
+  TC_TRY(ds->n_edges.alloc(ctx, f, "edge counts"));
+  TC_TRY(ds->nan_any.alloc(ctx, f, "NaN flags"));
+  TC_TRY(ds->bins_t.alloc(ctx, (size_t)(ds->groups - 1) * ds->gstride + (size_t)ds->wlast * ds->nt,
+                          "feature-group bin tiles"));
+  TC_TRY(ds->bins_cm.alloc(ctx, (size_t)f * ds->np, "column-major bins"));
+  TC_CUDA(ctx, cudaMemcpyAsync(ds->edges.p, ref->edges.p, ds->edges.bytes(), cudaMemcpyDeviceToDevice, st));
+  TC_CUDA(ctx, cudaMemcpyAsync(ds->n_edges.p, ref->n_edges.p, ds->n_edges.bytes(), cudaMemcpyDeviceToDevice, st));
+  TC_CUDA(ctx, cudaMemsetAsync(ds->nan_any.p, 0, ds->nan_any.bytes(), st));
+  TC_CUDA(ctx, cudaMemsetAsync(ds->bins_t.p, 0, ds->bins_t.bytes(), st));
+  if (n > 0) {
+    dim3 ag((n + AB_ROWS - 1) / AB_ROWS, ds->groups);
+    k_assign_bins<<<ag, 256, 0, st>>>(ds->X.p, n, f, ds->edges.p, ds->n_edges.p, ds->bins_t.p, ds->gstride,
+                                      ds->nt, ds->wlast, ds->bins_cm.p, ds->np, ds->nan_any.p);
+    TC_CUDA(ctx, cudaGetLastError());
+  }
+  TC_CUDA(ctx, cudaStreamSynchronize(st));
+  ds->h_edges = ref->h_edges;
+  ds->h_n_edges = ref->h_n_edges;
+  ds->quantized = true;
+  ds->max_bins = ref->max_bins;
+  return TC_OK;
+}
+
 }  // namespace tc
 
 extern "C" {
@@ -427,35 +460,8 @@ tc_status tc_apply_bins(tc_dataset* ds, const tc_dataset* ref) {
   if (!ds || !ref) return TC_ERR_INVALID_ARG;
   tc_ctx* ctx = ds->ctx;
   std::lock_guard<std::recursive_mutex> train_lock(ctx->train_mu);
-  if (ref->ctx != ctx) return ctx->fail(TC_ERR_INVALID_ARG, "the reference dataset belongs to another context");
-  if (!ref->quantized) return ctx->fail(TC_ERR_NOT_FITTED, "reference dataset not quantized");
-  if (ref->f != ds->f)
-    return ctx->fail(TC_ERR_INVALID_ARG, "feature counts differ (%u vs reference %u)", ds->f, ref->f);
   cudaSetDevice(ctx->device);
-  cudaStream_t st = ctx->stream;
-  const uint32_t n = ds->n, f = ds->f;
-  TC_TRY(ds->edges.alloc(ctx, (size_t)f * kSlots, "bin edges"));
-  TC_TRY(ds->n_edges.alloc(ctx, f, "edge counts"));
-  TC_TRY(ds->nan_any.alloc(ctx, f, "NaN flags"));
-  TC_TRY(ds->bins_t.alloc(ctx, (size_t)(ds->groups - 1) * ds->gstride + (size_t)ds->wlast * ds->nt,
-                          "feature-group bin tiles"));
-  TC_TRY(ds->bins_cm.alloc(ctx, (size_t)f * ds->np, "column-major bins"));
-  TC_CUDA(ctx, cudaMemcpyAsync(ds->edges.p, ref->edges.p, ds->edges.bytes(), cudaMemcpyDeviceToDevice, st));
-  TC_CUDA(ctx, cudaMemcpyAsync(ds->n_edges.p, ref->n_edges.p, ds->n_edges.bytes(), cudaMemcpyDeviceToDevice, st));
-  TC_CUDA(ctx, cudaMemsetAsync(ds->nan_any.p, 0, ds->nan_any.bytes(), st));
-  TC_CUDA(ctx, cudaMemsetAsync(ds->bins_t.p, 0, ds->bins_t.bytes(), st));
-  if (n > 0) {
-    dim3 ag((n + AB_ROWS - 1) / AB_ROWS, ds->groups);
-    k_assign_bins<<<ag, 256, 0, st>>>(ds->X.p, n, f, ds->edges.p, ds->n_edges.p, ds->bins_t.p, ds->gstride,
-                                      ds->nt, ds->wlast, ds->bins_cm.p, ds->np, ds->nan_any.p);
-    TC_CUDA(ctx, cudaGetLastError());
-  }
-  TC_CUDA(ctx, cudaStreamSynchronize(st));
-  ds->h_edges = ref->h_edges;
-  ds->h_n_edges = ref->h_n_edges;
-  ds->quantized = true;
-  ds->max_bins = ref->max_bins;
-  return TC_OK;
+  return tc::apply_bins(ds, ref);
 }
 
 tc_status tc_dataset_bins(const tc_dataset* ds, uint8_t* bins_out) {
