@@ -454,6 +454,9 @@ def suite_c1(eng, _capi, ref_ok):
     tr.step(100)
     dev = tr.stats().seconds - s0
     out = {"config": "binary 50k x 20, logloss, 100 trees, depth 6", "device_s_per_100_trees": dev}
+    prof = tr.profile(5)
+    out["kernel_ms_per_iteration"] = {k: [v[0] / 5, v[1] / 5] for k, v in prof.items() if not k.startswith("_")}
+    out["profiled_iteration_ms"] = prof["_iteration_ms"]
     if ref_ok:
         sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
         import _turbocat as ref

@@ -311,7 +311,15 @@ void tc_model_destroy(tc_model* m);
  * _SIGMOID (binary probability of class 1) or _SOFTMAX (multiclass).
  * Replaces Booster::predict_raw_nobinning_fast / predict_proba_nobinning_fast
  * (src/boosting/booster.cpp:899-945) and SymmetricEnsemble::predict_batch_raw_fast
- * (src/tree/symmetric_tree.cpp:1133-1149). */
+ * (src/tree/symmetric_tree.cpp:1133-1149).
+ * Requests of at most 64 rows (at most 512 features, 16 classes) are served
+ * by a persistent kernel of the context (a few SMs) that polls a pinned
+ * mailbox, so they cost no kernel launch; it serves one model at a time
+ * (restarted when another model is asked for or its model is destroyed) and
+ * ends by itself after 20 ms without a request (the next one relaunches it).
+ * A device-wide synchronisation therefore waits up to 20 ms after the last
+ * small request.  Values are identical for identical inputs; they may differ
+ * in the last bits from the same rows predicted in a larger request. */
 tc_status tc_predict(tc_ctx* ctx, const tc_model* m, const float* X, uint32_t n, uint16_t f,
                      int32_t transform, float* out);
 /* Same on device buffers, queued on `stream` (a cudaStream_t, NULL = the

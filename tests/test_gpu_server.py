@@ -207,3 +207,34 @@ def test_small_requests_match_oracle(engine, capi, K, T, D):
             want = 1.0 / (1.0 + np.exp(-raw))
         assert np.max(np.abs(got - want)) <= 1e-5, n
         assert np.max(np.abs(m.predict(X, "raw") - raw)) <= 1e-5 * scale, n
+
+
+def test_latency_worker_lifecycle(engine, capi):
+    """Small requests go through the persistent latency worker: results stay
+    equal (bits) across the worker ending on its own after an idle gap and
+    being relaunched, across switches between two models (the worker is
+    restarted for the other model), and after the model it serves is
+    destroyed (it is stopped first)."""
+    import time
+
+    F = 21
+    m1, a1 = _random_model(engine, capi, 501, 300, 6, F)
+    m2, a2 = _random_model(engine, capi, 502, 50, 4, F)
+    rng = np.random.default_rng(503)
+    X = rng.standard_normal((64, F)).astype(np.float32)
+    X[rng.random(X.shape) < 0.05] = np.nan
+    want1 = {n: m1.predict(X[:n], "sigmoid") for n in (1, 7, 64)}
+    want2 = {n: m2.predict(X[:n], "raw") for n in (1, 7, 64)}
+    for n in (1, 7, 64):
+        e1 = O.Ensemble(0.3, 1, 6, a1["depth"], a1["feature"], np.zeros((300, 6), np.uint8), a1["threshold"],
+                        a1["leaves"], a1["weights"])
+        p = 1.0 / (1.0 + np.exp(-O.predict(e1, X[:n])))
+        assert np.max(np.abs(want1[n] - p)) <= 1e-5
+    for rnd in range(3):
+        for n in (1, 7, 64):
+            assert np.array_equal(m1.predict(X[:n], "sigmoid"), want1[n]), (rnd, n)
+            assert np.array_equal(m2.predict(X[:n], "raw"), want2[n]), (rnd, n)
+        time.sleep(0.05)  # longer than the worker's idle limit: it ends and is relaunched
+        assert np.array_equal(m1.predict(X[:1], "sigmoid"), want1[1])
+    m1.close()  # stops the worker serving m1
+    assert np.array_equal(m2.predict(X[:7], "raw"), want2[7])

@@ -82,11 +82,17 @@ tc_status tc_ctx_create(int device, size_t mem_budget, tc_ctx** out) {
 void tc_ctx_destroy(tc_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
+  {
+    std::lock_guard<std::mutex> g(ctx->pred_mu);
+    tc::stop_latency_worker(ctx, nullptr);
+  }
   cudaStreamSynchronize(ctx->stream);
   cudaStreamSynchronize(ctx->pred_stream);
   for (auto& kv : ctx->allocs) cudaFree(kv.first);
   ctx->allocs.clear();
   if (ctx->pin_io) cudaFreeHost(ctx->pin_io);
+  if (ctx->lw_box) cudaFreeHost(ctx->lw_box);
+  if (ctx->lw_stream) cudaStreamDestroy(ctx->lw_stream);
   cudaStreamDestroy(ctx->stream);
   cudaStreamDestroy(ctx->pred_stream);
   delete ctx;

@@ -52,6 +52,17 @@ struct tc_ctx {
   size_t pin_floats = 0;
   void* small_scratch = nullptr;     // partials [blocks][rows][K] + counter
   size_t small_scratch_bytes = 0;
+  // latency worker: a persistent kernel serving small requests of one model
+  // through a pinned mailbox (tc_predict.cu); guarded by pred_mu
+  void* lw_box = nullptr;            // mailbox, host pointer (pinned, mapped)
+  void* lw_box_dev = nullptr;        // its device alias
+  void* lw_dev = nullptr;            // announcement words, counter, partials
+  cudaStream_t lw_stream = nullptr;
+  const tc_model* lw_model = nullptr;
+  bool lw_running = false;
+  int lw_blocks = 0;
+  uint32_t lw_seq = 0;
+  bool lw_enabled = true;
 
   tc_status fail(tc_status code, const char* fmt, ...) {
     char buf[512];
@@ -158,6 +169,10 @@ struct tc_model {
 };
 
 namespace tc {
+
+// Stops the latency worker (if one runs) and waits for it; with m, only if
+// it serves m.  Caller holds ctx->pred_mu (tc_predict.cu).
+void stop_latency_worker(tc_ctx* ctx, const tc_model* m);
 
 // Quantization entry (tc_data.cu).
 tc_status quantize(tc_dataset* ds, int max_bins, int compat_u8);

@@ -42,6 +42,7 @@
 // takes depends only on its model, so a request gives the same bits alone or
 // in a batch.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -434,17 +435,6 @@ __global__ void __launch_bounds__(PRED_THREADS, 2) k_predict(JobTable jt) {
   }
 }
 
-// Small requests (at most SMALL_ROWS rows): the trees are split over the
-// blocks of one launch instead of streamed through one block, as few blocks
-// as the (row, tree) walks need (one block for a single row).  Block b walks
-// trees [b*T/NB, (b+1)*T/NB) for every row of the request (row slot =
-// thread % RT, tree lane = thread / RT, trees in order within a lane) and
-// sums its lanes pairwise in a fixed order; with several blocks each stores
-// one partial per (row, class) and the last block to finish (completion
-// counter; nobody waits) adds them in block order.  The block that finishes
-// adds the base, applies the transform and writes the outputs (which may be
-// pinned host memory mapped into the device).  The rows come from device
-// memory or, for the smallest requests, from the launch parameters.
 constexpr int SMALL_ROWS = 64;
 constexpr int SMALL_INLINE = 928;  // floats of a request carried in the launch parameters (4 KB in all)
 struct SmallRows {
@@ -454,33 +444,30 @@ constexpr int SMALL_THREADS = 512;
 constexpr int SMALL_WALKS_PER_BLOCK = 4096;  // (row, tree) walks per block: one block for a single row
 constexpr int SMALL_MAX_F = 512;   // features of a small request (its rows fit in shared memory)
 
-__global__ void __launch_bounds__(SMALL_THREADS) k_predict_small(ModelDesc md, const float* __restrict__ X, uint32_t n,
-                                                                  int transform, float* __restrict__ partial,
-                                                                  uint32_t* __restrict__ counter,
-                                                                  float* __restrict__ out, SmallRows inl) {
-  extern __shared__ float sm_small[];
-  const int f = md.n_features, fs = f + 1;
+// Trees [t0, t1) for the n rows staged in s_x ([n][f+1]): row slot =
+// thread % RT, tree lane = thread / RT, trees in order within a lane, the
+// lanes summed pairwise in a fixed order.  Tree t's splits and leaves are
+// read at splits + (t - tb) * D and leaves + (t - tb) * 2^D (the model's
+// arrays with tb = 0, or a block's slice of them in shared memory).  Leaves
+// the block's sum of row r, class k in s_red[r * K + k] ([SMALL_THREADS][K]
+// scratch).
+__device__ __forceinline__ void small_trees(const ModelDesc& md, const float* __restrict__ s_x, uint32_t n, int t0,
+                                            int t1, float* __restrict__ s_red, const uint2* __restrict__ splits,
+                                            const float* __restrict__ leaves, int tb) {
+  const int fs = md.n_features + 1;
   const int K = md.n_classes, D = md.max_depth, L = 1 << D;
-  float* s_x = sm_small;                         // [n][f+1]
-  float* s_red = s_x + n * fs;                   // [SMALL_THREADS][K]
-  for (uint32_t i = threadIdx.x >> 5; i < n; i += blockDim.x >> 5)
-    for (int j = threadIdx.x & 31; j < f; j += 32) s_x[i * fs + j] = X ? X[(size_t)i * f + j] : inl.v[i * f + j];
-  __syncthreads();
   int RT = SMALL_ROWS;
   while (RT > 1 && (uint32_t)(RT >> 1) >= n) RT >>= 1;
   const int TG = blockDim.x / RT;
   const int row = threadIdx.x % RT, tg = threadIdx.x / RT;
-  const int T = md.n_trees, NB = gridDim.x;
-  const int t0 = (int)((long long)T * blockIdx.x / NB), t1 = (int)((long long)T * (blockIdx.x + 1) / NB);
   float acc[PRED_MAX_K];
 #pragma unroll
   for (int k = 0; k < PRED_MAX_K; ++k) acc[k] = 0.0f;
   if ((uint32_t)row < n) {
     const float* xr = s_x + row * fs;
-    for (int t = t0 + tg; t < t1; t += TG) {
-      // every split is loaded before any compare (one round trip to L2
-      // instead of one per level); padding splits give 0 bits
-      const uint2* sp = md.splits + (size_t)t * D;
+    // one tree: every split loaded before any compare; padding splits give 0 bits
+    auto leaf_of = [&](int t) -> float {
+      const uint2* sp = splits + (size_t)(t - tb) * D;
       uint2 q[kModelMaxDepth];
 #pragma unroll
       for (int d = 0; d < kModelMaxDepth; ++d)
@@ -489,12 +476,21 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_predict_small(ModelDesc md, c
 #pragma unroll
       for (int d = 0; d < kModelMaxDepth; ++d)
         if (d < D) idx = idx + idx + (uint32_t)(xr[q[d].x] >= __uint_as_float(q[d].y));  // false for NaN
-      const float v = md.leaves[(size_t)t * L + idx];
+      return leaves[(size_t)(t - tb) * L + idx];
+    };
+    auto add = [&](int t, float v) {
       const int cls = K == 1 ? 0 : t % K;
 #pragma unroll
       for (int k = 0; k < PRED_MAX_K; ++k)
         if (k == cls) acc[k] += v;
+    };
+    int t = t0 + tg;
+    for (; t + TG < t1; t += 2 * TG) {  // two trees in flight, added in order
+      const float v0 = leaf_of(t), v1 = leaf_of(t + TG);
+      add(t, v0);
+      add(t + TG, v1);
     }
+    for (; t < t1; t += TG) add(t, leaf_of(t));
   }
 #pragma unroll
   for (int k = 0; k < PRED_MAX_K; ++k)
@@ -505,51 +501,255 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_predict_small(ModelDesc md, c
       for (int k = 0; k < K; ++k) s_red[threadIdx.x * K + k] += s_red[(threadIdx.x + h * RT) * K + k];
     __syncthreads();
   }
-  if (NB > 1) {
-    if (tg == 0 && (uint32_t)row < n)
-      for (int k = 0; k < K; ++k) partial[((size_t)blockIdx.x * n + row) * K + k] = s_red[row * K + k];
-    __shared__ bool s_last;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      __threadfence();
-      s_last = atomicAdd(counter, 1u) == (uint32_t)NB - 1;
-    }
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-  }
-  for (uint32_t r = threadIdx.x; r < n; r += blockDim.x) {
-    float v[PRED_MAX_K];
+}
+
+// Raw scores v[0..K) of one row plus the base, transformed, into o[0..K).
+__device__ __forceinline__ void small_store(const ModelDesc& md, int transform, const float* v, float* o) {
+  const int K = md.n_classes;
+  if (transform == TC_TRANSFORM_SOFTMAX && K > 1) {
+    float mx = -INFINITY;
 #pragma unroll
-    for (int k = 0; k < PRED_MAX_K; ++k) v[k] = NB > 1 ? 0.0f : (k < K ? s_red[r * K + k] : 0.0f);
-    for (int b = 0; NB > 1 && b < NB; ++b)
+    for (int k = 0; k < PRED_MAX_K; ++k)
+      if (k < K) mx = fmaxf(mx, v[k] + md.base);
+    float sum = 0.0f, e[PRED_MAX_K];
 #pragma unroll
-      for (int k = 0; k < PRED_MAX_K; ++k)
-        if (k < K) v[k] += __ldcg(&partial[((size_t)b * n + r) * K + k]);
-    float* o = out + (size_t)r * K;
-    if (transform == TC_TRANSFORM_SOFTMAX && K > 1) {
-      float mx = -INFINITY;
+    for (int k = 0; k < PRED_MAX_K; ++k)
+      if (k < K) { e[k] = expf(v[k] + md.base - mx); sum += e[k]; }
 #pragma unroll
-      for (int k = 0; k < PRED_MAX_K; ++k)
-        if (k < K) mx = fmaxf(mx, v[k] + md.base);
-      float sum = 0.0f, e[PRED_MAX_K];
+    for (int k = 0; k < PRED_MAX_K; ++k)
+      if (k < K) o[k] = e[k] / sum;
+  } else {
 #pragma unroll
-      for (int k = 0; k < PRED_MAX_K; ++k)
-        if (k < K) { e[k] = expf(v[k] + md.base - mx); sum += e[k]; }
-#pragma unroll
-      for (int k = 0; k < PRED_MAX_K; ++k)
-        if (k < K) o[k] = e[k] / sum;
-    } else {
-#pragma unroll
-      for (int k = 0; k < PRED_MAX_K; ++k) {
-        if (k < K) {
-          const float raw = v[k] + md.base;
-          o[k] = transform == TC_TRANSFORM_SIGMOID ? sigmoidf_ref(raw) : raw;
-        }
+    for (int k = 0; k < PRED_MAX_K; ++k) {
+      if (k < K) {
+        const float raw = v[k] + md.base;
+        o[k] = transform == TC_TRANSFORM_SIGMOID ? sigmoidf_ref(raw) : raw;
       }
     }
   }
+}
+
+// With nb > 1 blocks taking part: store this block's sums
+// (partial[block][row][K]); the last of the nb blocks to finish (completion
+// counter; nobody waits) returns true and the blocks' sums are then
+// complete, to be added in block order.
+__device__ __forceinline__ bool small_publish(const ModelDesc& md, uint32_t n, const float* s_red, float* partial,
+                                              uint32_t* counter, uint32_t nb) {
+  const int K = md.n_classes;
+  for (uint32_t r = threadIdx.x; r < n; r += blockDim.x)
+    for (int k = 0; k < K; ++k) partial[((size_t)blockIdx.x * n + r) * K + k] = s_red[r * K + k];
+  __shared__ bool s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();  // the block's partials (ordered before it by the barrier) before the count
+    s_last = atomicAdd(counter, 1u) == nb - 1;
+    if (s_last) __threadfence();
+  }
+  __syncthreads();
+  return s_last;
+}
+
+// Row r's raw sums: this block's alone (nb == 1), or the nb blocks' partials
+// in block order, read from s_comb when the last block staged them there
+// (all loads in flight together), else from L2 one by one.
+__device__ __forceinline__ void small_row_sums(const ModelDesc& md, uint32_t n, uint32_t r, const float* s_red,
+                                               const float* partial, uint32_t nb, const float* s_comb, float* v) {
+  const int K = md.n_classes;
+#pragma unroll
+  for (int k = 0; k < PRED_MAX_K; ++k) v[k] = nb > 1 ? 0.0f : (k < K ? s_red[r * K + k] : 0.0f);
+  for (uint32_t b = 0; nb > 1 && b < nb; ++b)
+#pragma unroll
+    for (int k = 0; k < PRED_MAX_K; ++k)
+      if (k < K) v[k] += s_comb ? s_comb[((size_t)b * n + r) * K + k] : __ldcg(&partial[((size_t)b * n + r) * K + k]);
+}
+
+// Small requests (at most SMALL_ROWS rows): the trees are split over the
+// blocks of one launch instead of streamed through one block, as few blocks
+// as the (row, tree) walks need (one block for a single row).  Block b walks
+// trees [b*T/NB, (b+1)*T/NB) for every row of the request; with several
+// blocks each stores one partial per (row, class) and the last block to
+// finish adds them in block order.  The block that finishes adds the base,
+// applies the transform and writes the outputs (which may be pinned host
+// memory mapped into the device).  The rows come from device memory or, for
+// the smallest requests, from the launch parameters.
+__global__ void __launch_bounds__(SMALL_THREADS) k_predict_small(ModelDesc md, const float* __restrict__ X, uint32_t n,
+                                                                  int transform, float* __restrict__ partial,
+                                                                  uint32_t* __restrict__ counter,
+                                                                  float* __restrict__ out, SmallRows inl) {
+  extern __shared__ float sm_small[];
+  const int f = md.n_features, fs = f + 1;
+  const int K = md.n_classes;
+  float* s_x = sm_small;                         // [n][f+1]
+  float* s_red = s_x + n * fs;                   // [SMALL_THREADS][K]
+  for (uint32_t i = threadIdx.x >> 5; i < n; i += blockDim.x >> 5)
+    for (int j = threadIdx.x & 31; j < f; j += 32) s_x[i * fs + j] = X ? X[(size_t)i * f + j] : inl.v[i * f + j];
+  __syncthreads();
+  const int T = md.n_trees, NB = gridDim.x;
+  small_trees(md, s_x, n, (int)((long long)T * blockIdx.x / NB), (int)((long long)T * (blockIdx.x + 1) / NB), s_red,
+              md.splits, md.leaves, 0);
+  if (NB > 1 && !small_publish(md, n, s_red, partial, counter, NB)) return;
+  for (uint32_t r = threadIdx.x; r < n; r += blockDim.x) {
+    float v[PRED_MAX_K];
+    small_row_sums(md, n, r, s_red, partial, NB, nullptr, v);
+    small_store(md, transform, v, out + (size_t)r * K);
+  }
   if (NB > 1 && threadIdx.x == 0) *counter = 0u;  // re-armed for the next call
+}
+
+// ------------------------------------------------------- latency worker --
+// A persistent cooperative kernel serving small requests of one model
+// without a launch per request.  The host writes a request's rows into a
+// pinned mailbox mapped into the device, then its request word (sequence,
+// transform, rows); block 0 polls that word (system-scope acquire loads, a
+// short sleep between polls), copies the rows into device memory and
+// announces the request to the other blocks through a device word
+// (generation counter); every block walks its tree range, the last block
+// adds the partials in block order, writes the outputs into the mailbox and
+// publishes seq_done (system-scope release).  Every wait is bounded: block 0
+// stops after LW_IDLE_NS without a request or LW_LIFE_NS in all (or when the
+// host sets stop), announces that, and the others follow; their own waits
+// give up after LW_LIFE_NS + LW_IDLE_NS.  On exit block 0 sets `exited`; the
+// host then launches a new worker for the next request.
+struct LwBox {
+  uint32_t req;        // host -> device: sequence << 16 | transform << 8 | rows
+  uint32_t stop;
+  uint32_t pad0[14];
+  uint32_t seq_done;   // device -> host: sequence of the last answered request
+  uint32_t exited;
+  uint32_t pad1[14];
+  float x[SMALL_ROWS * SMALL_MAX_F];
+  float out[SMALL_ROWS * PRED_MAX_K];
+};
+constexpr uint64_t LW_IDLE_NS = 20000000ull;    // 20 ms without a request
+constexpr uint64_t LW_LIFE_NS = 2000000000ull;  // 2 s per launch
+constexpr int LW_MAX_BLOCKS = 32;
+constexpr int LW_FLAG_WORDS = 64;               // [0] blocks done with a request, [32] blocks that left
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ uint32_t ld_acquire_sys(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.sys.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_sys(uint32_t* p, uint32_t v) {
+  asm volatile("st.release.sys.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_acquire_gpu_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_gpu_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+constexpr uint32_t kLwEnd = 0xffffffffu;  // announcement: the worker ends (a request never has 255 rows)
+
+// Block b of the nb blocks serving a request of n rows takes rows
+// [n b / nb, n (b + 1) / nb) (nb = min(worker blocks, n)), loads them from the
+// pinned mailbox itself (16-byte loads of the aligned range, all in flight
+// together), walks every tree for them (the model from global memory, L2
+// resident) and writes their outputs into the mailbox; the last block to
+// finish (completion counter) publishes seq_done.  One thread of block 0
+// polls the request word (system-scope acquire loads over the bus) and
+// announces each request, or the end, to the other blocks through a device
+// word (generation counter).  Shared memory: [rows 64 x (f+1)][sums 512 x K].
+__global__ void __launch_bounds__(SMALL_THREADS) k_predict_worker(ModelDesc md, LwBox* box, uint32_t* flag,
+                                                                   uint32_t seen) {
+  extern __shared__ __align__(16) float sm_w[];
+  __shared__ uint32_t s_cmd, s_req;
+  const int f = md.n_features, fs = f + 1, K = md.n_classes, T = md.n_trees;
+  float* s_x = sm_w;                                   // [rows][f+1]
+  float* s_red = s_x + (size_t)SMALL_ROWS * fs;        // [SMALL_THREADS][K]
+  uint32_t* counter = flag;                            // blocks done with the current request
+  uint32_t* exits = flag + 32;                         // blocks that have left
+  // block 0's announcement: generation << 32 | request word (kLwEnd: leave),
+  // one 64-bit word, so a block that sees a generation sees its request
+  unsigned long long* ann = reinterpret_cast<unsigned long long*>(flag + 16);
+  const uint64_t t_start = global_ns();
+  uint32_t gen = 0;  // thread 0: the last generation announced / seen
+  for (;;) {
+    if (threadIdx.x == 0) {
+      uint32_t req = kLwEnd;
+      if (blockIdx.x == 0) {
+        const uint64_t t_idle = global_ns();
+        for (;;) {
+          const uint32_t r = ld_acquire_sys(&box->req);
+          if ((r >> 16) != seen) {
+            req = r;
+            break;
+          }
+          if (ld_acquire_sys(&box->stop)) break;
+          const uint64_t now = global_ns();
+          if (now - t_idle > LW_IDLE_NS || now - t_start > LW_LIFE_NS) break;
+        }
+        ++gen;
+        if (gridDim.x > 1) st_release_gpu_u64(ann, (unsigned long long)gen << 32 | req);
+      } else {
+        const uint64_t t_wait = global_ns();
+        for (;;) {
+          const unsigned long long a = ld_acquire_gpu_u64(ann);
+          if ((uint32_t)(a >> 32) != gen) {  // the latest announcement (earlier ones were not ours)
+            gen = (uint32_t)(a >> 32);
+            req = (uint32_t)a;
+            break;
+          }
+          if (global_ns() - t_wait > LW_LIFE_NS + LW_IDLE_NS) break;  // leaves
+        }
+      }
+      s_cmd = req == kLwEnd ? 2u : 1u;
+      s_req = req;
+    }
+    __syncthreads();
+    if (s_cmd != 1) break;
+    const uint32_t n = min(s_req & 0xffu, (uint32_t)SMALL_ROWS);
+    const int tr = (int)((s_req >> 8) & 0xffu);
+    const uint32_t nb = min(gridDim.x, max(n, 1u));
+    if (blockIdx.x < nb) {
+      const uint32_t rb0 = n * blockIdx.x / nb, rb1 = n * (blockIdx.x + 1) / nb, nr = rb1 - rb0;
+      // elements [rb0 f, rb1 f) of the rows, through the 16-byte units covering them
+      const uint32_t e0 = rb0 * (uint32_t)f, e1 = rb1 * (uint32_t)f;
+      const float4* src = reinterpret_cast<const float4*>(box->x);
+      for (uint32_t q = e0 / 4 + threadIdx.x; q < (e1 + 3) / 4; q += blockDim.x) {
+        const float4 v = __ldcv(src + q);
+        const float e[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const uint32_t i = 4 * q + c;
+          if (i >= e0 && i < e1) s_x[((i - e0) / f) * fs + (i - e0) % f] = e[c];
+        }
+      }
+      __syncthreads();
+      small_trees(md, s_x, nr, 0, T, s_red, md.splits, md.leaves, 0);
+      for (uint32_t r = threadIdx.x; r < nr; r += blockDim.x) {
+        float v[PRED_MAX_K];
+        small_row_sums(md, nr, r, s_red, nullptr, 1, nullptr, v);
+        small_store(md, tr, v, box->out + (size_t)(rb0 + r) * K);
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        if (nb == 1) {
+          // a release at system scope: the outputs (ordered before it by the
+          // barrier) are visible to whoever sees seq_done
+          st_release_sys(&box->seq_done, s_req >> 16);
+        } else {
+          // the block's outputs are visible system-wide before the count; the
+          // last block publishes seq_done
+          __threadfence_system();
+          if (atomicAdd(counter, 1u) == nb - 1) {
+            *counter = 0u;
+            st_release_sys(&box->seq_done, s_req >> 16);
+          }
+        }
+      }
+    }
+    seen = s_req >> 16;
+    __syncthreads();  // s_cmd / s_req are rewritten by the next poll
+  }
+  if (threadIdx.x == 0 && atomicAdd(exits, 1u) == gridDim.x - 1) st_release_sys(&box->exited, 1u);
 }
 
 // Stage sizes for a batch whose deepest model has depth max_depth: a leaf
@@ -764,6 +964,16 @@ ModelDesc model_desc(const tc_model* m) {
   d.n_features = m->info.n_features;
   d.base = m->info.base_prediction;
   return d;
+}
+
+void stop_latency_worker(tc_ctx* ctx, const tc_model* m) {
+  if (!ctx->lw_running || (m && ctx->lw_model != m)) return;
+  volatile LwBox* box = static_cast<volatile LwBox*>(ctx->lw_box);
+  box->stop = 1u;
+  cudaStreamSynchronize(ctx->lw_stream);
+  box->stop = 0u;
+  ctx->lw_running = false;
+  ctx->lw_model = nullptr;
 }
 
 tc_status predict_device(tc_ctx* ctx, const tc_model* m, const float* X, uint32_t n, uint32_t f, int transform,
@@ -1007,7 +1217,93 @@ tc_status tc_model_load_tcat(tc_ctx* ctx, const uint8_t* buf, size_t len, tc_mod
   return s;
 }
 
-void tc_model_destroy(tc_model* m) { delete m; }
+void tc_model_destroy(tc_model* m) {
+  if (!m) return;
+  if (m->ctx) {
+    std::lock_guard<std::mutex> g(m->ctx->pred_mu);
+    tc::stop_latency_worker(m->ctx, m);
+  }
+  delete m;
+}
+
+// Latency worker launch for model m (caller holds pred_mu; no worker runs).
+static tc_status lw_launch(tc_ctx* ctx, const tc_model* m) {
+  if (!ctx->lw_box) {
+    TC_CUDA(ctx, cudaHostAlloc(&ctx->lw_box, sizeof(LwBox), cudaHostAllocMapped));
+    std::memset(ctx->lw_box, 0, sizeof(LwBox));
+    TC_CUDA(ctx, cudaHostGetDevicePointer(&ctx->lw_box_dev, ctx->lw_box, 0));
+  }
+  if (!ctx->lw_dev)
+    TC_TRY(ctx->alloc(&ctx->lw_dev, LW_FLAG_WORDS * 4, "latency worker counters"));
+  if (!ctx->lw_stream) TC_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->lw_stream, cudaStreamNonBlocking));
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaFuncSetAttribute(k_predict_worker, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_done = true;
+  }
+  const int T = m->info.n_trees, K = m->info.n_classes, f = m->info.n_features;
+  const size_t smem = ((size_t)SMALL_ROWS * (f + 1) + (size_t)SMALL_THREADS * K) * sizeof(float);
+  // blocks: a 64-row request split so that a block walks ~4096 (row, tree) pairs
+  const long long want = ((long long)T * SMALL_ROWS + SMALL_WALKS_PER_BLOCK - 1) / SMALL_WALKS_PER_BLOCK;
+  int per_sm = 0;
+  TC_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_predict_worker, SMALL_THREADS, smem));
+  if (per_sm < 1) return ctx->fail(TC_ERR_INVALID_ARG, "latency worker does not fit a multiprocessor");
+  const int NB = (int)std::max<long long>(
+      1, std::min<long long>({want, (long long)SMALL_ROWS, (long long)LW_MAX_BLOCKS,
+                              (long long)std::max(1, ctx->sm_count / 4), (long long)per_sm * ctx->sm_count}));
+  volatile LwBox* box = static_cast<volatile LwBox*>(ctx->lw_box);
+  box->exited = 0u;
+  box->stop = 0u;
+  TC_CUDA(ctx, cudaMemsetAsync(ctx->lw_dev, 0, LW_FLAG_WORDS * 4, ctx->lw_stream));
+  ModelDesc md = model_desc(m);
+  LwBox* bd = static_cast<LwBox*>(ctx->lw_box_dev);
+  uint32_t* flag = static_cast<uint32_t*>(ctx->lw_dev);
+  uint32_t seen = box->seq_done;
+  void* args[] = {&md, &bd, &flag, &seen};
+  TC_CUDA(ctx, cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_predict_worker), dim3(NB),
+                                           dim3(SMALL_THREADS), args, smem, ctx->lw_stream));
+  ctx->lw_running = true;
+  ctx->lw_model = m;
+  ctx->lw_blocks = NB;
+  return TC_OK;
+}
+
+// Small request through the latency worker (caller holds pred_mu): rows into
+// the mailbox, then the request word, spin on seq_done.  A worker
+// that ended (idle, lifetime) is relaunched; it serves the pending request.
+static tc_status predict_worker(tc_ctx* ctx, const tc_model* m, const float* X, uint32_t n, uint32_t f,
+                                int32_t transform, float* out) {
+  if (ctx->lw_running && ctx->lw_model != m) tc::stop_latency_worker(ctx, nullptr);
+  if (ctx->lw_running && static_cast<volatile LwBox*>(ctx->lw_box)->exited) {  // ended (idle or lifetime)
+    cudaStreamSynchronize(ctx->lw_stream);
+    ctx->lw_running = false;
+  }
+  if (!ctx->lw_running) TC_TRY(lw_launch(ctx, m));
+  LwBox* box = static_cast<LwBox*>(ctx->lw_box);
+  volatile LwBox* vb = box;
+  std::memcpy(box->x, X, (size_t)n * f * sizeof(float));
+  const uint32_t seq = ctx->lw_seq = (ctx->lw_seq + 1u) & 0xffffu;  // 16-bit sequence; only inequality matters
+  std::atomic_thread_fence(std::memory_order_seq_cst);
+  vb->req = seq << 16 | (uint32_t)transform << 8 | n;
+  const auto t0 = std::chrono::steady_clock::now();
+  for (uint32_t spin = 1;; ++spin) {
+    if (vb->seq_done == seq) break;
+    if ((spin & 1023u) == 0u) {
+      if (vb->exited) {  // the worker ended before it saw the request
+        cudaStreamSynchronize(ctx->lw_stream);
+        ctx->lw_running = false;
+        TC_TRY(lw_launch(ctx, m));
+      }
+      if (std::chrono::steady_clock::now() - t0 > std::chrono::seconds(5)) {
+        tc::stop_latency_worker(ctx, nullptr);
+        return ctx->fail(TC_ERR_TIMEOUT, "latency worker did not answer request %u", seq);
+      }
+    }
+  }
+  std::atomic_thread_fence(std::memory_order_seq_cst);
+  std::memcpy(out, box->out, (size_t)n * m->info.n_classes * sizeof(float));
+  return TC_OK;
+}
 
 // Small request (n <= SMALL_ROWS): inputs and outputs through the context's
 // pinned mapped staging, one launch of k_predict_small, one synchronisation.
@@ -1082,6 +1378,7 @@ tc_status tc_predict(tc_ctx* ctx, const tc_model* m, const float* X, uint32_t n,
   const int K = m->info.n_classes;
   if (n <= (uint32_t)SMALL_ROWS && K <= PRED_MAX_K && f <= SMALL_MAX_F && m->info.n_trees > 0) {
     std::lock_guard<std::mutex> g(ctx->pred_mu);
+    if (ctx->lw_enabled) return predict_worker(ctx, m, X, n, f, transform, out);
     return predict_small(ctx, m, X, n, f, transform, out);
   }
   // input and output share one grow-only device buffer of the context, so a
