@@ -32,6 +32,7 @@
 // path launches one class and one level at a time with a host
 // synchronisation after every level.
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -1280,59 +1281,58 @@ __device__ __forceinline__ void node_reduce_body(const DevCfg& c, const DevPtrs&
 // rows per chunk for this level and the cumulative chunk counts over
 // (class, pair, feature group), which the histogram kernel decodes into work
 // items.
+constexpr int kPlanSegs = 4096;  // (class, pair) segment lengths the plan keeps in shared memory
+
 __device__ __forceinline__ void plan_body(const DevCfg& c, const DevPtrs& P, int d) {
-  __shared__ int s_go;
-  __shared__ uint32_t s_maxcnt;
-  __shared__ int s_hot;
   __shared__ long long s_rows;
   __shared__ int s_nodes;
-  __shared__ int s_warp[PLAN_THREADS / 32];
+  __shared__ int s_warp[32];
   __shared__ int s_carry;
+  __shared__ int s_len[kPlanSegs];  // [class][pair] rows of level d (0: the class grows no more)
   const int Pmax = 1 << (c.D - 1);
   const int L = 1 << c.D;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = (int)(blockDim.x >> 5);
+  const int np2 = pairs_at(d);
+  const int nsg = c.K * np2;
+  const bool cached = nsg <= kPlanSegs;
   if (tid == 0) { s_rows = 0; s_nodes = 0; }
-  for (int k = 0; k < c.K; ++k) {
+  __syncthreads();
+  // Per class, one warp each (classes w, w + warps, ...): no block barriers.
+  for (int k = warp; k < c.K; k += nwarps) {
     ClassState& cs = P.cs[k];
-    if (tid == 0) {
-      if (d == 0) { cs.done = 0; cs.depth = 0; }
-      if (d == 0 && c.nv > 0 && P.es->stopped) cs.done = 2;  // early-stopped: no more trees
-      s_go = 0;
-    }
-    __syncthreads();
-    const bool alive = !cs.done && (d == 0 || cs.depth == d) && d < c.D;
-    if (tid == 0) s_maxcnt = 0;
-    __syncthreads();
+    int done = cs.done, depth = cs.depth;
+    if (d == 0) { done = 0; depth = 0; }
+    if (d == 0 && c.nv > 0 && P.es->stopped) done = 2;  // early-stopped: no more trees
+    const bool alive = !done && (d == 0 || depth == d) && d < c.D;
+    int go = 0;
     if (alive) {
       const NodeStat* ns = P.nstat + ((size_t)k * (c.D + 1) + d) * L;
-      for (int q = tid; q < (1 << d); q += blockDim.x) {
-        if (ns[q].cnt >= (uint32_t)c.msl * 2u && (float)ns[q].H >= c.mcw * 2.0f) s_go = 1;
-        atomicMax(&s_maxcnt, ns[q].cnt);
+      uint32_t maxcnt = 0;
+      for (int q = lane; q < (1 << d); q += 32) {
+        const uint32_t cnt = ns[q].cnt;
+        if (cnt >= (uint32_t)c.msl * 2u && (float)ns[q].H >= c.mcw * 2.0f) go = 1;
+        maxcnt = max(maxcnt, cnt);
+      }
+      go = __any_sync(0xffffffffu, go);
+      for (int o = 16; o; o >>= 1) maxcnt = max(maxcnt, __shfl_xor_sync(0xffffffffu, maxcnt, o));
+      int hot = INT32_MAX;  // the largest node, the lowest index on a tie
+      for (int q = lane; q < (1 << d); q += 32)
+        if (ns[q].cnt == maxcnt) hot = min(hot, q);
+      for (int o = 16; o; o >>= 1) hot = min(hot, __shfl_xor_sync(0xffffffffu, hot, o));
+      if (lane == 0) {
+        const uint32_t tot = P.nstat[((size_t)k * (c.D + 1)) * L].cnt;  // rows of the level (the root's count)
+        cs.skew = (uint64_t)maxcnt * 8u > (uint64_t)tot ? 1 : 0;
+        cs.hot = hot == INT32_MAX ? 0 : hot;
       }
     }
-    if (tid == 0) s_hot = INT32_MAX;
-    __syncthreads();
-    if (alive) {
-      const NodeStat* ns = P.nstat + ((size_t)k * (c.D + 1) + d) * L;
-      for (int q = tid; q < (1 << d); q += blockDim.x)
-        if (ns[q].cnt == s_maxcnt) atomicMin(&s_hot, q);
-    }
-    __syncthreads();
-    if (tid == 0 && alive) {
-      uint32_t tot = 0;  // rows of the level (the root's count)
-      tot = P.nstat[((size_t)k * (c.D + 1)) * L].cnt;
-      cs.skew = (uint64_t)s_maxcnt * 8u > (uint64_t)tot ? 1 : 0;
-      cs.hot = s_hot == INT32_MAX ? 0 : s_hot;
-    }
-    if (tid == 0 && !cs.done && !(alive && s_go)) cs.done = 1;
-    __syncthreads();
-    if (cs.done == 1) {
+    if (!done && !(alive && go)) done = 1;
+    if (done == 1) {
+      // the tree is complete: its leaves (src/tree/symmetric_tree.cpp:357-367, 753-775)
       const int t = *P.iter * c.KT + c.k0 + k;
-      const int dep = cs.depth;
-      const NodeStat* ns = P.nstat + ((size_t)k * (c.D + 1) + dep) * L;
-      for (int q = tid; q < L; q += blockDim.x) {
+      const NodeStat* ns = P.nstat + ((size_t)k * (c.D + 1) + depth) * L;
+      for (int q = lane; q < L; q += 32) {
         float v = 0.0f;
-        if (q < (1 << dep)) {
+        if (q < (1 << depth)) {
           const double H = ns[q].H;
           if (H >= 1e-10) {
             double x = -ns[q].G / (H + (double)c.lam);
@@ -1345,45 +1345,53 @@ __device__ __forceinline__ void plan_body(const DevCfg& c, const DevPtrs& P, int
         }
         P.m_leaves[(size_t)t * L + q] = v;
       }
-      __syncthreads();
-      if (tid == 0) {
-        P.m_depth[t] = dep;
-        cs.done = 2;
-      }
-    } else if (!cs.done) {
-      // segment starts (exclusive scan over the pairs' lengths)
-      const int np2 = pairs_at(d);
-      if (tid == 0) s_carry = 0;
-      __syncthreads();
-      for (int base = 0; base < np2; base += blockDim.x) {
-        const int p = base + tid;
+      if (lane == 0) P.m_depth[t] = depth;
+      done = 2;
+    }
+    if (!done) {
+      // segment starts (exclusive scan over the pairs' lengths), 32 at a time
+      int carry = 0;
+      for (int base = 0; base < np2; base += 32) {
+        const int p = base + lane;
         const int len = p < np2 ? (d == 0 ? (int)c.n : P.seg_len[k * Pmax + p]) : 0;
         int x = len;
         for (int o = 1; o < 32; o <<= 1) {
           const int y = __shfl_up_sync(0xffffffffu, x, o);
           if (lane >= o) x += y;
         }
-        if (lane == 31) s_warp[warp] = x;
-        __syncthreads();
-        int before = s_carry;
-        for (int w = 0; w < warp; ++w) before += s_warp[w];
-        if (p < np2) P.seg_start[k * Pmax + p] = before + x - len;
-        __syncthreads();
-        if (tid == blockDim.x - 1) s_carry = before + x;
-        __syncthreads();
+        if (p < np2) {
+          P.seg_start[k * Pmax + p] = carry + x - len;
+          if (cached) s_len[k * np2 + p] = len;
+        }
+        carry += __shfl_sync(0xffffffffu, x, 31);
       }
-      if (tid == 0) { s_rows += s_carry; s_nodes += np2; }
+      if (lane == 0) {
+        atomicAdd(reinterpret_cast<unsigned long long*>(&s_rows), (unsigned long long)carry);
+        atomicAdd(&s_nodes, np2);
+      }
+    } else if (cached) {
+      for (int p = lane; p < np2; p += 32) s_len[k * np2 + p] = 0;
     }
-    __syncthreads();
+    __syncwarp();
+    if (lane == 0) {
+      if (d == 0) cs.depth = 0;
+      cs.done = done;
+    }
   }
+  __syncthreads();
+  // rows of segment sgi (class, pair) for the chunking below
+  auto seg_rows = [&](int sgi) -> int {
+    if (cached) return s_len[sgi];
+    const int k = sgi / np2, p = sgi % np2;
+    if (P.cs[k].done) return 0;
+    return d == 0 ? (int)c.n : P.seg_len[k * Pmax + p];
+  };
   // Rows per chunk for this level: the smallest R (from the even split up)
   // for which the level has at most target_items items.  Every group counts,
   // the narrow last one too: measured, items that all run in one wave beat
   // a second wave of cheap narrow items after the wide ones.
   __shared__ int s_R;
   __shared__ long long s_cnt;
-  const int np2 = pairs_at(d);
-  const int nsg = c.K * np2;
   const int gw = c.G;
   if (tid == 0) {
     int R = c.rows_fixed;
@@ -1396,13 +1404,7 @@ __device__ __forceinline__ void plan_body(const DevCfg& c, const DevPtrs& P, int
     if (tid == 0) s_cnt = 0;
     __syncthreads();
     long long mine = 0;
-    for (int sgi = tid; sgi < nsg; sgi += blockDim.x) {
-      const int k = sgi / np2, p = sgi % np2;
-      if (!P.cs[k].done) {
-        const int len = d == 0 ? (int)c.n : P.seg_len[k * Pmax + p];
-        mine += (len + Rt - 1) / Rt;
-      }
-    }
+    for (int sgi = tid; sgi < nsg; sgi += blockDim.x) mine += (seg_rows(sgi) + Rt - 1) / Rt;
     for (int o = 16; o; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
     if (lane == 0 && mine) atomicAdd(reinterpret_cast<unsigned long long*>(&s_cnt), (unsigned long long)mine);
     __syncthreads();
@@ -1421,14 +1423,7 @@ __device__ __forceinline__ void plan_body(const DevCfg& c, const DevPtrs& P, int
   // cumulative item counts over segments (class, pair): chunks x groups
   for (int base = 0; base < nsg; base += blockDim.x) {
     const int sgi = base + tid;
-    int chunks = 0;
-    if (sgi < nsg) {
-      const int k = sgi / np2, p = sgi % np2;
-      if (!P.cs[k].done) {
-        const int len = d == 0 ? (int)c.n : P.seg_len[k * Pmax + p];
-        chunks = (len + R - 1) / R * c.G;
-      }
-    }
+    const int chunks = sgi < nsg ? (seg_rows(sgi) + R - 1) / R * c.G : 0;
     int x = chunks;
     for (int o = 1; o < 32; o <<= 1) {
       const int y = __shfl_up_sync(0xffffffffu, x, o);
@@ -1752,6 +1747,7 @@ struct tc_trainer {
   bool given_gh = false;
   bool tuned = false;
   int hist_waves = 2;
+  int hist_rows_min = 512;  // smallest rows per histogram work item
   int64_t launches = 0;
   int launches_per_iter = 0;
   // profiling: when prof != nullptr every launch is bracketed by events
@@ -1898,6 +1894,7 @@ tc_status tc_trainer::configure(int J_, int waves) {
   cfg.W = W;
   cfg.hist_grid = hist_grid;
   cfg.target_items = waves * hist_grid;
+  cfg.rows_min = hist_rows_min;
   cfg.item_cap = (int)cap;
 
   TC_TRY(cum.alloc(ctx, (size_t)K * Pmax * G + 1, "chunk counts"));
@@ -1908,7 +1905,7 @@ tc_status tc_trainer::configure(int J_, int waves) {
 
 namespace {
 std::mutex g_tune_mu;
-std::map<std::string, std::pair<int, int>> g_tune_cache;  // shape -> (J, waves)
+std::map<std::string, std::array<int, 3>> g_tune_cache;  // shape -> (J, waves, rows_min)
 }  // namespace
 
 // Project autotuner: times a few iterations for every items-per-launch
@@ -1922,7 +1919,8 @@ tc_status tc_trainer::autotune() {
     std::lock_guard<std::mutex> g(g_tune_mu);
     auto it = g_tune_cache.find(key);
     if (it != g_tune_cache.end()) {
-      TC_TRY(configure(it->second.first, it->second.second));
+      hist_rows_min = it->second[2];
+      TC_TRY(configure(it->second[0], it->second[1]));
       tuned = true;
       return TC_OK;
     }
@@ -1933,13 +1931,23 @@ tc_status tc_trainer::autotune() {
   // parameter but are not tried
   const int jmax = 1;
   double best = 1e30;
-  int bj = J, bw = hist_waves;
+  int bj = J, bw = hist_waves, br = hist_rows_min;
+  // candidates (waves, rows_min): 1, 2, 4, 8 waves of items of at least 512
+  // rows; on small shapes also one wave of larger items (fewer items flush
+  // fewer partial histograms into the same accumulators)
+  std::vector<std::pair<int, int>> cand = {{1, 512}, {2, 512}, {4, 512}, {8, 512}};
+  if ((long long)cfg.n * (long long)((cfg.f + 31) / 32) <= 8LL * ctx->sm_count * 8192) {
+    cand.push_back({1, 2048});
+    cand.push_back({1, 8192});
+  }
   // every candidate restarts from the base prediction and replays the same
   // first iterations; the best of two timed runs of them counts
   const int trial_iters = 2;  // + 1 warm-up: 3 <= n_estimators iterations (checked by the caller)
   for (int rep = 0; rep < 2; ++rep) {
     for (int j = 1; j <= jmax; ++j) {
-      for (int waves : {1, 2, 4, 8}) {
+      for (const auto& wr : cand) {
+        const int waves = wr.first;
+        hist_rows_min = wr.second;
         TC_TRY(configure(j, waves));
         TC_TRY(init_predictions());
         enqueue_iteration(st);  // warm-up (first touch of the buffers)
@@ -1954,16 +1962,18 @@ tc_status tc_trainer::autotune() {
           best = ms;
           bj = j;
           bw = waves;
+          br = hist_rows_min;
         }
       }
     }
   }
+  hist_rows_min = br;
   TC_TRY(configure(bj, bw));
   TC_TRY(init_predictions());
   launches = 0;
   tuned = true;
   std::lock_guard<std::mutex> g(g_tune_mu);
-  g_tune_cache[key] = {bj, bw};
+  g_tune_cache[key] = {bj, bw, br};
   return TC_OK;
 }
 
