@@ -76,6 +76,10 @@ tc_status tc_ctx_memory(const tc_ctx* ctx, size_t* in_use, size_t* peak);
 tc_status tc_ctx_fail_next_allocs(tc_ctx* ctx, int count);
 /* Bounded wait (milliseconds) for all work queued by this context. */
 tc_status tc_ctx_synchronize(tc_ctx* ctx, int timeout_ms);
+/* Small predict requests (tc_predict, at most 64 rows) through the context's
+ * persistent latency worker (enabled = 1, the default) or by one kernel
+ * launch each (0); disabling stops a running worker. */
+tc_status tc_ctx_set_latency_worker(tc_ctx* ctx, int enabled);
 
 /* ---------------------------------------------------------------- dataset */
 

@@ -236,5 +236,21 @@ def test_latency_worker_lifecycle(engine, capi):
             assert np.array_equal(m2.predict(X[:n], "raw"), want2[n]), (rnd, n)
         time.sleep(0.05)  # longer than the worker's idle limit: it ends and is relaunched
         assert np.array_equal(m1.predict(X[:1], "sigmoid"), want1[1])
+    # one launch per request instead of the worker: the same values within
+    # the stated tolerance (the trees are split over blocks differently)
+    engine.set_latency_worker(False)
+    scale = 0.3 + (np.abs(a1["leaves"]).max(1) * a1["weights"]).sum()
+    for n in (1, 7, 64):
+        assert np.max(np.abs(m1.predict(X[:n], "raw") - engine_raw(m1, X[:n], a1))) <= 1e-5 * scale
+        assert np.max(np.abs(m1.predict(X[:n], "sigmoid") - want1[n])) <= 1e-5
+    engine.set_latency_worker(True)
     m1.close()  # stops the worker serving m1
     assert np.array_equal(m2.predict(X[:7], "raw"), want2[7])
+
+
+def engine_raw(m, X, a):
+    """FP64 oracle raw scores of a model built by _random_model (depth 6)."""
+    T = a["depth"].shape[0]
+    e = O.Ensemble(0.3, 1, 6, a["depth"], a["feature"], np.zeros((T, 6), np.uint8), a["threshold"], a["leaves"],
+                   a["weights"])
+    return O.predict(e, X)

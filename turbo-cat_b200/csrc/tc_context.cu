@@ -119,6 +119,15 @@ tc_status tc_ctx_fail_next_allocs(tc_ctx* ctx, int count) {
 
 // Polls the context stream instead of blocking in the driver so that a
 // stuck device turns into TC_ERR_TIMEOUT rather than a hung caller.
+tc_status tc_ctx_set_latency_worker(tc_ctx* ctx, int enabled) {
+  if (!ctx) return TC_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> g(ctx->pred_mu);
+  cudaSetDevice(ctx->device);
+  if (!enabled) tc::stop_latency_worker(ctx, nullptr);
+  ctx->lw_enabled = enabled != 0;
+  return TC_OK;
+}
+
 tc_status tc_ctx_synchronize(tc_ctx* ctx, int timeout_ms) {
   if (!ctx) return TC_ERR_INVALID_ARG;
   // not while another thread's training call may be capturing the stream

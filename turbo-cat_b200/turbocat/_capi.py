@@ -25,8 +25,8 @@ TRANSFORM = {"raw": 0, "sigmoid": 1, "softmax": 2}
 # every symbol include/tcgpu.h declares
 SYMBOLS = [
     "tc_ctx_create", "tc_ctx_destroy", "tc_last_error", "tc_ctx_memory", "tc_ctx_fail_next_allocs",
-    "tc_ctx_synchronize", "tc_dataset_upload", "tc_dataset_destroy", "tc_quantize", "tc_apply_bins",
-    "tc_dataset_bins",
+    "tc_ctx_synchronize", "tc_ctx_set_latency_worker", "tc_dataset_upload", "tc_dataset_destroy", "tc_quantize",
+    "tc_apply_bins", "tc_dataset_bins",
     "tc_trainer_create", "tc_trainer_step", "tc_trainer_reset", "tc_trainer_stats", "tc_trainer_profile",
     "tc_trainer_train_scores", "tc_trainer_sample_mask", "tc_trainer_set_validation", "tc_trainer_valid_loss",
     "tc_trainer_model", "tc_trainer_destroy", "tc_train", "tc_build_tree", "tc_histogram_root_noalloc",
@@ -337,6 +337,11 @@ class Engine:
 
     def synchronize(self, timeout_ms=10000):
         self._chk(lib().tc_ctx_synchronize(self.ctx, C.c_int(timeout_ms)))
+
+    def set_latency_worker(self, enabled):
+        """Small predict requests through the persistent latency worker (True,
+        the default) or one kernel launch each (False)."""
+        self._chk(lib().tc_ctx_set_latency_worker(self.ctx, C.c_int(1 if enabled else 0)))
 
     def close(self):
         if self.ctx:
