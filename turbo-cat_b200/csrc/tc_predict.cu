@@ -496,9 +496,22 @@ __device__ __forceinline__ void small_trees(const ModelDesc& md, const float* __
   for (int k = 0; k < PRED_MAX_K; ++k)
     if (k < K) s_red[threadIdx.x * K + k] = acc[k];
   __syncthreads();
-  for (int h = TG >> 1; h > 0; h >>= 1) {  // lanes pairwise, fixed order
+  // lanes pairwise, fixed order: thread t adds thread t + h * RT; once
+  // h * RT <= 16 every pair lies in warp 0, which finishes with shuffles
+  int h = TG >> 1;
+  for (; h > 0 && h * RT >= 32; h >>= 1) {
     if (tg < h)
       for (int k = 0; k < K; ++k) s_red[threadIdx.x * K + k] += s_red[(threadIdx.x + h * RT) * K + k];
+    __syncthreads();
+  }
+  if (h > 0) {
+    if (threadIdx.x < 32) {
+      for (int k = 0; k < K; ++k) {
+        float v = s_red[threadIdx.x * K + k];
+        for (int hh = h; hh > 0; hh >>= 1) v += __shfl_down_sync(0xffffffffu, v, hh * RT);
+        if (threadIdx.x < RT) s_red[threadIdx.x * K + k] = v;
+      }
+    }
     __syncthreads();
   }
 }
@@ -652,18 +665,26 @@ constexpr uint32_t kLwEnd = 0xffffffffu;  // announcement: the worker ends (a re
 // [n b / nb, n (b + 1) / nb) (nb = min(worker blocks, n)), loads them from the
 // pinned mailbox itself (16-byte loads of the aligned range, all in flight
 // together), walks every tree for them (the model from global memory, L2
-// resident) and writes their outputs into the mailbox; the last block to
+// resident; its splits in shared memory when they fit) and writes their
+// outputs into the mailbox; the last block to
 // finish (completion counter) publishes seq_done.  One thread of block 0
 // polls the request word (system-scope acquire loads over the bus) and
 // announces each request, or the end, to the other blocks through a device
 // word (generation counter).  Shared memory: [rows 64 x (f+1)][sums 512 x K].
 __global__ void __launch_bounds__(SMALL_THREADS) k_predict_worker(ModelDesc md, LwBox* box, uint32_t* flag,
-                                                                   uint32_t seen) {
+                                                                   uint32_t seen, int resident_splits) {
   extern __shared__ __align__(16) float sm_w[];
   __shared__ uint32_t s_cmd, s_req;
-  const int f = md.n_features, fs = f + 1, K = md.n_classes, T = md.n_trees;
+  const int f = md.n_features, fs = f + 1, K = md.n_classes, T = md.n_trees, D = md.max_depth;
   float* s_x = sm_w;                                   // [rows][f+1]
   float* s_red = s_x + (size_t)SMALL_ROWS * fs;        // [SMALL_THREADS][K]
+  // the model's splits, copied once per launch when they fit (leaves stay in L2)
+  uint2* s_sp = reinterpret_cast<uint2*>(s_red + (size_t)SMALL_THREADS * K);
+  const uint2* splits = md.splits;
+  if (resident_splits) {
+    for (int q = threadIdx.x; q < T * D; q += blockDim.x) s_sp[q] = md.splits[q];
+    splits = s_sp;
+  }
   uint32_t* counter = flag;                            // blocks done with the current request
   uint32_t* exits = flag + 32;                         // blocks that have left
   // block 0's announcement: generation << 32 | request word (kLwEnd: leave),
@@ -723,7 +744,7 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_predict_worker(ModelDesc md, 
         }
       }
       __syncthreads();
-      small_trees(md, s_x, nr, 0, T, s_red, md.splits, md.leaves, 0);
+      small_trees(md, s_x, nr, 0, T, s_red, splits, md.leaves, 0);
       for (uint32_t r = threadIdx.x; r < nr; r += blockDim.x) {
         float v[PRED_MAX_K];
         small_row_sums(md, nr, r, s_red, nullptr, 1, nullptr, v);
@@ -1241,8 +1262,11 @@ static tc_status lw_launch(tc_ctx* ctx, const tc_model* m) {
     cudaFuncSetAttribute(k_predict_worker, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr_done = true;
   }
-  const int T = m->info.n_trees, K = m->info.n_classes, f = m->info.n_features;
-  const size_t smem = ((size_t)SMALL_ROWS * (f + 1) + (size_t)SMALL_THREADS * K) * sizeof(float);
+  const int T = m->info.n_trees, K = m->info.n_classes, f = m->info.n_features, D = m->info.max_depth;
+  const size_t base_smem = ((size_t)SMALL_ROWS * (f + 1) + (size_t)SMALL_THREADS * K) * sizeof(float);
+  const size_t split_bytes = (size_t)T * D * sizeof(uint2);
+  int resident = base_smem % 8 == 0 && base_smem + split_bytes <= 160 * 1024 ? 1 : 0;
+  const size_t smem = base_smem + (resident ? split_bytes : 0);
   // blocks: a 64-row request split so that a block walks ~4096 (row, tree) pairs
   const long long want = ((long long)T * SMALL_ROWS + SMALL_WALKS_PER_BLOCK - 1) / SMALL_WALKS_PER_BLOCK;
   int per_sm = 0;
@@ -1259,7 +1283,7 @@ static tc_status lw_launch(tc_ctx* ctx, const tc_model* m) {
   LwBox* bd = static_cast<LwBox*>(ctx->lw_box_dev);
   uint32_t* flag = static_cast<uint32_t*>(ctx->lw_dev);
   uint32_t seen = box->seq_done;
-  void* args[] = {&md, &bd, &flag, &seen};
+  void* args[] = {&md, &bd, &flag, &seen, &resident};
   TC_CUDA(ctx, cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_predict_worker), dim3(NB),
                                            dim3(SMALL_THREADS), args, smem, ctx->lw_stream));
   ctx->lw_running = true;
