@@ -303,7 +303,12 @@ tc_status tc_model_import(tc_ctx* ctx, const tc_model_info* info, const int32_t*
                           const float* edges, const uint16_t* n_edges, tc_model** out);
 /* TCAT v3 stream (Booster::save_binary / load_binary,
  * src/boosting/booster.cpp:1049-1203 and src/tree/symmetric_tree.cpp:1199-1239).
- * tc_model_save_tcat: pass buf = NULL to query the size. */
+ * tc_model_save_tcat: pass buf = NULL to query the size.
+ * tc_model_load_tcat also reads single-output models of regular (depth-wise)
+ * trees (the reference's mode="small"; src/tree/tree.cpp:1748-1840): they
+ * predict through tc_predict / tc_predict_device as the reference predicts
+ * them (its binning against the model's edges, then the node walk) and save
+ * back byte for byte; tc_model_export and tc_server_add_model refuse them. */
 tc_status tc_model_save_tcat(const tc_model* m, uint8_t* buf, size_t* len);
 tc_status tc_model_load_tcat(tc_ctx* ctx, const uint8_t* buf, size_t len, tc_model** out);
 void tc_model_destroy(tc_model* m);

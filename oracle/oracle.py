@@ -82,6 +82,7 @@ class RefParams(C.Structure):
         ("min_child_weight", C.c_float),
         ("min_split_gain", C.c_float),
         ("max_delta_step", C.c_float),
+        ("regular", C.c_int32),
     ]
 
 
@@ -109,6 +110,7 @@ class Hyper:
     use_goss: bool = False          # GOSS row sampling (chosen over subsample)
     goss_top_rate: float = 0.2
     goss_other_rate: float = 0.1
+    regular_trees: bool = False     # reference probe only: regular (depth-wise) trees
 
     def tree(self) -> TreeParams:
         return TreeParams(self.max_depth, self.max_bins, self.min_samples_leaf, self.lambda_l2,
@@ -125,7 +127,8 @@ class Hyper:
         return RefParams(LOSS_IDS[self.loss], self.n_classes if self.loss == "softmax" else 2,
                          self.n_estimators, self.max_depth, self.max_bins, self.min_samples_leaf,
                          self.learning_rate, self.lambda_l2, self.lambda_l1,
-                         self.min_child_weight, self.min_split_gain, self.max_delta_step)
+                         self.min_child_weight, self.min_split_gain, self.max_delta_step,
+                         1 if self.regular_trees else 0)
 
 
 _lib = None
@@ -580,3 +583,113 @@ def early_stopping(ens: Ensemble, Xv, yv, loss: str, n_estimators: int, rounds: 
         if rounds >= 0 and it >= min_it and no_imp >= rounds:
             return np.array(losses), it, best_it
     return np.array(losses), -1, best_it
+
+
+# ------------------------------------------------ regular (depth-wise) trees --
+# Serving of models the reference trained with regular trees (mode="small").
+
+@dataclass
+class RegularModel:
+    base: float
+    task: int
+    n_classes: int
+    learning_rate: float
+    max_depth: int
+    lambda_l2: float
+    edges: list          # per feature: float32 array of its bin edges
+    weights: np.ndarray  # [T] float32
+    trees: list          # per tree: dict of node arrays (feature, split_bin, is_leaf, left, right, value)
+
+
+def parse_tcat_regular(data: bytes) -> RegularModel:
+    """TCAT v3 holding regular trees: Booster::save_binary / load_binary
+    (src/boosting/booster.cpp:1049-1110, 1140-1203) and Tree::save / load
+    (src/tree/tree.cpp:1748-1840): per tree depth u16, classes u32, nodes u32,
+    leaves u16, max_depth u16, lambda f32, then 16-byte nodes (feature u16,
+    bin u8, flags u8 = is_leaf | default_left << 1, left u16, right u16,
+    value f32, gain f32)."""
+    import struct
+
+    o = 0
+
+    def rd(fmt):
+        nonlocal o
+        v = struct.unpack_from("<" + fmt, data, o)
+        o += struct.calcsize("<" + fmt)
+        return v if len(v) > 1 else v[0]
+
+    assert data[:4] == b"TCAT"
+    o = 4
+    assert rd("I") == 3
+    base = rd("f")
+    task = rd("B")
+    ncls = rd("I")
+    lr = rd("f")
+    md = rd("H")
+    lam = rd("f")
+    assert rd("B") == 0, "symmetric model"
+    nf = rd("Q")
+    edges = []
+    for _ in range(nf):
+        k = rd("Q")
+        edges.append(np.frombuffer(data, np.float32, k, o).copy())
+        o += 4 * k
+    nt = rd("Q")
+    w = np.frombuffer(data, np.float32, nt, o).copy()
+    o += 4 * nt
+    trees = []
+    for _ in range(nt):
+        _depth, tcls, nn, _nl, _md, _lam = rd("HIIHHf")
+        rec = np.frombuffer(data, np.dtype([("feature", "<u2"), ("bin", "u1"), ("flags", "u1"), ("left", "<u2"),
+                                            ("right", "<u2"), ("value", "<f4"), ("gain", "<f4")]), nn, o)
+        o += 16 * nn
+        assert tcls <= 1, "multiclass regular trees"
+        trees.append(dict(feature=rec["feature"].astype(np.int64), split_bin=rec["bin"].astype(np.int64),
+                          is_leaf=(rec["flags"] & 1).astype(bool), left=rec["left"].astype(np.int64),
+                          right=rec["right"].astype(np.int64), value=rec["value"].copy()))
+    return RegularModel(base, task, ncls, lr, md, lam, edges, w, trees)
+
+
+def bin_regular(X, edges):
+    """The reference's binning of prediction rows for regular trees
+    (Booster::predict_raw_fast, src/boosting/booster.cpp:706-845): NaN -> 255;
+    a feature of at most 16 edges takes the number of edges <= x (its linear
+    scan), one of more edges std::lower_bound, the number of edges < x."""
+    X = np.asarray(X, np.float32)
+    out = np.zeros(X.shape, np.int64)
+    for j, e in enumerate(edges):
+        col = X[:, j]
+        if len(e) == 0:
+            b = np.zeros(len(col), np.int64)
+        elif len(e) <= 16:
+            b = np.searchsorted(e, col, side="right")
+        else:
+            b = np.searchsorted(e, col, side="left")
+        out[:, j] = np.where(np.isnan(col), 255, b)
+    return out
+
+
+def predict_regular(m: RegularModel, X, fp64=False):
+    """Raw scores (base included) of a regular-tree model
+    (TreeEnsemble::predict_batch_optimized, src/tree/tree.cpp:1471-1560): per
+    row, trees in order, walk to a leaf going right iff bin != 255 and
+    bin > split_bin, sum += weight * value (one fused multiply-add in the
+    reference's FP32 build; emulated through FP64), then + base."""
+    B = bin_regular(X, m.edges)
+    n = B.shape[0]
+    out = np.zeros(n, np.float64 if fp64 else np.float32)
+    for i in range(n):
+        row = B[i]
+        s = 0.0 if fp64 else np.float32(0.0)
+        for t, tr in enumerate(m.trees):
+            node = 0
+            while not tr["is_leaf"][node]:
+                b = row[tr["feature"][node]]
+                node = tr["right"][node] if (b != 255 and b > tr["split_bin"][node]) else tr["left"][node]
+            v = float(tr["value"][node])
+            if fp64:
+                s += float(m.weights[t]) * v
+            else:
+                s = np.float32(float(m.weights[t]) * v + float(s))
+        out[i] = (s + m.base) if fp64 else np.float32(s + np.float32(m.base))
+    return out

@@ -42,6 +42,7 @@ struct Params {
   float min_child_weight;
   float min_split_gain;
   float max_delta_step;
+  int32_t regular;         // 1: regular (depth-wise) trees instead of symmetric ones
 };
 
 Config make_config(const Params& p) {
@@ -67,7 +68,7 @@ Config make_config(const Params& p) {
   cfg.tree.min_samples_leaf = static_cast<uint32_t>(p.min_samples_leaf);
   cfg.tree.min_split_gain = p.min_split_gain;
   cfg.tree.max_delta_step = p.max_delta_step;
-  cfg.tree.use_symmetric = true;
+  cfg.tree.use_symmetric = p.regular == 0;
   cfg.verbosity = 0;
   return cfg;
 }

@@ -110,3 +110,26 @@ def noisy_binary_split(n=3000, nv=2000, f=10, seed=81, noise=2.0):
     w = rng.standard_normal(f)
     y = ((X @ w + rng.normal(0, noise, n + nv)) > 0).astype(np.float32)
     return X[:n], y[:n], X[n:], y[n:]
+
+
+def regular_case():
+    """Data of the regular-tree golden model: the binary generator with a
+    discrete feature (at most 16 bin edges, the reference's linear-scan
+    binning at prediction) and NaN values."""
+    X, y = binary_c1(3000, 12, seed=41)
+    X[:, 5] = np.round(X[:, 5] * 2) / 2
+    X[::13, 2] = np.nan
+    return X, y
+
+
+def regular_pred_matrix(X, edges):
+    """Prediction rows for the regular-tree golden model: the first 400
+    training rows, 200 of them with one feature set exactly to one of its bin
+    edges (where the two binning rules of the reference differ)."""
+    P = np.array(X[:400], np.float32)
+    for r in range(200):
+        j = r % P.shape[1]
+        e = edges[j]
+        if len(e):
+            P[r, j] = e[(7 * r) % len(e)]
+    return P

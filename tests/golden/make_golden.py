@@ -23,7 +23,23 @@ import oracle as O  # noqa: E402
 from datagen import GOLDEN_CASES, make_case  # noqa: E402
 
 
+def regular_golden():
+    """A model of regular (depth-wise) trees trained by the reference
+    (mode="small") and its raw predictions through the reference's own
+    prediction path for such models."""
+    from datagen import regular_case, regular_pred_matrix
+
+    X, y = regular_case()
+    hp = O.Hyper(loss="logloss", n_estimators=40, max_depth=5, learning_rate=0.2, regular_trees=True)
+    _, model, _, _, _ = O.ref_fit(X, y, hp)
+    m = O.parse_tcat_regular(model)
+    P = regular_pred_matrix(X, m.edges)
+    raw = O.ref_predict(model, P, proba=False)
+    np.savez_compressed(os.path.join(HERE, "regular_small.npz"), tcat=np.frombuffer(model, np.uint8), pred_raw=raw)
+
+
 def main():
+    regular_golden()
     for name, spec in GOLDEN_CASES.items():
         X, y, hp = make_case(spec)
         if hp.loss == "softmax":

@@ -455,3 +455,46 @@ def test_autotuner_and_profile(engine, capi):
     ex = tr.model().export()
     if ref.min_margin > MARGIN:
         assert np.array_equal(ex["feature"], ref.feature)
+
+
+def test_predict_regular_model_from_reference(engine, capi, tmp_path):
+    """A model of regular (depth-wise) trees trained by the reference
+    (mode="small", tests/golden/make_golden.py) served on the device: the
+    reference's own predictions (stored in the fixture) within 1e-6 of the
+    scale (the same FP32 fused multiply-adds in the same order; the number of
+    bit-identical rows is printed), through tc_predict (tile and small
+    requests) and the facade; the stream saves back byte for byte; the model
+    has no symmetric export and the server refuses it."""
+    from datagen import regular_case, regular_pred_matrix
+
+    g = np.load(f"{O.HERE}/../tests/golden/regular_small.npz")
+    data = g["tcat"].tobytes()
+    rm = O.parse_tcat_regular(data)
+    X, _ = regular_case()
+    P = regular_pred_matrix(X, rm.edges)
+    want = g["pred_raw"]
+    scale = abs(rm.base) + sum(float(np.abs(t["value"]).max()) * float(w) for t, w in zip(rm.trees, rm.weights))
+    m = engine.load_tcat(data)
+    assert m.info.n_trees == 40 and m.info.n_features == P.shape[1]
+    raw = m.predict(P, "raw")[:, 0]
+    print("regular-tree rows bit-identical to the reference:", int(np.sum(raw == want)), "of", len(want))
+    assert np.max(np.abs(raw - want)) <= 1e-6 * scale
+    for n in (1, 5, 64, 65):
+        assert np.max(np.abs(m.predict(P[:n], "raw")[:, 0] - want[:n])) <= 1e-6 * scale, n
+    prob = m.predict(P, "sigmoid")[:, 0]
+    assert np.max(np.abs(prob - 1.0 / (1.0 + np.exp(-want.astype(np.float64))))) <= 1e-6
+    assert m.tcat() == data
+    with pytest.raises(capi.TCError):
+        m.export()
+    srv = capi.Server(engine)
+    with pytest.raises(capi.TCError):
+        srv.add_model(m)
+    srv.close()
+    import turbocat
+
+    path = str(tmp_path / "regular.tcat")
+    with open(path, "wb") as fh:
+        fh.write(data)
+    clf = turbocat.TurboCatClassifier(verbosity=0).load(path)
+    p1 = clf.predict_proba(P)[:, 1]
+    assert np.max(np.abs(p1 - 1.0 / (1.0 + np.exp(-want.astype(np.float64))))) <= 1e-6

@@ -165,6 +165,15 @@ struct tc_model {
   DevBuf<float> d_bord;             // binned form: borders of every virtual feature, Eytzinger order
   DevBuf<uint2> d_vdesc;            // binned form: (feature, border offset | search steps << 24)
   int n_virtual = 0, n_bord = 0;
+  // regular (depth-wise) trees of a model the reference trained with
+  // mode="small" (served for prediction only; tc_predict.cu)
+  bool regular = false;
+  std::vector<uint8_t> tcat;        // the stream as loaded (saved back byte for byte)
+  DevBuf<uint4> d_rnodes;           // (feature | bin << 16 | leaf << 24, left, right, value bits), global indices
+  DevBuf<uint32_t> d_rroots;        // [T] first node of each tree
+  DevBuf<float> d_rweights;         // [T]
+  DevBuf<float> d_redges;           // [f][255] bin edges
+  DevBuf<int32_t> d_rnedges;        // [f]
   tc_status upload();
 };
 

@@ -773,6 +773,77 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_predict_worker(ModelDesc md, 
   if (threadIdx.x == 0 && atomicAdd(exits, 1u) == gridDim.x - 1) st_release_sys(&box->exited, 1u);
 }
 
+// ------------------------------------------------------ regular trees --
+// Models of regular (depth-wise) trees the reference trained with
+// mode="small" are served as the reference predicts them
+// (Booster::predict_raw_fast, src/boosting/booster.cpp:680-870, and
+// TreeEnsemble::predict_batch_optimized, src/tree/tree.cpp:1471-1560): each
+// row is binned against the model's edges (NaN -> 255; a feature of at most
+// 16 edges takes the number of edges <= x, one of more edges std::lower_bound,
+// the number of edges < x), then every tree is walked in order (right iff
+// bin != 255 and bin > the node's bin) and sum = fma(weight, leaf, sum) in
+// FP32, as the reference's build computes it; then + base and the transform.
+// A block takes RB rows: their bins in shared memory, one thread per row
+// walking the trees (nodes from L2).  Node children always follow their
+// parent (checked at load), so every walk ends.
+struct RegDesc {
+  const uint4* nodes;
+  const uint32_t* roots;
+  const float* weights;
+  const float* edges;   // [f][255]
+  const int32_t* nedges;
+  int32_t n_trees, n_features, n_nodes;
+  float base;
+};
+
+__global__ void __launch_bounds__(128) k_predict_regular(RegDesc rd, const float* __restrict__ X, uint32_t n,
+                                                         int rows_per_block, int transform, float* __restrict__ out) {
+  extern __shared__ uint8_t s_b[];  // [rows_per_block][f]
+  const int f = rd.n_features;
+  const uint32_t r0 = blockIdx.x * (uint32_t)rows_per_block;
+  const int nr = (int)min((uint32_t)rows_per_block, n - r0);
+  for (int q = threadIdx.x; q < nr * f; q += blockDim.x) {
+    const int r = q / f, j = q - r * f;
+    const float x = X[(size_t)(r0 + r) * f + j];
+    uint32_t b = 255;
+    if (!isnan(x)) {
+      const float* e = rd.edges + (size_t)j * 255;
+      const int ne = rd.nedges[j];
+      int lo = 0, hi = ne;  // first edge with x < e (at most 16 edges) or x <= e (more)
+      if (ne <= 16) {
+        while (lo < hi) {
+          const int mid = (lo + hi) >> 1;
+          if (e[mid] <= x) lo = mid + 1; else hi = mid;
+        }
+      } else {
+        while (lo < hi) {
+          const int mid = (lo + hi) >> 1;
+          if (e[mid] < x) lo = mid + 1; else hi = mid;
+        }
+      }
+      b = (uint32_t)lo;  // 255 beyond the last of 255 edges: routed left like NaN, as in the reference
+    }
+    s_b[q] = (uint8_t)b;
+  }
+  __syncthreads();
+  const int r = threadIdx.x;
+  if (r >= nr) return;
+  const uint8_t* row = s_b + (size_t)r * f;
+  float sum = 0.0f;
+  for (int t = 0; t < rd.n_trees; ++t) {
+    uint32_t node = rd.roots[t];
+    uint4 nd = rd.nodes[node];
+    for (int guard = 0; !(nd.x >> 24) && guard < rd.n_nodes; ++guard) {
+      const uint32_t b = row[nd.x & 0xffffu];
+      node = (b != 255u && b > ((nd.x >> 16) & 0xffu)) ? nd.z : nd.y;
+      nd = rd.nodes[node];
+    }
+    sum = fmaf(rd.weights[t], __uint_as_float(nd.w), sum);
+  }
+  const float raw = sum + rd.base;
+  out[r0 + r] = transform == TC_TRANSFORM_SIGMOID ? sigmoidf_ref(raw) : raw;
+}
+
 // Stage sizes for a batch whose deepest model has depth max_depth: a leaf
 // stage holds at least one tree per warp (16 KB at least); a split stage
 // holds the splits of as many trees as the leaf stage takes, for every depth
@@ -1000,7 +1071,21 @@ void stop_latency_worker(tc_ctx* ctx, const tc_model* m) {
 tc_status predict_device(tc_ctx* ctx, const tc_model* m, const float* X, uint32_t n, uint32_t f, int transform,
                          float* out, cudaStream_t stream) {
   if (n == 0) return TC_OK;
-  (void)f;
+  if (m->regular) {
+    RegDesc rd{m->d_rnodes.p, m->d_rroots.p, m->d_rweights.p, m->d_redges.p, m->d_rnedges.p,
+               m->info.n_trees, m->info.n_features, (int)m->d_rnodes.n, m->info.base_prediction};
+    const int rpb = (int)std::max<size_t>(1, std::min<size_t>(128, (size_t)160 * 1024 / std::max<uint32_t>(1, f)));
+    const size_t smem = (size_t)rpb * f;
+    static bool attr_done = false;
+    if (!attr_done) {
+      cudaFuncSetAttribute(k_predict_regular, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+      attr_done = true;
+    }
+    k_predict_regular<<<(n + rpb - 1) / rpb, 128, smem, stream>>>(rd, X, n, rpb, transform, out);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return ctx->cuda_fail(e, "k_predict_regular");
+    return TC_OK;
+  }
   JobTable jt{};
   jt.reqs = nullptr;
   jt.n_jobs = 1;
@@ -1053,6 +1138,8 @@ tc_status tc_model_info_get(const tc_model* m, tc_model_info* info) {
 tc_status tc_model_export(const tc_model* m, int32_t* depth, uint16_t* feature, uint8_t* bin, float* threshold,
                           float* gain, float* leaves, float* weights, float* edges, uint16_t* n_edges) {
   if (!m) return TC_ERR_INVALID_ARG;
+  if (m->regular)
+    return m->ctx->fail(TC_ERR_INVALID_ARG, "a model of regular trees has no symmetric-tree export");
   auto cp = [](void* dst, const auto& v) {
     if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
   };
@@ -1120,6 +1207,14 @@ tc_status tc_model_import(tc_ctx* ctx, const tc_model_info* info, const int32_t*
 // host-endian, size_t counts.
 tc_status tc_model_save_tcat(const tc_model* m, uint8_t* buf, size_t* len) {
   if (!m || !len) return TC_ERR_INVALID_ARG;
+  if (m->regular) {  // the stream as loaded (the reference's own bytes)
+    if (buf) {
+      if (*len < m->tcat.size()) return TC_ERR_INVALID_ARG;
+      std::memcpy(buf, m->tcat.data(), m->tcat.size());
+    }
+    *len = m->tcat.size();
+    return TC_OK;
+  }
   std::vector<uint8_t> b;
   put(b, "TCAT", 4);
   const uint32_t version = 3;
@@ -1173,8 +1268,95 @@ tc_status tc_model_save_tcat(const tc_model* m, uint8_t* buf, size_t* len) {
   return TC_OK;
 }
 
-// TCAT v3 reader (Booster::load_binary, src/boosting/booster.cpp:1120-1203);
-// symmetric models only.
+// The regular-tree branch of the TCAT v3 reader (Booster::load_binary,
+// src/boosting/booster.cpp:1140-1203; Tree::load, src/tree/tree.cpp:1795-1840):
+// single-output models (multiclass regular trees are refused).
+static tc_status load_regular(tc_ctx* ctx, Reader& r, tc_model_info info, const uint8_t* buf, size_t len,
+                              tc_model** out) {
+  if (info.task == TC_TASK_MULTICLASS) return ctx->fail(TC_ERR_FORMAT, "multiclass regular trees are not served");
+  info.n_classes = 1;
+  const uint64_t nf = r.get<uint64_t>();
+  if (!r.ok || nf == 0 || nf > 65535) return ctx->fail(TC_ERR_FORMAT, "TCAT feature count");
+  std::vector<float> edges((size_t)nf * 255, 0.0f);
+  std::vector<int32_t> ne(nf);
+  for (uint64_t j = 0; j < nf; ++j) {
+    const uint64_t k = r.get<uint64_t>();
+    if (!r.ok || k > 255) return ctx->fail(TC_ERR_FORMAT, "TCAT edge count");
+    ne[j] = (int32_t)k;
+    if (k && !r.bytes(&edges[j * 255], k * 4)) return ctx->fail(TC_ERR_FORMAT, "truncated TCAT edges");
+  }
+  const uint64_t nt = r.get<uint64_t>();
+  if (!r.ok || nt > (1ull << 24)) return ctx->fail(TC_ERR_FORMAT, "TCAT tree count");
+  std::vector<float> w(nt);
+  for (uint64_t t = 0; t < nt; ++t) w[t] = r.get<float>();
+  std::vector<uint4> nodes;
+  std::vector<uint32_t> roots(nt);
+  for (uint64_t t = 0; t < nt && r.ok; ++t) {
+    r.get<uint16_t>();  // depth
+    const uint32_t tcls = r.get<uint32_t>();
+    const uint32_t nn = r.get<uint32_t>();
+    r.get<uint16_t>();  // leaves
+    r.get<uint16_t>();  // max_depth
+    r.get<float>();     // lambda_l2
+    if (!r.ok) break;
+    if (tcls > 1) return ctx->fail(TC_ERR_FORMAT, "multiclass regular trees are not served");
+    if (nn == 0 || nn > 65535)
+      return ctx->fail(TC_ERR_FORMAT, "TCAT tree %llu has %u nodes", (unsigned long long)t, nn);
+    roots[t] = (uint32_t)nodes.size();
+    for (uint32_t i = 0; i < nn && r.ok; ++i) {
+      const uint16_t feat = r.get<uint16_t>();
+      const uint8_t bin = r.get<uint8_t>();
+      const uint8_t flags = r.get<uint8_t>();
+      const uint16_t lc = r.get<uint16_t>(), rc = r.get<uint16_t>();
+      const float value = r.get<float>();
+      r.get<float>();  // gain
+      const bool leaf = flags & 1u;
+      // children follow their parent (the reference adds them after it), so walks end
+      if (!leaf && (feat >= nf || lc <= i || rc <= i || lc >= nn || rc >= nn))
+        return ctx->fail(TC_ERR_FORMAT, "TCAT tree %llu node %u: bad split", (unsigned long long)t, i);
+      uint32_t vb;
+      std::memcpy(&vb, &value, 4);
+      nodes.push_back(make_uint4((uint32_t)feat | (uint32_t)bin << 16 | (leaf ? 1u : 0u) << 24,
+                                 leaf ? 0u : roots[t] + lc, leaf ? 0u : roots[t] + rc, vb));
+    }
+  }
+  if (!r.ok) return ctx->fail(TC_ERR_FORMAT, "truncated TCAT stream");
+  info.n_trees = (int)nt;
+  info.n_features = (int)nf;
+  cudaSetDevice(ctx->device);
+  tc_model* m = new tc_model();
+  m->ctx = ctx;
+  m->info = info;
+  m->regular = true;
+  m->tcat.assign(buf, buf + len);
+  m->weights = w;
+  auto up = [&]() -> tc_status {
+    TC_TRY(m->d_rnodes.alloc(ctx, std::max<size_t>(1, nodes.size()), "regular tree nodes"));
+    TC_TRY(m->d_rroots.alloc(ctx, std::max<size_t>(1, nt), "regular tree roots"));
+    TC_TRY(m->d_rweights.alloc(ctx, std::max<size_t>(1, nt), "regular tree weights"));
+    TC_TRY(m->d_redges.alloc(ctx, edges.size(), "regular model edges"));
+    TC_TRY(m->d_rnedges.alloc(ctx, ne.size(), "regular model edge counts"));
+    if (!nodes.empty())
+      TC_CUDA(ctx, cudaMemcpy(m->d_rnodes.p, nodes.data(), nodes.size() * sizeof(uint4), cudaMemcpyHostToDevice));
+    if (nt) {
+      TC_CUDA(ctx, cudaMemcpy(m->d_rroots.p, roots.data(), nt * 4, cudaMemcpyHostToDevice));
+      TC_CUDA(ctx, cudaMemcpy(m->d_rweights.p, w.data(), nt * 4, cudaMemcpyHostToDevice));
+    }
+    TC_CUDA(ctx, cudaMemcpy(m->d_redges.p, edges.data(), edges.size() * 4, cudaMemcpyHostToDevice));
+    TC_CUDA(ctx, cudaMemcpy(m->d_rnedges.p, ne.data(), ne.size() * 4, cudaMemcpyHostToDevice));
+    return TC_OK;
+  };
+  const tc_status s = up();
+  if (s != TC_OK) {
+    delete m;
+    return s;
+  }
+  *out = m;
+  return TC_OK;
+}
+
+// TCAT v3 reader (Booster::load_binary, src/boosting/booster.cpp:1120-1203):
+// symmetric models here, regular ones through load_regular.
 tc_status tc_model_load_tcat(tc_ctx* ctx, const uint8_t* buf, size_t len, tc_model** out) {
   if (!ctx || !buf || !out) return TC_ERR_INVALID_ARG;
   Reader r{buf, len};
@@ -1192,7 +1374,7 @@ tc_status tc_model_load_tcat(tc_ctx* ctx, const uint8_t* buf, size_t len, tc_mod
   info.lambda_l2 = r.get<float>();
   const uint8_t sym = r.get<uint8_t>();
   if (!r.ok) return ctx->fail(TC_ERR_FORMAT, "truncated TCAT header");
-  if (!sym) return ctx->fail(TC_ERR_FORMAT, "TCAT model holds regular trees; only symmetric trees are served");
+  if (!sym) return load_regular(ctx, r, info, buf, len, out);
   if (info.max_depth > kModelMaxDepth) return ctx->fail(TC_ERR_FORMAT, "TCAT max_depth %d too large", info.max_depth);
   info.n_classes = info.task == TC_TASK_MULTICLASS ? (int)ncls : 1;
   if (info.n_classes < 1 || info.n_classes > 16) return ctx->fail(TC_ERR_FORMAT, "TCAT class count %u", ncls);
@@ -1400,7 +1582,7 @@ tc_status tc_predict(tc_ctx* ctx, const tc_model* m, const float* X, uint32_t n,
   if (n == 0) return TC_OK;
   cudaSetDevice(ctx->device);
   const int K = m->info.n_classes;
-  if (n <= (uint32_t)SMALL_ROWS && K <= PRED_MAX_K && f <= SMALL_MAX_F && m->info.n_trees > 0) {
+  if (!m->regular && n <= (uint32_t)SMALL_ROWS && K <= PRED_MAX_K && f <= SMALL_MAX_F && m->info.n_trees > 0) {
     std::lock_guard<std::mutex> g(ctx->pred_mu);
     if (ctx->lw_enabled) return predict_worker(ctx, m, X, n, f, transform, out);
     return predict_small(ctx, m, X, n, f, transform, out);

@@ -268,6 +268,7 @@ tc_status tc_server_add_model(tc_server* s, const tc_model* m, int32_t* model_id
   tc_ctx* ctx = s->ctx;
   if (s->worker.joinable()) return ctx->fail(TC_ERR_BUSY, "models must be added before the first request");
   if (s->models.size() >= 64) return ctx->fail(TC_ERR_INVALID_ARG, "at most 64 resident models");
+  if (m->regular) return ctx->fail(TC_ERR_INVALID_ARG, "models of regular trees are served by tc_predict only");
   cudaSetDevice(ctx->device);
   s->models.push_back(model_desc(m));
   s->model_ptrs.push_back(m);
