@@ -460,11 +460,11 @@ def test_autotuner_and_profile(engine, capi):
 def test_predict_regular_model_from_reference(engine, capi, tmp_path):
     """A model of regular (depth-wise) trees trained by the reference
     (mode="small", tests/golden/make_golden.py) served on the device: the
-    reference's own predictions (stored in the fixture) within 1e-6 of the
-    scale (the same FP32 fused multiply-adds in the same order; the number of
-    bit-identical rows is printed), through tc_predict (tile and small
-    requests) and the facade; the stream saves back byte for byte; the model
-    has no symmetric export and the server refuses it."""
+    reference's own predictions (stored in the fixture) bit for bit (the same
+    binning, node walk and FP32 fused multiply-adds in tree order), through
+    tc_predict (tile and small requests) and the facade; the stream saves
+    back byte for byte; the model has no symmetric export and the server
+    refuses it."""
     from datagen import regular_case, regular_pred_matrix
 
     g = np.load(f"{O.HERE}/../tests/golden/regular_small.npz")
@@ -477,10 +477,11 @@ def test_predict_regular_model_from_reference(engine, capi, tmp_path):
     m = engine.load_tcat(data)
     assert m.info.n_trees == 40 and m.info.n_features == P.shape[1]
     raw = m.predict(P, "raw")[:, 0]
-    print("regular-tree rows bit-identical to the reference:", int(np.sum(raw == want)), "of", len(want))
-    assert np.max(np.abs(raw - want)) <= 1e-6 * scale
+    assert np.array_equal(raw, want)
     for n in (1, 5, 64, 65):
-        assert np.max(np.abs(m.predict(P[:n], "raw")[:, 0] - want[:n])) <= 1e-6 * scale, n
+        assert np.array_equal(m.predict(P[:n], "raw")[:, 0], want[:n]), n
+    p64 = O.predict_regular(rm, P, fp64=True)
+    assert np.max(np.abs(raw - p64)) <= 1e-6 * scale
     prob = m.predict(P, "sigmoid")[:, 0]
     assert np.max(np.abs(prob - 1.0 / (1.0 + np.exp(-want.astype(np.float64))))) <= 1e-6
     assert m.tcat() == data
