@@ -55,3 +55,44 @@ def test_threads_share_a_context(engine, capi):
         assert np.array_equal(ex["feature"], alone["feature"]) and np.array_equal(ex["bin"], alone["bin"])
         assert np.allclose(ex["leaves"], alone["leaves"], rtol=1e-5, atol=1e-6)
         assert results[("pred", i)]
+
+
+def test_threads_small_requests_two_models(engine, capi):
+    """Small requests (at most 64 rows: the latency worker) from several
+    threads at once, alternating between two models (the worker restarts for
+    the other model under the context's lock) while another thread trains:
+    every result equals the one predicted alone, bit for bit."""
+    X, y = binary_c1(20_000, 16, seed=72)
+    ds = engine.upload(X, y)
+    ds.quantize(255)
+    p1 = capi.params(loss="logloss", n_estimators=40, max_depth=6, learning_rate=0.1)
+    p2 = capi.params(loss="logloss", n_estimators=12, max_depth=4, learning_rate=0.3)
+    m1, _ = engine.train(ds, p1)
+    m2, _ = engine.train(ds, p2)
+    sizes = (1, 7, 64)
+    want = {(k, n): m.predict(X[:n], "sigmoid") for k, m in ((1, m1), (2, m2)) for n in sizes}
+    errors = []
+
+    def serve(i):
+        try:
+            for r in range(30):
+                k, m = ((1, m1), (2, m2))[(i + r) % 2]
+                n = sizes[(i + r) % 3]
+                if not np.array_equal(m.predict(X[:n], "sigmoid"), want[(k, n)]):
+                    raise AssertionError(f"small request changed under concurrency ({k}, {n})")
+        except Exception as e:  # surfaced below
+            errors.append(e)
+
+    def train():
+        try:
+            tr = engine.trainer(ds, p2)
+            tr.step(12)
+        except Exception as e:
+            errors.append(e)
+
+    ts = [threading.Thread(target=serve, args=(i,)) for i in range(4)] + [threading.Thread(target=train)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    assert not errors, errors
