@@ -92,6 +92,10 @@ void tc_ctx_destroy(tc_ctx* ctx) {
   ctx->allocs.clear();
   if (ctx->pin_io) cudaFreeHost(ctx->pin_io);
   if (ctx->lw_box) cudaFreeHost(ctx->lw_box);
+  for (int b = 0; b < 2; ++b) {
+    if (ctx->up_stage[b]) cudaFreeHost(ctx->up_stage[b]);
+    if (ctx->up_ev[b]) cudaEventDestroy(ctx->up_ev[b]);
+  }
   if (ctx->lw_stream) cudaStreamDestroy(ctx->lw_stream);
   cudaStreamDestroy(ctx->stream);
   cudaStreamDestroy(ctx->pred_stream);

@@ -19,6 +19,9 @@
 //      bytes wide) and column-major [f][np] (partition kernels, export).
 #include <algorithm>
 
+#include <cstring>
+#include <thread>
+
 #include "tc_internal.h"
 
 namespace tc {
@@ -393,6 +396,46 @@ tc_status apply_bins(tc_dataset* ds, const tc_dataset* ref) {
 
 }  // namespace tc
 
+namespace {
+
+constexpr size_t kUpChunk = (size_t)128 << 20;  // bytes of one pinned staging chunk
+
+// Host -> device copy of a large pageable buffer: chunks are copied into two
+// pinned staging buffers by host threads (each a slice of the chunk) while
+// the other buffer's chunk is on its way to the device, so the transfer runs
+// at the link's rate instead of the driver's single-threaded pageable copy.
+tc_status upload_staged(tc_ctx* ctx, void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  if (bytes <= 2 * kUpChunk) {
+    TC_CUDA(ctx, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+    return TC_OK;
+  }
+  for (int b = 0; b < 2; ++b) {
+    if (!ctx->up_stage[b]) TC_CUDA(ctx, cudaHostAlloc(&ctx->up_stage[b], kUpChunk, cudaHostAllocDefault));
+    if (!ctx->up_ev[b]) TC_CUDA(ctx, cudaEventCreateWithFlags(&ctx->up_ev[b], cudaEventDisableTiming));
+  }
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const int nt = (int)std::min(16u, std::max(1u, hw / 2));
+  const char* s = static_cast<const char*>(src);
+  char* d = static_cast<char*>(dst);
+  std::vector<std::thread> ts;
+  for (size_t off = 0, b = 0; off < bytes; off += kUpChunk, b ^= 1) {
+    const size_t len = std::min(kUpChunk, bytes - off);
+    TC_CUDA(ctx, cudaEventSynchronize(ctx->up_ev[b]));  // this buffer's previous chunk has left
+    char* stage = static_cast<char*>(ctx->up_stage[b]);
+    ts.clear();
+    for (int t = 0; t < nt; ++t) {
+      const size_t a = len * t / nt, e = len * (t + 1) / nt;
+      ts.emplace_back([=] { std::memcpy(stage + a, s + off + a, e - a); });
+    }
+    for (auto& th : ts) th.join();
+    TC_CUDA(ctx, cudaMemcpyAsync(d + off, stage, len, cudaMemcpyHostToDevice, st));
+    TC_CUDA(ctx, cudaEventRecord(ctx->up_ev[b], st));
+  }
+  return TC_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 tc_status tc_dataset_upload(tc_ctx* ctx, const float* X, uint32_t n, uint16_t f, const float* y,
@@ -420,7 +463,10 @@ tc_status tc_dataset_upload(tc_ctx* ctx, const float* X, uint32_t n, uint16_t f,
     return s;
   }
   cudaError_t e = cudaSuccess;
-  if (n > 0) e = cudaMemcpyAsync(ds->X.p, X, (size_t)n * f * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
+  if (n > 0 && upload_staged(ctx, ds->X.p, X, (size_t)n * f * sizeof(float), ctx->stream) != TC_OK) {
+    delete ds;
+    return TC_ERR_CUDA;
+  }
   if (e == cudaSuccess && y && n > 0)
     e = cudaMemcpyAsync(ds->y.p, y, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);

@@ -52,6 +52,10 @@ struct tc_ctx {
   size_t pin_floats = 0;
   void* small_scratch = nullptr;     // partials [blocks][rows][K] + counter
   size_t small_scratch_bytes = 0;
+  // staging of large uploads: two pinned chunks filled by host threads while
+  // the other one is copied to the device (tc_data.cu); guarded by train_mu
+  void* up_stage[2] = {nullptr, nullptr};
+  cudaEvent_t up_ev[2] = {nullptr, nullptr};
   // latency worker: a persistent kernel serving small requests of one model
   // through a pinned mailbox (tc_predict.cu); guarded by pred_mu
   void* lw_box = nullptr;            // mailbox, host pointer (pinned, mapped)
