@@ -423,9 +423,15 @@ tc_status upload_staged(tc_ctx* ctx, void* dst, const void* src, size_t bytes, c
     TC_CUDA(ctx, cudaEventSynchronize(ctx->up_ev[b]));  // this buffer's previous chunk has left
     char* stage = static_cast<char*>(ctx->up_stage[b]);
     ts.clear();
-    for (int t = 0; t < nt; ++t) {
-      const size_t a = len * t / nt, e = len * (t + 1) / nt;
-      ts.emplace_back([=] { std::memcpy(stage + a, s + off + a, e - a); });
+    size_t done_to = 0;  // bytes of the chunk copied on this thread when no helper thread could start
+    try {
+      for (int t = 0; t < nt; ++t) {
+        const size_t a = len * t / nt, e = len * (t + 1) / nt;
+        ts.emplace_back([=] { std::memcpy(stage + a, s + off + a, e - a); });
+        done_to = e;
+      }
+    } catch (const std::exception&) {
+      std::memcpy(stage + done_to, s + off + done_to, len - done_to);
     }
     for (auto& th : ts) th.join();
     TC_CUDA(ctx, cudaMemcpyAsync(d + off, stage, len, cudaMemcpyHostToDevice, st));
