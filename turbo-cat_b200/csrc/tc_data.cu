@@ -400,12 +400,17 @@ namespace {
 
 constexpr size_t kUpChunk = (size_t)128 << 20;  // bytes of one pinned staging chunk
 
-// Host -> device copy of a large pageable buffer: chunks are copied into two
+// Host -> device copy of a large pageable buffer (a page-locked one is copied
+// directly): chunks are copied into two
 // pinned staging buffers by host threads (each a slice of the chunk) while
 // the other buffer's chunk is on its way to the device, so the transfer runs
 // at the link's rate instead of the driver's single-threaded pageable copy.
 tc_status upload_staged(tc_ctx* ctx, void* dst, const void* src, size_t bytes, cudaStream_t st) {
-  if (bytes <= 2 * kUpChunk) {
+  cudaPointerAttributes pa;
+  bool pinned = false;
+  if (cudaPointerGetAttributes(&pa, src) == cudaSuccess) pinned = pa.type == cudaMemoryTypeHost;
+  else cudaGetLastError();
+  if (pinned || bytes <= 2 * kUpChunk) {  // page-locked already: one DMA at the link's rate
     TC_CUDA(ctx, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
     return TC_OK;
   }
