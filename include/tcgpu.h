@@ -99,13 +99,49 @@ tc_status tc_quantize(tc_dataset* ds, uint16_t max_bins, int compat_uint8_count,
                       uint16_t* n_edges_out);
 /* Bins ds with the edges of ref (a quantized dataset of the same context and
  * feature count): bin = number of ref's edges <= x, NaN -> 255, the same
- * assignment tc_quantize makes; ds can then be trained on or exported like a
- * quantized dataset.  Replaces Dataset::apply_bins (src/core/dataset.cpp:346-379)
- * for numeric features. */
+ * assignment tc_quantize makes for numeric features; ds can then be trained
+ * on, predicted from (tc_predict_dataset) or exported like a quantized
+ * dataset.  ref's categorical columns (tc_encode_categorical) are first
+ * replaced in ds's X by ref's global encoding of each row's category, 0.5
+ * for a category ref never saw, then binned the same way.  Replaces
+ * Dataset::apply_bins (src/core/dataset.cpp:346-379). */
 tc_status tc_apply_bins(tc_dataset* ds, const tc_dataset* ref);
 /* Host copy of the binned matrix, column-major [f][n]
  * (BinnedData::column, include/turbocat/dataset.hpp:27-82). */
 tc_status tc_dataset_bins(const tc_dataset* ds, uint8_t* bins_out);
+/* Host copy of the dataset's feature matrix X [n][f] as the device holds it
+ * (categorical columns hold their encodings once encoded). */
+tc_status tc_dataset_features(const tc_dataset* ds, float* X_out);
+
+/* Categorical target statistics (Dataset::compute_target_statistics,
+ * src/core/dataset.cpp:679-865). */
+#define TC_CAT_ORDERED 0 /* ordered TS: each row sees the rows before it in a random order */
+#define TC_CAT_CV 1      /* cross-validated TS: each row sees the rows of the other folds */
+typedef struct {
+  int32_t method;     /* TC_CAT_ORDERED or TC_CAT_CV */
+  float prior_weight; /* smoothing weight a of (sum + a * prior) / (count + a); the reference's is 1 */
+  int32_t cv_folds;   /* folds of TC_CAT_CV (2 .. 255); the reference's is 5 */
+  uint64_t seed;      /* draws the order / folds when `order` is NULL */
+} tc_cat_params;
+/* Replaces the categorical columns `features` of a labelled, not yet
+ * quantized dataset by their per-row target statistics and records each
+ * feature's global table (category -> (sum + a * prior) / (count + a) over all
+ * rows) for tc_apply_bins.  Category = (uint32)(int64) of the value; NaN rows
+ * get the prior (the mean label) and count in no statistic.  `order` (host,
+ * optional): TC_CAT_ORDERED, the processing order, a permutation of 0..n-1;
+ * TC_CAT_CV, each row's fold (< cv_folds).  NULL draws it from `seed` (the
+ * reference draws it from std::random_device, so its runs differ from one
+ * another; a given order reproduces them bit for bit).  tc_quantize then bins
+ * these columns by the reference's target-statistics rule: A = min(max_bins,
+ * U) edges, edge b = the distinct encoding of rank (b+1)*U/(A+1), bin =
+ * number of edges < x (src/core/dataset.cpp:183-240). */
+tc_status tc_encode_categorical(tc_dataset* ds, const uint16_t* features, uint16_t n_cat,
+                                const tc_cat_params* p, const uint32_t* order);
+/* One categorical feature's global table, sorted by category: with keys or
+ * vals NULL only *len is written (Dataset::target_stats,
+ * include/turbocat/dataset.hpp:207-226). */
+tc_status tc_category_table(const tc_dataset* ds, uint16_t feature, uint32_t* keys, float* vals,
+                            uint32_t* len);
 
 /* --------------------------------------------------------------- training */
 
@@ -336,6 +372,13 @@ tc_status tc_predict(tc_ctx* ctx, const tc_model* m, const float* X, uint32_t n,
  * without synchronising. */
 tc_status tc_predict_device(tc_ctx* ctx, const tc_model* m, const float* X_dev, uint32_t n,
                             uint16_t f, int32_t transform, float* out_dev, void* stream);
+/* Predicts a dataset's rows as the device holds them (after tc_apply_bins,
+ * categorical columns hold their encodings), into host `out`
+ * (Booster::predict_raw / predict_proba on a binned Dataset,
+ * src/boosting/booster.cpp:587-640; a split goes right iff x >= its
+ * threshold, which is bin > split bin for the training edges). */
+tc_status tc_predict_dataset(tc_ctx* ctx, const tc_model* m, const tc_dataset* ds, int32_t transform,
+                             float* out);
 
 /* ---------------------------------------------------------------- serving */
 

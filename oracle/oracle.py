@@ -693,3 +693,275 @@ def predict_regular(m: RegularModel, X, fp64=False):
                 s = np.float32(float(m.weights[t]) * v + float(s))
         out[i] = (s + m.base) if fp64 else np.float32(s + np.float32(m.base))
     return out
+
+
+# ------------------------------------------- categorical target statistics --
+# Dataset::compute_target_statistics and its two methods
+# (src/core/dataset.cpp:679-865), the target-statistics binning rule of
+# Dataset::compute_bins (src/core/dataset.cpp:183-240) and the categorical
+# branch of Dataset::apply_bins (src/core/dataset.cpp:362-372), restated in
+# float32 with the reference's order of additions.
+
+F32 = np.float32
+
+
+def category_of(v):
+    """static_cast<Index>(val) as x86-64 compiles it (truncate to int64, keep the low 32 bits)."""
+    return int(np.int64(np.trunc(v))) & 0xFFFFFFFF
+
+
+def label_prior(y) -> np.float32:
+    """std::accumulate(labels, 0.0f) / n_samples (src/core/dataset.cpp:685)."""
+    acc = np.add.accumulate(np.asarray(y, F32), dtype=F32)[-1] if len(y) else F32(0)
+    return F32(F32(acc) / F32(len(y)))
+
+
+def _smooth(s, c, wp, pw):
+    return F32(F32(F32(s) + wp) / F32(F32(c) + pw))
+
+
+def ordered_ts(X, y, feats, order, prior_weight=1.0):
+    """Ordered target statistics (src/core/dataset.cpp:722-780) with the
+    processing order `order` (row of each position).  Returns (encoded X copy,
+    {feature: (sorted categories, encodings)}, prior)."""
+    X = np.array(X, F32, copy=True)
+    y = np.asarray(y, F32)
+    prior = label_prior(y)
+    pw = F32(prior_weight)
+    wp = F32(pw * prior)
+    tables = {}
+    for j in feats:
+        col = X[:, j].copy()
+        run = {}
+        for row in order:
+            v = col[row]
+            if np.isnan(v):
+                X[row, j] = prior
+                continue
+            c = category_of(v)
+            s, k = run.get(c, (F32(0), 0))
+            X[row, j] = _smooth(s, k, wp, pw) if k else prior
+            run[c] = (F32(s + y[row]), k + 1)
+        keys = np.array(sorted(run), np.uint32)
+        tables[j] = (keys, np.array([_smooth(*run[int(c)], wp, pw) for c in keys], F32))
+    return X, tables, prior
+
+
+def cv_ts(X, y, feats, folds, n_folds, prior_weight=1.0):
+    """Cross-validated target statistics (src/core/dataset.cpp:783-865) with
+    each row's fold given."""
+    X = np.array(X, F32, copy=True)
+    y = np.asarray(y, F32)
+    prior = label_prior(y)
+    pw = F32(prior_weight)
+    wp = F32(pw * prior)
+    tables = {}
+    for j in feats:
+        col = X[:, j].copy()
+        fs = {}
+        for row in range(len(col)):
+            v = col[row]
+            if np.isnan(v):
+                continue
+            c = category_of(v)
+            st = fs.setdefault(c, [[F32(0), 0] for _ in range(n_folds)])
+            st[folds[row]][0] = F32(st[folds[row]][0] + y[row])
+            st[folds[row]][1] += 1
+        for row in range(len(col)):
+            v = col[row]
+            if np.isnan(v):
+                X[row, j] = prior
+                continue
+            st = fs[category_of(v)]
+            s, k = F32(0), 0
+            for q in range(n_folds):
+                if q != folds[row]:
+                    s = F32(s + st[q][0])
+                    k += st[q][1]
+            X[row, j] = _smooth(s, k, wp, pw)
+        keys = np.array(sorted(fs), np.uint32)
+        vals = []
+        for c in keys:
+            s, k = F32(0), 0
+            for q in range(n_folds):
+                s = F32(s + fs[int(c)][q][0])
+                k += fs[int(c)][q][1]
+            vals.append(_smooth(s, k, wp, pw))
+        tables[j] = (keys, np.array(vals, F32))
+    return X, tables, prior
+
+
+def quantize_ts(X, ts_feats, max_bins=255, compat_u8=True) -> Binned:
+    """compute_bins with target-statistics columns: numeric columns by the
+    quantile rule (quantize), TS columns by A = min(max_bins, U) edges, edge b
+    = the distinct value of rank (b+1)*U/(A+1), bin = number of edges < x
+    (std::lower_bound), NaN -> bin max_bins."""
+    X = np.ascontiguousarray(X, F32)
+    b = quantize(X, max_bins, compat_u8)
+    for j in ts_feats:
+        v = X[:, j]
+        ok = ~np.isnan(v)
+        u = np.unique(v[ok])
+        U = len(u)
+        b.edges[j] = 0
+        if U == 0:
+            b.edges[j, 0] = 0.0
+            b.n_edges[j] = 1
+            b.bins[j] = max_bins
+            continue
+        A = min(max_bins, (U & 255) if compat_u8 else U)
+        e = np.array([u[min((k + 1) * U // (A + 1), U - 1)] for k in range(A)], F32)
+        b.edges[j, :A] = e
+        b.n_edges[j] = A
+        bins = np.searchsorted(e, v, side="left")
+        bins[~ok] = max_bins
+        b.bins[j] = bins.astype(np.uint8)
+    return b
+
+
+def encode_test(X, tables):
+    """apply_bins' categorical branch: category -> global encoding, 0.5 for an
+    unseen one (include/turbocat/dataset.hpp:218-226); NaN stays NaN."""
+    X = np.array(X, F32, copy=True)
+    for j, (keys, vals) in tables.items():
+        lut = {int(k): v for k, v in zip(keys, vals)}
+        for r in range(X.shape[0]):
+            v = X[r, j]
+            if not np.isnan(v):
+                X[r, j] = lut.get(category_of(v), F32(0.5))
+    return X
+
+
+def recover_order(X, y, feat, enc, prior_weight=1.0):
+    """A processing order under which ordered_ts reproduces the per-row
+    encodings `enc` of one categorical column (the reference draws its order
+    from std::random_device).  Within a category the position of each row is
+    found by stepping the running (sum, count) and matching the encodings;
+    rows of equal (encoding, label) are interchangeable, and the label to take
+    next is the one whose successor encoding exists.  Raises when the
+    encodings fit no order."""
+    X = np.asarray(X, F32)
+    y = np.asarray(y, F32)
+    prior = label_prior(y)
+    pw = F32(prior_weight)
+    wp = F32(pw * prior)
+    col = X[:, feat]
+    by_cat = {}
+    nan_rows = []
+    for r in range(len(col)):
+        if np.isnan(col[r]):
+            if enc[r] != prior:
+                raise ValueError(f"NaN row {r} not encoded with the prior")
+            nan_rows.append(r)
+        else:
+            by_cat.setdefault(category_of(col[r]), []).append(r)
+    pos = {}
+    for c, rows in by_cat.items():
+        pool = {}
+        for r in rows:
+            pool.setdefault((enc[r].view(np.uint32).item(), y[r].item()), []).append(r)
+
+        def target(s, k):
+            return (prior if k == 0 else _smooth(s, k, wp, pw)).view(np.uint32).item()
+
+        def solve(s, k):  # depth-first over the label taken at each step
+            if k == len(rows):
+                return []
+            t = target(s, k)
+            for lab in sorted({lb for (e, lb), v in pool.items() if e == t and v}):
+                r = pool[(t, lab)].pop()
+                rest = solve(F32(s + F32(lab)), k + 1)
+                if rest is not None:
+                    return [r] + rest
+                pool[(t, lab)].append(r)
+            return None
+
+        import sys
+        sys.setrecursionlimit(max(sys.getrecursionlimit(), 4 * len(rows) + 100))
+        seq = solve(F32(0), 0)
+        if seq is None:
+            raise ValueError(f"category {c}: the encodings fit no order")
+        for k, r in enumerate(seq):
+            pos[r] = (k, c)
+    order = sorted(pos, key=lambda r: pos[r]) + nan_rows
+    return np.array(order, np.uint32)
+
+
+def recover_folds(X, y, feat, enc, n_folds, prior_weight=1.0):
+    """Fold ids under which cv_ts reproduces the per-row encodings `enc` of
+    one categorical column: per category, rows with equal out-of-fold
+    (sum, count) form whole folds of equal size and label sum; each group is
+    split into folds of that size.  Raises when that is impossible."""
+    X = np.asarray(X, F32)
+    y = np.asarray(y, F32)
+    prior = label_prior(y)
+    pw = F32(prior_weight)
+    wp = F32(pw * prior)
+    col = X[:, feat]
+    folds = np.zeros(len(col), np.uint32)
+    by_cat = {}
+    for r in range(len(col)):
+        if not np.isnan(col[r]):
+            by_cat.setdefault(category_of(col[r]), []).append(r)
+    for c, rows in by_cat.items():
+        N, P = len(rows), F32(np.add.accumulate(y[rows], dtype=F32)[-1])
+        groups = {}
+        for r in rows:
+            groups.setdefault(enc[r].view(np.uint32).item(), []).append(r)
+        q = 0
+        for e, grp in groups.items():
+            match = None
+            for nf in range(1, N + 1):  # fold size: the out-of-fold count is N - nf
+                if len(grp) % nf:
+                    continue
+                m = len(grp) // nf
+                pos = F32(np.add.accumulate(y[grp], dtype=F32)[-1]) / F32(m)
+                if _smooth(F32(P - pos), N - nf, wp, pw).view(np.uint32).item() == e:
+                    match = nf
+                    break
+            if match is None:
+                raise ValueError(f"category {c}: encoding fits no fold")
+            labs = sorted(grp, key=lambda r: y[r])
+            m = len(grp) // match
+            for i in range(m):  # deal rows so every fold gets the same label mix
+                for r in labs[i::m]:
+                    folds[r] = q
+                q += 1
+            if q > n_folds:
+                raise ValueError(f"category {c}: more than {n_folds} folds")
+    return folds
+
+
+def ref_cat_ts(X, y, cats, method="ordered", hp: Hyper | None = None, fit=False):
+    """The reference's target statistics, bins and (fit) model on one dataset:
+    (encodings [n_cat][n], Binned, {feature: (categories, encodings)}, TCAT or None)."""
+    X = np.ascontiguousarray(X, F32)
+    y = np.ascontiguousarray(y, F32)
+    n, f = X.shape
+    cats = np.ascontiguousarray(cats, np.uint16)
+    nc = len(cats)
+    hp = hp or Hyper(loss="logloss", n_estimators=1)
+    enc = np.zeros((nc, n), F32)
+    bins = np.zeros((f, n), np.uint8)
+    edges = np.zeros((f, 255), F32)
+    ne = np.zeros(f, np.uint16)
+    cap = n
+    tk = np.zeros((nc, cap), np.uint32)
+    tv = np.zeros((nc, cap), F32)
+    tl = np.zeros(nc, np.uint32)
+    mb = C.c_void_p()
+    ml = C.c_size_t()
+    rp = hp.ref()
+    R = ref()
+    rc = R.tcref_cat_ts(_ptr(X), C.c_uint32(n), C.c_uint16(f), _ptr(y), _ptr(cats), C.c_int32(nc),
+                        C.c_int32(1 if method == "cv" else 0), C.byref(rp), C.c_int32(1 if fit else 0), _ptr(enc),
+                        _ptr(bins), _ptr(edges), _ptr(ne), _ptr(tk), _ptr(tv), _ptr(tl), C.c_uint32(cap),
+                        C.byref(mb), C.byref(ml))
+    if rc < 0:
+        raise RuntimeError(R.tcref_last_error().decode())
+    model = None
+    if fit:
+        model = C.string_at(mb, ml.value)
+        R.tcref_free(mb)
+    tables = {int(cats[c]): (tk[c, :tl[c]].copy(), tv[c, :tl[c]].copy()) for c in range(nc)}
+    return enc, Binned(bins, edges, ne), tables, model

@@ -15,6 +15,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <exception>
+#include <algorithm>
 #include <memory>
 #include <numeric>
 #include <sstream>
@@ -298,6 +299,54 @@ int tcref_fit_timed(const float* X, uint32_t n, uint16_t f, const float* y, cons
     };
     booster.train(ds, nullptr, cb);
     return done < max_trees ? done : max_trees;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
+// Categorical target statistics (Dataset::from_dense with cat_features,
+// compute_target_statistics, compute_bins; python/bindings.cpp:207-224).
+// method: 0 ordered, 1 cross-validated.  enc_out [n_cat][n] = the per-row
+// encodings the reference drew (get_sample_categorical_encoding), bins /
+// edges as tcref_bin, and per categorical feature its global table
+// (target_stats) sorted by category: tab_len[c] entries at tab_keys /
+// tab_vals + c * tab_cap.  With fit != 0 it then trains on those bins
+// (Booster::train, symmetric trees) and returns the TCAT bytes.
+int tcref_cat_ts(const float* X, uint32_t n, uint16_t f, const float* y, const uint16_t* cats, int32_t n_cat,
+                 int32_t method, const Params* p, int32_t fit, float* enc_out, uint8_t* bins_out,
+                 float* edges_out, uint16_t* n_edges_out, uint32_t* tab_keys, float* tab_vals, uint32_t* tab_len,
+                 uint32_t tab_cap, char** model_bytes, size_t* model_len) {
+  try {
+    Config cfg = make_config(*p);
+    cfg.categorical.method = method == 1 ? CategoricalConfig::EncodingMethod::CrossValidatedTS
+                                         : CategoricalConfig::EncodingMethod::TargetStatistics;
+    std::vector<FeatureIndex> cf(cats, cats + n_cat);
+    Dataset ds;
+    ds.from_dense(X, n, f, y, nullptr, cf);
+    ds.compute_target_statistics(cfg);
+    for (int32_t c = 0; c < n_cat; ++c) {
+      for (uint32_t i = 0; i < n; ++i)
+        enc_out[static_cast<size_t>(c) * n + i] = ds.get_sample_categorical_encoding(cats[c], i);
+      std::vector<std::pair<Index, Float>> t(ds.target_stats()[cats[c]].begin(), ds.target_stats()[cats[c]].end());
+      std::sort(t.begin(), t.end());
+      tab_len[c] = static_cast<uint32_t>(t.size());
+      for (size_t k = 0; k < t.size() && k < tab_cap; ++k) {
+        tab_keys[static_cast<size_t>(c) * tab_cap + k] = t[k].first;
+        tab_vals[static_cast<size_t>(c) * tab_cap + k] = t[k].second;
+      }
+    }
+    ds.compute_bins(cfg);
+    copy_bins(ds, bins_out, edges_out, n_edges_out);
+    if (!fit) return 0;
+    Booster booster(cfg);
+    booster.train(ds, nullptr, nullptr);
+    std::ostringstream os;
+    booster.save_binary(os);
+    const std::string s = os.str();
+    *model_len = s.size();
+    *model_bytes = static_cast<char*>(std::malloc(s.size()));
+    std::memcpy(*model_bytes, s.data(), s.size());
+    return static_cast<int>(booster.n_trees());
   } catch (const std::exception& e) {
     return fail(e);
   }

@@ -133,3 +133,27 @@ def regular_pred_matrix(X, edges):
         if len(e):
             P[r, j] = e[(7 * r) % len(e)]
     return P
+
+
+def categorical_case(n=3000, f=6, n_classes=2, seed=5, n_cat=1, cardinality=25, nan_rate=0.03):
+    """Rows with categorical columns 2, 4, ... (integer category ids, some NaN)
+    whose category shifts the label's log-odds, plus standard-normal numeric
+    columns; labels are class ids."""
+    rng = np.random.default_rng(seed)
+    X = rng.standard_normal((n, f)).astype(np.float32)
+    logit = X[:, 0].astype(np.float64)
+    for c in range(n_cat):
+        j = 2 + 2 * c
+        cat = rng.integers(0, cardinality, n)
+        X[:, j] = cat.astype(np.float32)
+        X[rng.random(n) < nan_rate, j] = np.nan
+        logit = logit + (cat % 7 - 3) * 0.5
+    if n_classes == 2:
+        y = (rng.random(n) < 1.0 / (1.0 + np.exp(-logit))).astype(np.float32)
+    else:
+        y = np.clip(np.floor((logit + 4.0) / 8.0 * n_classes + rng.random(n) - 0.5), 0, n_classes - 1)
+        y = y.astype(np.float32)
+    return X, y
+
+
+CAT_HYPER = dict(loss="logloss", n_estimators=20, max_depth=4, learning_rate=0.2)

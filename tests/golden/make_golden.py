@@ -38,8 +38,37 @@ def regular_golden():
     np.savez_compressed(os.path.join(HERE, "regular_small.npz"), tcat=np.frombuffer(model, np.uint8), pred_raw=raw)
 
 
+def categorical_golden():
+    """The reference's categorical target statistics on one dataset, for both
+    methods: its per-row encodings, global tables, bins and edges, an order
+    (ordered) / folds (cv) under which the oracle reproduces them (the
+    reference draws its own from std::random_device), and for the ordered
+    method the model it trains on those bins."""
+    from datagen import CAT_HYPER, categorical_case
+
+    X, y = categorical_case()
+    hp = O.Hyper(**CAT_HYPER)
+    out = {}
+    for method in ("ordered", "cv"):
+        enc, rb, tables, model = O.ref_cat_ts(X, y, [2], method, hp, fit=method == "ordered")
+        e = enc[0]
+        if method == "ordered":
+            order = O.recover_order(X, y, 2, e)
+            Xo, tab, _ = O.ordered_ts(X, y, [2], order)
+            out["tcat"] = np.frombuffer(model, np.uint8)
+        else:
+            order = O.recover_folds(X, y, 2, e, 5)
+            Xo, tab, _ = O.cv_ts(X, y, [2], order, 5)
+        assert np.array_equal(Xo[:, 2].view(np.uint32), e.view(np.uint32)), method
+        keys, vals = tables[2]
+        out.update({f"{method}_enc": e, f"{method}_order": order, f"{method}_keys": keys, f"{method}_vals": vals,
+                    f"{method}_bins": rb.bins, f"{method}_edges": rb.edges, f"{method}_n_edges": rb.n_edges})
+    np.savez_compressed(os.path.join(HERE, "categorical_small.npz"), **out)
+
+
 def main():
     regular_golden()
+    categorical_golden()
     for name, spec in GOLDEN_CASES.items():
         X, y, hp = make_case(spec)
         if hp.loss == "softmax":
@@ -58,4 +87,7 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["categorical"]:
+        categorical_golden()
+    else:
+        main()

@@ -62,6 +62,17 @@ struct ModelPtr {
   ~ModelPtr() { tc_model_destroy(m); }
 };
 
+struct DatasetPtr {
+  tc_dataset* d = nullptr;
+  ~DatasetPtr() { tc_dataset_destroy(d); }
+};
+
+// Categorical features of a fit and their encoding (python/bindings.cpp:106-116, 201-224).
+struct CatSpec {
+  std::vector<uint16_t> features;
+  tc_cat_params params{TC_CAT_ORDERED, 1.0f, 5, 0};
+};
+
 // Host-side booster: the counterpart of turbocat::Booster for the symmetric path.
 class GpuBooster {
  public:
@@ -72,18 +83,31 @@ class GpuBooster {
   // With a validation set (Xv, yv, nv > 0) the fit follows Booster::train's
   // valid_data branch: validation loss every iteration, early stopping after
   // `es_rounds` iterations without improvement (src/boosting/booster.cpp:255-371).
+  // With categorical features the training set's categorical columns are
+  // replaced by their target statistics before binning (compute_target_statistics
+  // before compute_bins, python/bindings.cpp:218-224); the training set is
+  // kept, as the reference keeps train_data_, to encode the validation set and
+  // the rows of the binned predict path (Dataset::apply_bins).
+  std::unique_ptr<DatasetPtr> train_set;
+
   void fit(const float* X, uint32_t n, uint16_t f, const float* y, const tc_train_params& p,
-           const float* Xv = nullptr, const float* yv = nullptr, uint32_t nv = 0, int es_rounds = 50) {
+           const float* Xv = nullptr, const float* yv = nullptr, uint32_t nv = 0, int es_rounds = 50,
+           const CatSpec* cats = nullptr) {
     tc_ctx* ctx = device_context();
     tc_dataset* ds = nullptr;
     tc_dataset* vds = nullptr;
     check(tc_dataset_upload(ctx, X, n, f, y, &ds), ctx);
-    tc_status s = tc_quantize(ds, (uint16_t)p.max_bins, 1, nullptr, nullptr);
+    const bool keep = cats && !cats->features.empty();
+    tc_status s = TC_OK;
+    if (keep) s = tc_encode_categorical(ds, cats->features.data(), (uint16_t)cats->features.size(), &cats->params,
+                                        nullptr);
+    if (s == TC_OK) s = tc_quantize(ds, (uint16_t)p.max_bins, 1, nullptr, nullptr);
     tc_model* m = nullptr;
     if (s == TC_OK && nv == 0) s = tc_train(ctx, ds, &p, &m, &stats);
     if (s == TC_OK && nv > 0) {
       tc_trainer* tr = nullptr;
       s = tc_dataset_upload(ctx, Xv, nv, f, yv, &vds);
+      if (s == TC_OK && keep) s = tc_apply_bins(vds, ds);  // valid_data->apply_bins(*train_data_)
       if (s == TC_OK) s = tc_trainer_create(ctx, ds, &p, &tr);
       if (s == TC_OK) s = tc_trainer_set_validation(tr, vds, es_rounds);
       if (s == TC_OK) s = tc_trainer_step(tr, p.n_estimators, 1);
@@ -92,7 +116,12 @@ class GpuBooster {
       if (tr) tc_trainer_destroy(tr);
     }
     if (vds) tc_dataset_destroy(vds);
-    tc_dataset_destroy(ds);
+    if (keep && s == TC_OK) {
+      train_set.reset(new DatasetPtr());
+      train_set->d = ds;
+    } else {
+      tc_dataset_destroy(ds);
+    }
     check(s, ctx);
     model.reset(new ModelPtr());
     model->m = m;
@@ -103,6 +132,20 @@ class GpuBooster {
     tc_ctx* ctx = device_context();
     std::vector<float> out((size_t)n * info.n_classes);
     check(tc_predict(ctx, model->m, X, n, f, transform, out.data()), ctx);
+    return out;
+  }
+
+  // The reference's binned predict path (Dataset::apply_bins against the
+  // training set, then the tree walk; python/bindings.cpp:311-334): rows'
+  // categorical columns take the training set's global encodings.
+  std::vector<float> predict_binned(const float* X, uint32_t n, uint16_t f, int transform) const {
+    if (!train_set) return predict(X, n, f, transform);
+    tc_ctx* ctx = device_context();
+    std::vector<float> out((size_t)n * info.n_classes);
+    DatasetPtr t;
+    check(tc_dataset_upload(ctx, X, n, f, nullptr, &t.d), ctx);
+    check(tc_apply_bins(t.d, train_set->d), ctx);
+    check(tc_predict_dataset(ctx, model->m, t.d, transform, out.data()), ctx);
     return out;
   }
 
@@ -281,7 +324,11 @@ class TurboCatClassifier {
     if (early_stopping_metric != "loss" && early_stopping_metric != "logloss")
       warn("early_stopping_metric '" + early_stopping_metric + "' is not on the device path; the validation "
            "loss is used (the reference's fallback for metrics it does not know)");
-    (void)cat_encoding; (void)max_interactions;
+    // python/bindings.cpp:106-116: "cv" / "cross_validated", "onehot" / "one_hot", else ordered
+    if (cat_encoding == "cv" || cat_encoding == "cross_validated") cat_.params.method = TC_CAT_CV;
+    else if (cat_encoding == "onehot" || cat_encoding == "one_hot") onehot_ = true;
+    cat_.params.seed = p_.seed;  // the reference draws the order from std::random_device
+    (void)max_interactions;
     (void)interaction_method; (void)n_threads;
   }
 
@@ -295,7 +342,13 @@ class TurboCatClassifier {
     if (colsample_ < 1.0f && verbosity_ > 1) warn("colsample_bytree has no effect on symmetric trees");
     if (use_gradtree_ || use_ordered_ || auto_interactions_)
       warn("use_gradtree / use_ordered_boosting / auto_interactions are not on the device path and are ignored");
-    if (!cat_features.empty()) throw std::invalid_argument("cat_features are not supported on the device path");
+    CatSpec cats = cat_;
+    for (int c : cat_features) {
+      if (c < 0 || c >= (int)f) throw std::invalid_argument("cat_features index out of range");
+      cats.features.push_back((uint16_t)c);
+    }
+    if (!cats.features.empty() && onehot_)
+      throw std::invalid_argument("cat_encoding='onehot' is not on the device path (target statistics: 'ordered', 'cv')");
     const bool has_val = X_val.size() > 0 && y_val.size() > 0;
     if (has_val) {
       check_2d(X_val, "X_val");
@@ -320,9 +373,10 @@ class TurboCatClassifier {
       py::gil_scoped_release nogil;
       booster_.reset(new GpuBooster());
       if (has_val)
-        booster_->fit(X.data(), n, f, yp, p, X_val.data(), y_val.data(), (uint32_t)X_val.shape(0), es_rounds_);
+        booster_->fit(X.data(), n, f, yp, p, X_val.data(), y_val.data(), (uint32_t)X_val.shape(0), es_rounds_,
+                      &cats);
       else
-        booster_->fit(X.data(), n, f, yp, p);
+        booster_->fit(X.data(), n, f, yp, p, nullptr, nullptr, 0, 50, &cats);
     }
     n_features_ = f;
     is_fitted_ = true;
@@ -339,7 +393,11 @@ class TurboCatClassifier {
     std::vector<float> out;
     {
       py::gil_scoped_release nogil;
-      out = booster_->predict(X.data(), n, f, K > 1 ? TC_TRANSFORM_SOFTMAX : TC_TRANSFORM_SIGMOID);
+      // binary: the no-binning path on the raw rows (categorical columns
+      // compared as given); multiclass: the binned path, which encodes them
+      // (python/bindings.cpp:297-334)
+      out = K > 1 ? booster_->predict_binned(X.data(), n, f, TC_TRANSFORM_SOFTMAX)
+                  : booster_->predict(X.data(), n, f, TC_TRANSFORM_SIGMOID);
     }
     if (K > 1) {
       py::array_t<float> r({(py::ssize_t)n, (py::ssize_t)K});
@@ -438,6 +496,8 @@ class TurboCatClassifier {
   bool use_goss_, use_gradtree_, use_ordered_, auto_interactions_;
   int verbosity_;
   int es_rounds_ = 50;
+  CatSpec cat_;
+  bool onehot_ = false;
   std::unique_ptr<GpuBooster> booster_;
   uint32_t n_classes_ = 2;
   int n_features_ = 0;

@@ -18,6 +18,8 @@
 //      contiguous range; the last group's block is only 4, 8, 16 or 32
 //      bytes wide) and column-major [f][np] (partition kernels, export).
 #include <algorithm>
+#include <atomic>
+#include <cmath>
 
 #include <cstring>
 #include <thread>
@@ -117,7 +119,8 @@ __global__ void k_segment_scan(uint32_t* __restrict__ a, uint32_t m, uint32_t* _
 // offset for the tile + the count of equal digits before it in the tile.
 __global__ void k_radix_scatter(const uint32_t* __restrict__ kin, uint32_t* __restrict__ kout,
                                 uint32_t n, uint32_t n_tiles, int shift,
-                                const uint32_t* __restrict__ offsets) {
+                                const uint32_t* __restrict__ offsets,
+                                const uint32_t* __restrict__ vin = nullptr, uint32_t* __restrict__ vout = nullptr) {
   __shared__ uint32_t s_base[256];
   __shared__ uint32_t s_run[256];
   __shared__ uint32_t s_w[RS_THREADS / 32][256];
@@ -149,7 +152,11 @@ __global__ void k_radix_scatter(const uint32_t* __restrict__ kin, uint32_t* __re
       s_run[tid] = run;
     }
     __syncthreads();
-    if (valid) ko[s_base[d] + s_w[warp][d] + rank] = key;
+    if (valid) {
+      const uint32_t slot = s_base[d] + s_w[warp][d] + rank;
+      ko[slot] = key;
+      if (vout) vout[(size_t)j * n + slot] = vin[(size_t)j * n + idx];  // payload rides along
+    }
     __syncthreads();
     for (int w = 0; w < RS_THREADS / 32; ++w) s_w[w][tid] = 0;
     __syncthreads();
@@ -185,13 +192,16 @@ __device__ __forceinline__ uint32_t actual_bins(uint32_t U, int max_bins, int co
 // Picks edge b-1 = distinct value of rank floor(b*U/A) for b = 1 .. A-1.
 __global__ void k_unique_pick(const uint32_t* __restrict__ keys, uint32_t n, uint32_t n_tiles,
                               const uint32_t* __restrict__ tile_off, const uint32_t* __restrict__ U_,
-                              int max_bins, int compat_u8, float* __restrict__ edges) {
+                              int max_bins, int compat_u8, const uint8_t* __restrict__ ts,
+                              float* __restrict__ edges) {
   __shared__ uint32_t warp_sums[RS_THREADS / 32];
   __shared__ uint32_t run_s;
   const uint32_t j = blockIdx.y, tile = blockIdx.x;
   const uint32_t* kj = keys + (size_t)j * n;
   const uint64_t U = U_[j];
-  const uint64_t A = actual_bins((uint32_t)U, max_bins, compat_u8);
+  // numeric: edge b-1 = rank floor(b*U/A), b = 1 .. A-1; target statistics:
+  // edge b-1 = rank floor(b*U/(A+1)), b = 1 .. A (src/core/dataset.cpp:221-224)
+  const uint64_t A = actual_bins((uint32_t)U, max_bins, compat_u8) + (ts && ts[j] ? 1 : 0);
   if (A < 2) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (threadIdx.x == 0) run_s = tile_off[(size_t)j * n_tiles + tile];
@@ -224,7 +234,8 @@ __global__ void k_unique_pick(const uint32_t* __restrict__ keys, uint32_t n, uin
 }
 
 __global__ void k_edge_meta(const uint32_t* __restrict__ U_, uint32_t f, int max_bins, int compat_u8,
-                            float* __restrict__ edges, uint16_t* __restrict__ n_edges) {
+                            const uint8_t* __restrict__ ts, float* __restrict__ edges,
+                            uint16_t* __restrict__ n_edges) {
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= f) return;
   const uint32_t U = U_[j];
@@ -234,21 +245,25 @@ __global__ void k_edge_meta(const uint32_t* __restrict__ U_, uint32_t f, int max
     return;
   }
   const uint32_t A = actual_bins(U, max_bins, compat_u8);
-  n_edges[j] = (uint16_t)(A >= 2 ? A - 1 : 0);
+  n_edges[j] = (uint16_t)((ts && ts[j]) ? A : (A >= 2 ? A - 1 : 0));
 }
 
 constexpr int AB_ROWS = 256;
 
-// bin = #edges <= x (upper_bound), NaN -> 255; writes both bin layouts.
-// Block (row tile, group): 256 rows of the 32 features of group blockIdx.y.
+// bin = #edges <= x (upper_bound), NaN -> 255; target-statistics columns
+// (ts[j]) take #edges < x (lower_bound, src/core/dataset.cpp:226-235); writes
+// both bin layouts.  Block (row tile, group): 256 rows of the 32 features of
+// group blockIdx.y.
 __global__ void k_assign_bins(const float* __restrict__ X, uint32_t n, uint32_t f,
                               const float* __restrict__ edges, const uint16_t* __restrict__ n_edges,
+                              const uint8_t* __restrict__ ts,
                               uint8_t* __restrict__ bins_t, uint64_t gstride, uint32_t nt, uint32_t wlast,
                               uint8_t* __restrict__ bins_cm, uint32_t np, uint32_t* __restrict__ nan_any) {
   __shared__ float s_e[32][kSlots + 1];
   __shared__ int s_ne[32];
   __shared__ uint8_t s_b[32][AB_ROWS + 4];
   __shared__ int s_nan[32];
+  __shared__ int s_ts[32];
   const uint32_t j0 = blockIdx.y * 32, r0 = blockIdx.x * AB_ROWS;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
   for (int q = tid; q < 32 * kSlots; q += blockDim.x) {
@@ -257,6 +272,7 @@ __global__ void k_assign_bins(const float* __restrict__ X, uint32_t n, uint32_t 
   }
   if (tid < 32) {
     s_ne[tid] = (j0 + tid < f) ? (int)n_edges[j0 + tid] : 0;
+    s_ts[tid] = (ts && j0 + tid < f) ? (int)ts[j0 + tid] : 0;
     s_nan[tid] = 0;
   }
   __syncthreads();
@@ -271,11 +287,14 @@ __global__ void k_assign_bins(const float* __restrict__ X, uint32_t n, uint32_t 
         s_nan[lane] = 1;
       } else {
         int lo = 0, hi = s_ne[lane];
+        const bool lower = s_ts[lane] != 0;
         while (lo < hi) {
           const int mid = (lo + hi) >> 1;
-          if (x < s_e[lane][mid]) hi = mid; else lo = mid + 1;
+          const float e = s_e[lane][mid];
+          if (lower ? (x <= e) : (x < e)) hi = mid; else lo = mid + 1;
         }
         b = (uint8_t)lo;
+        if (lo == kNanBin) s_nan[lane] = 1;  // a target-statistics column's top bin shares the NaN slot
       }
     }
     s_b[lane][i] = b;
@@ -298,6 +317,256 @@ __global__ void k_assign_bins(const float* __restrict__ X, uint32_t n, uint32_t 
   }
 }
 
+// ------------------------------------------- categorical target statistics
+//
+// Dataset::compute_ordered_target_statistics / compute_cv_target_statistics
+// (src/core/dataset.cpp:722-865) on the device.  Each encoded column's rows
+// are keyed by category in processing order and stably sorted (the radix sort
+// above, the row index riding along), so every category becomes one
+// contiguous segment in processing order.  One thread then walks a segment
+// with the reference's float arithmetic: the running sums depend on the order
+// of the additions in float, so they are kept sequential in the reference's
+// order rather than scanned in parallel.  The walk writes each row's encoding
+// into X and the category's global entry into the table; segments come in
+// category order, so the table comes out sorted.
+
+constexpr uint32_t CAT_NAN = 0xFFFFFFFFu;  // key of NaN rows; category 0xFFFFFFFF shares it, the walk tells them apart
+constexpr int CAT_MAX_FOLDS = 32;
+constexpr int CAT_THREADS = 256;
+
+// static_cast<Index>(val) as x86-64 compiles it: truncate to 64 bits, keep the low 32.
+__device__ __forceinline__ uint32_t category_of(float x) { return (uint32_t)(unsigned long long)(long long)x; }
+
+// 32-bit integer finaliser ("lowbias32", C. Wellons' hash prospector).
+__host__ __device__ __forceinline__ uint32_t mix32(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+
+// Processing order of the ordered method and folds of the cross-validated
+// one.  Drawn from the seed: position p -> row by a 4-round Feistel bijection
+// on [0, 4^half) with cycle walking into [0, n) (a permutation with no sort
+// and no table); fold of a row = hash of the row mod folds.  Or given by the
+// caller (`given`: row of each position / fold of each row).
+struct CatOrder {
+  uint32_t key[4];
+  uint32_t half;
+  uint32_t folds;
+  int cv;
+  const uint32_t* given;
+};
+
+__device__ __forceinline__ uint32_t feistel(uint32_t x, const CatOrder& o) {
+  const uint32_t m = (1u << o.half) - 1u;
+  uint32_t l = x >> o.half, r = x & m;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const uint32_t t = l ^ (mix32(r ^ o.key[i]) & m);
+    l = r;
+    r = t;
+  }
+  return (l << o.half) | r;
+}
+
+__device__ __forceinline__ uint32_t order_row(uint32_t p, uint32_t n, const CatOrder& o) {
+  if (o.given) return o.given[p];
+  uint32_t x = p;
+  do x = feistel(x, o); while (x >= n);  // ends: p's cycle under the bijection returns to p < n
+  return x;
+}
+
+__device__ __forceinline__ uint32_t fold_of(uint32_t row, const CatOrder& o) {
+  return o.given ? o.given[row] : mix32(mix32(row ^ o.key[0]) + o.key[1]) % o.folds;
+}
+
+// std::accumulate(labels, 0.0f) / n (src/core/dataset.cpp:685): one thread
+// adds in row order, the block stages the labels through shared memory.
+__global__ void k_label_prior(const float* __restrict__ y, uint32_t n, float* __restrict__ prior) {
+  __shared__ float s[2048];
+  float acc = 0.0f;
+  for (uint32_t base = 0; base < n; base += 2048) {
+    const uint32_t m = min(2048u, n - base);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) s[i] = y[base + i];
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (uint32_t i = 0; i < m; ++i) acc = __fadd_rn(acc, s[i]);
+  }
+  if (threadIdx.x == 0) prior[0] = n ? __fdiv_rn(acc, __uint2float_rn(n)) : 0.0f;
+}
+
+// keys[c][p] = category of the row at position p of column feats[c],
+// rows[c][p] = that row (positions in processing order; rows in row order for
+// the cross-validated method).
+__global__ void k_cat_keys(const float* __restrict__ X, uint32_t n, uint32_t f,
+                           const uint16_t* __restrict__ feats, CatOrder o, uint32_t* __restrict__ keys,
+                           uint32_t* __restrict__ rows) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
+  if (p >= n) return;
+  const uint32_t row = o.cv ? p : order_row(p, n, o);
+  const float v = X[(size_t)row * f + feats[c]];
+  keys[(size_t)c * n + p] = isnan(v) ? CAT_NAN : category_of(v);
+  rows[(size_t)c * n + p] = row;
+}
+
+__device__ __forceinline__ uint32_t seg_flag(const uint32_t* kj, uint32_t idx, uint32_t n) {
+  return idx < n && (idx == 0 || kj[idx - 1] != kj[idx]);
+}
+
+__global__ void k_seg_count(const uint32_t* __restrict__ keys, uint32_t n, uint32_t n_tiles,
+                            uint32_t* __restrict__ tile_cnt) {
+  __shared__ uint32_t s;
+  if (threadIdx.x == 0) s = 0;
+  __syncthreads();
+  const uint32_t j = blockIdx.y, tile = blockIdx.x;
+  const uint32_t* kj = keys + (size_t)j * n;
+  uint32_t c = 0;
+  for (int it = 0; it < RS_ITEMS; ++it) c += seg_flag(kj, tile * RS_TILE + it * RS_THREADS + threadIdx.x, n);
+  for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(&s, c);
+  __syncthreads();
+  if (threadIdx.x == 0) tile_cnt[(size_t)j * n_tiles + tile] = s;
+}
+
+// starts[j][rank] = first sorted position of the rank-th segment of column j.
+__global__ void k_seg_starts(const uint32_t* __restrict__ keys, uint32_t n, uint32_t n_tiles,
+                             const uint32_t* __restrict__ tile_off, uint32_t* __restrict__ starts) {
+  __shared__ uint32_t warp_sums[RS_THREADS / 32];
+  __shared__ uint32_t run_s;
+  const uint32_t j = blockIdx.y, tile = blockIdx.x;
+  const uint32_t* kj = keys + (size_t)j * n;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) run_s = tile_off[(size_t)j * n_tiles + tile];
+  __syncthreads();
+  for (int it = 0; it < RS_ITEMS; ++it) {
+    const uint32_t idx = tile * RS_TILE + it * RS_THREADS + threadIdx.x;
+    const uint32_t fl = seg_flag(kj, idx, n);
+    uint32_t x = fl;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[warp] = x;
+    __syncthreads();
+    uint32_t before = run_s;
+    for (int w = 0; w < warp; ++w) before += warp_sums[w];
+    if (fl) starts[(size_t)j * n + before + x - 1] = idx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t t = 0;
+      for (int w = 0; w < RS_THREADS / 32; ++w) t += warp_sums[w];
+      run_s += t;
+    }
+    __syncthreads();
+  }
+}
+
+// One thread per category segment: the row encodings and the category's
+// global entry.  Ordered (src/core/dataset.cpp:738-780): a row sees the sum
+// and count of its category's rows before it, the prior when there are none.
+// Cross-validated (src/core/dataset.cpp:799-863): per-fold sums in row order,
+// a row sees the other folds' sums added in fold order.  Smoothing
+// (sum + a * prior) / (count + a); NaN rows get the prior and count nowhere.
+__global__ void k_cat_walk(const float* __restrict__ y, float* __restrict__ X, uint32_t n, uint32_t f,
+                           const uint16_t* __restrict__ feats, const uint32_t* __restrict__ keys,
+                           const uint32_t* __restrict__ rows, const uint32_t* __restrict__ starts,
+                           const uint32_t* __restrict__ nseg, const uint32_t* __restrict__ off,
+                           const float* __restrict__ prior_p, float pw, CatOrder o,
+                           uint32_t* __restrict__ tab_keys, float* __restrict__ tab_vals,
+                           uint32_t* __restrict__ tab_len) {
+  const uint32_t c = blockIdx.y, s = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t S = nseg[c];
+  if (s >= S) return;
+  const size_t base = (size_t)c * n;
+  const uint32_t begin = starts[base + s], end = s + 1 < S ? starts[base + s + 1] : n;
+  const uint32_t feat = feats[c];
+  const float prior = *prior_p;
+  const float wp = __fmul_rn(pw, prior);
+  auto smooth = [&](float sum, uint32_t cnt) {
+    return __fdiv_rn(__fadd_rn(sum, wp), __fadd_rn(__uint2float_rn(cnt), pw));
+  };
+  float total = 0.0f;
+  uint32_t count = 0;
+  if (!o.cv) {
+    for (uint32_t i = begin; i < end; ++i) {
+      const uint32_t row = rows[base + i];
+      float* xp = X + (size_t)row * f + feat;
+      if (isnan(*xp)) {
+        *xp = prior;
+        continue;
+      }
+      *xp = count ? smooth(total, count) : prior;
+      total = __fadd_rn(total, y[row]);
+      ++count;
+    }
+  } else {
+    float fs[CAT_MAX_FOLDS];
+    uint32_t fc[CAT_MAX_FOLDS];
+    for (uint32_t q = 0; q < o.folds; ++q) {
+      fs[q] = 0.0f;
+      fc[q] = 0;
+    }
+    for (uint32_t i = begin; i < end; ++i) {
+      const uint32_t row = rows[base + i];
+      if (isnan(X[(size_t)row * f + feat])) continue;
+      const uint32_t fd = fold_of(row, o);
+      fs[fd] = __fadd_rn(fs[fd], y[row]);
+      ++fc[fd];
+    }
+    for (uint32_t i = begin; i < end; ++i) {
+      const uint32_t row = rows[base + i];
+      float* xp = X + (size_t)row * f + feat;
+      if (isnan(*xp)) {
+        *xp = prior;
+        continue;
+      }
+      const uint32_t fd = fold_of(row, o);
+      float sum = 0.0f;
+      uint32_t cnt = 0;
+      for (uint32_t q = 0; q < o.folds; ++q) {
+        if (q == fd) continue;
+        sum = __fadd_rn(sum, fs[q]);
+        cnt += fc[q];
+      }
+      *xp = smooth(sum, cnt);
+    }
+    for (uint32_t q = 0; q < o.folds; ++q) {
+      total = __fadd_rn(total, fs[q]);
+      count += fc[q];
+    }
+  }
+  const uint32_t at = off[c] + s;
+  tab_keys[at] = keys[base + begin];
+  tab_vals[at] = count ? smooth(total, count) : prior;
+  if (s == S - 1) tab_len[c] = count ? S : S - 1;  // a last segment of NaN rows only is no category
+}
+
+// Dataset::apply_bins' categorical branch (src/core/dataset.cpp:362-372):
+// a row's category -> the reference's global encoding (binary search of the
+// sorted table), 0.5 for a category it never saw (encode_category's default,
+// include/turbocat/dataset.hpp:218-226); NaN stays NaN (bin 255).
+__global__ void k_cat_lookup(float* __restrict__ X, uint32_t n, uint32_t f, const uint16_t* __restrict__ feats,
+                             const uint32_t* __restrict__ off, const uint32_t* __restrict__ len,
+                             const uint32_t* __restrict__ tkeys, const float* __restrict__ tvals) {
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
+  if (r >= n) return;
+  float* xp = X + (size_t)r * f + feats[c];
+  const float x = *xp;
+  if (isnan(x)) return;
+  const uint32_t k = category_of(x);
+  const uint32_t b = off[c], e = off[c] + len[c];
+  uint32_t lo = b, hi = e;
+  while (lo < hi) {
+    const uint32_t mid = lo + (hi - lo) / 2;
+    if (tkeys[mid] < k) lo = mid + 1; else hi = mid;
+  }
+  *xp = (lo < e && tkeys[lo] == k) ? tvals[lo] : 0.5f;
+}
+
 }  // namespace
 
 tc_status quantize(tc_dataset* ds, int max_bins, int compat_u8) {
@@ -305,6 +574,7 @@ tc_status quantize(tc_dataset* ds, int max_bins, int compat_u8) {
   const uint32_t n = ds->n, f = ds->f;
   cudaStream_t st = ctx->stream;
   const uint32_t n_tiles = (uint32_t)((n + RS_TILE - 1) / RS_TILE);
+  const uint8_t* ts = ds->h_cat_feats.empty() ? nullptr : ds->ts.p;
   DevBuf<uint32_t> ka, kb, counts, tcnt, U;
   TC_TRY(ka.alloc(ctx, (size_t)n * f, "sort keys"));
   TC_TRY(kb.alloc(ctx, (size_t)n * f, "sort keys (alt)"));
@@ -334,16 +604,16 @@ tc_status quantize(tc_dataset* ds, int max_bins, int compat_u8) {
     k_unique_count<<<dim3(n_tiles, f), RS_THREADS, 0, st>>>(src, n, n_tiles, tcnt.p);
     k_segment_scan<<<f, 1024, 0, st>>>(tcnt.p, n_tiles, U.p);
     k_unique_pick<<<dim3(n_tiles, f), RS_THREADS, 0, st>>>(src, n, n_tiles, tcnt.p, U.p, max_bins,
-                                                            compat_u8, ds->edges.p);
+                                                            compat_u8, ts, ds->edges.p);
   } else {
     TC_CUDA(ctx, cudaMemsetAsync(U.p, 0, U.bytes(), st));
   }
-  k_edge_meta<<<(f + 127) / 128, 128, 0, st>>>(U.p, f, max_bins, compat_u8, ds->edges.p, ds->n_edges.p);
+  k_edge_meta<<<(f + 127) / 128, 128, 0, st>>>(U.p, f, max_bins, compat_u8, ts, ds->edges.p, ds->n_edges.p);
   TC_CUDA(ctx, cudaMemsetAsync(ds->bins_t.p, 0, ds->bins_t.bytes(), st));
   if (n > 0) {
     dim3 ag((n + AB_ROWS - 1) / AB_ROWS, ds->groups);
-    k_assign_bins<<<ag, 256, 0, st>>>(ds->X.p, n, f, ds->edges.p, ds->n_edges.p, ds->bins_t.p, ds->gstride,
-                                      ds->nt, ds->wlast, ds->bins_cm.p, ds->np, ds->nan_any.p);
+    k_assign_bins<<<ag, 256, 0, st>>>(ds->X.p, n, f, ds->edges.p, ds->n_edges.p, ts, ds->bins_t.p,
+                                      ds->gstride, ds->nt, ds->wlast, ds->bins_cm.p, ds->np, ds->nan_any.p);
   }
   TC_CUDA(ctx, cudaGetLastError());
   // host copy of the edges for model export / thresholds
@@ -370,6 +640,17 @@ tc_status apply_bins(tc_dataset* ds, const tc_dataset* ref) {
   if (ref == ds) return TC_OK;  // already binned with its own edges
   cudaStream_t st = ctx->stream;
   const uint32_t n = ds->n, f = ds->f;
+  if (!ref->h_cat_feats.empty() && ds->encoded_by != ref->id) {
+    if (!ds->h_cat_feats.empty() || ds->encoded_by)
+      return ctx->fail(TC_ERR_INVALID_ARG, "the dataset's categorical columns are already encoded");
+    const uint32_t nc = (uint32_t)ref->h_cat_feats.size();
+    if (n > 0) {
+      k_cat_lookup<<<dim3((n + CAT_THREADS - 1) / CAT_THREADS, nc), CAT_THREADS, 0, st>>>(
+          ds->X.p, n, f, ref->cat_feats.p, ref->cat_off.p, ref->cat_len.p, ref->cat_keys.p, ref->cat_vals.p);
+      TC_CUDA(ctx, cudaGetLastError());
+    }
+    ds->encoded_by = ref->id;
+  }
   TC_TRY(ds->edges.alloc(ctx, (size_t)f * kSlots, "bin edges"));
   TC_TRY(ds->n_edges.alloc(ctx, f, "edge counts"));
   TC_TRY(ds->nan_any.alloc(ctx, f, "NaN flags"));
@@ -382,8 +663,8 @@ tc_status apply_bins(tc_dataset* ds, const tc_dataset* ref) {
   TC_CUDA(ctx, cudaMemsetAsync(ds->bins_t.p, 0, ds->bins_t.bytes(), st));
   if (n > 0) {
     dim3 ag((n + AB_ROWS - 1) / AB_ROWS, ds->groups);
-    k_assign_bins<<<ag, 256, 0, st>>>(ds->X.p, n, f, ds->edges.p, ds->n_edges.p, ds->bins_t.p, ds->gstride,
-                                      ds->nt, ds->wlast, ds->bins_cm.p, ds->np, ds->nan_any.p);
+    k_assign_bins<<<ag, 256, 0, st>>>(ds->X.p, n, f, ds->edges.p, ds->n_edges.p, nullptr, ds->bins_t.p,
+                                      ds->gstride, ds->nt, ds->wlast, ds->bins_cm.p, ds->np, ds->nan_any.p);
     TC_CUDA(ctx, cudaGetLastError());
   }
   TC_CUDA(ctx, cudaStreamSynchronize(st));
@@ -391,6 +672,120 @@ tc_status apply_bins(tc_dataset* ds, const tc_dataset* ref) {
   ds->h_n_edges = ref->h_n_edges;
   ds->quantized = true;
   ds->max_bins = ref->max_bins;
+  return TC_OK;
+}
+
+namespace {
+uint64_t splitmix64(uint64_t& x) {  // S. Vigna's SplitMix64 step
+  uint64_t z = (x += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+}  // namespace
+
+tc_status encode_categorical(tc_dataset* ds, const uint16_t* feats, uint16_t nc, const tc_cat_params* p,
+                             const uint32_t* order) {
+  tc_ctx* ctx = ds->ctx;
+  const uint32_t n = ds->n, f = ds->f;
+  if (nc == 0) return TC_OK;
+  if (!feats || !p) return ctx->fail(TC_ERR_INVALID_ARG, "features and parameters are required");
+  if (ds->quantized) return ctx->fail(TC_ERR_INVALID_ARG, "encode the categorical columns before tc_quantize");
+  if (!ds->h_cat_feats.empty() || ds->encoded_by)
+    return ctx->fail(TC_ERR_INVALID_ARG, "the dataset's categorical columns are already encoded");
+  if (n == 0 || ds->y.n < n) return ctx->fail(TC_ERR_INVALID_ARG, "target statistics need rows and labels");
+  if (p->method != TC_CAT_ORDERED && p->method != TC_CAT_CV)
+    return ctx->fail(TC_ERR_INVALID_ARG, "unknown target-statistics method %d", p->method);
+  const bool cv = p->method == TC_CAT_CV;
+  if (cv && (p->cv_folds < 1 || p->cv_folds > CAT_MAX_FOLDS))
+    return ctx->fail(TC_ERR_INVALID_ARG, "cv_folds must be in [1, %d]", CAT_MAX_FOLDS);
+  if (!std::isfinite(p->prior_weight)) return ctx->fail(TC_ERR_INVALID_ARG, "prior_weight must be finite");
+  std::vector<uint8_t> seen(f, 0);
+  for (uint16_t c = 0; c < nc; ++c) {
+    if (feats[c] >= f) return ctx->fail(TC_ERR_INVALID_ARG, "categorical feature %u out of range", feats[c]);
+    if (seen[feats[c]]++) return ctx->fail(TC_ERR_INVALID_ARG, "categorical feature %u listed twice", feats[c]);
+  }
+  if (order) {  // checked here: the kernels index rows by it
+    if (cv) {
+      for (uint32_t i = 0; i < n; ++i)
+        if (order[i] >= (uint32_t)p->cv_folds) return ctx->fail(TC_ERR_INVALID_ARG, "fold %u of row %u", order[i], i);
+    } else {
+      std::vector<uint8_t> hit(n, 0);
+      for (uint32_t i = 0; i < n; ++i)
+        if (order[i] >= n || hit[order[i]]++) return ctx->fail(TC_ERR_INVALID_ARG, "order is not a permutation");
+    }
+  }
+  cudaStream_t st = ctx->stream;
+  const uint32_t n_tiles = (uint32_t)((n + RS_TILE - 1) / RS_TILE);
+  DevBuf<uint32_t> ka, kb, ra, rb, counts, tcnt, nseg, starts, given;
+  DevBuf<float> prior;
+  TC_TRY(ka.alloc(ctx, (size_t)nc * n, "category keys"));
+  TC_TRY(kb.alloc(ctx, (size_t)nc * n, "category keys (alt)"));
+  TC_TRY(ra.alloc(ctx, (size_t)nc * n, "category rows"));
+  TC_TRY(rb.alloc(ctx, (size_t)nc * n, "category rows (alt)"));
+  TC_TRY(counts.alloc(ctx, (size_t)nc * 256 * n_tiles, "radix counts"));
+  TC_TRY(tcnt.alloc(ctx, (size_t)nc * n_tiles, "segment tile counts"));
+  TC_TRY(nseg.alloc(ctx, nc, "segment counts"));
+  TC_TRY(starts.alloc(ctx, (size_t)nc * n, "segment starts"));
+  TC_TRY(prior.alloc(ctx, 1, "label prior"));
+  TC_TRY(ds->cat_feats.alloc(ctx, nc, "categorical features"));
+  TC_TRY(ds->cat_off.alloc(ctx, nc, "category table offsets"));
+  TC_TRY(ds->cat_len.alloc(ctx, nc, "category table lengths"));
+  TC_TRY(ds->ts.alloc(ctx, f, "target-statistics flags"));
+  CatOrder o{};
+  uint64_t sm = p->seed;
+  for (int i = 0; i < 4; ++i) o.key[i] = (uint32_t)splitmix64(sm);
+  o.half = 1;
+  while ((1ull << (2 * o.half)) < n) ++o.half;
+  o.folds = cv ? (uint32_t)p->cv_folds : 1u;
+  o.cv = cv ? 1 : 0;
+  if (order) {
+    TC_TRY(given.alloc(ctx, n, "given order"));
+    TC_CUDA(ctx, cudaMemcpyAsync(given.p, order, (size_t)n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    o.given = given.p;
+  }
+  TC_CUDA(ctx, cudaMemcpyAsync(ds->cat_feats.p, feats, nc * sizeof(uint16_t), cudaMemcpyHostToDevice, st));
+  k_label_prior<<<1, 1024, 0, st>>>(ds->y.p, n, prior.p);
+  k_cat_keys<<<dim3((n + CAT_THREADS - 1) / CAT_THREADS, nc), CAT_THREADS, 0, st>>>(ds->X.p, n, f,
+                                                                                   ds->cat_feats.p, o, ka.p, ra.p);
+  uint32_t *ks = ka.p, *kd = kb.p, *rs = ra.p, *rd = rb.p;
+  for (int shift = 0; shift < 32; shift += 8) {
+    k_radix_count<<<dim3(n_tiles, nc), RS_THREADS, 0, st>>>(ks, n, n_tiles, shift, counts.p);
+    k_segment_scan<<<nc, 1024, 0, st>>>(counts.p, 256 * n_tiles, nullptr);
+    k_radix_scatter<<<dim3(n_tiles, nc), RS_THREADS, 0, st>>>(ks, kd, n, n_tiles, shift, counts.p, rs, rd);
+    std::swap(ks, kd);
+    std::swap(rs, rd);
+  }
+  k_seg_count<<<dim3(n_tiles, nc), RS_THREADS, 0, st>>>(ks, n, n_tiles, tcnt.p);
+  k_segment_scan<<<nc, 1024, 0, st>>>(tcnt.p, n_tiles, nseg.p);
+  k_seg_starts<<<dim3(n_tiles, nc), RS_THREADS, 0, st>>>(ks, n, n_tiles, tcnt.p, starts.p);
+  TC_CUDA(ctx, cudaGetLastError());
+  std::vector<uint32_t> S(nc);
+  TC_CUDA(ctx, cudaMemcpyAsync(S.data(), nseg.p, nc * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  TC_CUDA(ctx, cudaStreamSynchronize(st));
+  ds->h_cat_off.assign(nc, 0);
+  size_t total = 0;
+  uint32_t smax = 0;
+  for (uint16_t c = 0; c < nc; ++c) {
+    ds->h_cat_off[c] = (uint32_t)total;
+    total += S[c];
+    smax = std::max(smax, S[c]);
+  }
+  TC_TRY(ds->cat_keys.alloc(ctx, total, "category table keys"));
+  TC_TRY(ds->cat_vals.alloc(ctx, total, "category table values"));
+  TC_CUDA(ctx, cudaMemcpyAsync(ds->cat_off.p, ds->h_cat_off.data(), nc * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+  k_cat_walk<<<dim3((smax + 127) / 128, nc), 128, 0, st>>>(ds->y.p, ds->X.p, n, f, ds->cat_feats.p, ks, rs, starts.p,
+                                                          nseg.p, ds->cat_off.p, prior.p, p->prior_weight, o,
+                                                          ds->cat_keys.p, ds->cat_vals.p, ds->cat_len.p);
+  TC_CUDA(ctx, cudaGetLastError());
+  ds->h_cat_len.assign(nc, 0);
+  TC_CUDA(ctx, cudaMemcpyAsync(ds->h_cat_len.data(), ds->cat_len.p, nc * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  TC_CUDA(ctx, cudaMemcpyAsync(&ds->cat_prior, prior.p, sizeof(float), cudaMemcpyDeviceToHost, st));
+  ds->h_ts.assign(f, 0);
+  for (uint16_t c = 0; c < nc; ++c) ds->h_ts[feats[c]] = 1;
+  TC_CUDA(ctx, cudaMemcpyAsync(ds->ts.p, ds->h_ts.data(), f, cudaMemcpyHostToDevice, st));
+  TC_CUDA(ctx, cudaStreamSynchronize(st));  // the host vectors above are read by the copies
+  ds->h_cat_feats.assign(feats, feats + nc);
   return TC_OK;
 }
 
@@ -455,8 +850,10 @@ tc_status tc_dataset_upload(tc_ctx* ctx, const float* X, uint32_t n, uint16_t f,
   std::lock_guard<std::recursive_mutex> train_lock(ctx->train_mu);
   *out = nullptr;
   cudaSetDevice(ctx->device);
+  static std::atomic<uint64_t> next_id{1};
   tc_dataset* ds = new tc_dataset();
   ds->ctx = ctx;
+  ds->id = next_id.fetch_add(1);
   ds->n = n;
   ds->f = f;
   ds->groups = (f + 31) / 32;
@@ -529,6 +926,43 @@ tc_status tc_dataset_bins(const tc_dataset* ds, uint8_t* bins_out) {
   cudaSetDevice(ctx->device);
   TC_CUDA(ctx, cudaMemcpy2DAsync(bins_out, ds->n, ds->bins_cm.p, ds->np, ds->n, ds->f,
                                  cudaMemcpyDeviceToHost, ctx->stream));
+  TC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return TC_OK;
+}
+
+tc_status tc_dataset_features(const tc_dataset* ds, float* X_out) {
+  if (!ds || (!X_out && ds->n)) return TC_ERR_INVALID_ARG;
+  tc_ctx* ctx = ds->ctx;
+  std::lock_guard<std::recursive_mutex> train_lock(ctx->train_mu);
+  cudaSetDevice(ctx->device);
+  if (ds->n == 0) return TC_OK;
+  TC_CUDA(ctx, cudaMemcpyAsync(X_out, ds->X.p, ds->X.bytes(), cudaMemcpyDeviceToHost, ctx->stream));
+  TC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return TC_OK;
+}
+
+tc_status tc_encode_categorical(tc_dataset* ds, const uint16_t* features, uint16_t n_cat,
+                                const tc_cat_params* p, const uint32_t* order) {
+  if (!ds) return TC_ERR_INVALID_ARG;
+  tc_ctx* ctx = ds->ctx;
+  std::lock_guard<std::recursive_mutex> train_lock(ctx->train_mu);
+  cudaSetDevice(ctx->device);
+  return tc::encode_categorical(ds, features, n_cat, p, order);
+}
+
+tc_status tc_category_table(const tc_dataset* ds, uint16_t feature, uint32_t* keys, float* vals, uint32_t* len) {
+  if (!ds || !len) return TC_ERR_INVALID_ARG;
+  tc_ctx* ctx = ds->ctx;
+  std::lock_guard<std::recursive_mutex> train_lock(ctx->train_mu);
+  size_t c = 0;
+  while (c < ds->h_cat_feats.size() && ds->h_cat_feats[c] != feature) ++c;
+  if (c == ds->h_cat_feats.size()) return ctx->fail(TC_ERR_INVALID_ARG, "feature %u is not an encoded column", feature);
+  *len = ds->h_cat_len[c];
+  if (!keys || !vals || *len == 0) return TC_OK;
+  cudaSetDevice(ctx->device);
+  const size_t at = ds->h_cat_off[c];
+  TC_CUDA(ctx, cudaMemcpyAsync(keys, ds->cat_keys.p + at, *len * sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  TC_CUDA(ctx, cudaMemcpyAsync(vals, ds->cat_vals.p + at, *len * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
   TC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return TC_OK;
 }

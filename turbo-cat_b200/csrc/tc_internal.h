@@ -146,6 +146,25 @@ struct tc_dataset {
   DevBuf<uint32_t> nan_any;  // [f] nonzero: the feature has NaN rows
   std::vector<float> h_edges;       // [f][255]
   std::vector<uint16_t> h_n_edges;  // [f]
+  // Categorical columns encoded by target statistics (tc_encode_categorical):
+  // X holds each row's encoding in those columns, and binning uses the
+  // reference's TS edge rule and lower_bound for them (ts[j] = 1).  Encoded
+  // column c (0 .. nc-1) is feature cat_feats[c]; its global table (sorted
+  // categories -> smoothed mean, for tc_apply_bins) is entries
+  // [cat_off[c], cat_off[c] + cat_len[c]) of cat_keys / cat_vals.
+  std::vector<uint8_t> h_ts;         // [f]
+  DevBuf<uint8_t> ts;                // [f]
+  std::vector<uint16_t> h_cat_feats; // [nc]
+  std::vector<uint32_t> h_cat_off;   // [nc]
+  std::vector<uint32_t> h_cat_len;   // [nc]
+  DevBuf<uint16_t> cat_feats;        // [nc]
+  DevBuf<uint32_t> cat_off;          // [nc]
+  DevBuf<uint32_t> cat_len;          // [nc]
+  DevBuf<uint32_t> cat_keys;         // [sum of the segment counts]
+  DevBuf<float> cat_vals;            // [sum of the segment counts]
+  float cat_prior = 0.0f;
+  uint64_t id = 0;                   // unique per dataset of the process
+  uint64_t encoded_by = 0;           // id of the dataset whose tables encoded X (tc_apply_bins)
 };
 
 // Flat device-resident symmetric ensemble (the FastFloatEnsemble layout,
@@ -189,6 +208,8 @@ void stop_latency_worker(tc_ctx* ctx, const tc_model* m);
 
 // Quantization entry (tc_data.cu).
 tc_status quantize(tc_dataset* ds, int max_bins, int compat_u8);
+tc_status encode_categorical(tc_dataset* ds, const uint16_t* feats, uint16_t nc, const tc_cat_params* p,
+                             const uint32_t* order);
 
 // Prediction (tc_predict.cu): raw scores [n][K] (+ transform) on device buffers.
 tc_status predict_device(tc_ctx* ctx, const tc_model* m, const float* X, uint32_t n, uint32_t f,

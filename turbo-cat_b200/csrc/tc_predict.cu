@@ -1574,6 +1574,21 @@ static tc_status predict_small(tc_ctx* ctx, const tc_model* m, const float* X, u
   return TC_OK;
 }
 
+// Grows the context's predict staging to `need` bytes (pred_mu held).
+static tc_status grow_pred_scratch(tc_ctx* ctx, size_t need) {
+  if (ctx->pred_scratch_bytes >= need) return TC_OK;
+  if (ctx->pred_scratch) {
+    cudaStreamSynchronize(ctx->pred_stream);
+    ctx->release(ctx->pred_scratch);
+    ctx->pred_scratch = nullptr;
+    ctx->pred_scratch_bytes = 0;
+  }
+  const size_t cap = std::max(need, (size_t)1 << 20);
+  TC_TRY(ctx->alloc(&ctx->pred_scratch, cap, "predict staging"));
+  ctx->pred_scratch_bytes = cap;
+  return TC_OK;
+}
+
 tc_status tc_predict(tc_ctx* ctx, const tc_model* m, const float* X, uint32_t n, uint16_t f, int32_t transform,
                      float* out) {
   if (!ctx || !m || (!X && n) || (!out && n)) return TC_ERR_INVALID_ARG;
@@ -1592,17 +1607,7 @@ tc_status tc_predict(tc_ctx* ctx, const tc_model* m, const float* X, uint32_t n,
   const size_t in_bytes = ((size_t)n * f * sizeof(float) + 255) / 256 * 256;
   const size_t need = in_bytes + (size_t)n * K * sizeof(float);
   std::lock_guard<std::mutex> g(ctx->pred_mu);
-  if (ctx->pred_scratch_bytes < need) {
-    if (ctx->pred_scratch) {
-      cudaStreamSynchronize(ctx->pred_stream);
-      ctx->release(ctx->pred_scratch);
-      ctx->pred_scratch = nullptr;
-      ctx->pred_scratch_bytes = 0;
-    }
-    const size_t cap = std::max(need, (size_t)1 << 20);
-    TC_TRY(ctx->alloc(&ctx->pred_scratch, cap, "predict staging"));
-    ctx->pred_scratch_bytes = cap;
-  }
+  TC_TRY(grow_pred_scratch(ctx, need));
   float* dx = static_cast<float*>(ctx->pred_scratch);
   float* dout = reinterpret_cast<float*>(static_cast<char*>(ctx->pred_scratch) + in_bytes);
   cudaStream_t st = ctx->pred_stream;  // not the training stream, which another thread may be capturing
@@ -1621,6 +1626,24 @@ tc_status tc_predict_device(tc_ctx* ctx, const tc_model* m, const float* X_dev, 
   cudaSetDevice(ctx->device);
   cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->pred_stream;
   return tc::predict_device(ctx, m, X_dev, n, f, transform, out_dev, st);
+}
+
+tc_status tc_predict_dataset(tc_ctx* ctx, const tc_model* m, const tc_dataset* ds, int32_t transform, float* out) {
+  if (!ctx || !m || !ds || (!out && ds->n)) return TC_ERR_INVALID_ARG;
+  if (ds->ctx != ctx) return ctx->fail(TC_ERR_INVALID_ARG, "the dataset belongs to another context");
+  if (ds->f != (uint32_t)m->info.n_features)
+    return ctx->fail(TC_ERR_INVALID_ARG, "the dataset has %u features, the model expects %d", ds->f, m->info.n_features);
+  if (ds->n == 0) return TC_OK;
+  cudaSetDevice(ctx->device);
+  const size_t bytes = (size_t)ds->n * m->info.n_classes * sizeof(float);
+  std::lock_guard<std::mutex> g(ctx->pred_mu);
+  TC_TRY(grow_pred_scratch(ctx, bytes));
+  float* dout = static_cast<float*>(ctx->pred_scratch);
+  cudaStream_t st = ctx->pred_stream;
+  TC_TRY(tc::predict_device(ctx, m, ds->X.p, ds->n, ds->f, transform, dout, st));
+  TC_CUDA(ctx, cudaMemcpyAsync(out, dout, bytes, cudaMemcpyDeviceToHost, st));
+  TC_CUDA(ctx, cudaStreamSynchronize(st));
+  return TC_OK;
 }
 
 }  // extern "C"

@@ -26,13 +26,13 @@ TRANSFORM = {"raw": 0, "sigmoid": 1, "softmax": 2}
 SYMBOLS = [
     "tc_ctx_create", "tc_ctx_destroy", "tc_last_error", "tc_ctx_memory", "tc_ctx_fail_next_allocs",
     "tc_ctx_synchronize", "tc_ctx_set_latency_worker", "tc_dataset_upload", "tc_dataset_destroy", "tc_quantize",
-    "tc_apply_bins", "tc_dataset_bins",
+    "tc_apply_bins", "tc_dataset_bins", "tc_dataset_features", "tc_encode_categorical", "tc_category_table",
     "tc_trainer_create", "tc_trainer_step", "tc_trainer_reset", "tc_trainer_stats", "tc_trainer_profile",
     "tc_trainer_train_scores", "tc_trainer_sample_mask", "tc_trainer_set_validation", "tc_trainer_valid_loss",
     "tc_trainer_model", "tc_trainer_destroy", "tc_train", "tc_build_tree", "tc_histogram_root_noalloc",
     "tc_model_info_get", "tc_model_export",
     "tc_model_import", "tc_model_save_tcat", "tc_model_load_tcat", "tc_model_destroy", "tc_predict",
-    "tc_predict_device", "tc_server_create", "tc_server_add_model", "tc_server_submit", "tc_server_poll",
+    "tc_predict_device", "tc_predict_dataset", "tc_server_create", "tc_server_add_model", "tc_server_submit", "tc_server_poll",
     "tc_server_replay", "tc_server_stats", "tc_server_destroy",
 ]
 
@@ -48,6 +48,13 @@ class TrainParams(C.Structure):
         ("seed", C.c_uint64), ("use_goss", C.c_int32), ("goss_top_rate", C.c_float),
         ("goss_other_rate", C.c_float),
     ]
+
+
+class CatParams(C.Structure):
+    _fields_ = [("method", C.c_int32), ("prior_weight", C.c_float), ("cv_folds", C.c_int32), ("seed", C.c_uint64)]
+
+
+CAT_METHOD = {"ordered": 0, "cv": 1}
 
 
 class TrainStats(C.Structure):
@@ -162,6 +169,13 @@ class Model:
                                               C.c_uint16(f), C.c_int32(TRANSFORM[transform]),
                                               C.c_void_p(out_ptr), C.c_void_p(stream)))
 
+    def predict_dataset(self, ds: "Dataset", transform="raw"):
+        """tc_predict_dataset: the dataset's rows as the device holds them."""
+        out = np.zeros((ds.n, self.info.n_classes), np.float32)
+        self.eng._chk(lib().tc_predict_dataset(self.eng.ctx, self.h, ds.h, C.c_int32(TRANSFORM[transform]),
+                                               _p(out)))
+        return out
+
     def close(self):
         if self.h and lib is not None:  # at interpreter exit the module globals may be gone
             lib().tc_model_destroy(self.h)
@@ -189,6 +203,29 @@ class Dataset:
         out = np.zeros((self.f, self.n), np.uint8)
         self.eng._chk(lib().tc_dataset_bins(self.h, _p(out)))
         return out
+
+    def features(self):
+        """The feature matrix as the device holds it (encoded categorical columns)."""
+        out = np.zeros((self.n, self.f), np.float32)
+        self.eng._chk(lib().tc_dataset_features(self.h, _p(out)))
+        return out
+
+    def encode_categorical(self, features, method="ordered", prior_weight=1.0, cv_folds=5, seed=0, order=None):
+        """Target statistics of the categorical columns (tc_encode_categorical);
+        `order`: the processing order (ordered) or each row's fold (cv)."""
+        feats = np.ascontiguousarray(features, np.uint16)
+        prm = CatParams(CAT_METHOD[method], prior_weight, cv_folds, seed)
+        o = None if order is None else np.ascontiguousarray(order, np.uint32)
+        self.eng._chk(lib().tc_encode_categorical(self.h, _p(feats), C.c_uint16(len(feats)), C.byref(prm), _p(o)))
+
+    def category_table(self, feature):
+        """(sorted categories, encodings) of one encoded column."""
+        n = C.c_uint32(0)
+        self.eng._chk(lib().tc_category_table(self.h, C.c_uint16(feature), None, None, C.byref(n)))
+        keys = np.zeros(n.value, np.uint32)
+        vals = np.zeros(n.value, np.float32)
+        self.eng._chk(lib().tc_category_table(self.h, C.c_uint16(feature), _p(keys), _p(vals), C.byref(n)))
+        return keys, vals
 
     def close(self):
         if self.h and lib is not None:  # at interpreter exit the module globals may be gone
