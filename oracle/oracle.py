@@ -857,9 +857,9 @@ def recover_order(X, y, feat, enc, prior_weight=1.0):
             by_cat.setdefault(category_of(col[r]), []).append(r)
     pos = {}
     for c, rows in by_cat.items():
-        pool = {}
+        pool = {}  # encoding bits -> label -> rows
         for r in rows:
-            pool.setdefault((enc[r].view(np.uint32).item(), y[r].item()), []).append(r)
+            pool.setdefault(enc[r].view(np.uint32).item(), {}).setdefault(y[r].item(), []).append(r)
 
         def target(s, k):
             return (prior if k == 0 else _smooth(s, k, wp, pw)).view(np.uint32).item()
@@ -867,13 +867,13 @@ def recover_order(X, y, feat, enc, prior_weight=1.0):
         def solve(s, k):  # depth-first over the label taken at each step
             if k == len(rows):
                 return []
-            t = target(s, k)
-            for lab in sorted({lb for (e, lb), v in pool.items() if e == t and v}):
-                r = pool[(t, lab)].pop()
+            cand = pool.get(target(s, k), {})
+            for lab in sorted(lb for lb, v in cand.items() if v):
+                r = cand[lab].pop()
                 rest = solve(F32(s + F32(lab)), k + 1)
                 if rest is not None:
                     return [r] + rest
-                pool[(t, lab)].append(r)
+                cand[lab].append(r)
             return None
 
         import sys
@@ -911,11 +911,12 @@ def recover_folds(X, y, feat, enc, n_folds, prior_weight=1.0):
         q = 0
         for e, grp in groups.items():
             match = None
+            gsum = F32(np.add.accumulate(y[grp], dtype=F32)[-1])
             for nf in range(1, N + 1):  # fold size: the out-of-fold count is N - nf
                 if len(grp) % nf:
                     continue
                 m = len(grp) // nf
-                pos = F32(np.add.accumulate(y[grp], dtype=F32)[-1]) / F32(m)
+                pos = gsum / F32(m)
                 if _smooth(F32(P - pos), N - nf, wp, pw).view(np.uint32).item() == e:
                     match = nf
                     break

@@ -220,7 +220,9 @@ __global__ void k_unique_pick(const uint32_t* __restrict__ keys, uint32_t n, uin
     for (int w = 0; w < warp; ++w) before += warp_sums[w];
     if (fl) {
       const uint64_t r = before + x - 1;  // distinct-value rank
-      const uint64_t b = (r * A + U - 1) / U;
+      // the smallest b with floor(b*U/A) >= r; b >= 1 (with A > U, as the
+      // target-statistics rule has for A = U, rank 0 is edge 0)
+      const uint64_t b = max((r * A + U - 1) / U, (uint64_t)1);
       if (b >= 1 && b <= A - 1 && (b * U) / A == r) edges[(size_t)j * kSlots + (b - 1)] = key_float(kj[idx]);
     }
     __syncthreads();
