@@ -471,6 +471,64 @@ def suite_c1(eng, _capi, ref_ok):
     return out
 
 
+def suite_cat(eng, _capi, ref_ok):
+    return {"cardinality_1000": _cat_case(eng, ref_ok, cardinality=1000),
+            "cardinality_8": _cat_case(eng, ref_ok, cardinality=8)}
+
+
+def _cat_case(eng, ref_ok, n=10_000_000, f=20, n_cat=4, cardinality=1000):
+    """Categorical target statistics at scale: n rows, n_cat categorical
+    columns of `cardinality` ids (3% NaN) among f, class-id labels.  Device:
+    tc_encode_categorical (ordered and cross-validated; host-synchronous
+    calls, wall time) and the binning after it; reference: its own
+    compute_target_statistics on a 1M-row slice, scaled to n."""
+    rng = np.random.default_rng(17)
+    X = rng.standard_normal((n, f), dtype=np.float32)
+    cats = list(range(1, 2 * n_cat, 2))
+    logit = X[:, 0].copy()
+    for j in cats:
+        c = rng.integers(0, cardinality, n)
+        X[:, j] = c
+        logit += ((c % 7) - 3) * 0.3
+        X[rng.random(n, dtype=np.float32) < 0.03, j] = np.nan
+    y = (rng.random(n, dtype=np.float32) < 1.0 / (1.0 + np.exp(-logit))).astype(np.float32)
+    out = {"config": f"categorical target statistics, {n} rows x {f} features, {n_cat} categorical "
+                     f"({cardinality} ids, 3% NaN)"}
+    for method in ("ordered", "cv"):
+        best = None
+        for _ in range(3):
+            ds = eng.upload(X, y)
+            t0 = time.perf_counter()
+            ds.encode_categorical(cats, method, seed=1)
+            t1 = time.perf_counter()
+            ds.quantize(255)
+            t2 = time.perf_counter()
+            ds.close()
+            best = min(best or (9e9, 9e9), (t1 - t0, t2 - t1))
+        out[f"{method}_encode_ms"] = best[0] * 1e3
+        out[f"{method}_rows_x_columns_per_s"] = n * n_cat / best[0]
+        out[f"{method}_quantize_after_ms"] = best[1] * 1e3
+    if ref_ok:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import ctypes as C
+
+        import oracle as O
+
+        m = 1_000_000
+        Xs, ys = np.ascontiguousarray(X[:m]), np.ascontiguousarray(y[:m])
+        cs = np.array(cats, np.uint16)
+        for method, mid in (("ordered", 0), ("cv", 1)):
+            sec = C.c_double()
+            rc = O.ref().tcref_cat_ts_timed(Xs.ctypes.data_as(C.c_void_p), C.c_uint32(m), C.c_uint16(f),
+                                            ys.ctypes.data_as(C.c_void_p), cs.ctypes.data_as(C.c_void_p),
+                                            C.c_int32(len(cats)), C.c_int32(mid), C.byref(sec))
+            if rc == 0:
+                out[f"reference_{method}_ms_1M_rows"] = sec.value * 1e3
+                out[f"reference_{method}_ms_scaled_to_n"] = sec.value * 1e3 * n / m
+        out["reference_threads"] = 1  # compute_target_statistics runs on one thread
+    return out
+
+
 def suite_c3(eng, _capi, iters=10):
     from datagen import multiclass_c3
 
@@ -686,6 +744,8 @@ def run_suite(args):
             r = c2_secondary(eng, _capi, peak, kind, steps=5)
         elif name == "goss":
             r = suite_goss(eng, _capi)
+        elif name == "cat":
+            r = suite_cat(eng, _capi, ref_ok)
         elif name == "c4dev":  # the four serving models' device-resident prediction only
             r = {"config": "serving models (1000xd6, 200xd4, 500xd8, 2000xd10) on 100 features, 1M resident rows",
                  "device_predict_1M_rows": _device_predict(_train_serving_models(eng, _capi), 100)}
@@ -707,7 +767,7 @@ def main():
     ap.add_argument("--no-c2", action="store_true", help="leave out the secondary regression configuration")
     ap.add_argument("--reference-seconds", type=float, default=240.0,
                     help="reference arm: stop building trees once this many seconds have passed")
-    ap.add_argument("--suite", default="", help="secondary configurations, e.g. c1,c2,c3,c4")
+    ap.add_argument("--suite", default="", help="secondary configurations, e.g. c1,c2,c3,c4,goss,cat")
     ap.add_argument("--rows", type=int, default=0,
                     help="rows of the workload (default: the configuration's 10M); a smaller case of the same "
                          "workload for profiler captures")

@@ -352,4 +352,25 @@ int tcref_cat_ts(const float* X, uint32_t n, uint16_t f, const float* y, const u
   }
 }
 
+// Seconds of the reference's compute_target_statistics alone on one dataset
+// (from_dense with the categorical features first, untimed); the CPU
+// baseline of the categorical encoding.
+int tcref_cat_ts_timed(const float* X, uint32_t n, uint16_t f, const float* y, const uint16_t* cats,
+                       int32_t n_cat, int32_t method, double* seconds) {
+  try {
+    Config cfg = Config::binary_classification();
+    cfg.categorical.method = method == 1 ? CategoricalConfig::EncodingMethod::CrossValidatedTS
+                                         : CategoricalConfig::EncodingMethod::TargetStatistics;
+    std::vector<FeatureIndex> cf(cats, cats + n_cat);
+    Dataset ds;
+    ds.from_dense(X, n, f, y, nullptr, cf);
+    const auto t0 = std::chrono::steady_clock::now();
+    ds.compute_target_statistics(cfg);
+    *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
 }  // extern "C"

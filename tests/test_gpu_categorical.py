@@ -41,10 +41,12 @@ def test_encode_matches_reference_run(engine, method):
     ds.close()
 
 
-def _odd_case(n, seed):
+def _odd_case(n, seed, labels="float"):
     """Three categorical columns: small ids, wide ids (category 0xFFFFFFFF from
     -1.0 next to NaN rows, 2^32 folding onto 0, fractions truncated) and a
-    high-cardinality one; float labels so that the order of additions shows."""
+    high-cardinality one.  Float labels make the order of the additions show
+    (the device's sequential walk); class ids add exactly in any order (its
+    parallel prefix / fold-total path)."""
     rng = np.random.default_rng(seed)
     X = rng.standard_normal((n, 7)).astype(np.float32)
     X[:, 1] = rng.integers(0, 9, n)
@@ -52,14 +54,17 @@ def _odd_case(n, seed):
     X[:, 5] = rng.integers(0, max(2, n // 3), n)
     for j in (1, 3, 5):
         X[rng.random(n) < 0.04, j] = np.nan
-    y = rng.random(n).astype(np.float32)
+    y = rng.random(n).astype(np.float32) if labels == "float" else rng.integers(0, 3, n).astype(np.float32)
     return X, y
 
 
-@pytest.mark.parametrize("method,n,pw", [("ordered", 1, 1.0), ("ordered", 5000, 1.0), ("ordered", 40_000, 2.5),
-                                         ("cv", 5000, 1.0), ("cv", 40_000, 0.5)])
-def test_encode_matches_oracle(engine, method, n, pw):
-    X, y = _odd_case(n, seed=n + int(pw * 10))
+@pytest.mark.parametrize("method,n,pw,labels", [
+    ("ordered", 1, 1.0, "float"), ("ordered", 5000, 1.0, "float"), ("ordered", 40_000, 2.5, "float"),
+    ("cv", 5000, 1.0, "float"), ("cv", 40_000, 0.5, "float"),
+    ("ordered", 1, 1.0, "class"), ("ordered", 70_000, 1.0, "class"), ("ordered", 70_000, 2.5, "class"),
+    ("cv", 70_000, 1.0, "class"), ("cv", 9000, 0.5, "class")])
+def test_encode_matches_oracle(engine, method, n, pw, labels):
+    X, y = _odd_case(n, seed=n + int(pw * 10), labels=labels)
     rng = np.random.default_rng(7)
     feats = [1, 3, 5]
     if method == "ordered":

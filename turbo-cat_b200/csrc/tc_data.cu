@@ -436,7 +436,8 @@ __global__ void k_seg_count(const uint32_t* __restrict__ keys, uint32_t n, uint3
 
 // starts[j][rank] = first sorted position of the rank-th segment of column j.
 __global__ void k_seg_starts(const uint32_t* __restrict__ keys, uint32_t n, uint32_t n_tiles,
-                             const uint32_t* __restrict__ tile_off, uint32_t* __restrict__ starts) {
+                             const uint32_t* __restrict__ tile_off, uint32_t* __restrict__ starts,
+                             uint32_t* __restrict__ segid) {
   __shared__ uint32_t warp_sums[RS_THREADS / 32];
   __shared__ uint32_t run_s;
   const uint32_t j = blockIdx.y, tile = blockIdx.x;
@@ -457,6 +458,7 @@ __global__ void k_seg_starts(const uint32_t* __restrict__ keys, uint32_t n, uint
     uint32_t before = run_s;
     for (int w = 0; w < warp; ++w) before += warp_sums[w];
     if (fl) starts[(size_t)j * n + before + x - 1] = idx;
+    if (segid && idx < n) segid[(size_t)j * n + idx] = before + x - 1;  // rank of idx's segment
     __syncthreads();
     if (threadIdx.x == 0) {
       uint32_t t = 0;
@@ -545,6 +547,269 @@ __global__ void k_cat_walk(const float* __restrict__ y, float* __restrict__ X, u
   tab_keys[at] = keys[base + begin];
   tab_vals[at] = count ? smooth(total, count) : prior;
   if (s == S - 1) tab_len[c] = count ? S : S - 1;  // a last segment of NaN rows only is no category
+}
+
+// ---- exact labels: every partial sum is an integer below 2^24 in magnitude,
+// so float adds them exactly in any order and the running sums can be
+// prefix sums (ordered) or atomic fold totals (cross-validated), one thread
+// per row instead of one per category.  Class ids always are; the sequential
+// walk above serves every other label.
+
+// flags[0] |= 1 if some label is not an integer of magnitude <= 2^24;
+// sum[0] += sum |label| (as integers).
+__global__ void k_label_exact(const float* __restrict__ y, uint32_t n, unsigned long long* __restrict__ sum,
+                              uint32_t* __restrict__ flags) {
+  unsigned long long s = 0;
+  uint32_t bad = 0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const float v = fabsf(y[i]);
+    if (!(v <= 16777216.0f) || v != truncf(v)) bad = 1;  // NaN fails the first test
+    else s += (unsigned long long)v;
+  }
+  for (int o = 16; o; o >>= 1) {
+    s += __shfl_xor_sync(0xffffffffu, s, o);
+    bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (s) atomicAdd(sum, s);
+    if (bad) atomicOr(flags, 1u);
+  }
+}
+
+// Per tile of sorted positions: sum of the labels and count of the rows that
+// are not NaN.
+__global__ void k_cat_tile_sums(const float* __restrict__ X, const float* __restrict__ y, uint32_t n, uint32_t f,
+                                const uint16_t* __restrict__ feats, const uint32_t* __restrict__ rows,
+                                uint32_t n_tiles, long long* __restrict__ tsum, uint32_t* __restrict__ tcnt) {
+  __shared__ long long ws[RS_THREADS / 32];
+  __shared__ uint32_t wc[RS_THREADS / 32];
+  const uint32_t c = blockIdx.y, tile = blockIdx.x, feat = feats[c];
+  long long sm = 0;
+  uint32_t k = 0;
+  for (int it = 0; it < RS_ITEMS; ++it) {
+    const uint32_t idx = tile * RS_TILE + it * RS_THREADS + threadIdx.x;
+    if (idx >= n) break;
+    const uint32_t row = rows[(size_t)c * n + idx];
+    if (!isnan(X[(size_t)row * f + feat])) {
+      sm += (long long)y[row];
+      ++k;
+    }
+  }
+  for (int o = 16; o; o >>= 1) {
+    sm += __shfl_xor_sync(0xffffffffu, sm, o);
+    k += __shfl_xor_sync(0xffffffffu, k, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    ws[threadIdx.x >> 5] = sm;
+    wc[threadIdx.x >> 5] = k;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long a = 0;
+    uint32_t b = 0;
+    for (int w = 0; w < RS_THREADS / 32; ++w) {
+      a += ws[w];
+      b += wc[w];
+    }
+    tsum[(size_t)c * n_tiles + tile] = a;
+    tcnt[(size_t)c * n_tiles + tile] = b;
+  }
+}
+
+// Exclusive scan of the tile totals of each column, in place (one thread per
+// column: a few thousand tiles).
+__global__ void k_cat_tile_scan(long long* __restrict__ tsum, uint32_t* __restrict__ tcnt, uint32_t n_tiles) {
+  if (threadIdx.x != 0) return;
+  long long a = 0;
+  uint32_t b = 0;
+  long long* ts = tsum + (size_t)blockIdx.x * n_tiles;
+  uint32_t* tc = tcnt + (size_t)blockIdx.x * n_tiles;
+  for (uint32_t t = 0; t < n_tiles; ++t) {
+    const long long x = ts[t];
+    const uint32_t y = tc[t];
+    ts[t] = a;
+    tc[t] = b;
+    a += x;
+    b += y;
+  }
+}
+
+// P[c][i] / C[c][i]: label sum / row count of the non-NaN rows at sorted
+// positions before i (i = 0 .. n).
+__global__ void k_cat_prefix(const float* __restrict__ X, const float* __restrict__ y, uint32_t n, uint32_t f,
+                             const uint16_t* __restrict__ feats, const uint32_t* __restrict__ rows, uint32_t n_tiles,
+                             const long long* __restrict__ toff, const uint32_t* __restrict__ tcoff,
+                             long long* __restrict__ P, uint32_t* __restrict__ C) {
+  __shared__ long long ws[RS_THREADS / 32];
+  __shared__ uint32_t wc[RS_THREADS / 32];
+  __shared__ long long run_s;
+  __shared__ uint32_t run_c;
+  const uint32_t c = blockIdx.y, tile = blockIdx.x, feat = feats[c];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const size_t base = (size_t)c * (n + 1);
+  if (threadIdx.x == 0) {
+    run_s = toff[(size_t)c * n_tiles + tile];
+    run_c = tcoff[(size_t)c * n_tiles + tile];
+  }
+  __syncthreads();
+  for (int it = 0; it < RS_ITEMS; ++it) {
+    const uint32_t idx = tile * RS_TILE + it * RS_THREADS + threadIdx.x;
+    long long v = 0;
+    uint32_t k = 0;
+    if (idx < n) {
+      const uint32_t row = rows[(size_t)c * n + idx];
+      if (!isnan(X[(size_t)row * f + feat])) {
+        v = (long long)y[row];
+        k = 1;
+      }
+    }
+    long long xs = v;
+    uint32_t xc = k;
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long a = __shfl_up_sync(0xffffffffu, xs, o);
+      const uint32_t b = __shfl_up_sync(0xffffffffu, xc, o);
+      if (lane >= o) {
+        xs += a;
+        xc += b;
+      }
+    }
+    if (lane == 31) {
+      ws[warp] = xs;
+      wc[warp] = xc;
+    }
+    __syncthreads();
+    long long bs = run_s;
+    uint32_t bc = run_c;
+    for (int w = 0; w < warp; ++w) {
+      bs += ws[w];
+      bc += wc[w];
+    }
+    if (idx < n) {
+      P[base + idx] = bs + xs - v;
+      C[base + idx] = bc + xc - k;
+      if (idx == n - 1) {
+        P[base + n] = bs + xs;
+        C[base + n] = bc + xc;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int w = 0; w < RS_THREADS / 32; ++w) {
+        run_s += ws[w];
+        run_c += wc[w];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Ordered method, one thread per sorted position: the rows of its category
+// before it are the positions [segment start, i).
+__global__ void k_cat_rows_ordered(float* __restrict__ X, uint32_t n, uint32_t f,
+                                   const uint16_t* __restrict__ feats, const uint32_t* __restrict__ rows,
+                                   const uint32_t* __restrict__ segid, const uint32_t* __restrict__ starts,
+                                   const long long* __restrict__ P, const uint32_t* __restrict__ C,
+                                   const float* __restrict__ prior_p, float pw) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
+  if (i >= n) return;
+  const size_t base = (size_t)c * n, pb = (size_t)c * (n + 1);
+  const uint32_t row = rows[base + i];
+  float* xp = X + (size_t)row * f + feats[c];
+  const float prior = *prior_p;
+  if (isnan(*xp)) {
+    *xp = prior;
+    return;
+  }
+  const uint32_t b = starts[base + segid[base + i]];
+  const uint32_t k = C[pb + i] - C[pb + b];
+  const float sum = __ll2float_rn(P[pb + i] - P[pb + b]);  // exact: |sum| <= 2^24
+  *xp = k ? __fdiv_rn(__fadd_rn(sum, __fmul_rn(pw, prior)), __fadd_rn(__uint2float_rn(k), pw)) : prior;
+}
+
+// Table entries of the ordered method from the prefix sums.
+__global__ void k_cat_table_prefix(const uint32_t* __restrict__ keys, uint32_t n, const uint32_t* __restrict__ starts,
+                                   const uint32_t* __restrict__ nseg, const uint32_t* __restrict__ off,
+                                   const long long* __restrict__ P, const uint32_t* __restrict__ C,
+                                   const float* __restrict__ prior_p, float pw, uint32_t* __restrict__ tab_keys,
+                                   float* __restrict__ tab_vals, uint32_t* __restrict__ tab_len) {
+  const uint32_t c = blockIdx.y, s = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t S = nseg[c];
+  if (s >= S) return;
+  const size_t base = (size_t)c * n, pb = (size_t)c * (n + 1);
+  const uint32_t b = starts[base + s], e = s + 1 < S ? starts[base + s + 1] : n;
+  const uint32_t k = C[pb + e] - C[pb + b];
+  const float prior = *prior_p;
+  const float sum = __ll2float_rn(P[pb + e] - P[pb + b]);
+  const uint32_t at = off[c] + s;
+  tab_keys[at] = keys[base + b];
+  tab_vals[at] = k ? __fdiv_rn(__fadd_rn(sum, __fmul_rn(pw, prior)), __fadd_rn(__uint2float_rn(k), pw)) : prior;
+  if (s == S - 1) tab_len[c] = k ? S : S - 1;
+}
+
+// Cross-validated method: per (category, fold) label sums and counts by
+// atomics (integers: exact in any order).
+__global__ void k_cat_fold_sums(const float* __restrict__ X, const float* __restrict__ y, uint32_t n, uint32_t f,
+                                const uint16_t* __restrict__ feats, const uint32_t* __restrict__ rows,
+                                const uint32_t* __restrict__ segid, const uint32_t* __restrict__ off, CatOrder o,
+                                unsigned long long* __restrict__ fsum, uint32_t* __restrict__ fcnt) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
+  if (i >= n) return;
+  const size_t base = (size_t)c * n;
+  const uint32_t row = rows[base + i];
+  if (isnan(X[(size_t)row * f + feats[c]])) return;
+  const size_t at = ((size_t)off[c] + segid[base + i]) * o.folds + fold_of(row, o);
+  atomicAdd(&fsum[at], (unsigned long long)(long long)y[row]);
+  atomicAdd(&fcnt[at], 1u);
+}
+
+__global__ void k_cat_rows_cv(float* __restrict__ X, uint32_t n, uint32_t f, const uint16_t* __restrict__ feats,
+                              const uint32_t* __restrict__ rows, const uint32_t* __restrict__ segid,
+                              const uint32_t* __restrict__ off, CatOrder o,
+                              const unsigned long long* __restrict__ fsum, const uint32_t* __restrict__ fcnt,
+                              const float* __restrict__ prior_p, float pw) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
+  if (i >= n) return;
+  const size_t base = (size_t)c * n;
+  const uint32_t row = rows[base + i];
+  float* xp = X + (size_t)row * f + feats[c];
+  const float prior = *prior_p;
+  if (isnan(*xp)) {
+    *xp = prior;
+    return;
+  }
+  const size_t at = ((size_t)off[c] + segid[base + i]) * o.folds;
+  const uint32_t fd = fold_of(row, o);
+  long long sm = 0;
+  uint32_t k = 0;
+  for (uint32_t q = 0; q < o.folds; ++q) {
+    if (q == fd) continue;
+    sm += (long long)fsum[at + q];
+    k += fcnt[at + q];
+  }
+  *xp = __fdiv_rn(__fadd_rn(__ll2float_rn(sm), __fmul_rn(pw, prior)), __fadd_rn(__uint2float_rn(k), pw));
+}
+
+__global__ void k_cat_table_cv(const uint32_t* __restrict__ keys, uint32_t n, const uint32_t* __restrict__ starts,
+                               const uint32_t* __restrict__ nseg, const uint32_t* __restrict__ off, CatOrder o,
+                               const unsigned long long* __restrict__ fsum, const uint32_t* __restrict__ fcnt,
+                               const float* __restrict__ prior_p, float pw, uint32_t* __restrict__ tab_keys,
+                               float* __restrict__ tab_vals, uint32_t* __restrict__ tab_len) {
+  const uint32_t c = blockIdx.y, s = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t S = nseg[c];
+  if (s >= S) return;
+  const size_t at = ((size_t)off[c] + s) * o.folds;
+  long long sm = 0;
+  uint32_t k = 0;
+  for (uint32_t q = 0; q < o.folds; ++q) {
+    sm += (long long)fsum[at + q];
+    k += fcnt[at + q];
+  }
+  const float prior = *prior_p;
+  const uint32_t t = off[c] + s;
+  tab_keys[t] = keys[(size_t)c * n + starts[(size_t)c * n + s]];
+  tab_vals[t] = k ? __fdiv_rn(__fadd_rn(__ll2float_rn(sm), __fmul_rn(pw, prior)), __fadd_rn(__uint2float_rn(k), pw))
+                  : prior;
+  if (s == S - 1) tab_len[c] = k ? S : S - 1;
 }
 
 // Dataset::apply_bins' categorical branch (src/core/dataset.cpp:362-372):
@@ -719,7 +984,8 @@ tc_status encode_categorical(tc_dataset* ds, const uint16_t* feats, uint16_t nc,
   }
   cudaStream_t st = ctx->stream;
   const uint32_t n_tiles = (uint32_t)((n + RS_TILE - 1) / RS_TILE);
-  DevBuf<uint32_t> ka, kb, ra, rb, counts, tcnt, nseg, starts, given;
+  DevBuf<uint32_t> ka, kb, ra, rb, counts, tcnt, nseg, starts, segid, given, lab_flag;
+  DevBuf<unsigned long long> lab_sum;
   DevBuf<float> prior;
   TC_TRY(ka.alloc(ctx, (size_t)nc * n, "category keys"));
   TC_TRY(kb.alloc(ctx, (size_t)nc * n, "category keys (alt)"));
@@ -729,7 +995,10 @@ tc_status encode_categorical(tc_dataset* ds, const uint16_t* feats, uint16_t nc,
   TC_TRY(tcnt.alloc(ctx, (size_t)nc * n_tiles, "segment tile counts"));
   TC_TRY(nseg.alloc(ctx, nc, "segment counts"));
   TC_TRY(starts.alloc(ctx, (size_t)nc * n, "segment starts"));
+  TC_TRY(segid.alloc(ctx, (size_t)nc * n, "segment of each position"));
   TC_TRY(prior.alloc(ctx, 1, "label prior"));
+  TC_TRY(lab_sum.alloc(ctx, 1, "label magnitude sum"));
+  TC_TRY(lab_flag.alloc(ctx, 1, "label flags"));
   TC_TRY(ds->cat_feats.alloc(ctx, nc, "categorical features"));
   TC_TRY(ds->cat_off.alloc(ctx, nc, "category table offsets"));
   TC_TRY(ds->cat_len.alloc(ctx, nc, "category table lengths"));
@@ -748,6 +1017,10 @@ tc_status encode_categorical(tc_dataset* ds, const uint16_t* feats, uint16_t nc,
   }
   TC_CUDA(ctx, cudaMemcpyAsync(ds->cat_feats.p, feats, nc * sizeof(uint16_t), cudaMemcpyHostToDevice, st));
   k_label_prior<<<1, 1024, 0, st>>>(ds->y.p, n, prior.p);
+  TC_CUDA(ctx, cudaMemsetAsync(lab_sum.p, 0, sizeof(unsigned long long), st));
+  TC_CUDA(ctx, cudaMemsetAsync(lab_flag.p, 0, sizeof(uint32_t), st));
+  k_label_exact<<<std::min<uint32_t>((n + 255) / 256, 4 * (uint32_t)ctx->sm_count), 256, 0, st>>>(ds->y.p, n, lab_sum.p,
+                                                                                             lab_flag.p);
   k_cat_keys<<<dim3((n + CAT_THREADS - 1) / CAT_THREADS, nc), CAT_THREADS, 0, st>>>(ds->X.p, n, f,
                                                                                    ds->cat_feats.p, o, ka.p, ra.p);
   uint32_t *ks = ka.p, *kd = kb.p, *rs = ra.p, *rd = rb.p;
@@ -760,11 +1033,18 @@ tc_status encode_categorical(tc_dataset* ds, const uint16_t* feats, uint16_t nc,
   }
   k_seg_count<<<dim3(n_tiles, nc), RS_THREADS, 0, st>>>(ks, n, n_tiles, tcnt.p);
   k_segment_scan<<<nc, 1024, 0, st>>>(tcnt.p, n_tiles, nseg.p);
-  k_seg_starts<<<dim3(n_tiles, nc), RS_THREADS, 0, st>>>(ks, n, n_tiles, tcnt.p, starts.p);
+  k_seg_starts<<<dim3(n_tiles, nc), RS_THREADS, 0, st>>>(ks, n, n_tiles, tcnt.p, starts.p, segid.p);
   TC_CUDA(ctx, cudaGetLastError());
   std::vector<uint32_t> S(nc);
+  unsigned long long h_lab_sum = 0;
+  uint32_t h_lab_flag = 1;
   TC_CUDA(ctx, cudaMemcpyAsync(S.data(), nseg.p, nc * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  TC_CUDA(ctx, cudaMemcpyAsync(&h_lab_sum, lab_sum.p, sizeof(h_lab_sum), cudaMemcpyDeviceToHost, st));
+  TC_CUDA(ctx, cudaMemcpyAsync(&h_lab_flag, lab_flag.p, sizeof(h_lab_flag), cudaMemcpyDeviceToHost, st));
   TC_CUDA(ctx, cudaStreamSynchronize(st));
+  // integer labels whose magnitudes sum to at most 2^24: every float partial
+  // sum is exact, so the sums need not be sequential
+  const bool exact = h_lab_flag == 0 && h_lab_sum <= (1ull << 24);
   ds->h_cat_off.assign(nc, 0);
   size_t total = 0;
   uint32_t smax = 0;
@@ -776,9 +1056,45 @@ tc_status encode_categorical(tc_dataset* ds, const uint16_t* feats, uint16_t nc,
   TC_TRY(ds->cat_keys.alloc(ctx, total, "category table keys"));
   TC_TRY(ds->cat_vals.alloc(ctx, total, "category table values"));
   TC_CUDA(ctx, cudaMemcpyAsync(ds->cat_off.p, ds->h_cat_off.data(), nc * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-  k_cat_walk<<<dim3((smax + 127) / 128, nc), 128, 0, st>>>(ds->y.p, ds->X.p, n, f, ds->cat_feats.p, ks, rs, starts.p,
-                                                          nseg.p, ds->cat_off.p, prior.p, p->prior_weight, o,
-                                                          ds->cat_keys.p, ds->cat_vals.p, ds->cat_len.p);
+  const dim3 rg((n + CAT_THREADS - 1) / CAT_THREADS, nc), sg((smax + 127) / 128, nc);
+  const float pw = p->prior_weight;
+  if (!exact) {
+    k_cat_walk<<<sg, 128, 0, st>>>(ds->y.p, ds->X.p, n, f, ds->cat_feats.p, ks, rs, starts.p, nseg.p, ds->cat_off.p,
+                                   prior.p, pw, o, ds->cat_keys.p, ds->cat_vals.p, ds->cat_len.p);
+  } else if (!cv) {
+    DevBuf<long long> tsum, P;
+    DevBuf<uint32_t> tcnt2, Cn;
+    TC_TRY(tsum.alloc(ctx, (size_t)nc * n_tiles, "tile label sums"));
+    TC_TRY(tcnt2.alloc(ctx, (size_t)nc * n_tiles, "tile row counts"));
+    TC_TRY(P.alloc(ctx, (size_t)nc * (n + 1), "label prefix sums"));
+    TC_TRY(Cn.alloc(ctx, (size_t)nc * (n + 1), "row prefix counts"));
+    k_cat_tile_sums<<<dim3(n_tiles, nc), RS_THREADS, 0, st>>>(ds->X.p, ds->y.p, n, f, ds->cat_feats.p, rs, n_tiles,
+                                                              tsum.p, tcnt2.p);
+    k_cat_tile_scan<<<nc, 32, 0, st>>>(tsum.p, tcnt2.p, n_tiles);
+    k_cat_prefix<<<dim3(n_tiles, nc), RS_THREADS, 0, st>>>(ds->X.p, ds->y.p, n, f, ds->cat_feats.p, rs, n_tiles,
+                                                           tsum.p, tcnt2.p, P.p, Cn.p);
+    k_cat_table_prefix<<<sg, 128, 0, st>>>(ks, n, starts.p, nseg.p, ds->cat_off.p, P.p, Cn.p, prior.p, pw,
+                                           ds->cat_keys.p, ds->cat_vals.p, ds->cat_len.p);
+    k_cat_rows_ordered<<<rg, CAT_THREADS, 0, st>>>(ds->X.p, n, f, ds->cat_feats.p, rs, segid.p, starts.p, P.p, Cn.p,
+                                                   prior.p, pw);
+    TC_CUDA(ctx, cudaGetLastError());
+    TC_CUDA(ctx, cudaStreamSynchronize(st));  // before the scratch buffers go
+  } else {
+    DevBuf<unsigned long long> fsum;
+    DevBuf<uint32_t> fcnt;
+    TC_TRY(fsum.alloc(ctx, total * o.folds, "fold label sums"));
+    TC_TRY(fcnt.alloc(ctx, total * o.folds, "fold row counts"));
+    TC_CUDA(ctx, cudaMemsetAsync(fsum.p, 0, fsum.bytes(), st));
+    TC_CUDA(ctx, cudaMemsetAsync(fcnt.p, 0, fcnt.bytes(), st));
+    k_cat_fold_sums<<<rg, CAT_THREADS, 0, st>>>(ds->X.p, ds->y.p, n, f, ds->cat_feats.p, rs, segid.p, ds->cat_off.p, o,
+                                                fsum.p, fcnt.p);
+    k_cat_table_cv<<<sg, 128, 0, st>>>(ks, n, starts.p, nseg.p, ds->cat_off.p, o, fsum.p, fcnt.p, prior.p, pw,
+                                       ds->cat_keys.p, ds->cat_vals.p, ds->cat_len.p);
+    k_cat_rows_cv<<<rg, CAT_THREADS, 0, st>>>(ds->X.p, n, f, ds->cat_feats.p, rs, segid.p, ds->cat_off.p, o, fsum.p,
+                                              fcnt.p, prior.p, pw);
+    TC_CUDA(ctx, cudaGetLastError());
+    TC_CUDA(ctx, cudaStreamSynchronize(st));
+  }
   TC_CUDA(ctx, cudaGetLastError());
   ds->h_cat_len.assign(nc, 0);
   TC_CUDA(ctx, cudaMemcpyAsync(ds->h_cat_len.data(), ds->cat_len.p, nc * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
