@@ -174,6 +174,34 @@ def test_fit_on_target_statistics_matches_reference(engine, capi):
         h.close()
 
 
+def test_validation_set_encoded_by_training_table(engine, capi):
+    """The binding's fit with cat_features and a validation set: the
+    validation rows are encoded by tc_apply_bins against the training set
+    (valid_data->apply_bins(*train_data_)), and the device's validation loss
+    is the logloss of the model's predictions on those encoded rows."""
+    X, y = categorical_case(n=8000, f=6, seed=41)
+    Xv, yv = categorical_case(n=3000, f=6, seed=42)
+    ds = engine.upload(X, y)
+    ds.encode_categorical([2], "ordered", seed=3)
+    ds.quantize(255)
+    vds = engine.upload(Xv, yv)
+    vds.apply_bins(ds)
+    tr = engine.trainer(ds, capi.params(loss="logloss", n_estimators=15, max_depth=4, learning_rate=0.3))
+    tr.set_validation(vds, 1000)
+    tr.step(15)
+    vl = tr.valid_loss()
+    m = tr.model()
+    keys, vals = ds.category_table(2)
+    Ev = O.encode_test(Xv, {2: (keys, vals)})
+    assert np.array_equal(_u32(vds.features()), _u32(Ev))
+    p = m.predict(Ev, "sigmoid")[:, 0].astype(np.float64)
+    p = np.clip(p, 1e-7, 1 - 1e-7)
+    ll = -np.mean(yv * np.log(p) + (1 - yv) * np.log(1 - p))
+    assert len(vl) == 15 and abs(vl[-1] - ll) <= 1e-5 * ll
+    for h in (m, tr, vds, ds):
+        h.close()
+
+
 def test_encode_rejects_bad_input(engine, capi):
     X, y = categorical_case(n=100, f=4, seed=1)
     ds = engine.upload(X, y)
