@@ -556,22 +556,29 @@ __global__ void k_cat_walk(const float* __restrict__ y, float* __restrict__ X, u
 // walk above serves every other label.
 
 // flags[0] |= 1 if some label is not an integer of magnitude <= 2^24;
-// sum[0] += sum |label| (as integers).
+// sum[0] += sum |label|, sum[1] += sum label (two's complement), as integers.
+// With exact labels the latter is the reference's float sum of the labels.
 __global__ void k_label_exact(const float* __restrict__ y, uint32_t n, unsigned long long* __restrict__ sum,
                               uint32_t* __restrict__ flags) {
-  unsigned long long s = 0;
+  unsigned long long s = 0, t = 0;
   uint32_t bad = 0;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const float v = fabsf(y[i]);
-    if (!(v <= 16777216.0f) || v != truncf(v)) bad = 1;  // NaN fails the first test
-    else s += (unsigned long long)v;
+    const float w = y[i], v = fabsf(w);
+    if (!(v <= 16777216.0f) || v != truncf(v)) {  // NaN fails the first test
+      bad = 1;
+    } else {
+      s += (unsigned long long)v;
+      t += (unsigned long long)(long long)w;
+    }
   }
   for (int o = 16; o; o >>= 1) {
     s += __shfl_xor_sync(0xffffffffu, s, o);
+    t += __shfl_xor_sync(0xffffffffu, t, o);
     bad |= __shfl_xor_sync(0xffffffffu, bad, o);
   }
   if ((threadIdx.x & 31) == 0) {
-    if (s) atomicAdd(sum, s);
+    if (s) atomicAdd(&sum[0], s);
+    if (t) atomicAdd(&sum[1], t);
     if (bad) atomicOr(flags, 1u);
   }
 }
@@ -997,7 +1004,7 @@ tc_status encode_categorical(tc_dataset* ds, const uint16_t* feats, uint16_t nc,
   TC_TRY(starts.alloc(ctx, (size_t)nc * n, "segment starts"));
   TC_TRY(segid.alloc(ctx, (size_t)nc * n, "segment of each position"));
   TC_TRY(prior.alloc(ctx, 1, "label prior"));
-  TC_TRY(lab_sum.alloc(ctx, 1, "label magnitude sum"));
+  TC_TRY(lab_sum.alloc(ctx, 2, "label sums"));
   TC_TRY(lab_flag.alloc(ctx, 1, "label flags"));
   TC_TRY(ds->cat_feats.alloc(ctx, nc, "categorical features"));
   TC_TRY(ds->cat_off.alloc(ctx, nc, "category table offsets"));
@@ -1016,8 +1023,7 @@ tc_status encode_categorical(tc_dataset* ds, const uint16_t* feats, uint16_t nc,
     o.given = given.p;
   }
   TC_CUDA(ctx, cudaMemcpyAsync(ds->cat_feats.p, feats, nc * sizeof(uint16_t), cudaMemcpyHostToDevice, st));
-  k_label_prior<<<1, 1024, 0, st>>>(ds->y.p, n, prior.p);
-  TC_CUDA(ctx, cudaMemsetAsync(lab_sum.p, 0, sizeof(unsigned long long), st));
+  TC_CUDA(ctx, cudaMemsetAsync(lab_sum.p, 0, lab_sum.bytes(), st));
   TC_CUDA(ctx, cudaMemsetAsync(lab_flag.p, 0, sizeof(uint32_t), st));
   k_label_exact<<<std::min<uint32_t>((n + 255) / 256, 4 * (uint32_t)ctx->sm_count), 256, 0, st>>>(ds->y.p, n, lab_sum.p,
                                                                                              lab_flag.p);
@@ -1036,15 +1042,21 @@ tc_status encode_categorical(tc_dataset* ds, const uint16_t* feats, uint16_t nc,
   k_seg_starts<<<dim3(n_tiles, nc), RS_THREADS, 0, st>>>(ks, n, n_tiles, tcnt.p, starts.p, segid.p);
   TC_CUDA(ctx, cudaGetLastError());
   std::vector<uint32_t> S(nc);
-  unsigned long long h_lab_sum = 0;
+  unsigned long long h_lab_sum[2] = {0, 0};
   uint32_t h_lab_flag = 1;
   TC_CUDA(ctx, cudaMemcpyAsync(S.data(), nseg.p, nc * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-  TC_CUDA(ctx, cudaMemcpyAsync(&h_lab_sum, lab_sum.p, sizeof(h_lab_sum), cudaMemcpyDeviceToHost, st));
+  TC_CUDA(ctx, cudaMemcpyAsync(h_lab_sum, lab_sum.p, sizeof(h_lab_sum), cudaMemcpyDeviceToHost, st));
   TC_CUDA(ctx, cudaMemcpyAsync(&h_lab_flag, lab_flag.p, sizeof(h_lab_flag), cudaMemcpyDeviceToHost, st));
   TC_CUDA(ctx, cudaStreamSynchronize(st));
   // integer labels whose magnitudes sum to at most 2^24: every float partial
   // sum is exact, so the sums need not be sequential
-  const bool exact = h_lab_flag == 0 && h_lab_sum <= (1ull << 24);
+  const bool exact = h_lab_flag == 0 && h_lab_sum[0] <= (1ull << 24);
+  // the prior, std::accumulate(labels, 0.0f) / n: with exact labels the float
+  // sum is the integer sum (converted exactly) and the division is done here
+  // in float; otherwise one device thread adds the labels in row order
+  const float h_prior = exact ? (float)(long long)h_lab_sum[1] / (float)n : 0.0f;
+  if (exact) TC_CUDA(ctx, cudaMemcpyAsync(prior.p, &h_prior, sizeof(float), cudaMemcpyHostToDevice, st));
+  else k_label_prior<<<1, 1024, 0, st>>>(ds->y.p, n, prior.p);
   ds->h_cat_off.assign(nc, 0);
   size_t total = 0;
   uint32_t smax = 0;
