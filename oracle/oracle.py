@@ -966,3 +966,154 @@ def ref_cat_ts(X, y, cats, method="ordered", hp: Hyper | None = None, fit=False)
         R.tcref_free(mb)
     tables = {int(cats[c]): (tk[c, :tl[c]].copy(), tv[c, :tl[c]].copy()) for c in range(nc)}
     return enc, Binned(bins, edges, ne), tables, model
+
+
+# ------------------------------------------------- regular (depth-wise) trees --
+# Tree::build / build_recursive_optimized (src/tree/tree.cpp:162-407),
+# SplitFinder::find_best_split(_feature) (src/tree/histogram.cpp:569-660),
+# Tree::make_leaf (src/tree/tree.cpp:655-683) and Booster::build_tree's
+# regular branch (src/boosting/booster.cpp:447-520), restated in FP64
+# arithmetic: the reference's histograms are FP32 sums, so this oracle agrees
+# with it wherever a node's top gain beats the runner-up by more than the
+# FP32 error (the margin each node records).
+
+
+def _regular_hist(bins, rows, g, h, max_bins, dt):
+    """The node's histogram as the reference builds it (CPUHistogramBuilder::
+    build, src/tree/histogram.cpp:62-176): per feature, the rows in order,
+    each added into its bin (FP32 adds in that order when dt is float32); one
+    row of max_bins slots per feature, a bin of max_bins or more (NaN: 255)
+    landing in the following feature's slots, as the reference's flat array
+    does."""
+    f = bins.shape[0]
+    idx = (np.arange(f)[:, None] * max_bins + bins[:, rows].astype(np.int64)).ravel()
+    size = f * max_bins + 256
+    G = np.zeros(size, dt)
+    H = np.zeros(size, dt)
+    np.add.at(G, idx, np.tile(np.asarray(g, dt)[rows], f))  # unbuffered: in index order
+    np.add.at(H, idx, np.tile(np.asarray(h, dt)[rows], f))
+    N = np.bincount(idx, None, size).astype(np.int64)
+    k = f * max_bins
+    return G[:k].reshape(f, max_bins), H[:k].reshape(f, max_bins), N[:k].reshape(f, max_bins)
+
+
+def build_regular_tree(b: Binned, g, h, hp: Hyper, rows=None, fp32=True):
+    """One regular tree from the given gradients.  fp32: the reference's
+    arithmetic (FP32 histograms in row order, the larger child's histogram as
+    parent - smaller, FP32 prefix sums and gains); else FP64.  Returns the
+    node arrays in the reference's numbering (children added in pairs, the
+    smaller child's subtree built first) with each split node's margin (top
+    gain - best gain of another partition) / |top gain| and each row's leaf."""
+    dt = np.float32 if fp32 else np.float64
+    bins = b.bins
+    n = bins.shape[1]
+    rows = np.arange(n) if rows is None else np.asarray(rows)
+    lam = dt(hp.lambda_l2)
+    half = dt(0.5)
+    gamma = dt(0.0)
+    msg = dt(hp.min_split_gain)
+    mcw = dt(hp.min_child_weight)
+    nb = int(hp.max_bins)
+    max_leaves = 64  # TreeConfig::max_leaves (include/turbocat/config.hpp:29)
+    keys = (("feature", 0), ("split_bin", 0), ("is_leaf", True), ("default_left", True), ("left", 0),
+            ("right", 0), ("value", 0.0), ("gain", 0.0), ("margin", np.inf))
+    nodes = {k: [v] for k, v in keys}
+    leaf_of = np.zeros(n, np.int64)
+    state = {"n_leaves": 0}
+
+    def add_node():
+        for k, v in keys:
+            nodes[k].append(v)
+        return len(nodes["value"]) - 1
+
+    def make_leaf(i, st, r):
+        v = dt(-st[0]) / dt(st[1] + lam)
+        if hp.max_delta_step > 0:
+            v = max(dt(-hp.max_delta_step), min(dt(hp.max_delta_step), v))
+        nodes["is_leaf"][i] = True
+        nodes["value"][i] = v
+        leaf_of[r] = i
+        state["n_leaves"] += 1
+
+    def rec(i, r, st, hist, depth):
+        G, H, C = st
+        if (depth >= hp.max_depth or state["n_leaves"] >= max_leaves or len(r) < 2 * hp.min_samples_leaf
+                or H < dt(2) * mcw):
+            make_leaf(i, st, r)
+            return
+        HG, HH, HN = hist
+        GL = np.cumsum(HG[:, : nb - 1], 1, dtype=dt)
+        HL = np.cumsum(HH[:, : nb - 1], 1, dtype=dt)
+        NL = np.cumsum(HN[:, : nb - 1], 1)
+        GR, HR, NR = (G - GL).astype(dt), (H - HL).astype(dt), C - NL
+        ok = (NL >= hp.min_samples_leaf) & (HL >= mcw) & (NR >= hp.min_samples_leaf) & (HR >= mcw)
+        with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
+            pg = dt(G * G) / dt(H + lam)
+            gain = (half * (((GL * GL) / (HL + lam) + (GR * GR) / (HR + lam)) - pg) - gamma).astype(dt)
+        gain = np.where(ok & (gain >= msg), gain, -np.inf)
+        flat = gain.ravel()
+        k = int(np.argmax(flat))  # first maximum in (feature, bin) order
+        if not np.isfinite(flat[k]) or flat[k] <= -1e30:
+            make_leaf(i, st, r)
+            return
+        top = flat[k]
+        other = flat[flat != top]
+        second = other.max() if other.size else -np.inf
+        fi, bi = divmod(k, nb - 1)
+        nodes["feature"][i], nodes["split_bin"][i] = fi, bi
+        nodes["is_leaf"][i] = False
+        nodes["gain"][i] = top
+        nodes["margin"][i] = float((top - second) / abs(top)) if np.isfinite(second) and top != 0 else np.inf
+        col = bins[fi, r]
+        go_left = np.where(col == 255, True, col <= bi)  # NaN: default_left (1 while partitioning)
+        rl, rr = r[go_left], r[~go_left]
+        if len(rl) != len(r) and len(rr) != len(r):
+            nodes["default_left"][i] = len(rl) >= len(rr)
+        li = add_node()
+        ri = add_node()
+        nodes["left"][i], nodes["right"][i] = li, ri
+        sl = (GL[fi, bi], HL[fi, bi], NL[fi, bi])
+        sr = (GR[fi, bi], HR[fi, bi], NR[fi, bi])
+        small_left = len(rl) <= len(rr)
+        hs = _regular_hist(bins, rl if small_left else rr, g, h, nb, dt)
+        hb = tuple((p - q).astype(p.dtype) for p, q in zip(hist, hs))  # larger = parent - smaller
+        if small_left:
+            rec(li, rl, sl, hs, depth + 1)
+            rec(ri, rr, sr, hb, depth + 1)
+        else:
+            rec(ri, rr, sr, hs, depth + 1)
+            rec(li, rl, sl, hb, depth + 1)
+
+    g_r = np.asarray(g, dt)[rows]
+    h_r = np.asarray(h, dt)[rows]
+    root = (np.add.accumulate(g_r, dtype=dt)[-1], np.add.accumulate(h_r, dtype=dt)[-1], len(rows))
+    rec(0, rows, root, _regular_hist(bins, rows, g, h, nb, dt), 0)
+    out = {k: np.array(v) for k, v in nodes.items()}
+    out["value"] = out["value"].astype(np.float32)
+    out["leaf_of"] = leaf_of
+    return out
+
+
+def fit_regular(b: Binned, y, hp: Hyper, grads=None, fp32=True):
+    """Booster::train with regular trees (binary logloss / MSE, all rows, no
+    sampling): base prediction, then per iteration the gradients of the FP32
+    predictions, one tree, predictions += lr * leaf (one FP32 rounding).  With `grads`
+    ((g, h) per iteration, e.g. the reference's own) the trees are built from
+    those instead (teacher forcing).  Returns (trees, FP32 train predictions)."""
+    y = np.asarray(y, np.float32)
+    base = init_prediction(hp.loss, y)
+    pred = np.full(len(y), base, np.float32)
+    lr = np.float32(hp.learning_rate)
+    trees = []
+    for it in range(hp.n_estimators):
+        if grads is None:
+            g, h = gradients(hp.loss, y, pred)
+        else:
+            g, h = grads[0][it], grads[1][it]
+        t = build_regular_tree(b, g, h, hp, fp32=fp32)
+        trees.append(t)
+        leaf = t["value"].astype(np.float32)[t["leaf_of"]]
+        # predictions += lr * leaf, a fused multiply-add in the reference's build:
+        # the product is exact in 80-bit precision, one rounding to float32
+        pred = (pred.astype(np.longdouble) + np.longdouble(lr) * leaf.astype(np.longdouble)).astype(np.float32)
+    return trees, pred, base

@@ -157,3 +157,13 @@ def categorical_case(n=3000, f=6, n_classes=2, seed=5, n_cat=1, cardinality=25, 
 
 
 CAT_HYPER = dict(loss="logloss", n_estimators=20, max_depth=4, learning_rate=0.2)
+
+
+def regular_train_case():
+    """Data of the regular-tree training fixture: the binary generator, no NaN
+    (the reference's NaN rows spill into the next feature's histogram from
+    parallel threads, which makes its own runs differ)."""
+    return binary_c1(4000, 10, seed=43)
+
+
+REGULAR_TRAIN_HYPER = dict(loss="logloss", n_estimators=12, max_depth=7, learning_rate=0.2, regular_trees=True)

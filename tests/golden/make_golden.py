@@ -66,8 +66,21 @@ def categorical_golden():
     np.savez_compressed(os.path.join(HERE, "categorical_small.npz"), **out)
 
 
+def regular_train_golden():
+    """Regular (depth-wise) trees the reference trains, for the training
+    oracle: depth 7, so that the 64-leaf cap binds in the recursion's order."""
+    from datagen import REGULAR_TRAIN_HYPER, regular_train_case
+
+    X, y = regular_train_case()
+    hp = O.Hyper(**REGULAR_TRAIN_HYPER)
+    _, model, _, _, tp = O.ref_fit(X, y, hp)
+    np.savez_compressed(os.path.join(HERE, "regular_train_small.npz"), tcat=np.frombuffer(model, np.uint8),
+                        train_raw=tp)
+
+
 def main():
     regular_golden()
+    regular_train_golden()
     categorical_golden()
     for name, spec in GOLDEN_CASES.items():
         X, y, hp = make_case(spec)
@@ -89,5 +102,7 @@ def main():
 if __name__ == "__main__":
     if sys.argv[1:] == ["categorical"]:
         categorical_golden()
+    elif sys.argv[1:] == ["regular_train"]:
+        regular_train_golden()
     else:
         main()
