@@ -273,6 +273,17 @@ void tc_trainer_destroy(tc_trainer* tr);
  * Booster::train (src/boosting/booster.cpp:47). */
 tc_status tc_train(tc_ctx* ctx, tc_dataset* ds, const tc_train_params* p, tc_model** out,
                    tc_train_stats* st);
+/* One-shot fit of regular (depth-wise) trees, the reference's mode="small"
+ * (Booster::train with use_symmetric = false, src/boosting/booster.cpp:447-520;
+ * Tree::build, src/tree/tree.cpp:162-407): per node the best (feature, bin)
+ * of SplitFinder (src/tree/histogram.cpp:569-690), the reference's stop rules
+ * including its 64-leaf cap in its recursion order (smaller child first), leaf
+ * -G/(H + lambda_l2).  Binary logloss, every row in every tree (subsample 1,
+ * no GOSS).  The model is a TCAT v3 regular-tree model in the reference's node
+ * numbering (tc_model_save_tcat writes it; tc_predict serves it as the
+ * reference predicts such models). */
+tc_status tc_train_regular(tc_ctx* ctx, tc_dataset* ds, const tc_train_params* p, tc_model** out,
+                           tc_train_stats* st);
 
 /* One symmetric tree on caller-given gradients/hessians [n] over all rows of
  * a quantized dataset.  Replaces SymmetricTree::build

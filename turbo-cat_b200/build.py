@@ -28,7 +28,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
                      f"-I{INCLUDE}", f"-I{CSRC}", "--expt-relaxed-constexpr", "-Xptxas", "-v"]
 
-CU_SOURCES = ["tc_context.cu", "tc_data.cu", "tc_train.cu", "tc_predict.cu", "tc_server.cu", "tc_noalloc.cu"]
+CU_SOURCES = ["tc_context.cu", "tc_data.cu", "tc_train.cu", "tc_predict.cu", "tc_server.cu", "tc_noalloc.cu",
+              "tc_regular.cu"]
 HOST_SOURCES = ["bindings.cpp"]
 
 LIB = os.path.join(PKG, "libtcgpu.so")
@@ -54,7 +55,7 @@ def _run(cmd, log):
 
 def build(force: bool = False) -> None:
     os.makedirs(OBJ, exist_ok=True)
-    headers = [os.path.join(INCLUDE, "tcgpu.h"), os.path.join(CSRC, "tc_internal.h")]
+    headers = [os.path.join(INCLUDE, "tcgpu.h"), os.path.join(CSRC, "tc_internal.h"), os.path.join(CSRC, "tc_loss.cuh")]
     jobs = []
     objs = []
     for src in CU_SOURCES:

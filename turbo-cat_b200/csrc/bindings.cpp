@@ -92,7 +92,7 @@ class GpuBooster {
 
   void fit(const float* X, uint32_t n, uint16_t f, const float* y, const tc_train_params& p,
            const float* Xv = nullptr, const float* yv = nullptr, uint32_t nv = 0, int es_rounds = 50,
-           const CatSpec* cats = nullptr) {
+           const CatSpec* cats = nullptr, bool regular = false) {
     tc_ctx* ctx = device_context();
     tc_dataset* ds = nullptr;
     tc_dataset* vds = nullptr;
@@ -103,7 +103,7 @@ class GpuBooster {
                                         nullptr);
     if (s == TC_OK) s = tc_quantize(ds, (uint16_t)p.max_bins, 1, nullptr, nullptr);
     tc_model* m = nullptr;
-    if (s == TC_OK && nv == 0) s = tc_train(ctx, ds, &p, &m, &stats);
+    if (s == TC_OK && nv == 0) s = regular ? tc_train_regular(ctx, ds, &p, &m, &stats) : tc_train(ctx, ds, &p, &m, &stats);
     if (s == TC_OK && nv > 0) {
       tc_trainer* tr = nullptr;
       s = tc_dataset_upload(ctx, Xv, nv, f, yv, &vds);
@@ -338,7 +338,6 @@ class TurboCatClassifier {
     const uint32_t n = (uint32_t)X.shape(0);
     const uint16_t f = (uint16_t)X.shape(1);
     if ((size_t)y.shape(0) != n) throw std::runtime_error("X and y have different numbers of rows");
-    if (mode_ == "small") warn("mode='small' (regular trees) is not on the device path; building symmetric trees");
     if (colsample_ < 1.0f && verbosity_ > 1) warn("colsample_bytree has no effect on symmetric trees");
     if (use_gradtree_ || use_ordered_ || auto_interactions_)
       warn("use_gradtree / use_ordered_boosting / auto_interactions are not on the device path and are ignored");
@@ -369,6 +368,17 @@ class TurboCatClassifier {
       p.loss = TC_LOSS_SOFTMAX;
       p.n_classes = (int)n_classes_;
     }
+    // mode="small": regular (depth-wise) trees where the device builds them --
+    // binary logloss on every row without a validation set or categorical
+    // columns (tc_train_regular); otherwise symmetric trees
+    bool regular = false;
+    if (mode_ == "small") {
+      regular = n_classes_ <= 2 && p.loss == TC_LOSS_LOGLOSS && p.subsample >= 1.0f && !p.use_goss && !has_val &&
+                cats.features.empty();
+      if (!regular)
+        warn("mode='small' (regular trees) is on the device path for binary logloss with subsample=1.0, no GOSS, "
+             "no validation set and no cat_features; building symmetric trees");
+    }
     {
       py::gil_scoped_release nogil;
       booster_.reset(new GpuBooster());
@@ -376,7 +386,7 @@ class TurboCatClassifier {
         booster_->fit(X.data(), n, f, yp, p, X_val.data(), y_val.data(), (uint32_t)X_val.shape(0), es_rounds_,
                       &cats);
       else
-        booster_->fit(X.data(), n, f, yp, p, nullptr, nullptr, 0, 50, &cats);
+        booster_->fit(X.data(), n, f, yp, p, nullptr, nullptr, 0, 50, &cats, regular);
     }
     n_features_ = f;
     is_fitted_ = true;

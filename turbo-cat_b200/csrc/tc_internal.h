@@ -210,6 +210,9 @@ void stop_latency_worker(tc_ctx* ctx, const tc_model* m);
 tc_status quantize(tc_dataset* ds, int max_bins, int compat_u8);
 tc_status encode_categorical(tc_dataset* ds, const uint16_t* feats, uint16_t nc, const tc_cat_params* p,
                              const uint32_t* order);
+// Regular (depth-wise) trees (tc_regular.cu).
+tc_status train_regular(tc_ctx* ctx, tc_dataset* ds, const tc_train_params* p, tc_model** out,
+                        tc_train_stats* stats);
 
 // Prediction (tc_predict.cu): raw scores [n][K] (+ transform) on device buffers.
 tc_status predict_device(tc_ctx* ctx, const tc_model* m, const float* X, uint32_t n, uint32_t f,

@@ -29,7 +29,7 @@ SYMBOLS = [
     "tc_apply_bins", "tc_dataset_bins", "tc_dataset_features", "tc_encode_categorical", "tc_category_table",
     "tc_trainer_create", "tc_trainer_step", "tc_trainer_reset", "tc_trainer_stats", "tc_trainer_profile",
     "tc_trainer_train_scores", "tc_trainer_sample_mask", "tc_trainer_set_validation", "tc_trainer_valid_loss",
-    "tc_trainer_model", "tc_trainer_destroy", "tc_train", "tc_build_tree", "tc_histogram_root_noalloc",
+    "tc_trainer_model", "tc_trainer_destroy", "tc_train", "tc_train_regular", "tc_build_tree", "tc_histogram_root_noalloc",
     "tc_model_info_get", "tc_model_export",
     "tc_model_import", "tc_model_save_tcat", "tc_model_load_tcat", "tc_model_destroy", "tc_predict",
     "tc_predict_device", "tc_predict_dataset", "tc_server_create", "tc_server_add_model", "tc_server_submit", "tc_server_poll",
@@ -330,6 +330,13 @@ class Engine:
         h = C.c_void_p()
         st = TrainStats()
         self._chk(lib().tc_train(self.ctx, ds.h, C.byref(p), C.byref(h), C.byref(st)))
+        return Model(self, h), st
+
+    def train_regular(self, ds: Dataset, p: TrainParams):
+        """tc_train_regular: regular (depth-wise) trees, the reference's mode="small"."""
+        h = C.c_void_p()
+        st = TrainStats()
+        self._chk(lib().tc_train_regular(self.ctx, ds.h, C.byref(p), C.byref(h), C.byref(st)))
         return Model(self, h), st
 
     def build_tree(self, ds: Dataset, g, h, p: TrainParams, want_hist=False):
