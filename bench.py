@@ -471,6 +471,40 @@ def suite_c1(eng, _capi, ref_ok):
     return out
 
 
+def suite_regular(eng, _capi, ref_ok):
+    """Regular (depth-wise) trees, the reference's mode="small": binary
+    50k x 20, logloss, depth 6, 100 trees, every row.  Device: tc_train_regular
+    (one-shot, wall time of the call); reference: its own Booster::train with
+    regular trees on the same data (timed trees through its callback)."""
+    from datagen import binary_c1
+
+    X, y = binary_c1()
+    ds = eng.upload(X, y)
+    ds.quantize(255)
+    prm = _capi.params(loss="logloss", n_estimators=100, max_depth=6, learning_rate=0.1)
+    eng.train_regular(ds, _capi.params(loss="logloss", n_estimators=2, max_depth=6))[0].close()  # warm-up
+    best = None
+    for _ in range(3):
+        t0 = time.perf_counter()
+        m, st = eng.train_regular(ds, prm)
+        dt = time.perf_counter() - t0
+        m.close()
+        best = dt if best is None else min(best, dt)
+    out = {"config": "regular trees, binary 50k x 20, logloss, depth 6, 100 trees", "device_s_per_100_trees": best,
+           "kernel_launches_per_fit": st.kernel_launches}
+    if ref_ok:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+
+        hp = O.Hyper(loss="logloss", n_estimators=100, max_depth=6, learning_rate=0.1, regular_trees=True)
+        setup, ends = O.ref_fit_timed(X, y, hp, 100, 60.0)
+        out["reference_cpu_s_per_100_trees"] = (ends[-1] - ends[0]) * 100.0 / max(1, len(ends) - 1) if len(ends) > 1 else None
+        out["reference_trees_timed"] = len(ends)
+        out["reference_threads"] = os.cpu_count()
+    ds.close()
+    return out
+
+
 def suite_cat(eng, _capi, ref_ok):
     return {"cardinality_1000": _cat_case(eng, ref_ok, cardinality=1000),
             "cardinality_8": _cat_case(eng, ref_ok, cardinality=8)}
@@ -746,6 +780,8 @@ def run_suite(args):
             r = suite_goss(eng, _capi)
         elif name == "cat":
             r = suite_cat(eng, _capi, ref_ok)
+        elif name == "regular":
+            r = suite_regular(eng, _capi, ref_ok)
         elif name == "c4dev":  # the four serving models' device-resident prediction only
             r = {"config": "serving models (1000xd6, 200xd4, 500xd8, 2000xd10) on 100 features, 1M resident rows",
                  "device_predict_1M_rows": _device_predict(_train_serving_models(eng, _capi), 100)}
@@ -767,7 +803,7 @@ def main():
     ap.add_argument("--no-c2", action="store_true", help="leave out the secondary regression configuration")
     ap.add_argument("--reference-seconds", type=float, default=240.0,
                     help="reference arm: stop building trees once this many seconds have passed")
-    ap.add_argument("--suite", default="", help="secondary configurations, e.g. c1,c2,c3,c4,goss,cat")
+    ap.add_argument("--suite", default="", help="secondary configurations, e.g. c1,c2,c3,c4,goss,cat,regular")
     ap.add_argument("--rows", type=int, default=0,
                     help="rows of the workload (default: the configuration's 10M); a smaller case of the same "
                          "workload for profiler captures")
