@@ -19,7 +19,8 @@
  *              per tree: depth, (feature, bin, float threshold, gain) per
  *              level padded to max_depth, 2^max_depth leaf values (padded)
  *
- * Threads: dataset and training calls (tc_dataset_*, tc_quantize, tc_train,
+ * Threads: dataset and training calls (tc_dataset_*, tc_quantize,
+ * tc_apply_bins, tc_encode_categorical, tc_train, tc_train_regular,
  * tc_build_tree, tc_trainer_*) on one context run one at a time; tc_predict
  * calls on one context run one at a time, on a stream of their own, so they
  * may run while another thread trains; tc_server_submit/poll may be called
