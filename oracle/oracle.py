@@ -1117,3 +1117,78 @@ def fit_regular(b: Binned, y, hp: Hyper, grads=None, fp32=True):
         # the product is exact in 80-bit precision, one rounding to float32
         pred = (pred.astype(np.longdouble) + np.longdouble(lr) * leaf.astype(np.longdouble)).astype(np.float32)
     return trees, pred, base
+
+
+def build_regular_tree_levelwise(b: Binned, g, h, hp: Hyper):
+    """The device's way to the same tree (FP64): grow every node level by
+    level (stop rules other than the leaf cap decided when a child is made),
+    then replay the reference's recursion -- smaller child first, a node
+    visited with 64 leaves made becomes a leaf -- to apply the cap and number
+    the nodes.  Equal to build_regular_tree(fp32=False) by construction of
+    the replay; checked by the tests."""
+    bins = b.bins
+    n = bins.shape[1]
+    g = np.asarray(g, np.float64)
+    h = np.asarray(h, np.float64)
+    lam, mcw, msl, nb = float(hp.lambda_l2), float(hp.min_child_weight), int(hp.min_samples_leaf), int(hp.max_bins)
+    grown = [dict(depth=0, split=False)]
+    slot = np.zeros(n, np.int64)
+    open_ids, d = [0], 0
+    while open_ids:
+        nxt, feat, thr, ls, rs = [], [], [], [], []
+        for a, gi in enumerate(open_ids):
+            rows = np.nonzero(slot == a)[0]
+            HG, HH, HN = _regular_hist(bins, rows, g, h, nb, np.float64)
+            G, H, C = g[rows].sum(), h[rows].sum(), len(rows)
+            GL, HL, CL = (np.cumsum(x[:, : nb - 1], 1) for x in (HG, HH, HN))
+            GR, HR, CR = G - GL, H - HL, C - CL
+            ok = (CL >= msl) & (CR >= msl) & (HL >= mcw) & (HR >= mcw)
+            gain = 0.5 * ((GL * GL / (HL + lam) + GR * GR / (HR + lam)) - G * G / (H + lam))
+            gain = np.where(ok & (gain >= hp.min_split_gain), gain, -np.inf).ravel()
+            k = int(np.argmax(gain))
+            nd = grown[gi]
+            if d == 0:
+                nd.update(G=G, H=H, C=C)
+            feat.append(-1), thr.append(0), ls.append(-1), rs.append(-1)
+            if (d == 0 and (C < 2 * msl or H < 2 * mcw)) or not np.isfinite(gain[k]):
+                continue
+            fi, bi = divmod(k, nb - 1)
+            nd.update(split=True, feature=fi, bin=bi)
+            feat[a], thr[a] = fi, bi
+            for side, (cg, ch, cc) in enumerate(((GL[fi, bi], HL[fi, bi], CL[fi, bi]),
+                                                 (GR[fi, bi], HR[fi, bi], CR[fi, bi]))):
+                c = dict(depth=d + 1, split=False, G=cg, H=ch, C=cc)
+                nd["right" if side else "left"] = len(grown)
+                if not (c["depth"] >= hp.max_depth or cc < 2 * msl or ch < 2 * mcw):
+                    (rs if side else ls)[a] = len(nxt)
+                    nxt.append(len(grown))
+                grown.append(c)
+        new = np.full(n, -1, np.int64)
+        for a in range(len(open_ids)):
+            if feat[a] < 0:
+                continue
+            rows = np.nonzero(slot == a)[0]
+            col = bins[feat[a], rows]
+            right = (col != 255) & (col > thr[a])
+            new[rows[right]] = rs[a]
+            new[rows[~right]] = ls[a]
+        slot, open_ids, d = new, nxt, d + 1
+    out = dict(feature=[0], split_bin=[0], is_leaf=[True], left=[0], right=[0], value=[0.0])
+    n_leaves, stack = 0, [(0, 0)]
+    while stack:
+        gi, fi = stack.pop()
+        nd = grown[gi]
+        if not nd["split"] or n_leaves >= 64:
+            out["value"][fi] = np.float32(-nd["G"] / (nd["H"] + lam))
+            n_leaves += 1
+            continue
+        li = len(out["value"])
+        for k, v in (("feature", 0), ("split_bin", 0), ("is_leaf", True), ("left", 0), ("right", 0), ("value", 0.0)):
+            out[k] += [v, v]
+        out["feature"][fi], out["split_bin"][fi], out["is_leaf"][fi] = nd["feature"], nd["bin"], False
+        out["left"][fi], out["right"][fi] = li, li + 1
+        small_left = grown[nd["left"]]["C"] <= grown[nd["right"]]["C"]
+        first, second = ((nd["left"], li), (nd["right"], li + 1)) if small_left else ((nd["right"], li + 1),
+                                                                                       (nd["left"], li))
+        stack += [second, first]
+    return {k: np.array(v) for k, v in out.items()}

@@ -57,3 +57,26 @@ def test_regular_training_oracle_matches_live_reference(n, f, depth, msl, mcw, l
     trees, _, _ = O.fit_regular(b, y, hp)
     for t, r in zip(trees, m.trees):
         assert _same_tree(t, r)
+
+
+@pytest.mark.parametrize("n,f,depth,msl,mcw,lam", [(3000, 10, 5, 1, 1.0, 1.0), (4000, 10, 7, 1, 1.0, 1.0),
+                                                     (5000, 8, 6, 20, 5.0, 3.0)])
+def test_level_wise_growth_with_replay_is_the_recursion(n, f, depth, msl, mcw, lam):
+    """The device grows a tree level by level and replays the reference's
+    recursion afterwards (the leaf cap, the numbering); in FP64 that gives
+    the recursion's tree exactly, the 64-leaf cap included (depth 7)."""
+    X, y = binary_c1(n, f, seed=n + depth)
+    hp = O.Hyper(loss="logloss", max_depth=depth, min_samples_leaf=msl, min_child_weight=mcw, lambda_l2=lam)
+    b = O.quantize(X)
+    p = np.full(n, O.init_prediction("logloss", y), np.float32)
+    for _ in range(3):
+        g, h = O.gradients("logloss", y, p)
+        t = O.build_regular_tree(b, g, h, hp, fp32=False)
+        lw = O.build_regular_tree_levelwise(b, g, h, hp)
+        for k in ("is_leaf", "left", "right"):
+            assert np.array_equal(t[k], lw[k])
+        assert np.array_equal(t["feature"][~t["is_leaf"]], lw["feature"][~lw["is_leaf"]])
+        assert np.array_equal(t["split_bin"][~t["is_leaf"]], lw["split_bin"][~lw["is_leaf"]])
+        assert np.array_equal(t["value"].view(np.uint32), lw["value"].astype(np.float32).view(np.uint32))
+        leaf = t["value"][t["leaf_of"]].astype(np.longdouble)
+        p = (p.astype(np.longdouble) + np.longdouble(np.float32(0.2)) * leaf).astype(np.float32)
