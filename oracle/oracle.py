@@ -997,6 +997,37 @@ def _regular_hist(bins, rows, g, h, max_bins, dt):
     return G[:k].reshape(f, max_bins), H[:k].reshape(f, max_bins), N[:k].reshape(f, max_bins)
 
 
+def _regular_scan(hist, st, hp: Hyper, dt):
+    """SplitFinder::find_best_split over a node's histogram (src/tree/histogram.cpp:569-660):
+    left = prefix over bins 0 .. max_bins-2, right = node stats - left, both
+    meeting min_samples_leaf and min_child_weight, gain 0.5 (GL^2/(HL+l) +
+    GR^2/(HR+l) - G^2/(H+l)), first maximum in (feature, bin) order.  Returns
+    (gain, runner-up gain of another partition, feature, bin, left stats,
+    right stats) or None."""
+    G, H, C = st
+    lam, half, gamma = dt(hp.lambda_l2), dt(0.5), dt(0.0)
+    msg, mcw, nb = dt(hp.min_split_gain), dt(hp.min_child_weight), int(hp.max_bins)
+    HG, HH, HN = hist
+    GL = np.cumsum(HG[:, : nb - 1], 1, dtype=dt)
+    HL = np.cumsum(HH[:, : nb - 1], 1, dtype=dt)
+    NL = np.cumsum(HN[:, : nb - 1], 1)
+    GR, HR, NR = (G - GL).astype(dt), (H - HL).astype(dt), C - NL
+    ok = (NL >= hp.min_samples_leaf) & (HL >= mcw) & (NR >= hp.min_samples_leaf) & (HR >= mcw)
+    with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
+        pg = dt(G * G) / dt(H + lam)
+        gain = (half * (((GL * GL) / (HL + lam) + (GR * GR) / (HR + lam)) - pg) - gamma).astype(dt)
+    gain = np.where(ok & (gain >= msg), gain, -np.inf)
+    flat = gain.ravel()
+    k = int(np.argmax(flat))  # first maximum in (feature, bin) order
+    if not np.isfinite(flat[k]) or flat[k] <= -1e30:
+        return None
+    top = flat[k]
+    other = flat[flat != top]
+    second = other.max() if other.size else -np.inf
+    fi, bi = divmod(k, nb - 1)
+    return top, second, fi, bi, (GL[fi, bi], HL[fi, bi], NL[fi, bi]), (GR[fi, bi], HR[fi, bi], NR[fi, bi])
+
+
 def build_regular_tree(b: Binned, g, h, hp: Hyper, rows=None, fp32=True):
     """One regular tree from the given gradients.  fp32: the reference's
     arithmetic (FP32 histograms in row order, the larger child's histogram as
@@ -1041,25 +1072,11 @@ def build_regular_tree(b: Binned, g, h, hp: Hyper, rows=None, fp32=True):
                 or H < dt(2) * mcw):
             make_leaf(i, st, r)
             return
-        HG, HH, HN = hist
-        GL = np.cumsum(HG[:, : nb - 1], 1, dtype=dt)
-        HL = np.cumsum(HH[:, : nb - 1], 1, dtype=dt)
-        NL = np.cumsum(HN[:, : nb - 1], 1)
-        GR, HR, NR = (G - GL).astype(dt), (H - HL).astype(dt), C - NL
-        ok = (NL >= hp.min_samples_leaf) & (HL >= mcw) & (NR >= hp.min_samples_leaf) & (HR >= mcw)
-        with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
-            pg = dt(G * G) / dt(H + lam)
-            gain = (half * (((GL * GL) / (HL + lam) + (GR * GR) / (HR + lam)) - pg) - gamma).astype(dt)
-        gain = np.where(ok & (gain >= msg), gain, -np.inf)
-        flat = gain.ravel()
-        k = int(np.argmax(flat))  # first maximum in (feature, bin) order
-        if not np.isfinite(flat[k]) or flat[k] <= -1e30:
+        sp = _regular_scan(hist, st, hp, dt)
+        if sp is None:
             make_leaf(i, st, r)
             return
-        top = flat[k]
-        other = flat[flat != top]
-        second = other.max() if other.size else -np.inf
-        fi, bi = divmod(k, nb - 1)
+        top, second, fi, bi, sl, sr = sp
         nodes["feature"][i], nodes["split_bin"][i] = fi, bi
         nodes["is_leaf"][i] = False
         nodes["gain"][i] = top
@@ -1072,8 +1089,6 @@ def build_regular_tree(b: Binned, g, h, hp: Hyper, rows=None, fp32=True):
         li = add_node()
         ri = add_node()
         nodes["left"][i], nodes["right"][i] = li, ri
-        sl = (GL[fi, bi], HL[fi, bi], NL[fi, bi])
-        sr = (GR[fi, bi], HR[fi, bi], NR[fi, bi])
         small_left = len(rl) <= len(rr)
         hs = _regular_hist(bins, rl if small_left else rr, g, h, nb, dt)
         hb = tuple((p - q).astype(p.dtype) for p, q in zip(hist, hs))  # larger = parent - smaller
@@ -1192,3 +1207,129 @@ def build_regular_tree_levelwise(b: Binned, g, h, hp: Hyper):
                                                                                        (nd["left"], li))
         stack += [second, first]
     return {k: np.array(v) for k, v in out.items()}
+
+
+def build_leafwise_tree(b: Binned, g, h, hp: Hyper, fp32=True, max_leaves=64):
+    """Tree::build_leafwise (src/tree/tree.cpp:685-907), the growth of the
+    reference's regression preset (GrowPolicy::Lossguide,
+    include/turbocat/config.hpp:266-274): the open leaf of the highest gain
+    splits next (a max-heap of candidates; equal gains from different nodes
+    do not occur in practice and are taken in insertion order here) until
+    max_leaves leaves exist; a child is scored only when it can split
+    (2 min_samples_leaf rows, 2 min_child_weight hessian) and one more leaf
+    fits; the smaller child's histogram is built and the larger's is parent -
+    smaller (built directly when the smaller cannot split).  fp32: the
+    reference's arithmetic; else FP64.  Node arrays as build_regular_tree."""
+    dt = np.float32 if fp32 else np.float64
+    bins = b.bins
+    n = bins.shape[1]
+    nb = int(hp.max_bins)
+    lam = dt(hp.lambda_l2)
+    mcw2 = dt(2) * dt(hp.min_child_weight)
+    msl2 = 2 * hp.min_samples_leaf
+    keys = (("feature", 0), ("split_bin", 0), ("is_leaf", True), ("default_left", True), ("left", 0),
+            ("right", 0), ("value", 0.0), ("gain", 0.0), ("margin", np.inf))
+    nodes = {k: [v] for k, v in keys}
+    leaf_of = np.zeros(n, np.int64)
+    state = {"n_leaves": 0, "depth": 0, "seq": 0}
+
+    def add_node():
+        for k, v in keys:
+            nodes[k].append(v)
+        return len(nodes["value"]) - 1
+
+    def make_leaf(i, st, r):
+        v = dt(-st[0]) / dt(st[1] + lam)
+        if hp.max_delta_step > 0:
+            v = max(dt(-hp.max_delta_step), min(dt(hp.max_delta_step), v))
+        nodes["is_leaf"][i] = True
+        nodes["value"][i] = v
+        leaf_of[r] = i
+        state["n_leaves"] += 1
+
+    rows = np.arange(n)
+    root = (np.add.accumulate(np.asarray(g, dt), dtype=dt)[-1], np.add.accumulate(np.asarray(h, dt), dtype=dt)[-1], n)
+    root_hist = _regular_hist(bins, rows, g, h, nb, dt)
+    sp = _regular_scan(root_hist, root, hp, dt)
+    if sp is None:
+        make_leaf(0, root, rows)
+        out = {k: np.array(v) for k, v in nodes.items()}
+        out["value"] = out["value"].astype(np.float32)
+        out["leaf_of"], out["depth"] = leaf_of, 0
+        return out
+    cands = [dict(node=0, split=sp, rows=rows, depth=0, stats=root, hist=root_hist, seq=0)]
+
+    def pop_best():
+        k = max(range(len(cands)), key=lambda j: (cands[j]["split"][0], -cands[j]["seq"]))
+        return cands.pop(k)
+
+    while cands and state["n_leaves"] < max_leaves:
+        c = pop_best()
+        i, (top, second, fi, bi, sl, sr), r, depth = c["node"], c["split"], c["rows"], c["depth"]
+        if depth >= hp.max_depth:
+            make_leaf(i, c["stats"], r)
+            continue
+        nodes["feature"][i], nodes["split_bin"][i] = fi, bi
+        nodes["is_leaf"][i] = False
+        nodes["gain"][i] = top
+        nodes["margin"][i] = float((top - second) / abs(top)) if np.isfinite(second) and top != 0 else np.inf
+        col = bins[fi, r]
+        go_left = np.where(col == 255, True, col <= bi)
+        rl, rr = r[go_left], r[~go_left]
+        if len(rl) != len(r) and len(rr) != len(r):
+            nodes["default_left"][i] = len(rl) >= len(rr)
+        li = add_node()
+        ri = add_node()
+        nodes["left"][i], nodes["right"][i] = li, ri
+        state["depth"] = max(state["depth"], depth + 1)
+        left_small = len(rl) <= len(rr)
+        lcan = len(rl) >= msl2 and sl[1] >= mcw2
+        rcan = len(rr) >= msl2 and sr[1] >= mcw2
+        hl = hr = None
+        if lcan or rcan:
+            if left_small:
+                if lcan:
+                    hl = _regular_hist(bins, rl, g, h, nb, dt)
+                if rcan:
+                    hr = (tuple((p - q).astype(p.dtype) for p, q in zip(c["hist"], hl)) if hl is not None
+                          else _regular_hist(bins, rr, g, h, nb, dt))
+            else:
+                if rcan:
+                    hr = _regular_hist(bins, rr, g, h, nb, dt)
+                if lcan:
+                    hl = (tuple((p - q).astype(p.dtype) for p, q in zip(c["hist"], hr)) if hr is not None
+                          else _regular_hist(bins, rl, g, h, nb, dt))
+        for node, can, hist, st, rr_ in ((li, lcan, hl, sl, rl), (ri, rcan, hr, sr, rr)):
+            if can and state["n_leaves"] + 1 < max_leaves:
+                csp = _regular_scan(hist, st, hp, dt)
+                if csp is not None:
+                    state["seq"] += 1
+                    cands.append(dict(node=node, split=csp, rows=rr_, depth=depth + 1, stats=st, hist=hist,
+                                      seq=state["seq"]))
+                    continue
+            make_leaf(node, st, rr_)
+    while cands:
+        c = pop_best()
+        make_leaf(c["node"], c["stats"], c["rows"])
+    out = {k: np.array(v) for k, v in nodes.items()}
+    out["value"] = out["value"].astype(np.float32)
+    out["leaf_of"], out["depth"] = leaf_of, state["depth"]
+    return out
+
+
+def fit_leafwise(b: Binned, y, hp: Hyper, fp32=True):
+    """Booster::train with leaf-wise regular trees (the reference's MSE
+    regression preset in mode="small"): base = mean label, per iteration the
+    MSE gradients, one tree, predictions += lr * leaf (one FP32 rounding)."""
+    y = np.asarray(y, np.float32)
+    base = init_prediction(hp.loss, y)
+    pred = np.full(len(y), base, np.float32)
+    lr = np.float32(hp.learning_rate)
+    trees = []
+    for _ in range(hp.n_estimators):
+        g, h = gradients(hp.loss, y, pred)
+        t = build_leafwise_tree(b, g, h, hp, fp32=fp32)
+        trees.append(t)
+        leaf = t["value"].astype(np.float32)[t["leaf_of"]]
+        pred = (pred.astype(np.longdouble) + np.longdouble(lr) * leaf.astype(np.longdouble)).astype(np.float32)
+    return trees, pred, base

@@ -167,3 +167,12 @@ def regular_train_case():
 
 
 REGULAR_TRAIN_HYPER = dict(loss="logloss", n_estimators=12, max_depth=7, learning_rate=0.2, regular_trees=True)
+
+
+def leafwise_case():
+    """Data of the leaf-wise (regression preset) fixture: the regression generator."""
+    return regression_c2(8000, 12, seed=8000)
+
+
+LEAFWISE_HYPER = dict(loss="mse", n_estimators=10, max_depth=8, learning_rate=0.1, min_samples_leaf=5,
+                      lambda_l2=0.0, regular_trees=True)

@@ -78,9 +78,20 @@ def regular_train_golden():
                         train_raw=tp)
 
 
+def leafwise_golden():
+    """Leaf-wise regular trees of the reference's regression preset
+    (mode="small" with MSE), for the leaf-wise training oracle."""
+    from datagen import LEAFWISE_HYPER, leafwise_case
+
+    X, y = leafwise_case()
+    _, model, _, _, _ = O.ref_fit(X, y, O.Hyper(**LEAFWISE_HYPER))
+    np.savez_compressed(os.path.join(HERE, "leafwise_small.npz"), tcat=np.frombuffer(model, np.uint8))
+
+
 def main():
     regular_golden()
     regular_train_golden()
+    leafwise_golden()
     categorical_golden()
     for name, spec in GOLDEN_CASES.items():
         X, y, hp = make_case(spec)
@@ -104,5 +115,7 @@ if __name__ == "__main__":
         categorical_golden()
     elif sys.argv[1:] == ["regular_train"]:
         regular_train_golden()
+    elif sys.argv[1:] == ["leafwise"]:
+        leafwise_golden()
     else:
         main()

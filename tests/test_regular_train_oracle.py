@@ -80,3 +80,35 @@ def test_level_wise_growth_with_replay_is_the_recursion(n, f, depth, msl, mcw, l
         assert np.array_equal(t["value"].view(np.uint32), lw["value"].astype(np.float32).view(np.uint32))
         leaf = t["value"][t["leaf_of"]].astype(np.longdouble)
         p = (p.astype(np.longdouble) + np.longdouble(np.float32(0.2)) * leaf).astype(np.float32)
+
+
+def test_leafwise_oracle_matches_reference_fixture():
+    """The regression preset grows leaf-wise trees in mode="small"
+    (GrowPolicy::Lossguide): the oracle's FP32 mode rebuilds the reference's,
+    bit for bit, from the stored fit."""
+    from datagen import LEAFWISE_HYPER, leafwise_case
+
+    g = np.load(f"{O.HERE}/../tests/golden/leafwise_small.npz")
+    m = O.parse_tcat_regular(g["tcat"].tobytes())
+    X, y = leafwise_case()
+    trees, _, base = O.fit_leafwise(O.quantize(X), y, O.Hyper(**LEAFWISE_HYPER))
+    assert np.float32(base) == np.float32(m.base)
+    for t, r in zip(trees, m.trees):
+        assert _same_tree(t, r)
+    # the 64-leaf bound only stops new candidates: open ones still end as leaves
+    assert max(int(t["is_leaf"].sum()) for t in trees) > 64
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference not built in this checkout")
+@pytest.mark.parametrize("n,f,depth,msl,lam", [(3000, 10, 6, 1, 1.0), (6000, 8, 5, 20, 3.0)])
+def test_leafwise_oracle_matches_live_reference(n, f, depth, msl, lam):
+    from datagen import regression_c2
+
+    X, y = regression_c2(n, f, seed=n + depth)
+    hp = O.Hyper(loss="mse", n_estimators=6, max_depth=depth, learning_rate=0.1, min_samples_leaf=msl,
+                 lambda_l2=lam, regular_trees=True)
+    b, model, _, _, _ = O.ref_fit(X, y, hp)
+    m = O.parse_tcat_regular(model)
+    trees, _, _ = O.fit_leafwise(b, y, hp)
+    for t, r in zip(trees, m.trees):
+        assert _same_tree(t, r)
