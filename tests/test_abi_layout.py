@@ -11,7 +11,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 PAIRS = [("TrainParams", "tc_train_params"), ("TrainStats", "tc_train_stats"), ("KernelTime", "tc_kernel_time"),
          ("Profile", "tc_profile"), ("ModelInfo", "tc_model_info"), ("ServerParams", "tc_server_params"),
-         ("ReplayRequest", "tc_replay_request")]
+         ("ReplayRequest", "tc_replay_request"), ("CatParams", "tc_cat_params")]
 
 
 def _probe(capi):
