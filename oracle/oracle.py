@@ -372,8 +372,10 @@ def ref_quantize(X, max_bins=255) -> Binned:
     return Binned(bins, edges, ne)
 
 
-def ref_fit(X, y, hp: Hyper, trace=False):
-    """Reference Booster::train; returns (Binned, TCAT bytes, grad trace, hess trace, train raw)."""
+def ref_fit(X, y, hp: Hyper, trace=False, want_pred=True):
+    """Reference Booster::train; returns (Binned, TCAT bytes, grad trace, hess trace, train raw).
+    want_pred=False skips the train predictions (the multiclass loop's
+    predictions are [n][K], which this wrapper does not collect)."""
     X = np.ascontiguousarray(X, np.float32)
     y = np.ascontiguousarray(y, np.float32)
     n, f = X.shape
@@ -382,7 +384,7 @@ def ref_fit(X, y, hp: Hyper, trace=False):
     ne = np.zeros(f, np.uint16)
     gt = np.zeros((hp.n_estimators, n), np.float32) if trace else None
     ht = np.zeros((hp.n_estimators, n), np.float32) if trace else None
-    tp = np.zeros(n, np.float32)
+    tp = np.zeros(n, np.float32) if want_pred else None
     mb = C.c_void_p()
     ml = C.c_size_t()
     rp = hp.ref()
@@ -1040,9 +1042,6 @@ def build_regular_tree(b: Binned, g, h, hp: Hyper, rows=None, fp32=True):
     n = bins.shape[1]
     rows = np.arange(n) if rows is None else np.asarray(rows)
     lam = dt(hp.lambda_l2)
-    half = dt(0.5)
-    gamma = dt(0.0)
-    msg = dt(hp.min_split_gain)
     mcw = dt(hp.min_child_weight)
     nb = int(hp.max_bins)
     max_leaves = 64  # TreeConfig::max_leaves (include/turbocat/config.hpp:29)
@@ -1333,3 +1332,27 @@ def fit_leafwise(b: Binned, y, hp: Hyper, fp32=True):
         leaf = t["value"].astype(np.float32)[t["leaf_of"]]
         pred = (pred.astype(np.longdouble) + np.longdouble(lr) * leaf.astype(np.longdouble)).astype(np.float32)
     return trees, pred, base
+
+
+def fit_regular_multiclass(b: Binned, y, hp: Hyper, K: int, fp32=True):
+    """Booster::train_multiclass (src/boosting/booster.cpp:1263-1395), the
+    reference's multiclass loop in every mode: base predictions 0, per
+    iteration the softmax gradients of all classes
+    (CrossEntropyLoss::compute_multiclass_gradients), then one regular
+    depth-wise tree per class on that class's gradient column, predictions
+    [:, k] += lr * leaf (one FP32 rounding).  Trees iteration-major,
+    class-minor, as the reference saves them."""
+    y = np.asarray(y, np.float32)
+    n = len(y)
+    pred = np.zeros((n, K), np.float32)
+    lr = np.longdouble(np.float32(hp.learning_rate))
+    trees = []
+    for _ in range(hp.n_estimators):
+        g, h = gradients("softmax", y, pred.ravel(), K)
+        g, h = g.reshape(n, K), h.reshape(n, K)
+        for k in range(K):
+            t = build_regular_tree(b, g[:, k].copy(), h[:, k].copy(), hp, fp32=fp32)
+            trees.append(t)
+            leaf = t["value"].astype(np.float32)[t["leaf_of"]]
+            pred[:, k] = (pred[:, k].astype(np.longdouble) + lr * leaf.astype(np.longdouble)).astype(np.float32)
+    return trees, pred

@@ -176,3 +176,12 @@ def leafwise_case():
 
 LEAFWISE_HYPER = dict(loss="mse", n_estimators=10, max_depth=8, learning_rate=0.1, min_samples_leaf=5,
                       lambda_l2=0.0, regular_trees=True)
+
+
+def multiclass_regular_case():
+    """Data of the multiclass regular-tree fixture: the multiclass generator."""
+    return multiclass_c3(4000, 10, 4, seed=7)
+
+
+MULTICLASS_REGULAR_HYPER = dict(loss="softmax", n_classes=4, n_estimators=5, max_depth=5, learning_rate=0.2,
+                                regular_trees=True)

@@ -88,10 +88,21 @@ def leafwise_golden():
     np.savez_compressed(os.path.join(HERE, "leafwise_small.npz"), tcat=np.frombuffer(model, np.uint8))
 
 
+def multiclass_regular_golden():
+    """The reference's multiclass loop (regular trees, one per class and
+    iteration), for the multiclass regular-tree oracle."""
+    from datagen import MULTICLASS_REGULAR_HYPER, multiclass_regular_case
+
+    X, y = multiclass_regular_case()
+    _, model, _, _, _ = O.ref_fit(X, y, O.Hyper(**MULTICLASS_REGULAR_HYPER), want_pred=False)
+    np.savez_compressed(os.path.join(HERE, "multiclass_regular_small.npz"), tcat=np.frombuffer(model, np.uint8))
+
+
 def main():
     regular_golden()
     regular_train_golden()
     leafwise_golden()
+    multiclass_regular_golden()
     categorical_golden()
     for name, spec in GOLDEN_CASES.items():
         X, y, hp = make_case(spec)
@@ -117,5 +128,7 @@ if __name__ == "__main__":
         regular_train_golden()
     elif sys.argv[1:] == ["leafwise"]:
         leafwise_golden()
+    elif sys.argv[1:] == ["multiclass_regular"]:
+        multiclass_regular_golden()
     else:
         main()

@@ -112,3 +112,20 @@ def test_leafwise_oracle_matches_live_reference(n, f, depth, msl, lam):
     trees, _, _ = O.fit_leafwise(b, y, hp)
     for t, r in zip(trees, m.trees):
         assert _same_tree(t, r)
+
+
+def test_multiclass_regular_oracle_matches_reference_fixture():
+    """The reference's multiclass loop builds one regular tree per class and
+    iteration on that class's softmax gradients (in every mode); the oracle
+    rebuilds every tree bit for bit."""
+    from datagen import MULTICLASS_REGULAR_HYPER, multiclass_regular_case
+
+    g = np.load(f"{O.HERE}/../tests/golden/multiclass_regular_small.npz")
+    m = O.parse_tcat_regular(g["tcat"].tobytes())
+    assert m.task == 1 and m.n_classes == 4
+    X, y = multiclass_regular_case()
+    hp = O.Hyper(**MULTICLASS_REGULAR_HYPER)
+    trees, _ = O.fit_regular_multiclass(O.quantize(X), y, hp, 4)
+    assert len(trees) == len(m.trees) == hp.n_estimators * 4
+    for t, r in zip(trees, m.trees):
+        assert _same_tree(t, r)
